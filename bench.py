@@ -1,0 +1,319 @@
+"""Benchmark of the coupled gauge + NRQCD timestep on B200.
+
+One step = one NRQCDField%Update (Crank-Nicolson step of quark and
+antiquark, 12 propagator columns) followed by one GaugeConfiguration%Update
+(leapfrog), the driver order of src/main.f90:344-348.
+
+Workload (plain FP64 at 64^3): transverse-polarised occupation initial
+condition n0 = 1, aQ = 0.5, coupling 0, ranlxd seed 1, links = 1; a0 = 0.05,
+a_s = 1; point sources at the origin; aM = 1.0, Wilson coefficients 1;
+Krylov residual 1e-12.  Synthetic, seeded fields; the working set (~3 GB)
+exceeds the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size L]
+
+For N > 1 (launched with torch.distributed.run) every rank evolves its own
+independent lattice (an ensemble member, seed 1 + rank); there is no
+data-path collective.  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "site-updates/s per 64^3 gauge+NRQCD step; CN s/step vs FP64 plain at ≤1e-10"
+MASS = 1.0
+WILSON = [1.0, 1.0, 1.0, 1.0]
+A = (0.05, 1.0, 1.0, 1.0)
+TOL = 1e-12
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=64)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(L, n_gpus):
+    return {"workload": f"coupled CN(12 columns)+leapfrog step, plain FP64, {L}^3 periodic lattice",
+            "lattice": [L, L, L], "spacings": list(A), "mass": MASS, "wilson_coefficients": WILSON,
+            "krylov_tol": TOL, "initial_condition": "transverse box n0=1 aQ=0.5 g=0 seed=1(+rank), U=1",
+            "sources": "point source at lattice index 1 (quark and antiquark)",
+            "l2": "inputs larger than L2 (working set ~3 GB > 126 MB)",
+            "parallelism": f"replicas x{n_gpus} (independent ensemble members)"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args, rank):
+    """The reference's CPU algorithm (oracle restatement) on the host cores."""
+    if rank != 0:
+        return
+    from oracle import oracle as oc
+    L = args.size
+    n = (L, L, L)
+    V = L ** 3
+    links, ef = oc.transverse_box(n, A, 0.5, 1.0, 0.0, 1, identity_links=True)
+    q = oc.single_point(n, 1)
+    an = oc.single_point(n, 1)
+
+    def step():
+        oc.cn_update(n, A, links, ef, MASS, WILSON, 1.0, q, an, tol=TOL)
+        oc.gauge_update(n, A, links, ef, 1.0)
+
+    t0 = time.perf_counter()
+    step()  # one warm-up step (the CPU path has no compilation or cache state to warm)
+    t_first = time.perf_counter() - t0
+    budget = 150.0
+    steps = max(1, min(args.steps, int(budget / max(t_first, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = V * steps / dt
+    cores = oc.num_threads()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(L, 1),
+            "cpu_baseline": {"value": value, "unit": "site-updates/s", "cores": cores, "kind": "port",
+                             "sample": f"{steps} coupled {L}^3 steps after 1 warm-up step (budget {budget:.0f} s); "
+                                       "FP64 C restatement of the reference algorithm (OpenMP), GMRES(30) to 1e-12"},
+            "e2e": {"value": value, "unit": "site-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(L):
+    """Bounded CPU-baseline sample (one coupled step of the same workload)."""
+    from oracle import oracle as oc
+    n = (L, L, L)
+    links, ef = oc.transverse_box(n, A, 0.5, 1.0, 0.0, 1, identity_links=True)
+    q = oc.single_point(n, 1)
+    an = oc.single_point(n, 1)
+    t0 = time.perf_counter()
+    oc.cn_update(n, A, links, ef, MASS, WILSON, 1.0, q, an, tol=TOL)
+    oc.gauge_update(n, A, links, ef, 1.0)
+    dt = time.perf_counter() - t0
+    return {"value": L ** 3 / dt, "unit": "site-updates/s", "cores": oc.num_threads(), "kind": "port",
+            "sample": f"1 coupled {L}^3 step ({dt:.1f} s), FP64 C restatement of the reference algorithm "
+                      "(OpenMP), GMRES(30) to 1e-12"}
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_
+        import datetime
+        dist = dist_
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice, nrqcd
+
+    L = args.size
+    V = L ** 3
+    torch.cuda.set_device(local)
+    lattice.InitModule([L, L, L], list(A), device=local)
+    ctx = lattice.context()
+    nrqcd.InitModule(MASS, WILSON, 1.0, TOL)
+    g = GaugeConfiguration()
+    g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=1 + rank, identity_links=True)
+    h = NRQCDField()
+    h.InitSinglePoint(1, 1)
+    lib = _capi.load()
+    stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(ctx))
+
+    iters = []
+
+    def step():
+        st = h.Update(g, MASS, WILSON, 1.0)
+        iters.append(st)
+        g.Update(1.0)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    lattice.synchronize()
+    iters.clear()
+    # ---------------- timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    _capi.profile_enable(ctx, True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    prof = _capi.profile_read(ctx)
+    _capi.profile_enable(ctx, False)
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * V * args.steps / (ms / 1000.0)
+    norm_q, norm_a = h.GetNorm_Quark(), h.GetNorm_AntiQ()
+
+    # ---------------- end-to-end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True)  # noqa: E731
+        links_h = pin((V, 3, 3, 3, 2), torch.float64)
+        ef_h = pin((V, 3, 8), torch.float64)
+        q_h = pin((V, 6, 6, 2), torch.float64)
+        a_h = pin((V, 6, 6, 2), torch.float64)
+        P = lambda t: ctypes.cast(t.data_ptr(), _capi._dp)  # noqa: E731
+        _capi.check(lib.nrq_gauge_download(g.handle, P(links_h), P(ef_h)), ctx, "download")
+        _capi.check(lib.nrq_heavy_download(h.handle, P(q_h), P(a_h)), ctx, "download")
+        e2e_steps = max(1, min(args.steps, 5))
+        h2d = (links_h.numel() + ef_h.numel() + q_h.numel() + a_h.numel()) * 8
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist is not None:
+            dist.barrier()
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            _capi.check(lib.nrq_gauge_upload(g.handle, P(links_h), P(ef_h)), ctx, "upload")
+            _capi.check(lib.nrq_heavy_upload(h.handle, P(q_h), P(a_h)), ctx, "upload")
+            step()
+            _capi.check(lib.nrq_heavy_download(h.handle, P(q_h), P(a_h)), ctx, "download")
+            _capi.check(lib.nrq_gauge_download(g.handle, P(links_h), P(ef_h)), ctx, "download")
+        e1.record(stream)
+        e1.synchronize()
+        ems = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * V * e2e_steps / (ems / 1000.0), "unit": "site-updates/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d), "steps": e2e_steps,
+               "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
+                       "nrq_heavy_download + nrq_gauge_download, pinned host buffers"}
+
+    if rank == 0:
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak, peak_src = 6650.0, "fallback"
+        if os.path.exists(peaks_path):
+            peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+        sten = prof["cn_stencil"]
+        achieved = sten["bytes"] / (sten["ms"] / 1000.0) / 1e9 if sten["ms"] > 0 else None
+        step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
+        its = [s["iterations"] for s in iters]
+        line = {
+            "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(L, world),
+            "roofline": {"bound": "hbm", "kernel": "k_cn_mv (CN 12-column stencil)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
+                         "traffic": None,
+                         "launches": sten["launches"], "avg_launch_ms": sten["ms"] / max(1, sten["launches"]),
+                         "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9},
+            "kernel_classes": prof,
+            "cn": {"iterations_per_step": float(np.mean(its)) if its else None,
+                   "matvecs_per_step": float(np.mean([s["matvecs"] for s in iters])) if iters else None,
+                   "max_rel_residual": max(s["max_rel_residual"] for s in iters) if iters else None,
+                   "norms": [norm_q, norm_a]},
+            "clocks": clk, "e2e": e2e, "gpu_launches": int(sum(v["launches"] for v in prof.values())),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_sample(min(L, 64))
+        print(json.dumps(line), flush=True)
+    del h, g
+    nrqcd.FinalizeModule()
+    lattice.FinalizeModule()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+/*
+ * nrqcd_b200 — C ABI of the B200 implementation of the two per-timestep hot
+ * paths of the NRQCD + classical-statistical SU(3) simulation
+ * (alexanderlehmann/NRQCD, Fortran 2008):
+ *
+ *   1. the SU(3) leapfrog of the gauge field      (GaugeConfiguration%Update)
+ *   2. the NRQCD Crank-Nicolson propagator step   (NRQCDField%Update)
+ *
+ * plus the observables those paths are checked with.  Every entry point is a
+ * plain C function over plain pointers and sizes so that the reference's
+ * Fortran can bind it with ISO_C_BINDING; each declaration names the
+ * reference procedure (file:line, paths within the reference project) whose
+ * call site it replaces.
+ *
+ * Host array layouts are the reference's Fortran arrays (column-major) with
+ * the memory index slowest; complex numbers are interleaved (re, im)
+ * doubles, i.e. Fortran complex(c_double_complex):
+ *   links(3,3,3,V)  : ((site*3 + dir)*3 + col)*3 + row      (complex)
+ *   efield(8,3,V)   : (site*3 + dir)*8 + a                  (real)
+ *   prop(6,6,V)     : (site*6 + col)*6 + row                (complex)
+ * site = lattice index - 1 = x + Nx*(y + Ny*z) (src/lattice.f90:883-898) —
+ * the single-rank memory order of the reference.
+ *
+ * All calls of one context are ordered on that context's CUDA stream.  Calls
+ * that return host scalars synchronise; update calls may return before the
+ * device work ends.  Calls are not re-entrant per context.  Every call
+ * returns an nrq_status; nonzero codes carry a message via nrq_last_error.
+ */
+#ifndef NRQCD_B200_H
+#define NRQCD_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  NRQ_OK = 0,
+  NRQ_ERR_NOT_INITIALISED = 1,     /* mirrors src/nrqcd.f90:206-211          */
+  NRQ_ERR_ALREADY_INITIALISED = 2, /* mirrors src/nrqcd.f90:180-181          */
+  NRQ_ERR_BAD_ARG = 3,
+  NRQ_ERR_CUDA = 4,
+  NRQ_ERR_NOT_CONVERGED = 5,       /* the reference never checks KSP convergence */
+  NRQ_ERR_TIMEOUT = 6,
+  NRQ_ERR_NONFINITE = 7,
+  NRQ_ERR_NO_DEVICE = 8,
+  NRQ_ERR_OOM = 9
+} nrq_status;
+
+typedef struct nrq_ctx nrq_ctx;     /* lattice + device + stream          */
+typedef struct nrq_gauge nrq_gauge; /* type(GaugeConfiguration)           */
+typedef struct nrq_heavy nrq_heavy; /* type(NRQCDField)                   */
+typedef struct nrq_cn nrq_cn;       /* module state of src/nrqcd.f90:120-158 */
+
+typedef struct {
+  int64_t iterations;      /* Krylov iterations of the last update (max over columns) */
+  int64_t matvecs;         /* stencil applications (12 columns each)  */
+  int64_t vector_streams;  /* 12-column vector passes (read or write)  */
+  double max_rel_residual; /* max over the 12 columns of ||b-Ax||/||b|| (true residual) */
+  int converged;           /* 1 when every column reached the tolerance */
+} nrq_cn_stats;
+
+/* ---- context: replaces lattice%InitModule (src/lattice.f90:124-228) and
+ *      halocomm%InitModule (src/halocomm.f90:70-90); on one GPU the halo
+ *      exchange becomes periodic indexing inside the kernels.               */
+int nrq_init(const int64_t extents[3], const double spacings[4] /* a0, ax, ay, az */,
+             int device, nrq_ctx **ctx);
+int nrq_finalize(nrq_ctx *ctx);
+const char *nrq_last_error(const nrq_ctx *ctx);
+const char *nrq_status_string(int status);
+int nrq_synchronize(nrq_ctx *ctx);
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on, so a
+ * caller can order its own work or time with CUDA events on it.            */
+void *nrq_cuda_stream(nrq_ctx *ctx);
+
+/* Per-kernel-class timing with CUDA events recorded around every launch on
+ * the context stream (off by default; enabling adds two event records per
+ * launch).  Classes: 0 CN stencil (matvec), 1 CN vector update, 2 CN
+ * scalar stages, 3 CN per-step gauge preparation, 4 leapfrog link update,
+ * 5 leapfrog E update.  nrq_profile_read synchronises and returns, per
+ * class, the launch count, summed device milliseconds and the algorithmic
+ * HBM bytes those launches had to move (each field read or written once);
+ * it then clears the counters.                                             */
+enum { NRQ_PROF_CLASSES = 6 };
+int nrq_profile_enable(nrq_ctx *ctx, int enable);
+int nrq_profile_read(nrq_ctx *ctx, int64_t launches[6], double milliseconds[6], double bytes[6]);
+
+/* ---- gauge configuration: src/gaugeconfiguration_su3.f90:33-116 -------- */
+int nrq_gauge_create(nrq_ctx *ctx, nrq_gauge **g);      /* Allocate (:124-140)   */
+int nrq_gauge_destroy(nrq_gauge *g);                    /* Deallocate            */
+int nrq_gauge_upload(nrq_gauge *g, const double *links, const double *efield);
+int nrq_gauge_download(const nrq_gauge *g, double *links, double *efield);
+int nrq_gauge_copy(nrq_gauge *dst, const nrq_gauge *src); /* configuration copies, src/main.f90:2320 */
+/* ColdInit, src/gaugeconfiguration_su3.f90:363-378 */
+int nrq_gauge_cold_init(nrq_gauge *g);
+/* TransversePolarisedOccupiedInit_Box, src/gaugeconfiguration_su3.f90:906-951
+ * (-> :1263-1446) after random%InitModule(seed) (src/random.f90:126-140);
+ * identity_links != 0 keeps U = 1 while drawing the same random stream.     */
+int nrq_gauge_transverse_box_init(nrq_gauge *g, double saturation_scale, double amplitude,
+                                  double coupling, int64_t seed, int identity_links);
+/* Update_Leapfrog(StepWidth), src/gaugeconfiguration_su3.f90:2082-2111 */
+int nrq_gauge_update(nrq_gauge *g, double stepwidth);
+/* GetEnergy, src/gaugeconfiguration_su3.f90:1769-1817 */
+int nrq_gauge_energy(nrq_gauge *g, double *energy);
+/* GetDeviationFromGaussLaw (:1480-1531) -> ref_measure, and the max-norm
+ * GetGdeviation of EquilibriumInit (:724-768) -> max_norm                   */
+int nrq_gauge_gauss(nrq_gauge *g, double *ref_measure, double *max_norm);
+
+/* ---- heavy-quark field: src/nrqcd.f90:58-117 -------------------------- */
+int nrq_heavy_create(nrq_ctx *ctx, nrq_heavy **h);      /* NRQCDField() (:235-248) */
+int nrq_heavy_destroy(nrq_heavy *h);                    /* Destructor (:255-260)   */
+int nrq_heavy_upload(nrq_heavy *h, const double *quark, const double *antiq);
+int nrq_heavy_download(const nrq_heavy *h, double *quark, double *antiq);
+int nrq_heavy_copy(nrq_heavy *dst, const nrq_heavy *src); /* assignment(=) (:219-228) */
+/* InitSinglePoint(LatticeIndex_quark, LatticeIndex_antiq), src/nrqcd.f90:324-350
+ * (1-based lattice indices)                                                 */
+int nrq_heavy_init_single_point(nrq_heavy *h, int64_t lattice_index_quark,
+                                int64_t lattice_index_antiq);
+/* GetNorm_Quark / GetNorm_AntiQ, src/nrqcd.f90:547-611 */
+int nrq_heavy_norms(nrq_heavy *h, double *norm_quark, double *norm_antiq);
+/* GetMesoncorrelator_{O1_1S0,O1_3S1,O8_1S0,O8_3S1}_ZeroMomentum,
+ * src/nrqcd.f90:1484-1661; out[8] = re/im of the four correlators          */
+int nrq_heavy_correlators(nrq_heavy *h, double out[8]);
+
+/* ---- Crank-Nicolson solver module: src/nrqcd.f90:167-212, 619-869 ------ */
+/* InitModule(Mass, WilsonCoeffs, StepWidth, kspTol); c = 4 complex (8 doubles).
+ * form: 0 = plain FP64 (BiCGStab, fused stencil/axpy/dot kernels).
+ * maxits bounds the Krylov iterations (the reference's PETSc default 1e4).  */
+int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, double tol,
+                int64_t maxits, int form, nrq_cn **cn);
+/* FinalizeModule, src/nrqcd.f90:199-212 */
+int nrq_cn_finalize(nrq_cn *cn);
+/* NRQCDField%Update(GaugeConf, Mass, WilsonCoeffs, StepWidth) =
+ * Update_CrankNicholson, src/nrqcd.f90:1053-1168: quark (+M, c) and
+ * antiquark (-M, conj c); per column RHS = A psi, solve A^H psi' = RHS with
+ * A the operator PETSc assembles (blocks transposed, src/nrqcd.f90:1014-1018).
+ * Returns NRQ_ERR_NOT_CONVERGED if a column missed the tolerance within
+ * maxits (the fields are still updated); stats may be NULL.                  */
+int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass,
+                        const double c[8], double stepwidth, nrq_cn_stats *stats);
+/* Apply the assembled operator A (herm = 0) or A^H (herm = 1) to all 6
+ * propagator columns of both species: quark with (+M, c), antiquark with
+ * (-M, conj c); out = A in.  MatMult of src/nrqcd.f90:1112, exposed for
+ * verification.                                                            */
+int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const double c[8],
+                 double stepwidth, int herm, const nrq_heavy *in, nrq_heavy *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

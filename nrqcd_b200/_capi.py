@@ -1,0 +1,143 @@
+"""ctypes binding of the C ABI in ``include/nrqcd_b200.h``.
+
+The shared library is built in-tree by ``nrqcd_b200/build.py``.  There is no
+fallback: if the library is missing or no CUDA device is present, the calls
+raise ``NrqcdError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libnrqcd_b200.so")
+
+NRQ_OK = 0
+NRQ_ERR_NOT_INITIALISED = 1
+NRQ_ERR_ALREADY_INITIALISED = 2
+NRQ_ERR_BAD_ARG = 3
+NRQ_ERR_CUDA = 4
+NRQ_ERR_NOT_CONVERGED = 5
+NRQ_ERR_TIMEOUT = 6
+NRQ_ERR_NONFINITE = 7
+NRQ_ERR_NO_DEVICE = 8
+NRQ_ERR_OOM = 9
+
+
+class NrqcdError(RuntimeError):
+    """Raised where the reference calls MPIStop (src/mpiinterface.f90:148-173)."""
+
+    def __init__(self, message, code=None):
+        super().__init__(message)
+        self.code = code
+
+
+class CnStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int64), ("matvecs", ctypes.c_int64),
+                ("vector_streams", ctypes.c_int64), ("max_rel_residual", ctypes.c_double),
+                ("converged", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_pp = ctypes.POINTER(ctypes.c_void_p)
+
+# name -> (restype, argtypes); every entry point of include/nrqcd_b200.h
+SIGNATURES = {
+    "nrq_init": (ctypes.c_int, [_i64p, _dp, ctypes.c_int, _pp]),
+    "nrq_finalize": (ctypes.c_int, [_vp]),
+    "nrq_last_error": (ctypes.c_char_p, [_vp]),
+    "nrq_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "nrq_synchronize": (ctypes.c_int, [_vp]),
+    "nrq_cuda_stream": (ctypes.c_void_p, [_vp]),
+    "nrq_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "nrq_profile_read": (ctypes.c_int, [_vp, _i64p, _dp, _dp]),
+    "nrq_gauge_create": (ctypes.c_int, [_vp, _pp]),
+    "nrq_gauge_destroy": (ctypes.c_int, [_vp]),
+    "nrq_gauge_upload": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_gauge_download": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_gauge_copy": (ctypes.c_int, [_vp, _vp]),
+    "nrq_gauge_cold_init": (ctypes.c_int, [_vp]),
+    "nrq_gauge_transverse_box_init": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                      ctypes.c_int64, ctypes.c_int]),
+    "nrq_gauge_update": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "nrq_gauge_energy": (ctypes.c_int, [_vp, _dp]),
+    "nrq_gauge_gauss": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_heavy_create": (ctypes.c_int, [_vp, _pp]),
+    "nrq_heavy_destroy": (ctypes.c_int, [_vp]),
+    "nrq_heavy_upload": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_heavy_download": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_heavy_copy": (ctypes.c_int, [_vp, _vp]),
+    "nrq_heavy_init_single_point": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64]),
+    "nrq_heavy_norms": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_heavy_correlators": (ctypes.c_int, [_vp, _dp]),
+    "nrq_cn_init": (ctypes.c_int, [_vp, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int64, ctypes.c_int, _pp]),
+    "nrq_cn_finalize": (ctypes.c_int, [_vp]),
+    "nrq_heavy_update_cn": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,
+                                           ctypes.POINTER(CnStats)]),
+    "nrq_cn_apply": (ctypes.c_int, [_vp, _vp, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise NrqcdError(f"CUDA extension not built: {path} missing (run python -m nrqcd_b200.build)")
+        lib = ctypes.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(rc: int, ctx=None, what: str = ""):
+    if rc != NRQ_OK:
+        lib = load()
+        msg = lib.nrq_status_string(rc).decode()
+        detail = lib.nrq_last_error(ctx).decode() if ctx else ""
+        raise NrqcdError(f"{what}: {msg}" + (f" ({detail})" if detail else ""), rc)
+
+
+def dptr(a: np.ndarray):
+    if not a.flags.c_contiguous:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data_as(_dp)
+
+
+def coeffs(c) -> np.ndarray:
+    """Wilson coefficients (4 complex) as 8 interleaved doubles."""
+    c = np.asarray(c, dtype=np.complex128).reshape(4)
+    out = np.empty(8)
+    out[0::2] = c.real
+    out[1::2] = c.imag
+    return out
+
+
+PROFILE_CLASSES = ("cn_stencil", "cn_vector", "cn_scalar", "cn_prepare", "leapfrog_links", "leapfrog_efield")
+
+
+def profile_enable(ctx, enable=True):
+    check(load().nrq_profile_enable(ctx, int(bool(enable))), ctx, "profile_enable")
+
+
+def profile_read(ctx) -> dict:
+    """Per kernel class: launches, device ms (CUDA events) and algorithmic bytes."""
+    n = np.zeros(6, dtype=np.int64)
+    ms = np.zeros(6)
+    by = np.zeros(6)
+    check(load().nrq_profile_read(ctx, n.ctypes.data_as(_i64p), dptr(ms), dptr(by)), ctx, "profile_read")
+    return {name: {"launches": int(n[k]), "ms": float(ms[k]), "bytes": float(by[k])}
+            for k, name in enumerate(PROFILE_CLASSES)}

@@ -1,0 +1,854 @@
+// C ABI (include/nrqcd_b200.h): handles, host<->device transfers, the
+// leapfrog sequencing, the Krylov driver of the Crank-Nicolson step, and the
+// initial-condition pipeline (host ranlxd stream, cuFFT, device kernels).
+#include <cufft.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/nrqcd_b200.h"
+#include "nrq_internal.h"
+#include "nrq_kernels.cuh"
+
+using nrq::cplx;
+
+namespace {
+
+// ---------------------------------------------------------------- ranlxd
+// Double-precision RANLUX (M. Luescher, ranlxd v2.1): 12 words of 48-bit
+// fractions, subtract-with-borrow x_n = x_{n-5} - x_{n-12} - c, pr recurrence
+// steps per 12 delivered numbers (pr = 397 at luxury level 2), seeded from a
+// 31-bit shift register — the generator of src/ranlxd_generator.f90:72-350
+// as random%InitModule uses it (src/random.f90:126-140).
+class Ranlxd {
+ public:
+  bool init(int level, int64_t seed) {
+    if (level == 1) pr_ = 202;
+    else if (level == 2) pr_ = 397;
+    else return false;
+    if (seed <= 0 || seed > 2147483647LL) return false;
+    int bits[31];
+    int64_t v = seed;
+    for (int k = 0; k < 31; ++k) {
+      bits[k] = (int)(v & 1);
+      v >>= 1;
+    }
+    int ib = 0, jb = 18;
+    const double unit = std::ldexp(1.0, -48);
+    for (int k = 0; k < 12; ++k) {
+      double acc = 0.0;
+      for (int l = 0; l < 48; ++l) {
+        acc = 2.0 * acc + (double)((bits[ib] + 1) & 1);
+        bits[ib] = (bits[ib] + bits[jb]) & 1;
+        ib = (ib + 1) % 31;
+        jb = (jb + 1) % 31;
+      }
+      w_[k] = unit * acc;
+    }
+    borrow_ = 0.0;
+    pos_ = 11;
+    lag_ = 7;
+    last_ = 0;
+    return true;
+  }
+  double next() {
+    pos_ = (pos_ + 1) % 12;
+    if (pos_ == last_) refill();
+    return w_[pos_];
+  }
+
+ private:
+  void refill() {
+    const double unit = std::ldexp(1.0, -48);
+    int i = pos_, j = lag_;
+    for (int k = 0; k < pr_; ++k) {
+      double y = (w_[j] - w_[i]) - borrow_;
+      if (y < 0.0) {
+        borrow_ = unit;
+        y += 1.0;
+      } else {
+        borrow_ = 0.0;
+      }
+      w_[i] = y;
+      i = (i + 1) % 12;
+      j = (j + 1) % 12;
+    }
+    pos_ = i;
+    lag_ = j;
+    last_ = i;
+  }
+  double w_[12];
+  double borrow_ = 0.0;
+  int pr_ = 397, pos_ = 11, lag_ = 7, last_ = 0;
+};
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+int ensure_stage(nrq_ctx *ctx, size_t bytes) {
+  if (ctx->stage_bytes >= bytes) return NRQ_OK;
+  if (ctx->d_stage) cudaFree(ctx->d_stage);
+  ctx->d_stage = nullptr;
+  ctx->stage_bytes = 0;
+  NRQ_CUDA_TRY(ctx, cudaMalloc(&ctx->d_stage, bytes));
+  ctx->stage_bytes = bytes;
+  return NRQ_OK;
+}
+
+int ensure_red(nrq_ctx *ctx, int64_t doubles) {
+  if (ctx->red_cap >= doubles) return NRQ_OK;
+  if (ctx->d_red) cudaFree(ctx->d_red);
+  ctx->d_red = nullptr;
+  ctx->red_cap = 0;
+  NRQ_CUDA_TRY(ctx, cudaMalloc(&ctx->d_red, sizeof(double) * doubles));
+  ctx->red_cap = doubles;
+  return NRQ_OK;
+}
+
+int set_device(nrq_ctx *ctx) {
+  NRQ_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  return NRQ_OK;
+}
+
+int check_launch(nrq_ctx *ctx, const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return NRQ_ERR_CUDA;
+  }
+  return NRQ_OK;
+}
+
+// final reduction of nq values over nb partial blocks into h_res[0..nq)
+int reduce_to_host(nrq_ctx *ctx, int64_t nb, int nq, unsigned maxmask) {
+  nrq::k_reduce_final<<<1, 256, 0, ctx->stream>>>(ctx->d_red, nb, nq, maxmask, ctx->d_res);
+  int rc = check_launch(ctx, "k_reduce_final");
+  if (rc) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(double) * nq, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return NRQ_OK;
+}
+
+// per-species, per-term coefficients; herm selects A^H
+nrq::CnCoef make_coef(const nrq_ctx *ctx, double mass, const double c_[8], double dt, bool herm) {
+  nrq::CnCoef C{};
+  const cplx kappa = {0.0, -dt / 2 * ctx->a[0]};
+  for (int sp = 0; sp < 2; ++sp) {
+    const double M = sp == 0 ? mass : -mass;
+    cplx c[4];
+    for (int k = 0; k < 4; ++k) c[k] = {c_[2 * k], sp == 0 ? c_[2 * k + 1] : -c_[2 * k + 1]};
+    cplx kin = (1.0 / M) * (kappa * c[0]);
+    cplx mag = (-1.0 / (2.0 * M)) * (kappa * c[1]);
+    cplx dar = (-1.0 / (8.0 * M * M)) * (kappa * c[2]);
+    cplx so = (-1.0 / (8.0 * M * M)) * (kappa * c[3]);
+    if (herm) {
+      kin = nrq::conj(kin);
+      mag = nrq::conj(mag);
+      dar = nrq::conj(dar);
+      so = nrq::conj(so);
+    }
+    C.kin[sp] = kin;
+    C.mag[sp] = mag;
+    C.dar[sp] = dar;
+    C.so[sp] = so;
+  }
+  C.dkin = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    C.inva2[i] = 1.0 / (ctx->a[i + 1] * ctx->a[i + 1]);
+    C.dkin += C.inva2[i];
+  }
+  return C;
+}
+
+}  // namespace
+
+// ====================================================================== context
+extern "C" const char *nrq_status_string(int s) {
+  switch (s) {
+    case NRQ_OK: return "ok";
+    case NRQ_ERR_NOT_INITIALISED: return "not initialised";
+    case NRQ_ERR_ALREADY_INITIALISED: return "already initialised";
+    case NRQ_ERR_BAD_ARG: return "bad argument";
+    case NRQ_ERR_CUDA: return "CUDA error";
+    case NRQ_ERR_NOT_CONVERGED: return "Krylov solve did not converge";
+    case NRQ_ERR_TIMEOUT: return "timeout";
+    case NRQ_ERR_NONFINITE: return "non-finite value";
+    case NRQ_ERR_NO_DEVICE: return "no CUDA device";
+    case NRQ_ERR_OOM: return "out of memory";
+    default: return "unknown status";
+  }
+}
+
+extern "C" const char *nrq_last_error(const nrq_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+extern "C" int nrq_init(const int64_t ext[3], const double a[4], int device, nrq_ctx **out) {
+  if (!ext || !a || !out) return NRQ_ERR_BAD_ARG;
+  *out = nullptr;
+  for (int k = 0; k < 3; ++k)
+    if (ext[k] < 1) return NRQ_ERR_BAD_ARG;
+  for (int k = 0; k < 4; ++k)
+    if (!(a[k] > 0.0)) return NRQ_ERR_BAD_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return NRQ_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = new (std::nothrow) nrq_ctx();
+  if (!ctx) return NRQ_ERR_OOM;
+  ctx->device = device;
+  for (int k = 0; k < 3; ++k) ctx->n[k] = ext[k];
+  for (int k = 0; k < 4; ++k) ctx->a[k] = a[k];
+  ctx->lat.nx = ext[0];
+  ctx->lat.ny = ext[1];
+  ctx->lat.nz = ext[2];
+  ctx->lat.V = ext[0] * ext[1] * ext[2];
+  ctx->lat.a0 = a[0];
+  for (int k = 0; k < 3; ++k) ctx->lat.a[k] = a[k + 1];
+  int rc = set_device(ctx);
+  if (rc == NRQ_OK) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) ctx->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&ctx->d_res, sizeof(double) * 64) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_res, sizeof(double) * 64) != cudaSuccess)
+      rc = NRQ_ERR_CUDA;
+  }
+  if (rc == NRQ_OK) rc = ensure_red(ctx, ((ctx->lat.V + 127) / 128) * 8 + 1024);
+  if (rc != NRQ_OK) {
+    nrq_finalize(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_finalize(nrq_ctx *ctx) {
+  if (!ctx) return NRQ_ERR_NOT_INITIALISED;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_red) cudaFree(ctx->d_red);
+  if (ctx->d_res) cudaFree(ctx->d_res);
+  if (ctx->h_res) cudaFreeHost(ctx->h_res);
+  if (ctx->d_stage) cudaFree(ctx->d_stage);
+  for (auto &r : ctx->prof_recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (auto e : ctx->prof_pool) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_synchronize(nrq_ctx *ctx) {
+  if (!ctx) return NRQ_ERR_NOT_INITIALISED;
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return NRQ_OK;
+}
+
+extern "C" void *nrq_cuda_stream(nrq_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int nrq_profile_enable(nrq_ctx *ctx, int enable) {
+  if (!ctx) return NRQ_ERR_NOT_INITIALISED;
+  ctx->prof = enable != 0;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_profile_read(nrq_ctx *ctx, int64_t launches[6], double ms[6], double bytes[6]) {
+  if (!ctx || !launches || !ms || !bytes) return NRQ_ERR_BAD_ARG;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < NRQ_PROF_CLASSES; ++k) {
+    launches[k] = 0;
+    ms[k] = 0.0;
+    bytes[k] = 0.0;
+  }
+  for (auto &r : ctx->prof_recs) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, r.a, r.b);
+    if (r.cls >= 0 && r.cls < NRQ_PROF_CLASSES) {
+      launches[r.cls] += 1;
+      ms[r.cls] += t;
+      bytes[r.cls] += r.bytes;
+    }
+    ctx->prof_pool.push_back(r.a);
+    ctx->prof_pool.push_back(r.b);
+  }
+  ctx->prof_recs.clear();
+  return NRQ_OK;
+}
+
+// ====================================================================== gauge
+extern "C" int nrq_gauge_create(nrq_ctx *ctx, nrq_gauge **out) {
+  if (!ctx || !out) return NRQ_ERR_BAD_ARG;
+  *out = nullptr;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  nrq_gauge *g = new (std::nothrow) nrq_gauge();
+  if (!g) return NRQ_ERR_OOM;
+  g->ctx = ctx;
+  const int64_t V = ctx->lat.V;
+  if (cudaMalloc(&g->U, sizeof(double2) * 27 * V) != cudaSuccess ||
+      cudaMalloc(&g->E, sizeof(double) * 24 * V) != cudaSuccess) {
+    cudaGetLastError();
+    if (g->U) cudaFree(g->U);
+    if (g->E) cudaFree(g->E);
+    delete g;
+    ctx->last_error = "nrq_gauge_create: device allocation failed";
+    return NRQ_ERR_OOM;
+  }
+  nrq::k_cold<<<nblk(V, 256), 256, 0, ctx->stream>>>(g->U, g->E, V);
+  rc = check_launch(ctx, "k_cold");
+  if (rc) {
+    nrq_gauge_destroy(g);
+    return rc;
+  }
+  *out = g;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_destroy(nrq_gauge *g) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  cudaSetDevice(g->ctx->device);
+  cudaStreamSynchronize(g->ctx->stream);
+  if (g->U) cudaFree(g->U);
+  if (g->E) cudaFree(g->E);
+  delete g;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_upload(nrq_gauge *g, const double *links, const double *efield) {
+  if (!g || !links || !efield) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  const int64_t V = ctx->lat.V;
+  int rc = set_device(ctx);
+  if (!rc) rc = ensure_stage(ctx, sizeof(double2) * 27 * V);
+  if (rc) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_stage, links, sizeof(double2) * 27 * V, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+  nrq::k_links_f2soa<<<nblk(V, 128), 128, 0, ctx->stream>>>((const double2 *)ctx->d_stage, g->U, V);
+  if ((rc = check_launch(ctx, "k_links_f2soa"))) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_stage, efield, sizeof(double) * 24 * V, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+  nrq::k_efield_f2soa<<<nblk(V, 128), 128, 0, ctx->stream>>>((const double *)ctx->d_stage, g->E, V);
+  return check_launch(ctx, "k_efield_f2soa");
+}
+
+extern "C" int nrq_gauge_download(const nrq_gauge *g, double *links, double *efield) {
+  if (!g || !links || !efield) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  const int64_t V = ctx->lat.V;
+  int rc = set_device(ctx);
+  if (!rc) rc = ensure_stage(ctx, sizeof(double2) * 27 * V);
+  if (rc) return rc;
+  nrq::k_links_soa2f<<<nblk(V, 128), 128, 0, ctx->stream>>>(g->U, (double2 *)ctx->d_stage, V);
+  if ((rc = check_launch(ctx, "k_links_soa2f"))) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(links, ctx->d_stage, sizeof(double2) * 27 * V, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  nrq::k_efield_soa2f<<<nblk(V, 128), 128, 0, ctx->stream>>>(g->E, (double *)ctx->d_stage, V);
+  if ((rc = check_launch(ctx, "k_efield_soa2f"))) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(efield, ctx->d_stage, sizeof(double) * 24 * V, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_copy(nrq_gauge *dst, const nrq_gauge *src) {
+  if (!dst || !src || dst->ctx != src->ctx) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = dst->ctx;
+  const int64_t V = ctx->lat.V;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(dst->U, src->U, sizeof(double2) * 27 * V, cudaMemcpyDeviceToDevice, ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(dst->E, src->E, sizeof(double) * 24 * V, cudaMemcpyDeviceToDevice, ctx->stream));
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_cold_init(nrq_gauge *g) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  nrq::k_cold<<<nblk(ctx->lat.V, 256), 256, 0, ctx->stream>>>(g->U, g->E, ctx->lat.V);
+  return check_launch(ctx, "k_cold");
+}
+
+extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, double coupling, int64_t seed,
+                                             int identity_links) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  const nrq::Lat L = ctx->lat;
+  const int64_t V = L.V;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  Ranlxd rng;
+  if (!rng.init(2, seed)) {
+    ctx->last_error = "transverse_box_init: seed must lie in [1, 2^31-1]";
+    return NRQ_ERR_BAD_ARG;
+  }
+  // real parts of complex Box-Muller normals, per site, per polarisation
+  // (gauge:1334-1340, random.f90:238-255): plane (pol*8 + a)
+  std::vector<double2> R((size_t)16 * V);
+  const double twopi = 2.0 * std::acos(-1.0);
+  for (int64_t s = 0; s < V; ++s)
+    for (int pol = 0; pol < 2; ++pol)
+      for (int a = 0; a < 8; ++a) {
+        double u1 = rng.next(), u2 = rng.next();
+        R[(size_t)(pol * 8 + a) * V + s] = make_double2(std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2), 0.0);
+      }
+  double2 *dR = nullptr, *dA = nullptr, *dEf = nullptr;
+  cufftHandle plan16 = 0, plan24 = 0;
+  bool p16 = false, p24 = false;
+  auto cleanup = [&]() {
+    if (p16) cufftDestroy(plan16);
+    if (p24) cufftDestroy(plan24);
+    if (dR) cudaFree(dR);
+    if (dA) cudaFree(dA);
+    if (dEf) cudaFree(dEf);
+  };
+  if (cudaMalloc(&dR, sizeof(double2) * 16 * V) != cudaSuccess ||
+      cudaMalloc(&dA, sizeof(double2) * 24 * V) != cudaSuccess ||
+      cudaMalloc(&dEf, sizeof(double2) * 24 * V) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    ctx->last_error = "transverse_box_init: device allocation failed";
+    return NRQ_ERR_OOM;
+  }
+  int dims[3] = {(int)L.nz, (int)L.ny, (int)L.nx};
+  if (cufftPlanMany(&plan16, 3, dims, nullptr, 1, (int)V, nullptr, 1, (int)V, CUFFT_Z2Z, 16) != CUFFT_SUCCESS) {
+    cleanup();
+    ctx->last_error = "transverse_box_init: cufftPlanMany failed";
+    return NRQ_ERR_CUDA;
+  }
+  p16 = true;
+  if (cufftPlanMany(&plan24, 3, dims, nullptr, 1, (int)V, nullptr, 1, (int)V, CUFFT_Z2Z, 24) != CUFFT_SUCCESS) {
+    cleanup();
+    ctx->last_error = "transverse_box_init: cufftPlanMany failed";
+    return NRQ_ERR_CUDA;
+  }
+  p24 = true;
+  cufftSetStream(plan16, ctx->stream);
+  cufftSetStream(plan24, ctx->stream);
+  if (cudaMemcpyAsync(dR, R.data(), sizeof(double2) * 16 * V, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+    cleanup();
+    return NRQ_ERR_CUDA;
+  }
+  bool ok = cufftExecZ2Z(plan16, (cufftDoubleComplex *)dR, (cufftDoubleComplex *)dR, CUFFT_FORWARD) == CUFFT_SUCCESS;
+  const double fwd_scale = ctx->a[1] * ctx->a[2] * ctx->a[3];
+  const double volume = (double)V * fwd_scale;
+  if (ok) {
+    nrq::k_ic_pspace<<<nblk(V, 128), 128, 0, ctx->stream>>>(L, dR, fwd_scale, Q, n0, coupling, dA, dEf);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  ok = ok && cufftExecZ2Z(plan24, (cufftDoubleComplex *)dA, (cufftDoubleComplex *)dA, CUFFT_INVERSE) == CUFFT_SUCCESS;
+  ok = ok && cufftExecZ2Z(plan24, (cufftDoubleComplex *)dEf, (cufftDoubleComplex *)dEf, CUFFT_INVERSE) == CUFFT_SUCCESS;
+  if (ok) {
+    nrq::k_ic_write<<<nblk(V, 128), 128, 0, ctx->stream>>>(L, dA, dEf, 1.0 / volume, identity_links, g->U, g->E);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  ok = ok && cudaStreamSynchronize(ctx->stream) == cudaSuccess;
+  cleanup();
+  if (!ok) {
+    ctx->last_error = "transverse_box_init: FFT or kernel failure";
+    return NRQ_ERR_CUDA;
+  }
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_update(nrq_gauge *g, double dt) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  const unsigned nb_ = nblk(ctx->lat.V, 128);
+  const double V = (double)ctx->lat.V;
+  auto links = [&]() {
+    ProfScope ps(ctx, 4, V * (192.0 + 432.0 + 432.0));
+    nrq::k_update_links<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+  };
+  auto efield = [&]() {
+    ProfScope ps(ctx, 5, V * (432.0 + 192.0 + 192.0));
+    nrq::k_update_efield<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+  };
+  // Update_Leapfrog ordering (gauge:2100-2110)
+  if (dt > 0) {
+    links();
+    efield();
+  } else {
+    efield();
+    links();
+  }
+  return check_launch(ctx, "leapfrog");
+}
+
+extern "C" int nrq_gauge_energy(nrq_gauge *g, double *energy) {
+  if (!g || !energy) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  const int64_t nb_ = nblk(ctx->lat.V, 256);
+  if ((rc = ensure_red(ctx, nb_ * 2))) return rc;
+  nrq::k_energy<<<(unsigned)nb_, 256, 0, ctx->stream>>>(ctx->lat, g->U, g->E, ctx->d_red);
+  if ((rc = check_launch(ctx, "k_energy"))) return rc;
+  if ((rc = reduce_to_host(ctx, nb_, 1, 0u))) return rc;
+  *energy = ctx->h_res[0];
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_gauss(nrq_gauge *g, double *ref_measure, double *max_norm) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  const int64_t nb_ = nblk(ctx->lat.V, 256);
+  if ((rc = ensure_red(ctx, nb_ * 2))) return rc;
+  nrq::k_gauss<<<(unsigned)nb_, 256, 0, ctx->stream>>>(ctx->lat, g->U, g->E, ctx->d_red);
+  if ((rc = check_launch(ctx, "k_gauss"))) return rc;
+  if ((rc = reduce_to_host(ctx, nb_, 2, 2u))) return rc;
+  if (ref_measure) *ref_measure = ctx->h_res[0];
+  if (max_norm) *max_norm = ctx->h_res[1];
+  return NRQ_OK;
+}
+
+// ====================================================================== heavy field
+extern "C" int nrq_heavy_create(nrq_ctx *ctx, nrq_heavy **out) {
+  if (!ctx || !out) return NRQ_ERR_BAD_ARG;
+  *out = nullptr;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  nrq_heavy *h = new (std::nothrow) nrq_heavy();
+  if (!h) return NRQ_ERR_OOM;
+  h->ctx = ctx;
+  if (cudaMalloc(&h->P, sizeof(double2) * 72 * ctx->lat.V) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    ctx->last_error = "nrq_heavy_create: device allocation failed";
+    return NRQ_ERR_OOM;
+  }
+  NRQ_CUDA_TRY(ctx, cudaMemsetAsync(h->P, 0, sizeof(double2) * 72 * ctx->lat.V, ctx->stream));
+  *out = h;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_heavy_destroy(nrq_heavy *h) {
+  if (!h) return NRQ_ERR_BAD_ARG;
+  cudaSetDevice(h->ctx->device);
+  cudaStreamSynchronize(h->ctx->stream);
+  if (h->P) cudaFree(h->P);
+  delete h;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_heavy_upload(nrq_heavy *h, const double *q, const double *a) {
+  if (!h || !q || !a) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = h->ctx;
+  const int64_t V = ctx->lat.V;
+  int rc = set_device(ctx);
+  if (!rc) rc = ensure_stage(ctx, sizeof(double2) * 72 * V);
+  if (rc) return rc;
+  double2 *stg = (double2 *)ctx->d_stage;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(stg, q, sizeof(double2) * 36 * V, cudaMemcpyHostToDevice, ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(stg + 36 * V, a, sizeof(double2) * 36 * V, cudaMemcpyHostToDevice, ctx->stream));
+  nrq::launch_prop_f2soa(stg, h->P, V, ctx->stream);
+  return check_launch(ctx, "k_prop_f2soa");
+}
+
+extern "C" int nrq_heavy_download(const nrq_heavy *h, double *q, double *a) {
+  if (!h || !q || !a) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = h->ctx;
+  const int64_t V = ctx->lat.V;
+  int rc = set_device(ctx);
+  if (!rc) rc = ensure_stage(ctx, sizeof(double2) * 72 * V);
+  if (rc) return rc;
+  double2 *stg = (double2 *)ctx->d_stage;
+  nrq::launch_prop_soa2f(h->P, stg, V, ctx->stream);
+  if ((rc = check_launch(ctx, "k_prop_soa2f"))) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(q, stg, sizeof(double2) * 36 * V, cudaMemcpyDeviceToHost, ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(a, stg + 36 * V, sizeof(double2) * 36 * V, cudaMemcpyDeviceToHost, ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return NRQ_OK;
+}
+
+extern "C" int nrq_heavy_copy(nrq_heavy *dst, const nrq_heavy *src) {
+  if (!dst || !src || dst->ctx != src->ctx) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = dst->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(dst->P, src->P, sizeof(double2) * 72 * ctx->lat.V, cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
+  return NRQ_OK;
+}
+
+extern "C" int nrq_heavy_init_single_point(nrq_heavy *h, int64_t lq, int64_t la) {
+  if (!h) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = h->ctx;
+  const int64_t V = ctx->lat.V;
+  if (lq < 1 || lq > V || la < 1 || la > V) {
+    ctx->last_error = "InitSinglePoint: lattice index out of range";
+    return NRQ_ERR_BAD_ARG;
+  }
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  nrq::launch_single_point(h->P, V, lq - 1, la - 1, ctx->stream);
+  return check_launch(ctx, "k_single_point");
+}
+
+extern "C" int nrq_heavy_norms(nrq_heavy *h, double *nq, double *na) {
+  if (!h) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = h->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  int64_t nb_ = nblk(ctx->lat.V, 256);
+  if ((rc = ensure_red(ctx, nb_ * 2))) return rc;
+  nrq::launch_norms(h->P, ctx->lat.V, ctx->d_red, nb_, ctx->stream);
+  if ((rc = check_launch(ctx, "k_norms"))) return rc;
+  if ((rc = reduce_to_host(ctx, nb_, 2, 0u))) return rc;
+  if (nq) *nq = std::sqrt(ctx->h_res[0]);
+  if (na) *na = std::sqrt(ctx->h_res[1]);
+  return NRQ_OK;
+}
+
+extern "C" int nrq_heavy_correlators(nrq_heavy *h, double out[8]) {
+  if (!h || !out) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = h->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  int64_t nb_ = nblk(ctx->lat.V, 128);
+  if ((rc = ensure_red(ctx, nb_ * 8))) return rc;
+  nrq::launch_correlators(h->P, ctx->lat.V, ctx->d_red, nb_, ctx->stream);
+  if ((rc = check_launch(ctx, "k_correlators"))) return rc;
+  if ((rc = reduce_to_host(ctx, nb_, 8, 0u))) return rc;
+  for (int k = 0; k < 8; ++k) out[k] = ctx->h_res[k];
+  return NRQ_OK;
+}
+
+// ====================================================================== CN solver
+extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, double tol,
+                           int64_t maxits, int form, nrq_cn **out) {
+  if (!ctx || !c || !out) return NRQ_ERR_BAD_ARG;
+  *out = nullptr;
+  if (mass == 0.0 || !(tol > 0.0) || maxits < 1 || form != 0) {
+    ctx->last_error = "nrq_cn_init: invalid mass, tolerance, maxits or form";
+    return NRQ_ERR_BAD_ARG;
+  }
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  nrq_cn *cn = new (std::nothrow) nrq_cn();
+  if (!cn) return NRQ_ERR_OOM;
+  cn->ctx = ctx;
+  cn->mass = mass;
+  for (int k = 0; k < 8; ++k) cn->c[k] = c[k];
+  cn->stepwidth = stepwidth;
+  cn->tol = tol;
+  cn->maxits = maxits;
+  cn->form = form;
+  const int64_t V = ctx->lat.V;
+  cn->nblocks = (V + nrq::CN_SITES_PER_BLOCK - 1) / nrq::CN_SITES_PER_BLOCK;
+  bool ok = true;
+  auto alloc = [&](void **p, size_t bytes) {
+    if (ok && cudaMalloc(p, bytes) != cudaSuccess) ok = false;
+  };
+  alloc((void **)&cn->Dsum, sizeof(double2) * 9 * V);
+  alloc((void **)&cn->Bsum, sizeof(double) * 9 * V);
+  alloc((void **)&cn->DE, sizeof(double2) * 54 * V);
+  for (double2 **pp : {&cn->b, &cn->x, &cn->r, &cn->rh, &cn->p, &cn->v, &cn->t})
+    alloc((void **)pp, sizeof(double2) * 72 * V);
+  alloc((void **)&cn->scal, sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE);
+  alloc((void **)&cn->partials, sizeof(double) * cn->nblocks * nrq::CN_COLS * 3);
+  if (ok && cudaMallocHost((void **)&cn->h_scal, sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE) != cudaSuccess)
+    ok = false;
+  if (!ok) {
+    cudaGetLastError();
+    nrq_cn_finalize(cn);
+    ctx->last_error = "nrq_cn_init: device allocation failed";
+    return NRQ_ERR_OOM;
+  }
+  NRQ_CUDA_TRY(ctx, cudaMemsetAsync(cn->scal, 0, sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE, ctx->stream));
+  *out = cn;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_finalize(nrq_cn *cn) {
+  if (!cn) return NRQ_ERR_NOT_INITIALISED;
+  cudaSetDevice(cn->ctx->device);
+  cudaStreamSynchronize(cn->ctx->stream);
+  for (void *p : {(void *)cn->Dsum, (void *)cn->Bsum, (void *)cn->DE, (void *)cn->b, (void *)cn->x, (void *)cn->r,
+                  (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->scal,
+                  (void *)cn->partials})
+    if (p) cudaFree(p);
+  if (cn->h_scal) cudaFreeHost(cn->h_scal);
+  delete cn;
+  return NRQ_OK;
+}
+
+namespace {
+// algorithmic bytes of one 12-column stencil launch: vector streams of
+// 12 x 6 complex per site plus the gauge inputs U and E read once
+double mv_bytes(const nrq_ctx *ctx, int mode) {
+  const int streams[5] = {2, 3, 5, 3, 3};
+  return (double)ctx->lat.V * (1152.0 * streams[mode] + 432.0 + 192.0);
+}
+void mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq::MvArgs &a) {
+  nrq_ctx *ctx = cn->ctx;
+  ProfScope ps(ctx, 0, mv_bytes(ctx, mode));
+  nrq::launch_cn_mv(mode, ctx->lat, C, g->U, cn->Dsum, cn->Bsum, cn->DE, a, ctx->stream);
+}
+void fin(nrq_cn *cn, int stage) {
+  nrq_ctx *ctx = cn->ctx;
+  ProfScope ps(ctx, 2, (double)cn->nblocks * 12 * 3 * 8);
+  nrq::launch_cn_finalize(stage, cn->nblocks, cn->partials, cn->scal, cn->tol, ctx->stream);
+}
+int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
+  nrq_ctx *ctx = cn->ctx;
+  ProfScope ps(ctx, 3, (double)ctx->lat.V * (432.0 + 192.0));
+  nrq::launch_cn_prepare(ctx->lat, g->U, g->E, cn->Dsum, cn->Bsum, cn->DE, ctx->stream);
+  return check_launch(ctx, "k_cn_prepare");
+}
+}  // namespace
+
+extern "C" int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const double c[8], double dt, int herm,
+                            const nrq_heavy *in, nrq_heavy *out) {
+  if (!cn || !g || !c || !in || !out || in == out) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = cn->ctx;
+  if (g->ctx != ctx || in->ctx != ctx || out->ctx != ctx || mass == 0.0) return NRQ_ERR_BAD_ARG;
+  int rc = set_device(ctx);
+  if (!rc) rc = cn_prepare(cn, g);
+  if (rc) return rc;
+  nrq::CnCoef C = make_coef(ctx, mass, c, dt, herm != 0);
+  nrq::MvArgs a{};
+  a.in = in->P;
+  a.out = out->P;
+  mv(cn, nrq::MV_PLAIN, C, g, a);
+  return check_launch(ctx, "k_cn_mv");
+}
+
+extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass, const double c[8],
+                                   double dt, nrq_cn_stats *stats) {
+  if (!cn || !h || !g || !c) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = cn->ctx;
+  if (g->ctx != ctx || h->ctx != ctx || mass == 0.0) return NRQ_ERR_BAD_ARG;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  cudaStream_t st = ctx->stream;
+  const nrq::Lat L = ctx->lat;
+  const nrq::CnCoef CA = make_coef(ctx, mass, c, dt, false);
+  const nrq::CnCoef CH = make_coef(ctx, mass, c, dt, true);
+  if ((rc = cn_prepare(cn, g))) return rc;
+  int64_t matvecs = 0, vstreams = 0;
+  // RHS = A psi ; extrapolated start x0 = 2 RHS - psi
+  {
+    nrq::MvArgs a{};
+    a.in = h->P;
+    a.out = cn->b;
+    a.out2 = cn->x;
+    mv(cn, nrq::MV_RHS, CA, g, a);
+    matvecs += 1;
+    vstreams += 1;  // extra write of x0
+  }
+  bool restart = true, just_restarted = false;
+  int64_t its = 0;
+  int status = NRQ_OK;
+  double *hs = cn->h_scal;
+  const size_t scal_bytes = sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE;
+  for (;;) {
+    if (restart) {
+      nrq::MvArgs a{};
+      a.in = cn->x;
+      a.bvec = cn->b;
+      a.out = cn->r;
+      a.out2 = cn->rh;
+      a.out3 = cn->p;
+      a.partials = cn->partials;
+      mv(cn, nrq::MV_RES, CH, g, a);
+      fin(cn, 0);
+      matvecs += 1;
+      vstreams += 3;  // b read, rh and p writes
+      restart = false;
+      just_restarted = true;
+    } else {
+      just_restarted = false;
+      if (its >= cn->maxits) {
+        status = NRQ_ERR_NOT_CONVERGED;
+        break;
+      }
+      nrq::MvArgs a{};
+      a.in = cn->p;
+      a.in2 = cn->rh;
+      a.out = cn->v;
+      a.partials = cn->partials;
+      a.scal = cn->scal;
+      mv(cn, nrq::MV_V, CH, g, a);
+      fin(cn, 1);
+      nrq::MvArgs b{};
+      b.in = cn->r;
+      b.in2 = cn->v;
+      b.out = cn->t;
+      b.partials = cn->partials;
+      b.scal = cn->scal;
+      mv(cn, nrq::MV_T, CH, g, b);
+      fin(cn, 2);
+      {
+        ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 8);
+        nrq::launch_vec_xr(L, cn->x, cn->r, cn->p, cn->v, cn->t, cn->rh, cn->scal, cn->partials, st);
+      }
+      fin(cn, 3);
+      {
+        ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 4);
+        nrq::launch_vec_p(L, cn->p, cn->r, cn->v, cn->scal, st);
+      }
+      matvecs += 2;
+      vstreams += 1 + 1 + 8 + 4;
+      ++its;
+    }
+    if ((rc = check_launch(ctx, "cn iteration"))) return rc;
+    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(hs, cn->scal, scal_bytes, cudaMemcpyDeviceToHost, st));
+    NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    bool all = true, brk = false, nonfin = false;
+    for (int k = 0; k < nrq::CN_COLS; ++k) {
+      const double *s = hs + k * nrq::SC_STRIDE;
+      all = all && s[nrq::SC_CONV] != 0.0;
+      brk = brk || s[nrq::SC_BREAK] != 0.0;
+      nonfin = nonfin || s[nrq::SC_NONFIN] != 0.0;
+    }
+    if (nonfin) {
+      status = NRQ_ERR_NONFINITE;
+      ctx->last_error = "CN solve: non-finite residual";
+      break;
+    }
+    if (all) {
+      // every column below tolerance: accept once a true residual b - A^H x
+      // (the restart pass) confirms it, otherwise recompute it first
+      if (just_restarted) break;
+      restart = true;
+      continue;
+    }
+    if (brk) restart = true;
+  }
+  // result -> propagator (swap buffers)
+  std::swap(h->P, cn->x);
+  double maxrel = 0.0;
+  bool conv = true;
+  for (int k = 0; k < nrq::CN_COLS; ++k) {
+    const double *s = hs + k * nrq::SC_STRIDE;
+    double rel = s[nrq::SC_BB] > 0 ? std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]) : 0.0;
+    maxrel = std::max(maxrel, rel);
+    conv = conv && s[nrq::SC_CONV] != 0.0;
+  }
+  cn->last_iterations = its;
+  cn->last_matvecs = matvecs;
+  cn->last_vecstreams = vstreams;
+  if (stats) {
+    stats->iterations = its;
+    stats->matvecs = matvecs;
+    stats->vector_streams = vstreams;
+    stats->max_rel_residual = maxrel;
+    stats->converged = conv ? 1 : 0;
+  }
+  return status;
+}

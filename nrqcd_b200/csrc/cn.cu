@@ -1,0 +1,746 @@
+// Heavy-quark kernels of the hot path (FP64): the Crank-Nicolson step of
+// src/nrqcd.f90:1053-1168 with the operator PETSc assembles in
+// BuildSystemMatrix (src/nrqcd.f90:1175-1387) applied matrix-free.
+//
+// Operator.  With kappa = -i a0 dt/2 the source writes, per row site x,
+// 6x6 blocks SubMat(x,y) = delta_xy 1 + kappa * (sum of terms); PETSc reads
+// each column-major block row-major (src/nrqcd.f90:1014-1018), so the
+// evolved operator holds SubMat^T.  Splitting the terms,
+//   A = 1 + sum_t alpha_t G_t,  t in {kinetic, magnetic, Darwin, spin-orbit}
+// with every G_t hermitian (c_t factored out), hence A^H = 1 + sum conj(alpha_t) G_t.
+// Per site, with E_j(y) = -Re(E~_j^a(y) T^a)/(a0 a_j) (= -F_0j of
+// gauge:1563-1581 for eigenphases inside the principal branch):
+//   G_kin  psi(x) = sum_i 1/a_i^2 [psi(x) - 1/2 (U_i(x)^T x 1) psi(x+i)
+//                                           - 1/2 (U_i(x-i)^* x 1) psi(x-i)]
+//   G_mag  psi(x) = (B(x)^T x 1) psi(x),  B = sum_i F_jk (nrqcd:1669-1693: B_i x 1, no sigma)
+//   G_dar  psi(x) = (D(x)^T x 1) psi(x),  D = sum_i [U_i E_i(x+i) U_i^+ - U_i(x-i)^+ E_i(x-i) U_i(x-i)]/(2a_i)
+//   G_so   psi(x) = sum_i sum_(j,k,eps) eps i [(DE_ij(x)^T x s_k^T) psi(x+i)
+//                                            - (DE_ij(x-i)^* x s_k^T) psi(x-i)]
+//          DE_ij(x) = (E_j(x) U_i(x) + U_i(x) E_j(x+i))/(2 a_i)
+//   alpha_kin = kappa c1/M, alpha_mag = -kappa c2/(2M), alpha_dar = -kappa c3/(8M^2),
+//   alpha_so = -kappa c4/(8M^2); antiquark: M -> -M, c -> conj(c).
+//
+// Layout: propagator planes (species*36 + col*6 + row), V complex each.
+// The matvec runs 12 warps per block, one warp per (species, column), all
+// warps over the same 32 sites so that the gauge-derived matrices are read
+// once from HBM and then from L1.
+#include "nrq_kernels.cuh"
+
+namespace nrq {
+
+// ------------------------------------------------------------ Jacobi log
+// Complex Jacobi eigen-decomposition of a general 3x3 matrix, the algorithm
+// of src/matrixoperations.f90:327-459 (d = U A U^+, rows of U normalised).
+__device__ void eigenc3(const m3 &Ain, cplx d[3], m3 &U) {
+  const double EPS = 9.860761315262648e-32;  // 2^-103
+  m3 A = Ain;
+  cplx ev0[3], ev1[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    ev0[p] = {0.0, 0.0};
+    ev1[p] = A.e[p * 4];
+    d[p] = ev1[p];
+  }
+  U = m3_id();
+  const double red = 0.01 / 81.0;
+  for (int sweep = 1; sweep <= 50; ++sweep) {
+    double off = 0.0;
+    for (int q = 1; q < 3; ++q)
+      for (int p = 0; p < q; ++p) {
+        double a1 = cabs_(A.e[p * 3 + q]), a2 = cabs_(A.e[q * 3 + p]);
+        off = off + a1 * a1 + a2 * a2;
+      }
+    if (off <= EPS) break;
+    double thresh = (sweep < 4) ? off * red : 0.0;
+    for (int q = 1; q < 3; ++q) {
+      for (int p = 0; p < q; ++p) {
+        double a1 = cabs_(A.e[p * 3 + q]), a2 = cabs_(A.e[q * 3 + p]);
+        off = a1 * a1 + a2 * a2;
+        double e1 = cabs_(ev1[p]), e2 = cabs_(ev1[q]);
+        if (sweep > 4 && off < EPS * (e1 * e1 + e2 * e2)) {
+          A.e[p * 3 + q] = {0.0, 0.0};
+          A.e[q * 3 + p] = {0.0, 0.0};
+        } else if (off > thresh) {
+          cplx delta = A.e[p * 3 + q] * A.e[q * 3 + p];
+          cplx x = 0.5 * (ev1[p] - ev1[q]);
+          cplx y = csqrt_(x * x + delta);
+          cplx t = x - y;
+          cplx s = x + y;
+          if (cabs_(t) < cabs_(s)) t = s;
+          t = cdiv({1.0, 0.0}, t);
+          delta = delta * t;
+          ev0[p] = ev0[p] + delta;
+          ev1[p] = d[p] + ev0[p];
+          ev0[q] = ev0[q] - delta;
+          ev1[q] = d[q] + ev0[q];
+          cplx invc = csqrt_(delta * t + cplx{1.0, 0.0});
+          s = cdiv(t, invc);
+          t = cdiv(t, invc + cplx{1.0, 0.0});
+          cplx sx = s * A.e[p * 3 + q], ty = t * A.e[p * 3 + q];
+          cplx sy = s * A.e[q * 3 + p], tx = t * A.e[q * 3 + p];
+          for (int j = 0; j < 3; ++j) {
+            x = A.e[j * 3 + p];
+            y = A.e[j * 3 + q];
+            A.e[j * 3 + p] = x + sy * (y - ty * x);
+            A.e[j * 3 + q] = y - sx * (x + tx * y);
+            x = A.e[p * 3 + j];
+            y = A.e[q * 3 + j];
+            A.e[p * 3 + j] = x + sx * (y - tx * x);
+            A.e[q * 3 + j] = y - sy * (x + ty * y);
+          }
+          A.e[p * 3 + q] = {0.0, 0.0};
+          A.e[q * 3 + p] = {0.0, 0.0};
+          for (int j = 0; j < 3; ++j) {
+            x = U.e[p * 3 + j];
+            y = U.e[q * 3 + j];
+            U.e[p * 3 + j] = x + sx * (y - tx * x);
+            U.e[q * 3 + j] = y - sy * (x + ty * y);
+          }
+        }
+      }
+    }
+    for (int p = 0; p < 3; ++p) {
+      ev0[p] = {0.0, 0.0};
+      d[p] = ev1[p];
+    }
+  }
+  for (int p = 0; p < 3; ++p) {
+    double nrm = 0.0;
+    for (int q = 0; q < 3; ++q) nrm += norm2(U.e[p * 3 + q]);
+    nrm = 1.0 / sqrt(nrm);
+    for (int q = 0; q < 3; ++q) U.e[p * 3 + q] = nrm * U.e[p * 3 + q];
+  }
+}
+
+// Re(LogU(P)/i) = Im(S^+ diag(i theta) S) for unitary P (matrixoperations:510-531)
+__device__ void field_strength_from_plaquette(const m3 &P, double scale_, double F[9]) {
+  cplx ev[3];
+  m3 S;
+  eigenc3(P, ev, S);
+  double th[3];
+  for (int k = 0; k < 3; ++k) th[k] = atan2(ev[k].im, ev[k].re);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        // Re(conj(S[k][r]) * S[k][c])
+        cplx a = S.e[k * 3 + r], b = S.e[k * 3 + c];
+        acc += th[k] * (a.re * b.re + a.im * b.im);
+      }
+      F[r * 3 + c] = acc * scale_;
+    }
+}
+
+// E_j(y) entering the CN operator: -Re(sum_a E~^a T^a)/a0/a_j (real symmetric)
+__device__ __forceinline__ m3 efield_cn(const Lat &L, const double *__restrict__ E, int64_t y, int j) {
+  const int64_t V = L.V;
+  const double h = 0.5, s8 = 0.5 / 1.7320508075688772, d8 = 1.0 / 1.7320508075688772;
+  const double *e = E + (int64_t)(j * 8) * V + y;
+  double e1 = __ldg(e), e3 = __ldg(e + 2 * V), e4 = __ldg(e + 3 * V), e6 = __ldg(e + 5 * V),
+         e8 = __ldg(e + 7 * V);
+  const double f = -1.0 / L.a0 / L.a[j];
+  m3 M = m3_zero();
+  M.e[0].re = (h * e3 + s8 * e8) * f;
+  M.e[4].re = (-h * e3 + s8 * e8) * f;
+  M.e[8].re = (-d8 * e8) * f;
+  M.e[1].re = M.e[3].re = (h * e1) * f;
+  M.e[2].re = M.e[6].re = (h * e4) * f;
+  M.e[5].re = M.e[7].re = (h * e6) * f;
+  return M;
+}
+
+__global__ void __launch_bounds__(128) k_cn_prepare(Lat L, const double2 *__restrict__ U,
+                                                    const double *__restrict__ E, double2 *__restrict__ Dsum,
+                                                    double *__restrict__ Bsum, double2 *__restrict__ DE) {
+  int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (x >= L.V) return;
+  const int64_t V = L.V;
+  // Darwin
+  m3 D = m3_zero();
+  for (int i = 0; i < 3; ++i) {
+    int64_t xp = nb(L, x, i, +1), xm = nb(L, x, i, -1);
+    m3 u = load_link(U, V, x, i), um = load_link(U, V, xm, i);
+    m3 t1 = mul_nd(mul(u, efield_cn(L, E, xp, i)), u);
+    m3 t2 = mul(mul_dn(um, efield_cn(L, E, xm, i)), um);
+    D = add(D, scale(sub(t1, t2), 1.0 / (2.0 * L.a[i])));
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) st(Dsum + (int64_t)k * V + x, D.e[k]);
+  // magnetic: B_i = F_jk with (i,j,k) cyclic
+  double B[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < 3; ++i) {
+    int j = (i + 1) % 3, k = (i + 2) % 3;
+    // P_jk = U_j(x) U_k(x+j) U_j(x+k)^+ U_k(x)^+
+    m3 P = mul_nd(mul_nd(mul(load_link(U, V, x, j), load_link(U, V, nb(L, x, j, +1), k)),
+                         load_link(U, V, nb(L, x, k, +1), j)),
+                  load_link(U, V, x, k));
+    double F[9];
+    field_strength_from_plaquette(P, 1.0 / L.a[j] / L.a[k], F);
+    for (int m = 0; m < 9; ++m) B[m] += F[m];
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) Bsum[(int64_t)k * V + x] = B[k];
+  // spin-orbit colour matrices
+  for (int i = 0; i < 3; ++i) {
+    int64_t xp = nb(L, x, i, +1);
+    m3 u = load_link(U, V, x, i);
+    for (int perm = 0; perm < 2; ++perm) {
+      int j = perm == 0 ? (i + 1) % 3 : (i + 2) % 3;
+      m3 d = scale(add(mul(efield_cn(L, E, x, j), u), mul(u, efield_cn(L, E, xp, j))), 0.5 / L.a[i]);
+      double2 *dst = DE + (int64_t)((i * 2 + perm) * 9) * V + x;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) st(dst + (int64_t)k * V, d.e[k]);
+    }
+  }
+}
+
+void launch_cn_prepare(Lat L, const double2 *U, const double *E, double2 *Dsum, double *Bsum, double2 *DE,
+                       cudaStream_t st) {
+  int64_t nb_ = (L.V + 127) / 128;
+  k_cn_prepare<<<(unsigned)nb_, 128, 0, st>>>(L, U, E, Dsum, Bsum, DE);
+}
+
+// ------------------------------------------------------------ matvec
+// u = s_k^T w (transposed reference Pauli matrix, src/su2.f90:68-79), index 2c+s
+__device__ __forceinline__ void sigmaT(int k, const cplx w[6], cplx u[6]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    cplx w0 = w[2 * c], w1 = w[2 * c + 1];
+    if (k == 0) {
+      u[2 * c] = w1;
+      u[2 * c + 1] = w0;
+    } else if (k == 1) {
+      u[2 * c] = -times_i(w1);
+      u[2 * c + 1] = times_i(w0);
+    } else {
+      u[2 * c] = w0;
+      u[2 * c + 1] = -w1;
+    }
+  }
+}
+
+// acc[2c+s] += sum_c' M[c'][c] u[2c'+s]    (M^T x 1)
+__device__ __forceinline__ void apply_T(const double2 *__restrict__ Mp, int64_t V, int64_t y, const cplx u[6],
+                                        cplx acc[6]) {
+#pragma unroll
+  for (int cp = 0; cp < 3; ++cp)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cplx m = ldg(Mp + (int64_t)(cp * 3 + c) * V + y);
+      cmac(acc[2 * c], m, u[2 * cp]);
+      cmac(acc[2 * c + 1], m, u[2 * cp + 1]);
+    }
+}
+// acc[2c+s] += sum_c' conj(M[c][c']) u[2c'+s]    (M^* x 1)
+__device__ __forceinline__ void apply_C(const double2 *__restrict__ Mp, int64_t V, int64_t y, const cplx u[6],
+                                        cplx acc[6]) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int cp = 0; cp < 3; ++cp) {
+      cplx m = ldg(Mp + (int64_t)(c * 3 + cp) * V + y);
+      cmac_cj(acc[2 * c], m, u[2 * cp]);
+      cmac_cj(acc[2 * c + 1], m, u[2 * cp + 1]);
+    }
+}
+
+__device__ __forceinline__ cplx scal_c(const double *sc, int col, int slot) {
+  return {sc[col * SC_STRIDE + slot], sc[col * SC_STRIDE + slot + 1]};
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(384) k_cn_mv(Lat L, CnCoef C, const double2 *__restrict__ U,
+                                               const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
+                                               const double2 *__restrict__ DE, MvArgs A) {
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;  // column index 0..11
+  const int sp = w / 6;
+  const int64_t V = L.V;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  const bool active = x0 < V;
+  const int64_t x = active ? x0 : 0;
+  const int64_t pb = (int64_t)(w * 6) * V;  // (sp*36 + col*6) = w*6
+  cplx als = {0.0, 0.0};
+  if (MODE == MV_T) als = scal_c(A.scal, w, SC_ALPHA);
+
+  auto load_in = [&](int64_t y, cplx v[6]) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      v[r] = ldg(A.in + pb + (int64_t)r * V + y);
+      if (MODE == MV_T) v[r] = v[r] - als * ldg(A.in2 + pb + (int64_t)r * V + y);
+    }
+  };
+
+  cplx w0[6], acc[6];
+  load_in(x, w0);
+#pragma unroll
+  for (int r = 0; r < 6; ++r) acc[r] = w0[r];
+  const cplx ak = C.kin[sp], am = C.mag[sp], ad = C.dar[sp], aso = C.so[sp];
+  // diagonal colour block: (ak*dkin) 1 + ad D^T + am B^T
+  {
+    cplx Cd[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int cp = 0; cp < 3; ++cp) {
+        cplx dv = ldg(Dsum + (int64_t)(cp * 3 + c) * V + x);
+        double bv = __ldg(Bsum + (int64_t)(cp * 3 + c) * V + x);
+        cplx v = ad * dv + bv * am;
+        if (c == cp) v = v + C.dkin * ak;
+        Cd[c * 3 + cp] = v;
+      }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int cp = 0; cp < 3; ++cp) {
+        cmac(acc[2 * c], Cd[c * 3 + cp], w0[2 * cp]);
+        cmac(acc[2 * c + 1], Cd[c * 3 + cp], w0[2 * cp + 1]);
+      }
+  }
+  const cplx cs0 = times_i(aso);   // eps = +1 permutation
+  const cplx cs1 = -times_i(aso);  // eps = -1 permutation
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+    const cplx ck = (-0.5 * C.inva2[i]) * ak;
+    const int k0 = (i + 2) % 3, k1 = (i + 1) % 3;
+    cplx wv[6], t[6], u[6];
+    // ---- +i neighbour: blocks from site x
+    {
+      const int64_t y = nb(L, x, i, +1);
+      load_in(y, wv);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) t[r] = ck * wv[r];
+      apply_T(U + (int64_t)(i * 9) * V, V, x, t, acc);
+      sigmaT(k0, wv, u);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) t[r] = cs0 * u[r];
+      apply_T(DE + (int64_t)((i * 2 + 0) * 9) * V, V, x, t, acc);
+      sigmaT(k1, wv, u);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) t[r] = cs1 * u[r];
+      apply_T(DE + (int64_t)((i * 2 + 1) * 9) * V, V, x, t, acc);
+    }
+    // ---- -i neighbour: blocks from site y = x-i
+    {
+      const int64_t y = nb(L, x, i, -1);
+      load_in(y, wv);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) t[r] = ck * wv[r];
+      apply_C(U + (int64_t)(i * 9) * V, V, y, t, acc);
+      sigmaT(k0, wv, u);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) t[r] = -(cs0 * u[r]);
+      apply_C(DE + (int64_t)((i * 2 + 0) * 9) * V, V, y, t, acc);
+      sigmaT(k1, wv, u);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) t[r] = -(cs1 * u[r]);
+      apply_C(DE + (int64_t)((i * 2 + 1) * 9) * V, V, y, t, acc);
+    }
+  }
+
+  // ---------------- epilogue by mode
+  double q[3] = {0.0, 0.0, 0.0};
+  if (MODE == MV_PLAIN) {
+    if (active)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) st(A.out + pb + (int64_t)r * V + x, acc[r]);
+  } else if (MODE == MV_RHS) {
+    if (active)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        st(A.out + pb + (int64_t)r * V + x, acc[r]);
+        st(A.out2 + pb + (int64_t)r * V + x, 2.0 * acc[r] - w0[r]);
+      }
+  } else if (MODE == MV_RES) {
+    if (active)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        cplx b = ldg(A.bvec + pb + (int64_t)r * V + x);
+        cplx rr = b - acc[r];
+        st(A.out + pb + (int64_t)r * V + x, rr);
+        st(A.out2 + pb + (int64_t)r * V + x, rr);
+        st(A.out3 + pb + (int64_t)r * V + x, rr);
+        q[0] += norm2(rr);
+        q[1] += norm2(b);
+      }
+  } else if (MODE == MV_V) {
+    if (active)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        st(A.out + pb + (int64_t)r * V + x, acc[r]);
+        cplx h = ldg(A.in2 + pb + (int64_t)r * V + x);
+        cplx d = {0.0, 0.0};
+        cmac_cj(d, h, acc[r]);
+        q[0] += d.re;
+        q[1] += d.im;
+      }
+  } else if (MODE == MV_T) {
+    if (active)
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        st(A.out + pb + (int64_t)r * V + x, acc[r]);
+        cplx d = {0.0, 0.0};
+        cmac_cj(d, acc[r], w0[r]);  // (t . s)
+        q[0] += d.re;
+        q[1] += d.im;
+        q[2] += norm2(acc[r]);
+      }
+  }
+  if (MODE == MV_RES || MODE == MV_V || MODE == MV_T) {
+    constexpr int NQ = (MODE == MV_T) ? 3 : 2;
+#pragma unroll
+    for (int k = 0; k < NQ; ++k) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) q[k] += __shfl_down_sync(0xffffffffu, q[k], o);
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) A.partials[((int64_t)blockIdx.x * CN_COLS + w) * NQ + k] = q[k];
+  }
+}
+
+void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,
+                  const double2 *DE, const MvArgs &a, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  dim3 blk(32 * CN_COLS);
+  switch (mode) {
+    case MV_PLAIN: k_cn_mv<MV_PLAIN><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_RHS: k_cn_mv<MV_RHS><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_RES: k_cn_mv<MV_RES><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_V: k_cn_mv<MV_V><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    default: k_cn_mv<MV_T><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+  }
+}
+
+// ------------------------------------------------------------ BiCGStab vector updates
+// s = r - alpha v ; x += alpha p + omega s ; r = s - omega t ; partials (rh.r), (r.r)
+__global__ void __launch_bounds__(384) k_vec_xr(int64_t V, double2 *__restrict__ X, double2 *__restrict__ R,
+                                                const double2 *__restrict__ P, const double2 *__restrict__ Vv,
+                                                const double2 *__restrict__ T, const double2 *__restrict__ RH,
+                                                const double *__restrict__ scal, double *__restrict__ partials) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  const bool active = x0 < V;
+  const int64_t pb = (int64_t)(w * 6) * V;
+  const cplx al = scal_c(scal, w, SC_ALPHA), om = scal_c(scal, w, SC_OMEGA);
+  double q[3] = {0.0, 0.0, 0.0};
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int64_t o = pb + (int64_t)r * V + x0;
+      cplx s = ld(R + o) - al * ldg(Vv + o);
+      cplx xn = ld(X + o) + al * ldg(P + o) + om * s;
+      cplx rn = s - om * ldg(T + o);
+      st(X + o, xn);
+      st(R + o, rn);
+      cplx d = {0.0, 0.0};
+      cmac_cj(d, ldg(RH + o), rn);
+      q[0] += d.re;
+      q[1] += d.im;
+      q[2] += norm2(rn);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q[k] += __shfl_down_sync(0xffffffffu, q[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) partials[((int64_t)blockIdx.x * CN_COLS + w) * 3 + k] = q[k];
+}
+
+// p = r + beta (p - omega v)
+__global__ void __launch_bounds__(384) k_vec_p(int64_t V, double2 *__restrict__ P, const double2 *__restrict__ R,
+                                               const double2 *__restrict__ Vv, const double *__restrict__ scal) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  if (x0 >= V) return;
+  const int64_t pb = (int64_t)(w * 6) * V;
+  const cplx be = scal_c(scal, w, SC_BETA), om = scal_c(scal, w, SC_OMEGA);
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    const int64_t o = pb + (int64_t)r * V + x0;
+    st(P + o, ldg(R + o) + be * (ld(P + o) - om * ldg(Vv + o)));
+  }
+}
+
+void launch_vec_xr(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *v, const double2 *t,
+                   const double2 *rh, const double *scal, double *partials, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  k_vec_xr<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, x, r, p, v, t, rh, scal, partials);
+}
+void launch_vec_p(Lat L, double2 *p, const double2 *r, const double2 *v, const double *scal, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  k_vec_p<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, p, r, v, scal);
+}
+
+// ------------------------------------------------------------ scalar stages
+__device__ __forceinline__ cplx cdiv_safe(cplx a, cplx b) { return cdiv(a, b); }
+
+__global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restrict__ partials,
+                              double *__restrict__ scal, double tol) {
+  const int col = blockIdx.x;
+  const int nq = (stage == 0 || stage == 1) ? 2 : 3;
+  __shared__ double sh[3][256];
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int k = 0; k < nq; ++k) acc[k] += partials[(b * CN_COLS + col) * nq + k];
+  for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int wd = blockDim.x / 2; wd > 0; wd >>= 1) {
+    if (threadIdx.x < wd)
+      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + wd];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double *sc = scal + col * SC_STRIDE;
+  const double q0 = sh[0][0], q1 = sh[1][0], q2 = sh[2][0];
+  const bool conv = sc[SC_CONV] != 0.0;
+  if (stage == 0) {  // rr, bb after a (re)start
+    sc[SC_RR] = q0;
+    sc[SC_BB] = q1;
+    sc[SC_RHO] = q0;
+    sc[SC_RHO + 1] = 0.0;
+    sc[SC_CONV] = (q0 <= tol * tol * q1 || q1 == 0.0) ? 1.0 : 0.0;
+    sc[SC_BREAK] = 0.0;
+    sc[SC_NONFIN] = (isfinite(q0) && isfinite(q1)) ? 0.0 : 1.0;
+    sc[SC_ALPHA] = sc[SC_ALPHA + 1] = sc[SC_OMEGA] = sc[SC_OMEGA + 1] = sc[SC_BETA] = sc[SC_BETA + 1] = 0.0;
+  } else if (stage == 1) {  // alpha = rho / (rh . v)
+    cplx den = {q0, q1};
+    cplx rho = {sc[SC_RHO], sc[SC_RHO + 1]};
+    cplx al = {0.0, 0.0};
+    if (!conv) {
+      if (den.re == 0.0 && den.im == 0.0) sc[SC_BREAK] = 1.0;
+      else al = cdiv(rho, den);
+    }
+    sc[SC_ALPHA] = al.re;
+    sc[SC_ALPHA + 1] = al.im;
+  } else if (stage == 2) {  // omega = (t.s)/(t.t)
+    cplx om = {0.0, 0.0};
+    if (!conv && q2 > 0.0) om = (1.0 / q2) * cplx{q0, q1};
+    sc[SC_OMEGA] = om.re;
+    sc[SC_OMEGA + 1] = om.im;
+  } else {  // stage 3: rho_new = rh.r, rr = r.r
+    if (!conv) {
+      sc[SC_RR] = q2;
+      if (!isfinite(q2)) sc[SC_NONFIN] = 1.0;
+      bool cv = q2 <= tol * tol * sc[SC_BB];
+      cplx rho = {sc[SC_RHO], sc[SC_RHO + 1]};
+      cplx rhon = {q0, q1};
+      cplx al = {sc[SC_ALPHA], sc[SC_ALPHA + 1]}, om = {sc[SC_OMEGA], sc[SC_OMEGA + 1]};
+      cplx be = {0.0, 0.0};
+      if (cv) {
+        sc[SC_CONV] = 1.0;
+      } else if ((om.re == 0.0 && om.im == 0.0) || (rho.re == 0.0 && rho.im == 0.0)) {
+        sc[SC_BREAK] = 1.0;
+      } else {
+        be = cdiv(rhon, rho) * cdiv(al, om);
+      }
+      sc[SC_BETA] = be.re;
+      sc[SC_BETA + 1] = be.im;
+      sc[SC_RHO] = rhon.re;
+      sc[SC_RHO + 1] = rhon.im;
+    } else {
+      sc[SC_BETA] = sc[SC_BETA + 1] = 0.0;
+    }
+  }
+}
+
+void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
+                        cudaStream_t st) {
+  k_cn_finalize<<<CN_COLS, 256, 0, st>>>(stage, nblocks, partials, scal, tol);
+}
+
+// ------------------------------------------------------------ propagator I/O, norms, correlators
+// Fortran prop(6,6,V): (site*6 + col)*6 + row ; f holds quark then antiquark (2*V*36)
+__global__ void k_prop_f2soa(const double2 *__restrict__ f, double2 *__restrict__ P, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+    for (int k = 0; k < 36; ++k) P[(int64_t)(sp * 36 + k) * V + s] = f[(int64_t)sp * 36 * V + s * 36 + k];
+}
+__global__ void k_prop_soa2f(const double2 *__restrict__ P, double2 *__restrict__ f, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+    for (int k = 0; k < 36; ++k) f[(int64_t)sp * 36 * V + s * 36 + k] = P[(int64_t)(sp * 36 + k) * V + s];
+}
+void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st) {
+  k_prop_f2soa<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(f, P, V);
+}
+void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st) {
+  k_prop_soa2f<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(P, f, V);
+}
+
+__global__ void k_single_point(double2 *__restrict__ P, int64_t V, int64_t sq, int64_t sa) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  const double v = 1.0 / sqrt(6.0);
+  for (int sp = 0; sp < 2; ++sp) {
+    const int64_t src = sp == 0 ? sq : sa;
+#pragma unroll
+    for (int k = 0; k < 36; ++k) {
+      const int col = k / 6, row = k % 6;
+      P[(int64_t)(sp * 36 + k) * V + s] = make_double2((s == src && col == row) ? v : 0.0, 0.0);
+    }
+  }
+}
+void launch_single_point(double2 *P, int64_t V, int64_t sq, int64_t sa, cudaStream_t st) {
+  k_single_point<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(P, V, sq, sa);
+}
+
+__global__ void __launch_bounds__(256) k_norms(const double2 *__restrict__ P, int64_t V, double *partials) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (s < V)
+    for (int sp = 0; sp < 2; ++sp)
+      for (int k = 0; k < 36; ++k) v[sp] += norm2(ldg(P + (int64_t)(sp * 36 + k) * V + s));
+  __shared__ double sh[8][2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 2; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if (lane == 0) {
+    sh[warp][0] = v[0];
+    sh[warp][1] = v[1];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      a += sh[k][0];
+      b += sh[k][1];
+    }
+    partials[blockIdx.x * 2] = a;
+    partials[blockIdx.x * 2 + 1] = b;
+  }
+}
+void launch_norms(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st) {
+  nblk = (V + 255) / 256;
+  k_norms<<<(unsigned)nblk, 256, 0, st>>>(P, V, partials);
+}
+
+// Sparse Gamma tables for the zero-momentum meson correlators
+// (src/nrqcd.f90:1484-1661): entries (row, col, re, im) of Gamma = T^a x s_k,
+// 1 x s_k or T^a x 1 (index 2*colour + spin), with the reference's matrices.
+struct GamEntry {
+  double re, im;
+  int r, c;
+};
+struct GamTable {
+  int ngam[3];       // O1_3S1, O8_1S0, O8_3S1
+  int start[3][24];  // entry offset per Gamma
+  int count[3][24];
+  GamEntry e[3 * 24 * 8];
+};
+__constant__ GamTable c_gam;
+
+__global__ void __launch_bounds__(128) k_correlators(const double2 *__restrict__ P, int64_t V, double *partials) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (s < V) {
+    // Q[r][c] = quark (row r, col c), A likewise
+    auto q = [&](int r, int c) { return ldg(P + (int64_t)(c * 6 + r) * V + s); };
+    auto a = [&](int r, int c) { return ldg(P + (int64_t)(36 + c * 6 + r) * V + s); };
+    // O1_1S0 = i Tr(A^+ Q) = i sum_{rc} conj(A[r][c]) Q[r][c]
+    cplx t = {0.0, 0.0};
+    for (int r = 0; r < 6; ++r)
+      for (int c = 0; c < 6; ++c) cmac_cj(t, a(r, c), q(r, c));
+    cplx o = times_i(t);
+    v[0] = o.re;
+    v[1] = o.im;
+    const double wts[3] = {1.0 / 3.0, 6.0 / 8.0, 6.0 / 24.0};
+    for (int kind = 0; kind < 3; ++kind) {
+      cplx sum = {0.0, 0.0};
+      for (int g = 0; g < c_gam.ngam[kind]; ++g) {
+        const int st0 = c_gam.start[kind][g], n = c_gam.count[kind][g];
+        // Tr(A^+ G Q G) = sum conj(A[d1][d0]) G[d1][d2] Q[d2][d3] G[d3][d0]
+        for (int e1 = 0; e1 < n; ++e1) {
+          const GamEntry ga = c_gam.e[st0 + e1];  // (d1, d2)
+          for (int e2 = 0; e2 < n; ++e2) {
+            const GamEntry gb = c_gam.e[st0 + e2];  // (d3, d0)
+            cplx gg = cplx{ga.re, ga.im} * cplx{gb.re, gb.im};
+            cplx qa = q(ga.c, gb.r);
+            cplx term = {0.0, 0.0};
+            cmac_cj(term, a(ga.r, gb.c), qa);
+            cmac(sum, gg, term);
+          }
+        }
+      }
+      cplx ov = times_i(sum) * wts[kind];
+      v[2 + 2 * kind] = ov.re;
+      v[3 + 2 * kind] = ov.im;
+    }
+  }
+  __shared__ double sh[4][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 8; ++k)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if (lane == 0)
+    for (int k = 0; k < 8; ++k) sh[warp][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double acc = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) acc += sh[k][threadIdx.x];
+    partials[blockIdx.x * 8 + threadIdx.x] = acc;
+  }
+}
+
+static void build_gamma_table(GamTable &T) {
+  // reference generators (row-major) and Pauli matrices (su2.f90 arrays)
+  double Tre[8][9] = {{0}}, Tim[8][9] = {{0}};
+  const double h = 0.5, s8 = 0.5 / 1.7320508075688772, d8 = 1.0 / 1.7320508075688772;
+  Tre[0][1] = Tre[0][3] = h;
+  Tim[1][1] = h; Tim[1][3] = -h;
+  Tre[2][0] = h; Tre[2][4] = -h;
+  Tre[3][2] = Tre[3][6] = h;
+  Tim[4][2] = h; Tim[4][6] = -h;
+  Tre[5][5] = Tre[5][7] = h;
+  Tim[6][5] = h; Tim[6][7] = -h;
+  Tre[7][0] = s8; Tre[7][4] = s8; Tre[7][8] = -d8;
+  double Sre[3][4] = {{0, 1, 1, 0}, {0, 0, 0, 0}, {1, 0, 0, -1}};
+  double Sim[3][4] = {{0, 0, 0, 0}, {0, 1, -1, 0}, {0, 0, 0, 0}};
+  int ne = 0;
+  auto add_gamma = [&](int kind, int g, const double *Are, const double *Aim, const double *Bre,
+                       const double *Bim) {
+    T.start[kind][g] = ne;
+    int cnt = 0;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        for (int s = 0; s < 2; ++s)
+          for (int t = 0; t < 2; ++t) {
+            double ar = Are[r * 3 + c], ai = Aim[r * 3 + c], br = Bre[s * 2 + t], bi = Bim[s * 2 + t];
+            double vr = ar * br - ai * bi, vi = ar * bi + ai * br;
+            if (vr != 0.0 || vi != 0.0) {
+              T.e[ne++] = GamEntry{vr, vi, 2 * r + s, 2 * c + t};
+              ++cnt;
+            }
+          }
+    T.count[kind][g] = cnt;
+  };
+  double I3re[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, I3im[9] = {0};
+  double I2re[4] = {1, 0, 0, 1}, I2im[4] = {0};
+  T.ngam[0] = 3;
+  for (int k = 0; k < 3; ++k) add_gamma(0, k, I3re, I3im, Sre[k], Sim[k]);
+  T.ngam[1] = 8;
+  for (int a = 0; a < 8; ++a) add_gamma(1, a, Tre[a], Tim[a], I2re, I2im);
+  T.ngam[2] = 24;
+  int g = 0;
+  for (int k = 0; k < 3; ++k)
+    for (int a = 0; a < 8; ++a) add_gamma(2, g++, Tre[a], Tim[a], Sre[k], Sim[k]);
+}
+
+void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st) {
+  static GamTable T;
+  static bool built = false;
+  if (!built) {
+    build_gamma_table(T);
+    built = true;
+  }
+  cudaMemcpyToSymbolAsync(c_gam, &T, sizeof(T), 0, cudaMemcpyHostToDevice, st);
+  nblk = (V + 127) / 128;
+  k_correlators<<<(unsigned)nblk, 128, 0, st>>>(P, V, partials);
+}
+
+}  // namespace nrq

@@ -1,0 +1,341 @@
+// Gauge-field kernels of the hot path (FP64):
+//   - leapfrog link update  U <- exp(i dt E^a T^a) U   (gauge:2118-2140)
+//   - leapfrog E update from the U/D staples           (gauge:2147-2259)
+//   - energy (gauge:1769-1817) and both Gauss-law measures (gauge:1480-1531,
+//     :724-768) as deterministic two-stage FP64 reductions
+//   - layout transposes between the reference's Fortran arrays and the
+//     structure-of-arrays planes held in HBM
+//   - the device part of the transverse-polarised initial condition
+//     (gauge:1263-1446): momentum-space construction between two FFTs.
+// Paths are those of the reference project (src/gaugeconfiguration_su3.f90
+// abbreviated "gauge").
+#include "nrq_kernels.cuh"
+
+namespace nrq {
+
+// ------------------------------------------------------------ layout moves
+// Fortran links(3,3,3,V): element (row, col, dir, site) at ((site*3+dir)*3+col)*3+row
+__global__ void k_links_f2soa(const double2 *__restrict__ f, double2 *__restrict__ U, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  const double2 *src = f + s * 27;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) U[(int64_t)(d * 9 + r * 3 + c) * V + s] = src[(d * 3 + c) * 3 + r];
+}
+__global__ void k_links_soa2f(const double2 *__restrict__ U, double2 *__restrict__ f, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+  double2 *dst = f + s * 27;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) dst[(d * 3 + c) * 3 + r] = U[(int64_t)(d * 9 + r * 3 + c) * V + s];
+}
+// Fortran efield(8,3,V): (site*3+dir)*8 + a
+__global__ void k_efield_f2soa(const double *__restrict__ f, double *__restrict__ E, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+#pragma unroll
+  for (int k = 0; k < 24; ++k) E[(int64_t)k * V + s] = f[s * 24 + k];
+}
+__global__ void k_efield_soa2f(const double *__restrict__ E, double *__restrict__ f, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+#pragma unroll
+  for (int k = 0; k < 24; ++k) f[s * 24 + k] = E[(int64_t)k * V + s];
+}
+
+__global__ void k_cold(double2 *__restrict__ U, double *__restrict__ E, int64_t V) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+      U[(int64_t)(d * 9 + k) * V + s] = make_double2((k % 4 == 0) ? 1.0 : 0.0, 0.0);
+#pragma unroll
+  for (int k = 0; k < 24; ++k) E[(int64_t)k * V + s] = 0.0;
+}
+
+// ------------------------------------------------------------ leapfrog
+__global__ void __launch_bounds__(128) k_update_links(Lat L, double2 *__restrict__ U,
+                                                      const double *__restrict__ E, double dt) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= L.V) return;
+  const int64_t V = L.V;
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) {
+    double al[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) al[a] = __ldg(E + (int64_t)(d * 8 + a) * V + s) * dt;
+    m3 G = expi_herm(algebra_matrix(al));
+    m3 u = load_link(U, V, s, d);
+    store_link(U, V, s, d, mul(G, u));
+  }
+}
+
+__global__ void __launch_bounds__(128) k_update_efield(Lat L, const double2 *__restrict__ U,
+                                                       double *__restrict__ E, double dt) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= L.V) return;
+  const int64_t V = L.V;
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+    m3 sum = m3_zero();
+    const int64_t xpi = nb(L, s, i, +1);
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+      if (k == i) continue;
+      const double r = L.a0 / L.a[k];
+      const double coef = dt * (r * r);
+      const int64_t xpk = nb(L, s, k, +1), xmk = nb(L, s, k, -1);
+      const int64_t xpimk = nb(L, xmk, i, +1);
+      // U staple  U_k(x+i) U_i(x+k)^+ U_k(x)^+
+      m3 su = mul_nd(mul_nd(load_link(U, V, xpi, k), load_link(U, V, xpk, i)), load_link(U, V, s, k));
+      // D staple  U_k(x+i-k)^+ U_i(x-k)^+ U_k(x-k)
+      m3 sd = mul(dag(mul(load_link(U, V, xmk, i), load_link(U, V, xpimk, k))), load_link(U, V, xmk, k));
+#pragma unroll
+      for (int m = 0; m < 9; ++m) sum.e[m] = sum.e[m] + coef * (su.e[m] + sd.e[m]);
+    }
+    m3 ls = mul(load_link(U, V, s, i), sum);
+    cplx tr[8];
+    traces_with_generators(ls, tr);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      double *e = E + (int64_t)(i * 8 + a) * V + s;
+      *e = *e - 2.0 * tr[a].im;
+    }
+  }
+}
+
+// ------------------------------------------------------------ reductions
+// Block-level sum of nq values per thread into partials[block*nq + q].
+template <int NQ>
+__device__ __forceinline__ void block_sum_store(double v[NQ], double *partials) {
+  __shared__ double sh[32][NQ];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sh[warp][q] = v[q];
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double t = (lane < nw) ? sh[lane][q] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+      if (lane == 0) partials[blockIdx.x * NQ + q] = t;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_energy(Lat L, const double2 *__restrict__ U,
+                                                const double *__restrict__ E, double *partials) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (s < L.V) {
+    const int64_t V = L.V;
+    double loc = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      double sq = 0.0;
+      for (int a = 0; a < 8; ++a) {
+        double ea = E[(int64_t)(i * 8 + a) * V + s] / L.a[i] / L.a0;
+        sq += ea * ea;
+      }
+      loc += sq / 2.0;
+      for (int j = i + 1; j < 3; ++j) {
+        // Re Tr( U_i(x) U_j(x+i) U_i(x+j)^+ U_j(x)^+ ) = Re sum (M1 .* conj(M2)), M2 = U_j(x) U_i(x+j)
+        m3 m1 = mul(load_link(U, V, s, i), load_link(U, V, nb(L, s, i, +1), j));
+        m3 m2 = mul(load_link(U, V, s, j), load_link(U, V, nb(L, s, j, +1), i));
+        double tr = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) tr += m1.e[k].re * m2.e[k].re + m1.e[k].im * m2.e[k].im;
+        loc += 2.0 * 3.0 * ((1.0 - tr / 3.0) / L.a[i] / L.a[j]);
+      }
+    }
+    v[0] = loc;
+  }
+  block_sum_store<1>(v, partials);
+}
+
+// G-like covariant backward divergence pieces for the two Gauss measures.
+__global__ void __launch_bounds__(256) k_gauss(Lat L, const double2 *__restrict__ U,
+                                               const double *__restrict__ E, double *partials) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};  // [0] reference sum measure, [1] max-norm
+  if (s < L.V) {
+    const int64_t V = L.V;
+    m3 G = m3_zero();
+    double refsum = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      const int64_t xm = nb(L, s, i, -1);
+      double al[8], aln[8];
+      for (int a = 0; a < 8; ++a) {
+        al[a] = E[(int64_t)(i * 8 + a) * V + s];
+        aln[a] = E[(int64_t)(i * 8 + a) * V + xm];
+      }
+      m3 Em = algebra_matrix(al), En = algebra_matrix(aln);
+      m3 un = load_link(U, V, xm, i);
+      m3 T = mul(mul_dn(un, En), un);
+      m3 Dd = sub(Em, T);
+      // reference measure: sum_a 2|Im Tr(T^a D)|, D = (E - U^+ E' U)/a_i^2/a0
+      m3 D = scale(Dd, 1.0 / (L.a[i] * L.a[i]) / L.a0);
+      cplx tr[8];
+      traces_with_generators(D, tr);
+      for (int a = 0; a < 8; ++a) refsum += 2.0 * fabs(tr[a].im);
+      G = add(G, scale(Dd, 1.0 / L.a[i]));
+    }
+    G = scale(G, 1.0 / L.a0);
+    cplx tr[8];
+    traces_with_generators(G, tr);
+    double mx = 0.0;
+    for (int a = 0; a < 8; ++a) mx = fmax(mx, 2.0 * hypot(tr[a].re, tr[a].im));
+    v[0] = refsum;
+    v[1] = mx;
+  }
+  // sum for [0], max for [1]
+  __shared__ double sh[32][2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] += __shfl_down_sync(0xffffffffu, v[0], o);
+    v[1] = fmax(v[1], __shfl_down_sync(0xffffffffu, v[1], o));
+  }
+  if (lane == 0) {
+    sh[warp][0] = v[0];
+    sh[warp][1] = v[1];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    double t0 = (lane < nw) ? sh[lane][0] : 0.0, t1 = (lane < nw) ? sh[lane][1] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t0 += __shfl_down_sync(0xffffffffu, t0, o);
+      t1 = fmax(t1, __shfl_down_sync(0xffffffffu, t1, o));
+    }
+    if (lane == 0) {
+      partials[blockIdx.x * 2] = t0;
+      partials[blockIdx.x * 2 + 1] = t1;
+    }
+  }
+}
+
+// Final deterministic reduction: out[q] = op over nblk partials[b*nq+q]
+// (op: 0 sum, 1 max selected by mask bit q).
+__global__ void k_reduce_final(const double *__restrict__ partials, int64_t nblk, int nq,
+                               unsigned maxmask, double *out) {
+  __shared__ double sh[256];
+  for (int q = 0; q < nq; ++q) {
+    const bool isMax = (maxmask >> q) & 1u;
+    double acc = 0.0;
+    for (int64_t b = threadIdx.x; b < nblk; b += blockDim.x) {
+      double v = partials[b * nq + q];
+      acc = isMax ? fmax(acc, v) : acc + v;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x] = isMax ? fmax(sh[threadIdx.x], sh[threadIdx.x + w])
+                                                    : sh[threadIdx.x] + sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = sh[0];
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------ initial condition
+// p-space construction of TransversePolarisedOccupiedInit (gauge:1349-1381)
+// R: 16 complex planes (pol*8 + a) holding x2p of the real normals (unscaled
+// FFT); writes A, Ef: 24 complex planes (i*8 + a) in p-space.
+__global__ void k_ic_pspace(Lat L, const double2 *__restrict__ R, double fwd_scale, double Q,
+                            double n0, double g, double2 *__restrict__ A, double2 *__restrict__ Ef) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= L.V) return;
+  const int64_t V = L.V;
+  int64_t pos[3];
+  coords(L, s, pos[0], pos[1], pos[2]);
+  const int64_t ext[3] = {L.nx, L.ny, L.nz};
+  const double pi = 3.141592653589793;
+  cplx p[3];
+  double pn2 = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    double ang = pi * (double)pos[i] / (double)ext[i];
+    double mag = 2.0 * sin(ang) / L.a[i];
+    p[i] = {mag * cos(-ang), mag * sin(-ang)};
+    double ab = hypot(p[i].re, p[i].im);
+    pn2 += ab * ab;
+  }
+  double pn = sqrt(pn2);
+  cplx eps1[3], eps2[3];
+  bool zero = !(pn > 1e-12);
+  if (!zero) {
+    const double tol = 1e-12;
+    if (hypot(p[0].re, p[0].im) > tol) {
+      double a0 = hypot(p[0].re, p[0].im), a1 = hypot(p[1].re, p[1].im);
+      double n12 = sqrt(a0 * a0 + a1 * a1);
+      eps1[0] = (-1.0 / n12) * p[1];
+      eps1[1] = (1.0 / n12) * p[0];
+      eps1[2] = {0.0, 0.0};
+      double den = pn * n12;
+      eps2[0] = (1.0 / den) * (conj(p[0]) * p[2]);
+      eps2[1] = (1.0 / den) * (conj(p[1]) * p[2]);
+      eps2[2] = {-n12 / pn, 0.0};
+    } else {
+      double a1 = hypot(p[1].re, p[1].im), a2 = hypot(p[2].re, p[2].im);
+      double n23 = sqrt(a1 * a1 + a2 * a2);
+      eps1[0] = {0.0, 0.0};
+      eps1[1] = (1.0 / n23) * p[2];
+      eps1[2] = (-1.0 / n23) * p[1];
+      eps2[0] = {1.0, 0.0};
+      eps2[1] = {0.0, 0.0};
+      eps2[2] = {0.0, 0.0};
+    }
+  }
+  double occ = (pn < Q) ? n0 : g * g / 2.0;
+  double pa = zero ? 0.0 : sqrt(occ / pn * 2.0);
+  double pe = zero ? 0.0 : sqrt(occ * pn * 2.0);
+  for (int a = 0; a < 8; ++a) {
+    cplx r1 = fwd_scale * ldg(R + (int64_t)a * V + s);
+    cplx r2 = fwd_scale * ldg(R + (int64_t)(8 + a) * V + s);
+    for (int i = 0; i < 3; ++i) {
+      cplx m = zero ? cplx{0.0, 0.0} : r1 * eps1[i] + r2 * eps2[i];
+      st(A + (int64_t)(i * 8 + a) * V + s, pa * m);
+      st(Ef + (int64_t)(i * 8 + a) * V + s, times_i(pe * m));
+    }
+  }
+}
+
+// links = exp(i Re(A) a_i) (or 1), E = Re(Ef) a0 a_i after the backward FFT
+// (scale 1/Volume folded in here), gauge:1431-1443.
+__global__ void k_ic_write(Lat L, const double2 *__restrict__ A, const double2 *__restrict__ Ef,
+                           double inv_volume, int identity_links, double2 *__restrict__ U,
+                           double *__restrict__ E) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= L.V) return;
+  const int64_t V = L.V;
+  for (int i = 0; i < 3; ++i) {
+    double as[8];
+    for (int a = 0; a < 8; ++a) {
+      as[a] = __ldg(&A[(int64_t)(i * 8 + a) * V + s].x) * inv_volume * L.a[i];
+      E[(int64_t)(i * 8 + a) * V + s] = __ldg(&Ef[(int64_t)(i * 8 + a) * V + s].x) * inv_volume * L.a0 * L.a[i];
+    }
+    m3 G = identity_links ? m3_id() : expi_herm(algebra_matrix(as));
+    store_link(U, V, s, i, G);
+  }
+}
+
+}  // namespace nrq

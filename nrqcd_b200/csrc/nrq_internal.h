@@ -1,0 +1,117 @@
+// Host-side handle definitions behind the C ABI (include/nrqcd_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "nrq_common.cuh"
+
+struct nrq_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  nrq::Lat lat{};
+  int64_t n[3] = {0, 0, 0};
+  double a[4] = {0, 0, 0, 0};
+  // reduction scratch (device + pinned host mirror)
+  double *d_red = nullptr;     // partial sums, red_cap doubles
+  int64_t red_cap = 0;
+  double *d_res = nullptr;     // final results, 64 doubles
+  double *h_res = nullptr;     // pinned, 64 doubles
+  // staging buffer for layout transposes (device), grown on demand
+  void *d_stage = nullptr;
+  size_t stage_bytes = 0;
+  std::string last_error;
+  int sm_count = 148;
+  // opt-in per-class kernel timing (events recorded on `stream`)
+  bool prof = false;
+  struct ProfRec {
+    int cls;
+    double bytes;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfRec> prof_recs;
+  std::vector<cudaEvent_t> prof_pool;
+};
+
+// RAII helper: records a start event on construction and an end event plus
+// the algorithmic byte count on destruction when profiling is on.
+struct ProfScope {
+  nrq_ctx *ctx;
+  int cls;
+  double bytes;
+  cudaEvent_t a = nullptr;
+  ProfScope(nrq_ctx *c, int k, double by) : ctx(c), cls(k), bytes(by) {
+    if (!ctx->prof) return;
+    a = take();
+    cudaEventRecord(a, ctx->stream);
+  }
+  ~ProfScope() {
+    if (!ctx->prof || !a) return;
+    cudaEvent_t b = take();
+    cudaEventRecord(b, ctx->stream);
+    ctx->prof_recs.push_back({cls, bytes, a, b});
+  }
+  cudaEvent_t take() {
+    if (!ctx->prof_pool.empty()) {
+      cudaEvent_t e = ctx->prof_pool.back();
+      ctx->prof_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+};
+
+struct nrq_gauge {
+  nrq_ctx *ctx = nullptr;
+  double2 *U = nullptr;  // 27 planes of V complex: (dir*9 + row*3 + col)
+  double *E = nullptr;   // 24 planes of V reals  : (dir*8 + a)
+};
+
+struct nrq_heavy {
+  nrq_ctx *ctx = nullptr;
+  // 72 planes of V complex: (species*36 + col*6 + row); species 0 quark, 1 antiquark
+  double2 *P = nullptr;
+};
+
+struct nrq_cn_stats_internal;
+
+struct nrq_cn {
+  nrq_ctx *ctx = nullptr;
+  double mass = 1.0;
+  double c[8] = {1, 0, 1, 0, 1, 0, 1, 0};
+  double stepwidth = 1.0;
+  double tol = 1e-12;
+  int64_t maxits = 10000;
+  int form = 0;
+  // per-step derived gauge data
+  double2 *Dsum = nullptr;  // 9 planes
+  double *Bsum = nullptr;   // 9 planes
+  double2 *DE = nullptr;    // 54 planes: ((i*2 + perm)*9 + r*3 + c)
+  // Krylov vectors, 72 planes each
+  double2 *b = nullptr, *x = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr,
+          *t = nullptr;
+  double *scal = nullptr;     // device scalars per column
+  double *h_scal = nullptr;   // pinned mirror
+  int *d_flags = nullptr;
+  int64_t nblocks = 0;
+  double *partials = nullptr;  // nblocks * 12 * 4
+  unsigned int *counter = nullptr;
+  // statistics of the last update
+  int64_t last_iterations = 0;
+  int64_t last_matvecs = 0;
+  int64_t last_vecstreams = 0;
+};
+
+// error helpers
+#define NRQ_CUDA_TRY(ctx, expr)                                              \
+  do {                                                                       \
+    cudaError_t _e = (expr);                                                 \
+    if (_e != cudaSuccess) {                                                 \
+      if (ctx) (ctx)->last_error = std::string(#expr) + ": " + cudaGetErrorString(_e); \
+      return NRQ_ERR_CUDA;                                                   \
+    }                                                                        \
+  } while (0)

@@ -1,0 +1,80 @@
+// Kernel declarations shared between the kernel translation units and the
+// C-ABI translation unit.
+#pragma once
+#include "nrq_common.cuh"
+
+namespace nrq {
+
+// ---------------- gauge.cu
+__global__ void k_links_f2soa(const double2 *__restrict__ f, double2 *__restrict__ U, int64_t V);
+__global__ void k_links_soa2f(const double2 *__restrict__ U, double2 *__restrict__ f, int64_t V);
+__global__ void k_efield_f2soa(const double *__restrict__ f, double *__restrict__ E, int64_t V);
+__global__ void k_efield_soa2f(const double *__restrict__ E, double *__restrict__ f, int64_t V);
+__global__ void k_cold(double2 *__restrict__ U, double *__restrict__ E, int64_t V);
+__global__ void k_update_links(Lat L, double2 *__restrict__ U, const double *__restrict__ E, double dt);
+__global__ void k_update_efield(Lat L, const double2 *__restrict__ U, double *__restrict__ E, double dt);
+__global__ void k_energy(Lat L, const double2 *__restrict__ U, const double *__restrict__ E, double *partials);
+__global__ void k_gauss(Lat L, const double2 *__restrict__ U, const double *__restrict__ E, double *partials);
+__global__ void k_reduce_final(const double *__restrict__ partials, int64_t nblk, int nq, unsigned maxmask,
+                               double *out);
+__global__ void k_ic_pspace(Lat L, const double2 *__restrict__ R, double fwd_scale, double Q, double n0,
+                            double g, double2 *__restrict__ A, double2 *__restrict__ Ef);
+__global__ void k_ic_write(Lat L, const double2 *__restrict__ A, const double2 *__restrict__ Ef,
+                           double inv_volume, int identity_links, double2 *__restrict__ U,
+                           double *__restrict__ E);
+
+// ---------------- cn.cu
+// Per-species, per-term complex coefficients of the assembled CN operator:
+//   out = in + sum_t alpha_t G_t in      (t = kinetic, magnetic, Darwin, spin-orbit)
+struct CnCoef {
+  cplx kin[2], mag[2], dar[2], so[2];
+  double dkin;       // sum_i 1/a_i^2
+  double inva2[3];   // 1/a_i^2
+};
+
+enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4 };
+
+struct MvArgs {
+  const double2 *in;  // operand (PLAIN/RHS: psi, RES: x, V: p, T: r)
+  const double2 *in2; // T: v ; RHS: (unused)
+  double2 *out;       // PLAIN: A in ; RHS: b ; RES: r ; V: v ; T: t
+  double2 *out2;      // RHS: x0 = 2b - psi ; RES: rh
+  double2 *out3;      // RES: p
+  const double2 *bvec;// RES: b
+  const double *scal; // per-column scalars
+  double *partials;   // per block, per column, NQ doubles
+};
+
+constexpr int CN_SITES_PER_BLOCK = 32;
+constexpr int CN_COLS = 12;  // 2 species x 6 propagator columns
+constexpr int SC_STRIDE = 16; // doubles per column in the scalar array
+// scalar slots (per column)
+enum {
+  SC_RHO = 0,    // complex (2)
+  SC_ALPHA = 2,  // complex
+  SC_OMEGA = 4,  // complex
+  SC_BETA = 6,   // complex
+  SC_RR = 8,
+  SC_BB = 9,
+  SC_CONV = 10,  // 1.0 when converged
+  SC_BREAK = 11, // 1.0 on breakdown (restart requested)
+  SC_NONFIN = 12
+};
+
+void launch_cn_prepare(Lat L, const double2 *U, const double *E, double2 *Dsum, double *Bsum, double2 *DE,
+                       cudaStream_t st);
+void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,
+                  const double2 *DE, const MvArgs &a, cudaStream_t st);
+void launch_vec_xr(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *v, const double2 *t,
+                   const double2 *rh, const double *scal, double *partials, cudaStream_t st);
+void launch_vec_p(Lat L, double2 *p, const double2 *r, const double2 *v, const double *scal, cudaStream_t st);
+// finalize stages: 0 = after RES (rr, bb), 1 = alpha (rh.v), 2 = omega (t.s, t.t), 3 = beta (rh.r, r.r)
+void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
+                        cudaStream_t st);
+void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st);
+void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);
+void launch_single_point(double2 *P, int64_t V, int64_t sq, int64_t sa, cudaStream_t st);
+void launch_norms(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st);
+void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st);
+
+}  // namespace nrq

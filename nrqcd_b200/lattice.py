@@ -1,0 +1,74 @@
+"""Lattice module: host mirror of ``lattice%InitModule`` (src/lattice.f90:124-228).
+
+On one GPU the whole periodic lattice lives in one device's memory, so the
+reference's MPI domain decomposition and halo lists (src/halocomm.f90) become
+periodic indexing inside the kernels.  ``InitModule`` creates the device
+context every other object of this package is bound to.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+
+modulename = "lattice"
+
+_ctx = None
+_extents = None
+_spacings = None
+
+
+def InitModule(LatticeExtensions, LatticeSpacings, device: int = 0):
+    """Extents (Nx,Ny,Nz) and spacings (a0,ax,ay,az) as in the reference."""
+    global _ctx, _extents, _spacings
+    if _ctx is not None:
+        raise _capi.NrqcdError(f"Error in init of {modulename}: already initialised.",
+                               _capi.NRQ_ERR_ALREADY_INITIALISED)
+    ext = np.ascontiguousarray(LatticeExtensions, dtype=np.int64).reshape(3)
+    sp = np.ascontiguousarray(LatticeSpacings, dtype=np.float64).reshape(4)
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    rc = lib.nrq_init(ext.ctypes.data_as(_capi._i64p), _capi.dptr(sp), int(device), ctypes.byref(h))
+    _capi.check(rc, None, f"Error in init of {modulename}")
+    _ctx, _extents, _spacings = h, ext.copy(), sp.copy()
+
+
+def FinalizeModule():
+    global _ctx
+    if _ctx is None:
+        raise _capi.NrqcdError(f"Error in finalization of {modulename}: is not initialised.",
+                               _capi.NRQ_ERR_NOT_INITIALISED)
+    _capi.load().nrq_finalize(_ctx)
+    _ctx = None
+
+
+def IsModuleInitialised() -> bool:
+    return _ctx is not None
+
+
+def context():
+    if _ctx is None:
+        raise _capi.NrqcdError(f"Error in {modulename}: is not initialised.", _capi.NRQ_ERR_NOT_INITIALISED)
+    return _ctx
+
+
+def GetLatticeExtension(i: int) -> int:
+    return int(_extents[i - 1])
+
+
+def GetLatticeSpacing(i: int) -> float:
+    return float(_spacings[i])
+
+
+def GetLatticeSize() -> int:
+    return int(np.prod(_extents))
+
+
+def GetVolume() -> float:
+    return float(np.prod(_extents * _spacings[1:]))
+
+
+def synchronize():
+    _capi.check(_capi.load().nrq_synchronize(context()), context(), "synchronize")

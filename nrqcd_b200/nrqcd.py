@@ -1,0 +1,181 @@
+"""Host mirror of the ``nrqcd`` module (src/nrqcd.f90).
+
+``InitModule``/``FinalizeModule`` hold the solver state the reference keeps
+in module globals (src/nrqcd.f90:120-158); ``NRQCDField`` mirrors
+``type(NRQCDField)`` (src/nrqcd.f90:58-117).  Propagators live on the device;
+``QuarkProp``/``AntiQProp`` download host copies in the reference's layout
+prop(6,6,V) read as complex128 (V, 6, 6) [site, col, row].
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi, lattice
+from .gaugeconfiguration_su3 import GaugeConfiguration
+
+modulename = "nrqcd"
+nDof = 6
+nWilsonCoefficients = 4
+
+_cn = None
+_settings = None
+
+FORM_PLAIN_FP64 = 0
+
+
+def InitModule(Mass, WilsonCoeffs, StepWidth, kspTol, maxits=10000, form=FORM_PLAIN_FP64):
+    """src/nrqcd.f90:167-192 (kspTol = relative residual of every column solve)."""
+    global _cn, _settings
+    if _cn is not None:
+        raise _capi.NrqcdError(f"Error in init of {modulename}: already initialised.",
+                               _capi.NRQ_ERR_ALREADY_INITIALISED)
+    if not lattice.IsModuleInitialised():
+        raise _capi.NrqcdError(f"Error in init of {modulename}: lattice is not initialised.",
+                               _capi.NRQ_ERR_NOT_INITIALISED)
+    ctx = lattice.context()
+    c = _capi.coeffs(WilsonCoeffs)
+    h = ctypes.c_void_p()
+    rc = _capi.load().nrq_cn_init(ctx, float(Mass), _capi.dptr(c), float(StepWidth), float(kspTol),
+                                  int(maxits), int(form), ctypes.byref(h))
+    _capi.check(rc, ctx, f"Error in init of {modulename}")
+    _cn = h
+    _settings = dict(Mass=float(Mass), WilsonCoeffs=c, StepWidth=float(StepWidth), kspTol=float(kspTol))
+
+
+def FinalizeModule():
+    global _cn
+    if _cn is None:
+        raise _capi.NrqcdError(f"Error in finalization of {modulename}: is not initialised.",
+                               _capi.NRQ_ERR_NOT_INITIALISED)
+    _capi.load().nrq_cn_finalize(_cn)
+    _cn = None
+
+
+def IsModuleInitialised() -> bool:
+    return _cn is not None
+
+
+def solver_handle():
+    if _cn is None:
+        raise _capi.NrqcdError(f"Error in {modulename}: is not initialised.", _capi.NRQ_ERR_NOT_INITIALISED)
+    return _cn
+
+
+class NRQCDField:
+    def __init__(self):
+        self._ctx = lattice.context()
+        self._h = ctypes.c_void_p()
+        _capi.check(_capi.load().nrq_heavy_create(self._ctx, ctypes.byref(self._h)), self._ctx,
+                    f"Error in Allocate of {modulename}")
+        self.V = lattice.GetLatticeSize()
+        self.last_stats = None
+
+    def Destructor(self):
+        if self._h:
+            _capi.load().nrq_heavy_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            if lattice.IsModuleInitialised():
+                self.Destructor()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _call(self, name, *args):
+        _capi.check(getattr(_capi.load(), name)(self._h, *args), self._ctx, f"{modulename}:{name}")
+
+    # ------------------------------------------------------------ data
+    def upload(self, quark: np.ndarray, antiq: np.ndarray):
+        q = np.ascontiguousarray(quark, dtype=np.complex128).reshape(self.V, 6, 6)
+        a = np.ascontiguousarray(antiq, dtype=np.complex128).reshape(self.V, 6, 6)
+        self._call("nrq_heavy_upload", q.ctypes.data_as(_capi._dp), a.ctypes.data_as(_capi._dp))
+
+    def download(self, quark=None, antiq=None):
+        if quark is None:
+            quark = np.empty((self.V, 6, 6), dtype=np.complex128)
+        if antiq is None:
+            antiq = np.empty((self.V, 6, 6), dtype=np.complex128)
+        self._call("nrq_heavy_download", quark.ctypes.data_as(_capi._dp), antiq.ctypes.data_as(_capi._dp))
+        return quark, antiq
+
+    @property
+    def QuarkProp(self):
+        return self.download()[0]
+
+    @property
+    def AntiQProp(self):
+        return self.download()[1]
+
+    def Assign(self, other: "NRQCDField"):
+        """assignment(=), src/nrqcd.f90:219-228"""
+        _capi.check(_capi.load().nrq_heavy_copy(self._h, other._h), self._ctx, "NRQCDField assign")
+
+    # ------------------------------------------------------------ inits
+    def InitSinglePoint(self, LatticeIndex_quark: int, LatticeIndex_antiq: int):
+        """src/nrqcd.f90:324-350 (1-based lattice indices)."""
+        self._call("nrq_heavy_init_single_point", int(LatticeIndex_quark), int(LatticeIndex_antiq))
+
+    # ------------------------------------------------------------ evolution
+    def Update(self, GaugeConf: GaugeConfiguration, Mass, WilsonCoeffs, StepWidth: float = 1.0,
+               raise_on_nonconvergence: bool = True):
+        """Update_CrankNicholson, src/nrqcd.f90:1053-1168."""
+        st = _capi.CnStats()
+        c = _capi.coeffs(WilsonCoeffs)
+        rc = _capi.load().nrq_heavy_update_cn(solver_handle(), self._h, GaugeConf.handle, float(Mass),
+                                              _capi.dptr(c), float(StepWidth), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if rc == _capi.NRQ_ERR_NOT_CONVERGED and not raise_on_nonconvergence:
+            return self.last_stats
+        _capi.check(rc, self._ctx, f"Error in Update of {modulename}")
+        return self.last_stats
+
+    # ------------------------------------------------------------ observables
+    def _norms(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._call("nrq_heavy_norms", ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def GetNorm_Quark(self) -> float:
+        return self._norms()[0]
+
+    def GetNorm_AntiQ(self) -> float:
+        return self._norms()[1]
+
+    def _correlators(self):
+        out = np.empty(8)
+        self._call("nrq_heavy_correlators", _capi.dptr(out))
+        return out[0::2] + 1j * out[1::2]
+
+    def GetMesoncorrelator_O1_1S0_ZeroMomentum(self) -> complex:
+        return complex(self._correlators()[0])
+
+    def GetMesoncorrelator_O1_3S1_ZeroMomentum(self) -> complex:
+        return complex(self._correlators()[1])
+
+    def GetMesoncorrelator_O8_1S0_ZeroMomentum(self) -> complex:
+        return complex(self._correlators()[2])
+
+    def GetMesoncorrelator_O8_3S1_ZeroMomentum(self) -> complex:
+        return complex(self._correlators()[3])
+
+    def GetMesoncorrelators(self) -> dict:
+        c = self._correlators()
+        return {"o1_1s0": complex(c[0]), "o1_3s1": complex(c[1]), "o8_1s0": complex(c[2]),
+                "o8_3s1": complex(c[3])}
+
+
+def apply_operator(GaugeConf: GaugeConfiguration, Mass, WilsonCoeffs, StepWidth, herm: bool,
+                   field_in: NRQCDField, field_out: NRQCDField):
+    """field_out = A field_in (herm=False) or A^H field_in, quark and antiquark
+    operators as assembled in BuildSystemMatrix (MatMult of src/nrqcd.f90:1112)."""
+    c = _capi.coeffs(WilsonCoeffs)
+    rc = _capi.load().nrq_cn_apply(solver_handle(), GaugeConf.handle, float(Mass), _capi.dptr(c),
+                                   float(StepWidth), int(bool(herm)), field_in.handle, field_out.handle)
+    _capi.check(rc, lattice.context(), "apply_operator")

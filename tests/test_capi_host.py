@@ -1,0 +1,61 @@
+"""C ABI: the library loads and exports every entry point the header declares;
+without a GPU the product fails loudly (no CPU fallback)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from tests.conftest import ROOT, gpu_available
+
+HEADER = os.path.join(ROOT, "include", "nrqcd_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nrq_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from nrqcd_b200 import build
+    if not os.path.exists(build.LIB):
+        build.build()
+    return ctypes.CDLL(build.LIB)
+
+
+def test_header_symbols_exported(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 25
+    for s in syms:
+        assert hasattr(lib, s), s
+
+
+def test_python_binding_covers_header():
+    from nrqcd_b200 import _capi
+    assert set(declared_symbols()) == set(_capi.SIGNATURES)
+
+
+def test_status_strings(lib):
+    lib.nrq_status_string.restype = ctypes.c_char_p
+    assert lib.nrq_status_string(0) == b"ok"
+    assert b"converge" in lib.nrq_status_string(5)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-device path")
+def test_no_device_fails_loudly():
+    from nrqcd_b200 import NrqcdError, lattice
+    with pytest.raises(NrqcdError) as e:
+        lattice.InitModule([4, 4, 4], [0.05, 1, 1, 1])
+    assert e.value.code == 8  # NRQ_ERR_NO_DEVICE
+    assert not lattice.IsModuleInitialised()
+
+
+def test_module_guards_without_device():
+    from nrqcd_b200 import NrqcdError, nrqcd
+    with pytest.raises(NrqcdError):
+        nrqcd.FinalizeModule()
+    if not gpu_available():
+        with pytest.raises(NrqcdError):
+            nrqcd.InitModule(1.0, [1, 1, 1, 1], 1.0, 1e-12)

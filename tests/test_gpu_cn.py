@@ -1,0 +1,157 @@
+"""GPU parity of the Crank-Nicolson hot path against the oracle (through the C ABI).
+
+Tolerances: the matvec is FP64 against the FP64 oracle (1e-13 relative).
+Solves run to kspTol = 1e-13 on both sides; the propagators then agree to a
+few 1e-13 absolute (point-source amplitude 1/sqrt 6)."""
+import os
+
+import numpy as np
+import pytest
+
+from nrqcd_b200 import GaugeConfiguration, NRQCDField, nrqcd
+from tests.gpu_util import lattice_ctx
+
+pytestmark = pytest.mark.gpu
+
+A = (0.05, 1.0, 1.0, 1.0)
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def hot(oracle, n, seed=5, Q=3.0):
+    return oracle.transverse_box(n, A, Q, 1.0, 0.0, seed, identity_links=False)
+
+
+@pytest.mark.parametrize("herm", [False, True])
+@pytest.mark.parametrize("n", [(4, 4, 4), (6, 5, 7)])
+def test_operator_matches_oracle(oracle, herm, n):
+    links, ef = hot(oracle, n)
+    V = int(np.prod(n))
+    rng = np.random.default_rng(3)
+    q = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    an = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    M, c, dt = 1.3, [1.0, 0.9 + 0.1j, 1.1, 0.8 - 0.2j], 1.0
+    with lattice_ctx(n, A, cn=(M, c, dt, 1e-12)):
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        fin, fout = NRQCDField(), NRQCDField()
+        fin.upload(q, an)
+        nrqcd.apply_operator(g, M, c, dt, herm, fin, fout)
+        oq, oa = fout.download()
+    eq = oracle.cn_apply(n, A, links, ef, M, c, dt, int(herm), q)
+    ea = oracle.cn_apply(n, A, links, ef, -M, np.conj(c), dt, int(herm), an)
+    scale = np.abs(q).max()
+    assert np.abs(oq - eq).max() < 1e-13 * scale
+    assert np.abs(oa - ea).max() < 1e-13 * scale
+
+
+@pytest.mark.parametrize("name", ["free_kat_8x8x8_M1", "free_kat_6x4x10_M2"])
+def test_free_known_answer_on_gpu(name):
+    g0 = np.load(os.path.join(GOLD, name + ".npz"))
+    n, a, M = tuple(int(v) for v in g0["n"]), tuple(float(v) for v in g0["a"]), float(g0["mass"])
+    with lattice_ctx(n, a, cn=(M, [1, 1, 1, 1], 1.0, 1e-14)):
+        g = GaugeConfiguration()
+        g.ColdInit()
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        for s in range(int(g0["nsteps"])):
+            st = h.Update(g, M, [1, 1, 1, 1], 1.0)
+            assert st["converged"] == 1
+            q, an = h.download()
+            eye = np.eye(6)
+            assert np.abs(q - g0["amp_q"][s][:, None, None] * eye).max() < 1e-13
+            assert np.abs(an - g0["amp_a"][s][:, None, None] * eye).max() < 1e-13
+            assert abs(h.GetMesoncorrelator_O1_1S0_ZeroMomentum() - g0["o1_1s0"][s]) < 1e-13
+            assert abs(h.GetNorm_Quark() - 1) < 1e-13 and abs(h.GetNorm_AntiQ() - 1) < 1e-13
+
+
+@pytest.mark.parametrize("n", [(6, 6, 6), (8, 4, 6)])
+def test_cn_step_matches_oracle(oracle, n):
+    links, ef = hot(oracle, n)
+    M, c = 1.0, [1, 1, 1, 1]
+    q = oracle.single_point(n, 1)
+    an = oracle.single_point(n, 1)
+    with lattice_ctx(n, A, cn=(M, c, 1.0, 1e-13)):
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        for _ in range(3):
+            st = h.Update(g, M, c, 1.0)
+            assert st["converged"] == 1 and st["max_rel_residual"] < 1e-13
+            oracle.cn_update(n, A, links, ef, M, c, 1.0, q, an, tol=1e-14)
+        gq, ga = h.download()
+        nq, na = h.GetNorm_Quark(), h.GetNorm_AntiQ()
+        corr = h.GetMesoncorrelators()
+    assert np.abs(gq - q).max() < 5e-13 and np.abs(ga - an).max() < 5e-13
+    assert abs(nq - 1) < 1e-12 and abs(na - 1) < 1e-12
+    oc = oracle.meson_correlators(n, q, an)
+    for k in oc:
+        assert abs(corr[k] - oc[k]) < 1e-12, k
+
+
+def test_correlators_random_fields(oracle):
+    n = (4, 4, 4)
+    V = 64
+    rng = np.random.default_rng(8)
+    q = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    an = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    with lattice_ctx(n, A):
+        h = NRQCDField()
+        h.upload(q, an)
+        corr = h.GetMesoncorrelators()
+        nq = h.GetNorm_Quark()
+    oc = oracle.meson_correlators(n, q, an)
+    for k in oc:
+        assert abs(corr[k] - oc[k]) < 1e-11 * max(1, abs(oc[k])), k
+    assert abs(nq - oracle.heavy_norm(n, q)) < 1e-12 * nq
+
+
+def test_forward_backward_returns_initial_propagator(oracle):
+    n = (8, 8, 8)
+    links, ef = hot(oracle, n, seed=4, Q=2.0)
+    with lattice_ctx(n, A, cn=(1.0, [1, 1, 1, 1], 1.0, 1e-14)):
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        q0, a0 = h.download()
+        for _ in range(4):
+            h.Update(g, 1.0, [1, 1, 1, 1], 1.0)
+        for _ in range(4):
+            h.Update(g, 1.0, [1, 1, 1, 1], -1.0)
+        q, an = h.download()
+    assert np.abs(q - q0).max() < 1e-12 and np.abs(an - a0).max() < 1e-12
+
+
+def test_coupled_step_matches_oracle(oracle):
+    """Driver order of src/main.f90:344-348: CN step, then leapfrog."""
+    n = (8, 8, 8)
+    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 1, identity_links=True)
+    M, c = 1.0, [1, 1, 1, 1]
+    q = oracle.single_point(n, 1)
+    an = oracle.single_point(n, 1)
+    with lattice_ctx(n, A, cn=(M, c, 1.0, 1e-13)):
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        for _ in range(5):
+            h.Update(g, M, c)
+            g.Update()
+            oracle.cn_update(n, A, links, ef, M, c, 1.0, q, an, tol=1e-14)
+            oracle.gauge_update(n, A, links, ef, 1.0)
+        gq, ga = h.download()
+        lg, eg = g.download()
+    assert np.abs(lg - links).max() < 1e-13 and np.abs(eg - ef).max() < 1e-13
+    assert np.abs(gq - q).max() < 5e-13 and np.abs(ga - an).max() < 5e-13
+
+
+def test_errors_fail_loudly():
+    from nrqcd_b200 import NrqcdError
+    n = (4, 4, 4)
+    with lattice_ctx(n, A, cn=(1.0, [1, 1, 1, 1], 1.0, 1e-12)):
+        h = NRQCDField()
+        with pytest.raises(NrqcdError):
+            h.InitSinglePoint(0, 1)
+        with pytest.raises(NrqcdError):
+            nrqcd.InitModule(1.0, [1, 1, 1, 1], 1.0, 1e-12)

@@ -1,0 +1,78 @@
+"""Oracle checks: ranlxd, FFT conventions, initial condition, leapfrog."""
+import numpy as np
+import pytest
+
+
+def test_ranlxd_state_roundtrip_and_uniformity(oracle):
+    r = oracle.Ranlxd(2, 1)
+    x = r.draw(200000)
+    assert 0.0 <= x.min() and x.max() < 1.0
+    assert abs(x.mean() - 0.5) < 3e-3 and abs(x.var() - 1 / 12) < 2e-3
+    # 48-bit fractions
+    assert np.all(np.ldexp(x, 48) == np.floor(np.ldexp(x, 48)))
+    st = r.get_state()
+    a = r.draw(1000)
+    r.reset(st)
+    b = r.draw(1000)
+    assert np.array_equal(a, b)
+    # different seeds, different streams; same seed, same stream
+    assert not np.array_equal(oracle.Ranlxd(2, 1).draw(10), oracle.Ranlxd(2, 2).draw(10))
+    assert np.array_equal(oracle.Ranlxd(2, 7).draw(50), oracle.Ranlxd(2, 7).draw(50))
+    with pytest.raises(ValueError):
+        oracle.Ranlxd(3, 1)
+    with pytest.raises(ValueError):
+        oracle.Ranlxd(2, 0)
+
+
+def test_box_muller_normals(oracle):
+    z = oracle.Ranlxd(2, 11).normal_cmplx(100000)
+    assert abs(z.real.mean()) < 0.02 and abs(z.real.var() - 1) < 0.02
+    assert abs(z.imag.var() - 1) < 0.02
+
+
+@pytest.mark.parametrize("n", [(6, 4, 5), (8, 8, 8), (12, 9, 10)])
+def test_fft_conventions(oracle, n):
+    rng = np.random.default_rng(0)
+    V = int(np.prod(n))
+    d = rng.normal(size=V) + 1j * rng.normal(size=V)
+    ref = np.fft.fftn(d.reshape(n[2], n[1], n[0])).reshape(-1)
+    f = oracle.fft3d(d, n, -1, 1.0)
+    assert np.abs(f - ref).max() < 1e-13 * np.abs(ref).max()
+    back = oracle.fft3d(f, n, +1, 1.0 / V)
+    assert np.abs(back - d).max() < 1e-14 * 10
+
+
+def test_transverse_ic_is_gauss_exact_and_transverse(oracle):
+    n, a = (16, 16, 16), (0.05, 1.0, 1.0, 1.0)
+    links, ef = oracle.transverse_box(n, a, 0.5, 1.0, 0.0, 1, identity_links=True)
+    assert np.all(links[:, :, 0, 0] == 1) and np.abs(ef).max() > 1e-4
+    assert oracle.gauss_maxnorm(n, a, links, ef) < 1e-12
+    assert oracle.gauss_ref(n, a, links, ef) < 1e-12
+    # projection is a no-op on this field
+    e0 = ef.copy()
+    assert oracle.gauss_project(n, a, links, ef, tol=1e-3) == 0
+    assert np.array_equal(ef, e0)
+
+
+def test_non_identity_ic_links_are_unitary(oracle):
+    n, a = (8, 8, 8), (0.05, 1.0, 1.0, 1.0)
+    links, ef = oracle.transverse_box(n, a, 2.0, 1.0, 0.0, 3, identity_links=False)
+    U = np.swapaxes(links, 2, 3)  # [site, dir, row, col]
+    err = np.abs(U @ np.conj(np.swapaxes(U, 2, 3)) - np.eye(3)).max()
+    assert err < 1e-14
+
+
+def test_leapfrog_reversible_and_energy_bounded(oracle):
+    n, a = (16, 16, 16), (0.05, 1.0, 1.0, 1.0)
+    links, ef = oracle.transverse_box(n, a, 0.5, 1.0, 0.0, 1, identity_links=True)
+    l0, e0 = links.copy(), ef.copy()
+    E0 = oracle.energy(n, a, links, ef)
+    es = []
+    for _ in range(40):
+        oracle.gauge_update(n, a, links, ef, 1.0)
+        es.append(oracle.energy(n, a, links, ef))
+    assert max(abs(e - E0) for e in es) / E0 < 0.03
+    assert oracle.gauss_maxnorm(n, a, links, ef) < 1e-12
+    for _ in range(40):
+        oracle.gauge_update(n, a, links, ef, -1.0)
+    assert np.abs(links - l0).max() < 1e-13 and np.abs(ef - e0).max() < 1e-15
