@@ -248,6 +248,7 @@ __device__ __forceinline__ cplx scal_c(const double *sc, int col, int slot) {
   return {sc[col * SC_STRIDE + slot], sc[col * SC_STRIDE + slot + 1]};
 }
 
+#ifdef NRQ_MV_V1
 template <int MODE>
 __global__ void __launch_bounds__(384) k_cn_mv(Lat L, CnCoef C, const double2 *__restrict__ U,
                                                const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
@@ -411,6 +412,8 @@ void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
     default: k_cn_mv<MV_T><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
   }
 }
+
+#endif  // NRQ_MV_V1
 
 // ------------------------------------------------------------ BiCGStab vector updates
 // s = r - alpha v ; x += alpha p + omega s ; r = s - omega t ; partials (rh.r), (r.r)

@@ -1,0 +1,226 @@
+// The 12-column stencil of the assembled Crank-Nicolson operator
+// (src/nrqcd.f90:1175-1387 with PETSc's block transposition), applied
+// matrix-free: out = in + sum_t alpha_t G_t in for both species at once.
+// See cn.cu for the operator; this file holds its stencil kernel.
+//
+// Work split.  A block covers 32 consecutive sites with 6 warps, one warp per
+// (species, output colour c).  A thread owns the output rows (c, s=0,1) of
+// all 6 propagator columns of its species (12 complex accumulators).  Per
+// neighbour it builds its two rows of the species-specific 6x6 block
+//   W = ck (K0^T x 1) + cs0 (X0^T x s_k0^T) + cs1 (X1^T x s_k1^T)
+// once (12 complex entries, colour row c) and reuses them from registers for
+// the 6 columns: 36 complex multiply-adds per column per neighbour, the
+// minimum for a dense 6x6 block.  The three colour warps of a species read
+// the same neighbour spinors; those reads hit L1.
+#include "nrq_kernels.cuh"
+
+namespace nrq {
+
+// entry (s, sp) of the transposed reference Pauli matrix s_k^T
+// (src/su2.f90:68-79 holds s_2 transposed, so s_2^T = [[0,-i],[i,0]])
+__device__ __forceinline__ cplx sigT(int k, int s, int t) {
+  if (k == 0) return (s != t) ? cplx{1.0, 0.0} : cplx{0.0, 0.0};
+  if (k == 1) {
+    if (s == 0 && t == 1) return {0.0, -1.0};
+    if (s == 1 && t == 0) return {0.0, 1.0};
+    return {0.0, 0.0};
+  }
+  if (s != t) return {0.0, 0.0};
+  return (s == 0) ? cplx{1.0, 0.0} : cplx{-1.0, 0.0};
+}
+
+__device__ __forceinline__ cplx scal_col(const double *sc, int col12, int slot) {
+  return {sc[col12 * SC_STRIDE + slot], sc[col12 * SC_STRIDE + slot + 1]};
+}
+
+#ifndef NRQ_MV_V1
+template <int MODE>
+__global__ void __launch_bounds__(192, 2) k_cn_mv2(Lat L, CnCoef C, const double2 *__restrict__ U,
+                                                   const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
+                                                   const double2 *__restrict__ DE, MvArgs A) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;  // 0..5
+  const int sp = warp / 3, c = warp % 3;
+  const int64_t V = L.V;
+  const int64_t x0 = (int64_t)blockIdx.x * 32 + lane;
+  const bool active = x0 < V;
+  const int64_t x = active ? x0 : 0;
+  const int64_t pb = (int64_t)(sp * 36) * V;
+
+  cplx al[6];
+  if (MODE == MV_T) {
+#pragma unroll
+    for (int col = 0; col < 6; ++col) al[col] = scal_col(A.scal, sp * 6 + col, SC_ALPHA);
+  }
+  // 6-component spinor of column col at site y (MV_T: s = r - alpha v on the fly)
+  auto load_w = [&](int64_t y, int col, cplx w[6]) {
+    const double2 *p = A.in + pb + (int64_t)(col * 6) * V + y;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) w[r] = ldg(p + (int64_t)r * V);
+    if (MODE == MV_T) {
+      const double2 *q = A.in2 + pb + (int64_t)(col * 6) * V + y;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) w[r] = w[r] - al[col] * ldg(q + (int64_t)r * V);
+    }
+  };
+
+  const cplx ak = C.kin[sp], am = C.mag[sp], ad = C.dar[sp], aso = C.so[sp];
+  cplx acc[6][2];
+  // ---- diagonal block: [1 + ak dkin] 1 + ad D^T + am B^T, colour row c
+  {
+    cplx Cd[3];
+#pragma unroll
+    for (int cp = 0; cp < 3; ++cp) {
+      cplx dv = ldg(Dsum + (int64_t)(cp * 3 + c) * V + x);
+      double bv = __ldg(Bsum + (int64_t)(cp * 3 + c) * V + x);
+      Cd[cp] = ad * dv + bv * am;
+    }
+    Cd[c] = Cd[c] + C.dkin * ak + cplx{1.0, 0.0};
+#pragma unroll
+    for (int col = 0; col < 6; ++col) {
+      cplx w[6];
+      load_w(x, col, w);
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        cplx a_ = Cd[0] * w[s];
+        cmac(a_, Cd[1], w[2 + s]);
+        cmac(a_, Cd[2], w[4 + s]);
+        acc[col][s] = a_;
+      }
+    }
+  }
+  const cplx cs0 = times_i(aso);   // eps = +1 permutation (j,k) = (i+1, i+2)
+  const cplx cs1 = -times_i(aso);  // eps = -1 permutation (j,k) = (i+2, i+1)
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+    const cplx ck = (-0.5 * C.inva2[i]) * ak;
+    const int k0 = (i + 2) % 3, k1 = (i + 1) % 3;
+#pragma unroll 1
+    for (int dir = 0; dir < 2; ++dir) {
+      // dir 0: neighbour x+i, blocks from site x (transposed)
+      // dir 1: neighbour x-i, blocks from site x-i (complex conjugated)
+      const int64_t y = nb(L, x, i, dir == 0 ? +1 : -1);
+      const int64_t ms = dir == 0 ? x : y;
+      const double2 *Up = U + (int64_t)(i * 9) * V + ms;
+      const double2 *D0 = DE + (int64_t)((i * 2 + 0) * 9) * V + ms;
+      const double2 *D1 = DE + (int64_t)((i * 2 + 1) * 9) * V + ms;
+      const cplx s0 = dir == 0 ? cs0 : -cs0, s1 = dir == 0 ? cs1 : -cs1;
+      cplx Wm[2][3][2];
+#pragma unroll
+      for (int cp = 0; cp < 3; ++cp) {
+        cplx u, d0, d1;
+        if (dir == 0) {  // M^T[c][cp] = M[cp][c]
+          u = ldg(Up + (int64_t)(cp * 3 + c) * V);
+          d0 = ldg(D0 + (int64_t)(cp * 3 + c) * V);
+          d1 = ldg(D1 + (int64_t)(cp * 3 + c) * V);
+        } else {         // M^*[c][cp]
+          u = conj(ldg(Up + (int64_t)(c * 3 + cp) * V));
+          d0 = conj(ldg(D0 + (int64_t)(c * 3 + cp) * V));
+          d1 = conj(ldg(D1 + (int64_t)(c * 3 + cp) * V));
+        }
+        const cplx ku = ck * u, e0 = s0 * d0, e1 = s1 * d1;
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+          for (int t = 0; t < 2; ++t) {
+            cplx v = sigT(k0, s, t) * e0 + sigT(k1, s, t) * e1;
+            if (s == t) v = v + ku;
+            Wm[s][cp][t] = v;
+          }
+      }
+#pragma unroll 2
+      for (int col = 0; col < 6; ++col) {
+        cplx w[6];
+        load_w(y, col, w);
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+          for (int cp = 0; cp < 3; ++cp) {
+            cmac(acc[col][s], Wm[s][cp][0], w[2 * cp]);
+            cmac(acc[col][s], Wm[s][cp][1], w[2 * cp + 1]);
+          }
+      }
+    }
+  }
+
+  // ---------------- epilogue by mode; rows (c, s) of the 6 columns
+  constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V) ? 2 : 0);
+  double q[6][3];
+#pragma unroll
+  for (int col = 0; col < 6; ++col)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[col][k] = 0.0;
+  if (active) {
+#pragma unroll
+    for (int col = 0; col < 6; ++col)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int64_t o = pb + (int64_t)(col * 6 + 2 * c + s) * V + x;
+        const cplx y_ = acc[col][s];
+        if (MODE == MV_PLAIN) {
+          st(A.out + o, y_);
+        } else if (MODE == MV_RHS) {
+          st(A.out + o, y_);
+          st(A.out2 + o, 2.0 * y_ - ldg(A.in + o));
+        } else if (MODE == MV_RES) {
+          const cplx b = ldg(A.bvec + o);
+          const cplx r = b - y_;
+          st(A.out + o, r);
+          st(A.out2 + o, r);
+          st(A.out3 + o, r);
+          q[col][0] += norm2(r);
+          q[col][1] += norm2(b);
+        } else if (MODE == MV_V) {
+          st(A.out + o, y_);
+          cplx d = {0.0, 0.0};
+          cmac_cj(d, ldg(A.in2 + o), y_);
+          q[col][0] += d.re;
+          q[col][1] += d.im;
+        } else {  // MV_T
+          st(A.out + o, y_);
+          const cplx s_ = ldg(A.in + o) - al[col] * ldg(A.in2 + o);
+          cplx d = {0.0, 0.0};
+          cmac_cj(d, y_, s_);
+          q[col][0] += d.re;
+          q[col][1] += d.im;
+          q[col][2] += norm2(y_);
+        }
+      }
+  }
+  if constexpr (NQ > 0) {
+    __shared__ double sh[6][6][3];
+#pragma unroll
+    for (int col = 0; col < 6; ++col)
+#pragma unroll
+      for (int k = 0; k < NQ; ++k) {
+        double v = q[col][k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) sh[warp][col][k] = v;
+      }
+    __syncthreads();
+    if (threadIdx.x < 12 * NQ) {
+      const int col12 = threadIdx.x / NQ, k = threadIdx.x % NQ;
+      const int spp = col12 / 6, col = col12 % 6;
+      const double v = sh[spp * 3 + 0][col][k] + sh[spp * 3 + 1][col][k] + sh[spp * 3 + 2][col][k];
+      A.partials[((int64_t)blockIdx.x * CN_COLS + col12) * NQ + k] = v;
+    }
+  }
+}
+
+void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,
+                  const double2 *DE, const MvArgs &a, cudaStream_t st) {
+  const unsigned nb_ = (unsigned)((L.V + 31) / 32);
+  const dim3 blk(192);
+  switch (mode) {
+    case MV_PLAIN: k_cn_mv2<MV_PLAIN><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_RHS: k_cn_mv2<MV_RHS><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_RES: k_cn_mv2<MV_RES><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_V: k_cn_mv2<MV_V><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    default: k_cn_mv2<MV_T><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+  }
+}
+
+#endif  // NRQ_MV_V1
+
+}  // namespace nrq
