@@ -44,7 +44,8 @@ typedef enum {
   NRQ_ERR_TIMEOUT = 6,
   NRQ_ERR_NONFINITE = 7,
   NRQ_ERR_NO_DEVICE = 8,
-  NRQ_ERR_OOM = 9
+  NRQ_ERR_OOM = 9,
+  NRQ_ERR_CAPACITY = 10            /* lattice larger than a fixed scratch array */
 } nrq_status;
 
 typedef struct nrq_ctx nrq_ctx;     /* lattice + device + stream          */
@@ -144,6 +145,33 @@ int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
  * verification.                                                            */
 int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const double c[8],
                  double stepwidth, int herm, const nrq_heavy *in, nrq_heavy *out);
+
+/* ---- energy without any device allocation ---------------------------- */
+/* No counterpart in the reference.  This is for callers that cannot call
+ * cudaMalloc, for example a driver port whose fields live in device memory
+ * owned by another runtime (OpenACC or CUDA Fortran data regions, a
+ * framework's caching allocator) and that must not grow the device footprint
+ * inside its time loop.  Computes the same energy as nrq_gauge_energy without
+ * a context or handle.  It allocates nothing.
+ *
+ * Inputs are in caller-owned device memory in the device plane layout:
+ *   links_soa  : 27 planes of V complex (interleaved re, im),
+ *                plane = dir*9 + row*3 + col
+ *   efield_soa : 24 planes of V doubles, plane = dir*8 + a
+ * The energy goes to energy_out, one double of device-accessible memory.
+ * The launches go onto `stream`, a cudaStream_t of the current device
+ * (NULL = default stream), and the function returns without synchronising.
+ *
+ * Partial sums go into a fixed 128 KiB device array in the library.  That
+ * caps the lattice at NRQ_NOALLOC_MAX_SITES sites (for example 160^3);
+ * larger lattices return NRQ_ERR_CAPACITY.  The first call on a device looks
+ * up the array's address and caches it, so make that first call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised.                                              */
+#define NRQ_NOALLOC_MAX_SITES 4194304
+int nrq_gauge_energy_noalloc(const int64_t extents[3], const double spacings[4],
+                             const double *links_soa, const double *efield_soa,
+                             double *energy_out, void *stream);
 
 #ifdef __cplusplus
 }

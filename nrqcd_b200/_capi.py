@@ -24,6 +24,7 @@ NRQ_ERR_TIMEOUT = 6
 NRQ_ERR_NONFINITE = 7
 NRQ_ERR_NO_DEVICE = 8
 NRQ_ERR_OOM = 9
+NRQ_ERR_CAPACITY = 10
 
 
 class NrqcdError(RuntimeError):
@@ -83,6 +84,7 @@ SIGNATURES = {
     "nrq_heavy_update_cn": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,
                                            ctypes.POINTER(CnStats)]),
     "nrq_cn_apply": (ctypes.c_int, [_vp, _vp, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    "nrq_gauge_energy_noalloc": (ctypes.c_int, [_i64p, _dp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

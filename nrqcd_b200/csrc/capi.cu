@@ -178,6 +178,7 @@ extern "C" const char *nrq_status_string(int s) {
     case NRQ_ERR_NONFINITE: return "non-finite value";
     case NRQ_ERR_NO_DEVICE: return "no CUDA device";
     case NRQ_ERR_OOM: return "out of memory";
+    case NRQ_ERR_CAPACITY: return "lattice exceeds the fixed scratch capacity of a no-allocation entry point";
     default: return "unknown status";
   }
 }
