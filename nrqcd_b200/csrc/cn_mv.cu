@@ -14,7 +14,22 @@
 // the same neighbour spinors; those reads hit L1.
 #include "nrq_kernels.cuh"
 
+// tuning parameters of the stencil kernel (blocks per SM for the register
+// budget, unroll depth of the direction and column loops)
+#ifndef NRQ_MV_MINB
+#define NRQ_MV_MINB 2
+#endif
+#ifndef NRQ_MV_UNROLL_DIR
+#define NRQ_MV_UNROLL_DIR 1
+#endif
+#ifndef NRQ_MV_UNROLL_COL
+#define NRQ_MV_UNROLL_COL 2
+#endif
+
 namespace nrq {
+
+constexpr int kMvUnrollDir = NRQ_MV_UNROLL_DIR;
+constexpr int kMvUnrollCol = NRQ_MV_UNROLL_COL;
 
 // entry (s, sp) of the transposed reference Pauli matrix s_k^T
 // (src/su2.f90:68-79 holds s_2 transposed, so s_2^T = [[0,-i],[i,0]])
@@ -35,7 +50,7 @@ __device__ __forceinline__ cplx scal_col(const double *sc, int col12, int slot) 
 
 #ifndef NRQ_MV_V1
 template <int MODE>
-__global__ void __launch_bounds__(192, 2) k_cn_mv2(Lat L, CnCoef C, const double2 *__restrict__ U,
+__global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, const double2 *__restrict__ U,
                                                    const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
                                                    const double2 *__restrict__ DE, MvArgs A) {
   const int lane = threadIdx.x & 31;
@@ -91,11 +106,11 @@ __global__ void __launch_bounds__(192, 2) k_cn_mv2(Lat L, CnCoef C, const double
   }
   const cplx cs0 = times_i(aso);   // eps = +1 permutation (j,k) = (i+1, i+2)
   const cplx cs1 = -times_i(aso);  // eps = -1 permutation (j,k) = (i+2, i+1)
-#pragma unroll 1
+#pragma unroll kMvUnrollDir
   for (int i = 0; i < 3; ++i) {
     const cplx ck = (-0.5 * C.inva2[i]) * ak;
     const int k0 = (i + 2) % 3, k1 = (i + 1) % 3;
-#pragma unroll 1
+#pragma unroll kMvUnrollDir
     for (int dir = 0; dir < 2; ++dir) {
       // dir 0: neighbour x+i, blocks from site x (transposed)
       // dir 1: neighbour x-i, blocks from site x-i (complex conjugated)
@@ -128,7 +143,7 @@ __global__ void __launch_bounds__(192, 2) k_cn_mv2(Lat L, CnCoef C, const double
             Wm[s][cp][t] = v;
           }
       }
-#pragma unroll 2
+#pragma unroll kMvUnrollCol
       for (int col = 0; col < 6; ++col) {
         cplx w[6];
         load_w(y, col, w);
