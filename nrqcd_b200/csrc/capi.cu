@@ -87,6 +87,12 @@ class Ranlxd {
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// per-column Krylov scalars followed by one int error flag written by the
+// stencil kernels (NRQ_ERR_TIMEOUT when a bounded wait expired)
+constexpr size_t kScalDoubles = (size_t)nrq::CN_COLS * nrq::SC_STRIDE;
+constexpr size_t kScalBytes = sizeof(double) * (kScalDoubles + 2);
+inline int *scal_err(double *scal) { return (int *)(scal + kScalDoubles); }
+
 int ensure_stage(nrq_ctx *ctx, size_t bytes) {
   if (ctx->stage_bytes >= bytes) return NRQ_OK;
   if (ctx->d_stage) cudaFree(ctx->d_stage);
@@ -658,19 +664,21 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
   alloc((void **)&cn->Dsum, sizeof(double2) * 9 * V);
   alloc((void **)&cn->Bsum, sizeof(double) * 9 * V);
   alloc((void **)&cn->DE, sizeof(double2) * 54 * V);
-  for (double2 **pp : {&cn->b, &cn->x, &cn->r, &cn->rh, &cn->p, &cn->v, &cn->t})
+  for (double2 **pp : {&cn->b, &cn->x, &cn->r, &cn->rh, &cn->p, &cn->v, &cn->t, &cn->s})
     alloc((void **)pp, sizeof(double2) * 72 * V);
-  alloc((void **)&cn->scal, sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE);
-  alloc((void **)&cn->partials, sizeof(double) * cn->nblocks * nrq::CN_COLS * 3);
-  if (ok && cudaMallocHost((void **)&cn->h_scal, sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE) != cudaSuccess)
-    ok = false;
+  alloc((void **)&cn->scal, kScalBytes);
+  alloc((void **)&cn->partials, sizeof(double) * 3 * cn->nblocks * nrq::CN_COLS * 3);
+  if (ok && cudaMallocHost((void **)&cn->h_scal, kScalBytes) != cudaSuccess) ok = false;
+  // the TMA-staged stencil needs 16-byte plane strides for the real-valued
+  // magnetic planes (V even) and tiles no wider than the lattice
+  cn->use_tma = (V % 2 == 0) && V >= 64;
   if (!ok) {
     cudaGetLastError();
     nrq_cn_finalize(cn);
     ctx->last_error = "nrq_cn_init: device allocation failed";
     return NRQ_ERR_OOM;
   }
-  NRQ_CUDA_TRY(ctx, cudaMemsetAsync(cn->scal, 0, sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE, ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaMemsetAsync(cn->scal, 0, kScalBytes, ctx->stream));
   *out = cn;
   return NRQ_OK;
 }
@@ -680,7 +688,7 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
   cudaSetDevice(cn->ctx->device);
   cudaStreamSynchronize(cn->ctx->stream);
   for (void *p : {(void *)cn->Dsum, (void *)cn->Bsum, (void *)cn->DE, (void *)cn->b, (void *)cn->x, (void *)cn->r,
-                  (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->scal,
+                  (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->s, (void *)cn->scal,
                   (void *)cn->partials})
     if (p) cudaFree(p);
   if (cn->h_scal) cudaFreeHost(cn->h_scal);
@@ -698,12 +706,18 @@ double mv_bytes(const nrq_ctx *ctx, int mode) {
 void mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq::MvArgs &a) {
   nrq_ctx *ctx = cn->ctx;
   ProfScope ps(ctx, 0, mv_bytes(ctx, mode));
+  if (cn->use_tma && nrq::launch_cn_mv3(mode, ctx->lat, C, g->U, cn->Dsum, cn->Bsum, cn->DE, a,
+                                        scal_err(cn->scal), ctx->sm_count, ctx->stream) == 0)
+    return;
+  cn->use_tma = false;  // tensor maps unavailable: register-tiled stencil from here on
   nrq::launch_cn_mv(mode, ctx->lat, C, g->U, cn->Dsum, cn->Bsum, cn->DE, a, ctx->stream);
 }
 void fin(nrq_cn *cn, int stage) {
   nrq_ctx *ctx = cn->ctx;
-  ProfScope ps(ctx, 2, (double)cn->nblocks * 12 * 3 * 8);
-  nrq::launch_cn_finalize(stage, cn->nblocks, cn->partials, cn->scal, cn->tol, ctx->stream);
+  // the TMA-staged stencil leaves one partial row per (unit, colour warp)
+  const int64_t rows = (stage <= 2 && cn->use_tma) ? 3 * cn->nblocks : cn->nblocks;
+  ProfScope ps(ctx, 2, (double)rows * 12 * 3 * 8);
+  nrq::launch_cn_finalize(stage, rows, cn->partials, cn->scal, cn->tol, ctx->stream);
 }
 int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
   nrq_ctx *ctx = cn->ctx;
@@ -756,7 +770,6 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   int64_t its = 0;
   int status = NRQ_OK;
   double *hs = cn->h_scal;
-  const size_t scal_bytes = sizeof(double) * nrq::CN_COLS * nrq::SC_STRIDE;
   for (;;) {
     if (restart) {
       nrq::MvArgs a{};
@@ -786,15 +799,29 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       a.scal = cn->scal;
       mv(cn, nrq::MV_V, CH, g, a);
       fin(cn, 1);
+      const bool tma = cn->use_tma;
       nrq::MvArgs b{};
-      b.in = cn->r;
-      b.in2 = cn->v;
+      if (tma) {  // s = r - alpha v materialised, then t = A^H s
+        {
+          ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 3);
+          nrq::launch_vec_s(L, cn->s, cn->r, cn->v, cn->scal, st);
+        }
+        b.in = cn->s;
+        vstreams += 3;
+      } else {    // s formed on the fly inside the stencil
+        b.in = cn->r;
+        b.in2 = cn->v;
+      }
       b.out = cn->t;
       b.partials = cn->partials;
       b.scal = cn->scal;
       mv(cn, nrq::MV_T, CH, g, b);
       fin(cn, 2);
-      {
+      if (tma) {
+        ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 7);
+        nrq::launch_vec_xr_s(L, cn->x, cn->r, cn->p, cn->s, cn->t, cn->rh, cn->scal, cn->partials, st);
+        vstreams -= 1;
+      } else {
         ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 8);
         nrq::launch_vec_xr(L, cn->x, cn->r, cn->p, cn->v, cn->t, cn->rh, cn->scal, cn->partials, st);
       }
@@ -808,8 +835,14 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       ++its;
     }
     if ((rc = check_launch(ctx, "cn iteration"))) return rc;
-    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(hs, cn->scal, scal_bytes, cudaMemcpyDeviceToHost, st));
+    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(hs, cn->scal, kScalBytes, cudaMemcpyDeviceToHost, st));
     NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (*scal_err(hs) != 0) {
+      status = NRQ_ERR_TIMEOUT;
+      ctx->last_error = "CN stencil: a bounded pipeline wait expired";
+      NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, sizeof(int), st));
+      break;
+    }
     bool all = true, brk = false, nonfin = false;
     for (int k = 0; k < nrq::CN_COLS; ++k) {
       const double *s = hs + k * nrq::SC_STRIDE;

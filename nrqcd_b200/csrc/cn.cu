@@ -21,9 +21,9 @@
 //   alpha_so = -kappa c4/(8M^2); antiquark: M -> -M, c -> conj(c).
 //
 // Layout: propagator planes (species*36 + col*6 + row), V complex each.
-// The matvec runs 12 warps per block, one warp per (species, column), all
-// warps over the same 32 sites so that the gauge-derived matrices are read
-// once from HBM and then from L1.
+// The stencil kernels live in cn_mv3.cu (TMA-staged) and cn_mv.cu
+// (register-tiled); this file holds the per-step preparation, the BiCGStab
+// vector updates and scalar stages, and the propagator I/O and observables.
 #include "nrq_kernels.cuh"
 
 namespace nrq {
@@ -131,6 +131,67 @@ __device__ void field_strength_from_plaquette(const m3 &P, double scale_, double
     }
 }
 
+// Same quantity for plaquettes inside the principal branch with small
+// angles, without an eigen-decomposition.  For unitary P = exp(iH) whose
+// eigenphases satisfy |theta| < pi/2, K = (P - P^+)/(2i) = sin(H) and
+// H = asin(K) = sum_n c_n K^(2n+1), c_n = (2n)!/(4^n (n!)^2 (2n+1)).  The
+// powers of K are reduced with Cayley-Hamilton (K^3 = t1 K^2 - t2 K + t3 1
+// with the real invariants of the hermitian K), so the series runs on three
+// real coefficients and H = f0 1 + f1 K + f2 K^2 is assembled once.  Used
+// when |K|_F <= 0.3 and Re Tr P > 2 (all eigenphases then lie within
+// |theta| < 0.31); the Jacobi route handles every other plaquette.  Both
+// return Re(LogU(P)/i) to rounding.
+__device__ bool field_strength_small_angle(const m3 &P, double scale_, double F[9]) {
+  const double trP = P.e[0].re + P.e[4].re + P.e[8].re;
+  m3 K;
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      // (P[r][c] - conj(P[c][r])) / (2i)
+      cplx d = P.e[r * 3 + c] - conj(P.e[c * 3 + r]);
+      K.e[r * 3 + c] = {0.5 * d.im, -0.5 * d.re};
+    }
+  double nf2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) nf2 += norm2(K.e[k]);
+  if (!(trP > 2.0) || !(nf2 <= 0.09)) return false;
+  const double rho = sqrt(nf2);
+  const m3 K2 = mul(K, K);
+  const double t1 = K.e[0].re + K.e[4].re + K.e[8].re;
+  const double trK2 = K2.e[0].re + K2.e[4].re + K2.e[8].re;
+  const double t2 = 0.5 * (t1 * t1 - trK2);
+  // det K (real for hermitian K)
+  const cplx det = K.e[0] * (K.e[4] * K.e[8] - K.e[5] * K.e[7]) - K.e[1] * (K.e[3] * K.e[8] - K.e[5] * K.e[6]) +
+                   K.e[2] * (K.e[3] * K.e[7] - K.e[4] * K.e[6]);
+  const double t3 = det.re;
+  // K^m = a 1 + b K + d K^2 ; start m = 1
+  double a = 0.0, b = 1.0, d = 0.0;
+  double f0 = 0.0, f1 = 1.0, f2 = 0.0;  // c_0 K
+  double cn = 1.0, pw = rho;            // c_n (n = 0) and rho^(2n+1)
+  for (int n = 1; n <= 40; ++n) {
+    // two multiplications by K: K^(2n+1) from K^(2n-1)
+    for (int rep = 0; rep < 2; ++rep) {
+      const double an = d * t3, bn = a - d * t2, dn = b + d * t1;
+      a = an;
+      b = bn;
+      d = dn;
+    }
+    cn *= (double)(2 * n - 1) * (double)(2 * n - 1) / ((double)(2 * n) * (double)(2 * n + 1));
+    pw *= nf2;
+    f0 += cn * a;
+    f1 += cn * b;
+    f2 += cn * d;
+    if (cn * pw < 1e-19 * rho) break;
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double h = f1 * K.e[k].re + f2 * K2.e[k].re + ((k % 4 == 0) ? f0 : 0.0);
+    F[k] = h * scale_;
+  }
+  return true;
+}
+
 // E_j(y) entering the CN operator: -Re(sum_a E~^a T^a)/a0/a_j (real symmetric)
 __device__ __forceinline__ m3 efield_cn(const Lat &L, const double *__restrict__ E, int64_t y, int j) {
   const int64_t V = L.V;
@@ -175,7 +236,8 @@ __global__ void __launch_bounds__(128) k_cn_prepare(Lat L, const double2 *__rest
                          load_link(U, V, nb(L, x, k, +1), j)),
                   load_link(U, V, x, k));
     double F[9];
-    field_strength_from_plaquette(P, 1.0 / L.a[j] / L.a[k], F);
+    if (!field_strength_small_angle(P, 1.0 / L.a[j] / L.a[k], F))
+      field_strength_from_plaquette(P, 1.0 / L.a[j] / L.a[k], F);
     for (int m = 0; m < 9; ++m) B[m] += F[m];
   }
 #pragma unroll
@@ -200,220 +262,10 @@ void launch_cn_prepare(Lat L, const double2 *U, const double *E, double2 *Dsum, 
   k_cn_prepare<<<(unsigned)nb_, 128, 0, st>>>(L, U, E, Dsum, Bsum, DE);
 }
 
-// ------------------------------------------------------------ matvec
-// u = s_k^T w (transposed reference Pauli matrix, src/su2.f90:68-79), index 2c+s
-__device__ __forceinline__ void sigmaT(int k, const cplx w[6], cplx u[6]) {
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    cplx w0 = w[2 * c], w1 = w[2 * c + 1];
-    if (k == 0) {
-      u[2 * c] = w1;
-      u[2 * c + 1] = w0;
-    } else if (k == 1) {
-      u[2 * c] = -times_i(w1);
-      u[2 * c + 1] = times_i(w0);
-    } else {
-      u[2 * c] = w0;
-      u[2 * c + 1] = -w1;
-    }
-  }
-}
-
-// acc[2c+s] += sum_c' M[c'][c] u[2c'+s]    (M^T x 1)
-__device__ __forceinline__ void apply_T(const double2 *__restrict__ Mp, int64_t V, int64_t y, const cplx u[6],
-                                        cplx acc[6]) {
-#pragma unroll
-  for (int cp = 0; cp < 3; ++cp)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      cplx m = ldg(Mp + (int64_t)(cp * 3 + c) * V + y);
-      cmac(acc[2 * c], m, u[2 * cp]);
-      cmac(acc[2 * c + 1], m, u[2 * cp + 1]);
-    }
-}
-// acc[2c+s] += sum_c' conj(M[c][c']) u[2c'+s]    (M^* x 1)
-__device__ __forceinline__ void apply_C(const double2 *__restrict__ Mp, int64_t V, int64_t y, const cplx u[6],
-                                        cplx acc[6]) {
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int cp = 0; cp < 3; ++cp) {
-      cplx m = ldg(Mp + (int64_t)(c * 3 + cp) * V + y);
-      cmac_cj(acc[2 * c], m, u[2 * cp]);
-      cmac_cj(acc[2 * c + 1], m, u[2 * cp + 1]);
-    }
-}
-
 __device__ __forceinline__ cplx scal_c(const double *sc, int col, int slot) {
   return {sc[col * SC_STRIDE + slot], sc[col * SC_STRIDE + slot + 1]};
 }
 
-#ifdef NRQ_MV_V1
-template <int MODE>
-__global__ void __launch_bounds__(384) k_cn_mv(Lat L, CnCoef C, const double2 *__restrict__ U,
-                                               const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
-                                               const double2 *__restrict__ DE, MvArgs A) {
-  const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;  // column index 0..11
-  const int sp = w / 6;
-  const int64_t V = L.V;
-  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
-  const bool active = x0 < V;
-  const int64_t x = active ? x0 : 0;
-  const int64_t pb = (int64_t)(w * 6) * V;  // (sp*36 + col*6) = w*6
-  cplx als = {0.0, 0.0};
-  if (MODE == MV_T) als = scal_c(A.scal, w, SC_ALPHA);
-
-  auto load_in = [&](int64_t y, cplx v[6]) {
-#pragma unroll
-    for (int r = 0; r < 6; ++r) {
-      v[r] = ldg(A.in + pb + (int64_t)r * V + y);
-      if (MODE == MV_T) v[r] = v[r] - als * ldg(A.in2 + pb + (int64_t)r * V + y);
-    }
-  };
-
-  cplx w0[6], acc[6];
-  load_in(x, w0);
-#pragma unroll
-  for (int r = 0; r < 6; ++r) acc[r] = w0[r];
-  const cplx ak = C.kin[sp], am = C.mag[sp], ad = C.dar[sp], aso = C.so[sp];
-  // diagonal colour block: (ak*dkin) 1 + ad D^T + am B^T
-  {
-    cplx Cd[9];
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int cp = 0; cp < 3; ++cp) {
-        cplx dv = ldg(Dsum + (int64_t)(cp * 3 + c) * V + x);
-        double bv = __ldg(Bsum + (int64_t)(cp * 3 + c) * V + x);
-        cplx v = ad * dv + bv * am;
-        if (c == cp) v = v + C.dkin * ak;
-        Cd[c * 3 + cp] = v;
-      }
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int cp = 0; cp < 3; ++cp) {
-        cmac(acc[2 * c], Cd[c * 3 + cp], w0[2 * cp]);
-        cmac(acc[2 * c + 1], Cd[c * 3 + cp], w0[2 * cp + 1]);
-      }
-  }
-  const cplx cs0 = times_i(aso);   // eps = +1 permutation
-  const cplx cs1 = -times_i(aso);  // eps = -1 permutation
-#pragma unroll 1
-  for (int i = 0; i < 3; ++i) {
-    const cplx ck = (-0.5 * C.inva2[i]) * ak;
-    const int k0 = (i + 2) % 3, k1 = (i + 1) % 3;
-    cplx wv[6], t[6], u[6];
-    // ---- +i neighbour: blocks from site x
-    {
-      const int64_t y = nb(L, x, i, +1);
-      load_in(y, wv);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) t[r] = ck * wv[r];
-      apply_T(U + (int64_t)(i * 9) * V, V, x, t, acc);
-      sigmaT(k0, wv, u);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) t[r] = cs0 * u[r];
-      apply_T(DE + (int64_t)((i * 2 + 0) * 9) * V, V, x, t, acc);
-      sigmaT(k1, wv, u);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) t[r] = cs1 * u[r];
-      apply_T(DE + (int64_t)((i * 2 + 1) * 9) * V, V, x, t, acc);
-    }
-    // ---- -i neighbour: blocks from site y = x-i
-    {
-      const int64_t y = nb(L, x, i, -1);
-      load_in(y, wv);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) t[r] = ck * wv[r];
-      apply_C(U + (int64_t)(i * 9) * V, V, y, t, acc);
-      sigmaT(k0, wv, u);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) t[r] = -(cs0 * u[r]);
-      apply_C(DE + (int64_t)((i * 2 + 0) * 9) * V, V, y, t, acc);
-      sigmaT(k1, wv, u);
-#pragma unroll
-      for (int r = 0; r < 6; ++r) t[r] = -(cs1 * u[r]);
-      apply_C(DE + (int64_t)((i * 2 + 1) * 9) * V, V, y, t, acc);
-    }
-  }
-
-  // ---------------- epilogue by mode
-  double q[3] = {0.0, 0.0, 0.0};
-  if (MODE == MV_PLAIN) {
-    if (active)
-#pragma unroll
-      for (int r = 0; r < 6; ++r) st(A.out + pb + (int64_t)r * V + x, acc[r]);
-  } else if (MODE == MV_RHS) {
-    if (active)
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        st(A.out + pb + (int64_t)r * V + x, acc[r]);
-        st(A.out2 + pb + (int64_t)r * V + x, 2.0 * acc[r] - w0[r]);
-      }
-  } else if (MODE == MV_RES) {
-    if (active)
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        cplx b = ldg(A.bvec + pb + (int64_t)r * V + x);
-        cplx rr = b - acc[r];
-        st(A.out + pb + (int64_t)r * V + x, rr);
-        st(A.out2 + pb + (int64_t)r * V + x, rr);
-        st(A.out3 + pb + (int64_t)r * V + x, rr);
-        q[0] += norm2(rr);
-        q[1] += norm2(b);
-      }
-  } else if (MODE == MV_V) {
-    if (active)
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        st(A.out + pb + (int64_t)r * V + x, acc[r]);
-        cplx h = ldg(A.in2 + pb + (int64_t)r * V + x);
-        cplx d = {0.0, 0.0};
-        cmac_cj(d, h, acc[r]);
-        q[0] += d.re;
-        q[1] += d.im;
-      }
-  } else if (MODE == MV_T) {
-    if (active)
-#pragma unroll
-      for (int r = 0; r < 6; ++r) {
-        st(A.out + pb + (int64_t)r * V + x, acc[r]);
-        cplx d = {0.0, 0.0};
-        cmac_cj(d, acc[r], w0[r]);  // (t . s)
-        q[0] += d.re;
-        q[1] += d.im;
-        q[2] += norm2(acc[r]);
-      }
-  }
-  if (MODE == MV_RES || MODE == MV_V || MODE == MV_T) {
-    constexpr int NQ = (MODE == MV_T) ? 3 : 2;
-#pragma unroll
-    for (int k = 0; k < NQ; ++k) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) q[k] += __shfl_down_sync(0xffffffffu, q[k], o);
-    }
-    if (lane == 0)
-#pragma unroll
-      for (int k = 0; k < NQ; ++k) A.partials[((int64_t)blockIdx.x * CN_COLS + w) * NQ + k] = q[k];
-  }
-}
-
-void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,
-                  const double2 *DE, const MvArgs &a, cudaStream_t st) {
-  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
-  dim3 blk(32 * CN_COLS);
-  switch (mode) {
-    case MV_PLAIN: k_cn_mv<MV_PLAIN><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
-    case MV_RHS: k_cn_mv<MV_RHS><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
-    case MV_RES: k_cn_mv<MV_RES><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
-    case MV_V: k_cn_mv<MV_V><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
-    default: k_cn_mv<MV_T><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
-  }
-}
-
-#endif  // NRQ_MV_V1
 
 // ------------------------------------------------------------ BiCGStab vector updates
 // s = r - alpha v ; x += alpha p + omega s ; r = s - omega t ; partials (rh.r), (r.r)
@@ -465,6 +317,67 @@ __global__ void __launch_bounds__(384) k_vec_p(int64_t V, double2 *__restrict__ 
     const int64_t o = pb + (int64_t)r * V + x0;
     st(P + o, ldg(R + o) + be * (ld(P + o) - om * ldg(Vv + o)));
   }
+}
+
+// s = r - alpha v (materialised for the TMA-staged stencil)
+__global__ void __launch_bounds__(384) k_vec_s(int64_t V, double2 *__restrict__ S, const double2 *__restrict__ R,
+                                               const double2 *__restrict__ Vv, const double *__restrict__ scal) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  if (x0 >= V) return;
+  const int64_t pb = (int64_t)(w * 6) * V;
+  const cplx al = scal_c(scal, w, SC_ALPHA);
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    const int64_t o = pb + (int64_t)r * V + x0;
+    st(S + o, ldg(R + o) - al * ldg(Vv + o));
+  }
+}
+
+// x += alpha p + omega s ; r = s - omega t ; partials (rh.r), (r.r)   (s materialised)
+__global__ void __launch_bounds__(384) k_vec_xr_s(int64_t V, double2 *__restrict__ X, double2 *__restrict__ R,
+                                                  const double2 *__restrict__ P, const double2 *__restrict__ S,
+                                                  const double2 *__restrict__ T, const double2 *__restrict__ RH,
+                                                  const double *__restrict__ scal, double *__restrict__ partials) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  const bool active = x0 < V;
+  const int64_t pb = (int64_t)(w * 6) * V;
+  const cplx al = scal_c(scal, w, SC_ALPHA), om = scal_c(scal, w, SC_OMEGA);
+  double q[3] = {0.0, 0.0, 0.0};
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int64_t o = pb + (int64_t)r * V + x0;
+      const cplx s = ldg(S + o);
+      const cplx xn = ld(X + o) + al * ldg(P + o) + om * s;
+      const cplx rn = s - om * ldg(T + o);
+      st(X + o, xn);
+      st(R + o, rn);
+      cplx d = {0.0, 0.0};
+      cmac_cj(d, ldg(RH + o), rn);
+      q[0] += d.re;
+      q[1] += d.im;
+      q[2] += norm2(rn);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q[k] += __shfl_down_sync(0xffffffffu, q[k], o);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) partials[((int64_t)blockIdx.x * CN_COLS + w) * 3 + k] = q[k];
+}
+
+void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  k_vec_s<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, s, r, v, scal);
+}
+void launch_vec_xr_s(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *s, const double2 *t,
+                     const double2 *rh, const double *scal, double *partials, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  k_vec_xr_s<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, x, r, p, s, t, rh, scal, partials);
 }
 
 void launch_vec_xr(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *v, const double2 *t,

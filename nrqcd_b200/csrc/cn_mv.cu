@@ -1,4 +1,6 @@
-// The 12-column stencil of the assembled Crank-Nicolson operator
+// Register-tiled 12-column stencil of the assembled Crank-Nicolson operator
+// (used where the TMA-staged stencil of cn_mv3.cu cannot describe the
+// lattice with tensor maps, i.e. odd V or V < 64)
 // (src/nrqcd.f90:1175-1387 with PETSc's block transposition), applied
 // matrix-free: out = in + sum_t alpha_t G_t in for both species at once.
 // See cn.cu for the operator; this file holds its stencil kernel.
@@ -48,7 +50,6 @@ __device__ __forceinline__ cplx scal_col(const double *sc, int col12, int slot) 
   return {sc[col12 * SC_STRIDE + slot], sc[col12 * SC_STRIDE + slot + 1]};
 }
 
-#ifndef NRQ_MV_V1
 template <int MODE>
 __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, const double2 *__restrict__ U,
                                                    const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
@@ -72,7 +73,7 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, co
     const double2 *p = A.in + pb + (int64_t)(col * 6) * V + y;
 #pragma unroll
     for (int r = 0; r < 6; ++r) w[r] = ldg(p + (int64_t)r * V);
-    if (MODE == MV_T) {
+    if (MODE == MV_T && A.in2 != nullptr) {
       const double2 *q = A.in2 + pb + (int64_t)(col * 6) * V + y;
 #pragma unroll
       for (int r = 0; r < 6; ++r) w[r] = w[r] - al[col] * ldg(q + (int64_t)r * V);
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, co
           q[col][1] += d.im;
         } else {  // MV_T
           st(A.out + o, y_);
-          const cplx s_ = ldg(A.in + o) - al[col] * ldg(A.in2 + o);
+          const cplx s_ = A.in2 ? ldg(A.in + o) - al[col] * ldg(A.in2 + o) : ldg(A.in + o);
           cplx d = {0.0, 0.0};
           cmac_cj(d, y_, s_);
           q[col][0] += d.re;
@@ -235,7 +236,5 @@ void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
     default: k_cn_mv2<MV_T><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
   }
 }
-
-#endif  // NRQ_MV_V1
 
 }  // namespace nrq

@@ -93,7 +93,9 @@ struct nrq_cn {
   double2 *DE = nullptr;    // 54 planes: ((i*2 + perm)*9 + r*3 + c)
   // Krylov vectors, 72 planes each
   double2 *b = nullptr, *x = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr,
-          *t = nullptr;
+          *t = nullptr, *s = nullptr;
+  // TMA-staged stencil usable for this lattice (else the register-tiled one)
+  bool use_tma = false;
   double *scal = nullptr;     // device scalars per column
   double *h_scal = nullptr;   // pinned mirror
   int *d_flags = nullptr;

@@ -68,6 +68,14 @@ void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
 void launch_vec_xr(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *v, const double2 *t,
                    const double2 *rh, const double *scal, double *partials, cudaStream_t st);
 void launch_vec_p(Lat L, double2 *p, const double2 *r, const double2 *v, const double *scal, cudaStream_t st);
+void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st);
+void launch_vec_xr_s(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *s, const double2 *t,
+                     const double2 *rh, const double *scal, double *partials, cudaStream_t st);
+// TMA-staged stencil (cn_mv3.cu); returns nonzero if the tensor maps cannot
+// describe this lattice (then the caller uses launch_cn_mv).  For MV_T its
+// input is the materialised s = r - alpha v.
+int launch_cn_mv3(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,
+                  const double2 *DE, const MvArgs &a, int *err, int sm_count, cudaStream_t st);
 // finalize stages: 0 = after RES (rr, bb), 1 = alpha (rh.v), 2 = omega (t.s, t.t), 3 = beta (rh.r, r.r)
 void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
                         cudaStream_t st);
