@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--size", type=int, default=64)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-forms", action="store_true")
     return p.parse_args()
 
 
@@ -166,6 +167,44 @@ def cpu_baseline_sample(L):
                       "(OpenMP), GMRES(30) to 1e-12"}
 
 
+# ------------------------------------------------------------------ CN forms
+FORMS = {"plain_fp64_bicgstab": 0, "precision_fp32_chebyshev_fp64_refinement": 1}
+
+
+def measure_cn_forms(g, stream, steps, tol=1e-10):
+    """CN-only seconds per step of every solver form at the same residual,
+    on the same gauge field (the headline's comparison at <= 1e-10)."""
+    import torch
+    from nrqcd_b200 import NRQCDField, nrqcd
+    out = {}
+    for name, form in FORMS.items():
+        if nrqcd.IsModuleInitialised():
+            nrqcd.FinalizeModule()
+        nrqcd.InitModule(MASS, WILSON, 1.0, tol, form=form)
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        for _ in range(2):
+            h.Update(g, MASS, WILSON, 1.0)
+        stats = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            stats.append(h.Update(g, MASS, WILSON, 1.0))
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"s_per_step": ms / 1000.0, "tol": tol,
+                     "max_rel_residual": max(st["max_rel_residual"] for st in stats),
+                     "stencil_launches_per_step": float(np.mean([st["matvecs"] for st in stats])),
+                     "norms": [h.GetNorm_Quark(), h.GetNorm_AntiQ()]}
+        del h
+        nrqcd.FinalizeModule()
+    base = out["plain_fp64_bicgstab"]["s_per_step"]
+    for v in out.values():
+        v["speedup_vs_plain_fp64"] = base / v["s_per_step"]
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 def main():
     args = parse()
@@ -278,6 +317,12 @@ def main():
                "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
                        "nrq_heavy_download + nrq_gauge_download, pinned host buffers"}
 
+    forms = None
+    if not args.no_forms:
+        nrqcd.FinalizeModule()
+        forms = measure_cn_forms(g, stream, max(2, min(args.steps, 5)))
+        nrqcd.InitModule(MASS, WILSON, 1.0, TOL)
+
     if rank == 0:
         peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
         peak, peak_src = 6650.0, "fallback"
@@ -304,6 +349,7 @@ def main():
                    "max_rel_residual": max(s["max_rel_residual"] for s in iters) if iters else None,
                    "norms": [norm_q, norm_a]},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(sum(v["launches"] for v in prof.values())),
+            "cn_forms_at_1e-10": forms,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(min(L, 64))

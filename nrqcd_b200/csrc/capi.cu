@@ -4,6 +4,7 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <new>
 #include <string>
@@ -640,8 +641,12 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
                            int64_t maxits, int form, nrq_cn **out) {
   if (!ctx || !c || !out) return NRQ_ERR_BAD_ARG;
   *out = nullptr;
-  if (mass == 0.0 || !(tol > 0.0) || maxits < 1 || form != 0) {
+  if (mass == 0.0 || !(tol > 0.0) || maxits < 1 || form < 0 || form > 1) {
     ctx->last_error = "nrq_cn_init: invalid mass, tolerance, maxits or form";
+    return NRQ_ERR_BAD_ARG;
+  }
+  if (form == 1 && (c[1] != 0.0 || c[3] != 0.0 || c[5] != 0.0 || c[7] != 0.0)) {
+    ctx->last_error = "nrq_cn_init: the precision form needs real Wilson coefficients";
     return NRQ_ERR_BAD_ARG;
   }
   int rc = set_device(ctx);
@@ -669,6 +674,15 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
   alloc((void **)&cn->scal, kScalBytes);
   alloc((void **)&cn->partials, sizeof(double) * 3 * cn->nblocks * nrq::CN_COLS * 3);
   if (ok && cudaMallocHost((void **)&cn->h_scal, kScalBytes) != cudaSuccess) ok = false;
+  if (form == 1) {
+    alloc((void **)&cn->U32, sizeof(float2) * 27 * V);
+    alloc((void **)&cn->DE32, sizeof(float2) * 54 * V);
+    alloc((void **)&cn->D32, sizeof(float2) * 9 * V);
+    alloc((void **)&cn->B32, sizeof(float) * 9 * V);
+    for (float2 **pp : {&cn->r32, &cn->dA32, &cn->dB32, &cn->e32}) alloc((void **)pp, sizeof(float2) * 72 * V);
+    alloc((void **)&cn->bounds, sizeof(double) * (4 * ((V + 255) / 256) + 8));
+    if (ok && cudaMallocHost((void **)&cn->h_bounds, sizeof(double) * 8) != cudaSuccess) ok = false;
+  }
   // the TMA-staged stencil needs 16-byte plane strides for the real-valued
   // magnetic planes (V even) and tiles no wider than the lattice
   cn->use_tma = (V % 2 == 0) && V >= 64;
@@ -689,9 +703,11 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
   cudaStreamSynchronize(cn->ctx->stream);
   for (void *p : {(void *)cn->Dsum, (void *)cn->Bsum, (void *)cn->DE, (void *)cn->b, (void *)cn->x, (void *)cn->r,
                   (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->s, (void *)cn->scal,
-                  (void *)cn->partials})
+                  (void *)cn->partials, (void *)cn->U32, (void *)cn->DE32, (void *)cn->D32, (void *)cn->B32,
+                  (void *)cn->r32, (void *)cn->dA32, (void *)cn->dB32, (void *)cn->e32, (void *)cn->bounds})
     if (p) cudaFree(p);
   if (cn->h_scal) cudaFreeHost(cn->h_scal);
+  if (cn->h_bounds) cudaFreeHost(cn->h_bounds);
   delete cn;
   return NRQ_OK;
 }
@@ -743,6 +759,185 @@ extern "C" int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const d
   return check_launch(ctx, "k_cn_mv");
 }
 
+
+namespace {
+// Chebyshev parameters for A^H = 1 + i tau H with spec(H) in [lo, hi]:
+// theta (centre), delta (half-length), sigma = theta/delta
+struct ChebSeg {
+  std::complex<double> theta, delta, sigma;
+};
+ChebSeg cheb_segment(double tau, double lo, double hi) {
+  ChebSeg s;
+  s.theta = std::complex<double>(1.0, tau * 0.5 * (lo + hi));
+  double half = std::fabs(tau) * 0.5 * (hi - lo);
+  if (half < 1e-14) half = 1e-14;
+  s.delta = std::complex<double>(0.0, half);
+  s.sigma = s.theta / s.delta;
+  return s;
+}
+// |T_m(sigma)| via the recurrence T_{k+1} = 2 sigma T_k - T_{k-1}
+double cheb_gain(std::complex<double> sigma, int m) {
+  std::complex<double> t0(1.0, 0.0), t1 = sigma;
+  if (m == 0) return 1.0;
+  for (int k = 1; k < m; ++k) {
+    std::complex<double> t2 = 2.0 * sigma * t1 - t0;
+    t0 = t1;
+    t1 = t2;
+  }
+  return std::abs(t1);
+}
+
+// Precision form: FP64 refinement around FP32 Chebyshev inner solves.
+int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass, const double c[8], double dt,
+                        nrq_cn_stats *stats) {
+  nrq_ctx *ctx = cn->ctx;
+  cudaStream_t st = ctx->stream;
+  const nrq::Lat L = ctx->lat;
+  const int64_t V = L.V;
+  if (c[1] != 0.0 || c[3] != 0.0 || c[5] != 0.0 || c[7] != 0.0) {
+    ctx->last_error = "precision form: Wilson coefficients must be real";
+    return NRQ_ERR_BAD_ARG;
+  }
+  const nrq::CnCoef CA = make_coef(ctx, mass, c, dt, false);
+  const nrq::CnCoef CH = make_coef(ctx, mass, c, dt, true);
+  const double tau = std::fabs(dt) * ctx->a[0] / 2.0;
+  int rc = cn_prepare(cn, g);
+  if (rc) return rc;
+  {
+    ProfScope ps(ctx, 3, (double)V * (1080.0 + 540.0));
+    nrq::launch_cn_to_f32(V, g->U, cn->DE, cn->Dsum, cn->Bsum, cn->U32, cn->DE32, cn->D32, cn->B32, st);
+  }
+  // spectral enclosure of H per species
+  {
+    ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 216.0));
+    const int64_t nblk = (V + 255) / 256;
+    nrq::launch_cn_bounds(L, CH, dt > 0 ? tau : -tau, g->U, cn->Dsum, cn->Bsum, cn->DE, cn->bounds,
+                          cn->bounds + 4 * nblk, st);
+    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(cn->h_bounds, cn->bounds + 4 * nblk, sizeof(double) * 4,
+                                      cudaMemcpyDeviceToHost, st));
+  }
+  int64_t matvecs = 0, vstreams = 0;
+  {  // RHS = A psi ; x0 = 2 RHS - psi
+    nrq::MvArgs a{};
+    a.in = h->P;
+    a.out = cn->b;
+    a.out2 = cn->x;
+    mv(cn, nrq::MV_RHS, CA, g, a);
+    matvecs += 1;
+    vstreams += 1;
+  }
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  ChebSeg seg[2];
+  for (int sp = 0; sp < 2; ++sp) {
+    double lo = cn->h_bounds[2 * sp], hi = cn->h_bounds[2 * sp + 1];
+    if (!std::isfinite(lo) || !std::isfinite(hi) || hi < lo) {
+      ctx->last_error = "precision form: invalid spectral bounds";
+      return NRQ_ERR_NONFINITE;
+    }
+    cn->last_lo[sp] = lo;
+    cn->last_hi[sp] = hi;
+    // A^H = 1 + i (dt a0/2) H: the sign of dt enters through tau
+    seg[sp] = cheb_segment(dt > 0 ? tau : -tau, lo, hi);
+  }
+  // inner steps: enough for a 1e-6 reduction on the enclosing segment
+  int m = 1;
+  while (m < 40 && std::min(cheb_gain(seg[0].sigma, m), cheb_gain(seg[1].sigma, m)) < 1e6) ++m;
+  // per-step Chebyshev coefficients (identical for every outer pass)
+  std::vector<nrq::ChebCoef> coef(m);
+  {
+    std::complex<double> rho[2];
+    for (int sp = 0; sp < 2; ++sp) rho[sp] = 1.0 / seg[sp].sigma;
+    for (int k = 0; k < m; ++k)
+      for (int sp = 0; sp < 2; ++sp) {
+        std::complex<double> rn = 1.0 / (2.0 * seg[sp].sigma - rho[sp]);
+        std::complex<double> c1 = rn * rho[sp], c2 = 2.0 * rn / seg[sp].delta;
+        coef[k].c1[sp] = {c1.real(), c1.imag()};
+        coef[k].c2[sp] = {c2.real(), c2.imag()};
+        rho[sp] = rn;
+      }
+  }
+  int status = NRQ_OK;
+  double *hs = cn->h_scal;
+  int64_t outer = 0, inner = 0;
+  bool conv = false;
+  for (outer = 0; outer < 8; ++outer) {
+    nrq::MvArgs a{};
+    a.in = cn->x;
+    a.bvec = cn->b;
+    a.r32 = cn->r32;
+    a.d32 = cn->dA32;
+    a.partials = cn->partials;
+    for (int sp = 0; sp < 2; ++sp) {
+      std::complex<double> it = 1.0 / seg[sp].theta;
+      a.inv_theta[sp] = {it.real(), it.imag()};
+    }
+    mv(cn, nrq::MV_RESC, CH, g, a);
+    fin(cn, 0);
+    matvecs += 1;
+    vstreams += 3;
+    if ((rc = check_launch(ctx, "cn residual"))) return rc;
+    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(hs, cn->scal, kScalBytes, cudaMemcpyDeviceToHost, st));
+    NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (*scal_err(hs) != 0) {
+      NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, sizeof(int), st));
+      ctx->last_error = "CN stencil: a bounded pipeline wait expired";
+      return NRQ_ERR_TIMEOUT;
+    }
+    bool all = true, nonfin = false;
+    for (int k = 0; k < nrq::CN_COLS; ++k) {
+      all = all && hs[k * nrq::SC_STRIDE + nrq::SC_CONV] != 0.0;
+      nonfin = nonfin || hs[k * nrq::SC_STRIDE + nrq::SC_NONFIN] != 0.0;
+    }
+    if (nonfin) {
+      ctx->last_error = "CN solve: non-finite residual";
+      status = NRQ_ERR_NONFINITE;
+      break;
+    }
+    if (all) {
+      conv = true;
+      break;
+    }
+    if (outer == 7) break;
+    // FP32 inner Chebyshev solve of A^H e = r, then x += e
+    float2 *dcur = cn->dA32, *dnext = cn->dB32;
+    for (int k = 0; k < m; ++k) {
+      ProfScope ps(ctx, 0, (double)V * (576.0 * 6 + 756.0));
+      nrq::launch_cheb32(k == 0, L, CH, cn->U32, cn->D32, cn->B32, cn->DE32, dcur, dnext, cn->r32, cn->e32, coef[k],
+                         st);
+      std::swap(dcur, dnext);
+    }
+    inner += m;
+    {
+      ProfScope ps(ctx, 1, (double)V * (1152.0 * 2 + 576.0));
+      nrq::launch_add_e(72 * V, cn->x, cn->e32, st);
+    }
+    matvecs += m;
+    vstreams += 3;
+  }
+  if (status == NRQ_OK && !conv) status = NRQ_ERR_NOT_CONVERGED;
+  std::swap(h->P, cn->x);
+  double maxrel = 0.0;
+  for (int k = 0; k < nrq::CN_COLS; ++k) {
+    const double *s = hs + k * nrq::SC_STRIDE;
+    double rel = s[nrq::SC_BB] > 0 ? std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]) : 0.0;
+    maxrel = std::max(maxrel, rel);
+  }
+  cn->last_iterations = inner;
+  cn->last_inner = inner;
+  cn->last_outer = outer;
+  cn->last_matvecs = matvecs;
+  cn->last_vecstreams = vstreams;
+  if (stats) {
+    stats->iterations = inner;
+    stats->matvecs = matvecs;
+    stats->vector_streams = vstreams;
+    stats->max_rel_residual = maxrel;
+    stats->converged = conv ? 1 : 0;
+  }
+  return status;
+}
+}  // namespace
+
 extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass, const double c[8],
                                    double dt, nrq_cn_stats *stats) {
   if (!cn || !h || !g || !c) return NRQ_ERR_BAD_ARG;
@@ -750,6 +945,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   if (g->ctx != ctx || h->ctx != ctx || mass == 0.0) return NRQ_ERR_BAD_ARG;
   int rc = set_device(ctx);
   if (rc) return rc;
+  if (cn->form == 1) return cn_update_precision(cn, h, g, mass, c, dt, stats);
   cudaStream_t st = ctx->stream;
   const nrq::Lat L = ctx->lat;
   const nrq::CnCoef CA = make_coef(ctx, mass, c, dt, false);

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, co
   }
 
   // ---------------- epilogue by mode; rows (c, s) of the 6 columns
-  constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V) ? 2 : 0);
+  constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
   double q[6][3];
 #pragma unroll
   for (int col = 0; col < 6; ++col)
@@ -192,6 +192,14 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, co
           cmac_cj(d, ldg(A.in2 + o), y_);
           q[col][0] += d.re;
           q[col][1] += d.im;
+        } else if (MODE == MV_RESC) {
+          const cplx b = ldg(A.bvec + o);
+          const cplx r = b - y_;
+          const cplx dd = r * A.inv_theta[sp];
+          A.r32[o] = make_float2((float)r.re, (float)r.im);
+          A.d32[o] = make_float2((float)dd.re, (float)dd.im);
+          q[col][0] += norm2(r);
+          q[col][1] += norm2(b);
         } else {  // MV_T
           st(A.out + o, y_);
           const cplx s_ = A.in2 ? ldg(A.in + o) - al[col] * ldg(A.in2 + o) : ldg(A.in + o);
@@ -233,6 +241,7 @@ void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
     case MV_RHS: k_cn_mv2<MV_RHS><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
     case MV_RES: k_cn_mv2<MV_RES><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
     case MV_V: k_cn_mv2<MV_V><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
+    case MV_RESC: k_cn_mv2<MV_RESC><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
     default: k_cn_mv2<MV_T><<<nb_, blk, 0, st>>>(L, C, U, Dsum, Bsum, DE, a); break;
   }
 }

@@ -390,7 +390,7 @@ __global__ void __launch_bounds__(mv3::kThreads, 1)
     }
 
     // ------------------------------------------------------------ epilogue
-    constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V) ? 2 : 0);
+    constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
     double q[kCols][3];
 #pragma unroll
     for (int j = 0; j < kCols; ++j) q[j][0] = q[j][1] = q[j][2] = 0.0;
@@ -420,6 +420,14 @@ __global__ void __launch_bounds__(mv3::kThreads, 1)
             cmac_cj(d, ldg(A.in2 + o), y_);
             q[j][0] += d.re;
             q[j][1] += d.im;
+          } else if (MODE == MV_RESC) {
+            const cplx bb = ldg(A.bvec + o);
+            const cplx r = bb - y_;
+            const cplx dd = r * A.inv_theta[sp];
+            A.r32[o] = make_float2((float)r.re, (float)r.im);
+            A.d32[o] = make_float2((float)dd.re, (float)dd.im);
+            q[j][0] += norm2(r);
+            q[j][1] += norm2(bb);
           } else {  // MV_T: in = s
             st(A.out + o, y_);
             cplx d = {0.0, 0.0};
@@ -499,6 +507,7 @@ int launch_cn_mv3(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
     case MV_RHS: go(k_cn_mv3<MV_RHS>); break;
     case MV_RES: go(k_cn_mv3<MV_RES>); break;
     case MV_V: go(k_cn_mv3<MV_V>); break;
+    case MV_RESC: go(k_cn_mv3<MV_RESC>); break;
     default: go(k_cn_mv3<MV_T>); break;
   }
   return 0;

@@ -96,6 +96,16 @@ struct nrq_cn {
           *t = nullptr, *s = nullptr;
   // TMA-staged stencil usable for this lattice (else the register-tiled one)
   bool use_tma = false;
+  // precision form (form 1): FP32 copies of the per-step matrices and the
+  // FP32 Chebyshev vectors; spectral bounds of the hermitian part
+  float2 *U32 = nullptr, *DE32 = nullptr, *D32 = nullptr;
+  float *B32 = nullptr;
+  float2 *r32 = nullptr, *dA32 = nullptr, *dB32 = nullptr, *e32 = nullptr;
+  double *bounds = nullptr;    // partial blocks, then 4 final values
+  double *h_bounds = nullptr;  // pinned
+  int64_t last_inner = 0;      // FP32 Chebyshev steps of the last update
+  int64_t last_outer = 0;      // FP64 refinement passes of the last update
+  double last_lo[2] = {0, 0}, last_hi[2] = {0, 0};
   double *scal = nullptr;     // device scalars per column
   double *h_scal = nullptr;   // pinned mirror
   int *d_flags = nullptr;

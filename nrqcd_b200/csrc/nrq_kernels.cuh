@@ -32,7 +32,7 @@ struct CnCoef {
   double inva2[3];   // 1/a_i^2
 };
 
-enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4 };
+enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4, MV_RESC = 5 };
 
 struct MvArgs {
   const double2 *in;  // operand (PLAIN/RHS: psi, RES: x, V: p, T: r)
@@ -43,6 +43,16 @@ struct MvArgs {
   const double2 *bvec;// RES: b
   const double *scal; // per-column scalars
   double *partials;   // per block, per column, NQ doubles
+  // MV_RESC (residual for the FP32 Chebyshev inner solve): r32 = f32(b - A^H x),
+  // d32 = f32((b - A^H x) / theta_species)
+  float2 *r32;
+  float2 *d32;
+  cplx inv_theta[2];
+};
+
+// per-species coefficients of one Chebyshev step: d' = c1 d + c2 r
+struct ChebCoef {
+  cplx c1[2], c2[2];
 };
 
 constexpr int CN_SITES_PER_BLOCK = 32;
@@ -79,6 +89,14 @@ int launch_cn_mv3(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
 // finalize stages: 0 = after RES (rr, bb), 1 = alpha (rh.v), 2 = omega (t.s, t.t), 3 = beta (rh.r, r.r)
 void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
                         cudaStream_t st);
+void launch_cn_to_f32(int64_t V, const double2 *U, const double2 *DE, const double2 *D, const double *B, float2 *U32,
+                      float2 *DE32, float2 *D32, float *B32, cudaStream_t st);
+void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, const double2 *Dsum, const double *Bsum,
+                      const double2 *DE, double *partials, double *out, cudaStream_t st);
+void launch_cheb32(bool first, Lat L, const CnCoef &C, const float2 *U, const float2 *Dsum, const float *Bsum,
+                   const float2 *DE, const float2 *D, float2 *Dn, float2 *R, float2 *E, const ChebCoef &K,
+                   cudaStream_t st);
+void launch_add_e(int64_t n, double2 *X, const float2 *E, cudaStream_t st);
 void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st);
 void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);
 void launch_single_point(double2 *P, int64_t V, int64_t sq, int64_t sa, cudaStream_t st);

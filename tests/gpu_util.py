@@ -8,7 +8,7 @@ from nrqcd_b200 import lattice, nrqcd
 
 @contextlib.contextmanager
 def lattice_ctx(n, a, cn=None):
-    """cn = (Mass, WilsonCoeffs, StepWidth, kspTol) opens the nrqcd module too."""
+    """cn = (Mass, WilsonCoeffs, StepWidth, kspTol[, maxits, form]) opens the nrqcd module too."""
     lattice.InitModule(list(n), list(a), device=0)
     try:
         if cn is not None:
