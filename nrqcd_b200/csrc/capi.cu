@@ -839,15 +839,14 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     // A^H = 1 + i (dt a0/2) H: the sign of dt enters through tau
     seg[sp] = cheb_segment(dt > 0 ? tau : -tau, lo, hi);
   }
-  // inner steps: enough for a 1e-6 reduction on the enclosing segment
-  int m = 1;
-  while (m < 40 && std::min(cheb_gain(seg[0].sigma, m), cheb_gain(seg[1].sigma, m)) < 1e6) ++m;
-  // per-step Chebyshev coefficients (identical for every outer pass)
-  std::vector<nrq::ChebCoef> coef(m);
+  // Chebyshev coefficients along the enclosing segments (the sequence does
+  // not depend on how many steps an inner solve takes)
+  const int kMaxInner = 40;
+  std::vector<nrq::ChebCoef> coef(kMaxInner);
   {
     std::complex<double> rho[2];
     for (int sp = 0; sp < 2; ++sp) rho[sp] = 1.0 / seg[sp].sigma;
-    for (int k = 0; k < m; ++k)
+    for (int k = 0; k < kMaxInner; ++k)
       for (int sp = 0; sp < 2; ++sp) {
         std::complex<double> rn = 1.0 / (2.0 * seg[sp].sigma - rho[sp]);
         std::complex<double> c1 = rn * rho[sp], c2 = 2.0 * rn / seg[sp].delta;
@@ -856,6 +855,14 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
         rho[sp] = rn;
       }
   }
+  // smallest inner step count whose guaranteed gain reaches `gain` on both
+  // species (FP32 inner arithmetic caps a pass at about 1e6)
+  auto inner_steps = [&](double gain) {
+    gain = std::min(std::max(gain, 10.0), 1e6);
+    int m = 1;
+    while (m < kMaxInner && std::min(cheb_gain(seg[0].sigma, m), cheb_gain(seg[1].sigma, m)) < gain) ++m;
+    return m;
+  };
   int status = NRQ_OK;
   double *hs = cn->h_scal;
   int64_t outer = 0, inner = 0;
@@ -898,6 +905,13 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
       break;
     }
     if (outer == 7) break;
+    // gain needed to bring the worst column to 0.3 tol in this pass
+    double worst = 0.0;
+    for (int kk = 0; kk < nrq::CN_COLS; ++kk) {
+      const double *s = hs + kk * nrq::SC_STRIDE;
+      if (s[nrq::SC_BB] > 0) worst = std::max(worst, std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]));
+    }
+    const int m = inner_steps(worst / (0.3 * cn->tol));
     // FP32 inner Chebyshev solve of A^H e = r, then x += e
     float2 *dcur = cn->dA32, *dnext = cn->dB32;
     for (int k = 0; k < m; ++k) {
