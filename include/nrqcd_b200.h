@@ -125,7 +125,9 @@ int nrq_heavy_correlators(nrq_heavy *h, double out[8]);
 
 /* ---- Crank-Nicolson solver module: src/nrqcd.f90:167-212, 619-869 ------ */
 /* InitModule(Mass, WilsonCoeffs, StepWidth, kspTol); c = 4 complex (8 doubles).
- * form: 0 = plain FP64 (BiCGStab, fused stencil/axpy/dot kernels).
+ * form: 0 = plain FP64 (BiCGStab, fused stencil/axpy/dot kernels);
+ *       1 = precision (FP32 Chebyshev inner iterations inside FP64
+ *           iterative refinement to the same tol; real Wilson coefficients).
  * maxits bounds the Krylov iterations (the reference's PETSc default 1e4).  */
 int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, double tol,
                 int64_t maxits, int form, nrq_cn **cn);
@@ -145,6 +147,59 @@ int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
  * verification.                                                            */
 int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const double c[8],
                  double stepwidth, int herm, const nrq_heavy *in, nrq_heavy *out);
+
+/* ---- batching: many fields, one gauge field, one launch per kernel ---- */
+/* No single counterpart in the reference, whose driver advances one
+ * NRQCDField per NRQCDField%Update call (src/nrqcd.f90:1053), field after
+ * field where it evolves several (src/main.f90:983-985).  A batch holds n fields (propagator sources x
+ * heavy masses) of one context; nrq_cn_batch_update advances every field by
+ * one Crank-Nicolson step in the gauge field g with the precision form of
+ * nrq_heavy_update_cn (form 1) at tolerance tol, each kernel launch covering
+ * every field.  The result of field i equals that of nrq_heavy_update_cn on
+ * field i alone to within the tolerance.  Fields must be distinct and belong
+ * to ctx; masses[i] is the heavy mass of fields[i].
+ *
+ * The first update (and the first after c or stepwidth change) calibrates:
+ * it runs the refinement adaptively with host synchronisation, times the
+ * candidate kernel tiles (fields per tile x block order) and keeps the
+ * fastest, and records the per-pass inner step counts as the schedule.
+ * Later updates replay the schedule without host synchronisation, as one
+ * CUDA graph when use_graph != 0, and verify every field's FP64 residual at
+ * the end; a field that missed the tolerance gets adaptive passes and
+ * extends the schedule.  The fields' device buffers are exchanged with the
+ * batch's work buffers on every update (as in nrq_heavy_update_cn).        */
+typedef struct nrq_cn_batch nrq_cn_batch;
+int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *fields, const double *masses,
+                        double tol, nrq_cn_batch **batch);
+int nrq_cn_batch_destroy(nrq_cn_batch *batch);
+/* stats: iterations = FP32 inner steps, matvecs = stencil applications per
+ * field, max_rel_residual = max over fields and columns.                    */
+int nrq_cn_batch_update(nrq_cn_batch *batch, const nrq_gauge *g, const double c[8], double stepwidth,
+                        int use_graph, nrq_cn_stats *stats);
+/* Relative residual ||b - A^H x|| / ||b|| of every field (max over its 12
+ * columns) after the last update, in the order of `fields`.                 */
+int nrq_cn_batch_residuals(const nrq_cn_batch *batch, double *rel);
+/* Tuning and schedule: the chosen fields per tile and block order, the
+ * measured milliseconds per Chebyshev launch of the candidates
+ * (tile 1 order 0, tile 1 order 1, tile 2 order 0, tile 2 order 1; -1 where
+ * not applicable), and the inner steps of each refinement pass (up to 16). */
+int nrq_cn_batch_info(const nrq_cn_batch *batch, int *nf_tile, int *order, double candidate_ms[4],
+                      int *npasses, int steps[16]);
+
+/* An ensemble of independent members (batch[i], gauge[i]); the members may
+ * sit on contexts of different lattice sizes on the same device.  One step
+ * advances every member by the coupled timestep of the reference's driver
+ * loop (src/main.f90:346-348): the batch's Crank-Nicolson update, then the
+ * leapfrog of its gauge field.  With use_graph != 0 the step after the
+ * calibration is captured once as one CUDA graph (one child graph per
+ * member, members independent) and every later step is one graph launch.
+ * stats aggregate over members (max residual, sum of matvecs).             */
+typedef struct nrq_ensemble nrq_ensemble;
+int nrq_ensemble_create(int nmembers, nrq_cn_batch *const *batches, nrq_gauge *const *gauges,
+                        nrq_ensemble **ens);
+int nrq_ensemble_destroy(nrq_ensemble *ens);
+int nrq_ensemble_step(nrq_ensemble *ens, const double c[8], double stepwidth, int use_graph,
+                      nrq_cn_stats *stats);
 
 /* ---- energy without any device allocation ---------------------------- */
 /* No counterpart in the reference.  This is for callers that cannot call

@@ -48,6 +48,7 @@ _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _pp = ctypes.POINTER(ctypes.c_void_p)
+_ip = ctypes.POINTER(ctypes.c_int)
 
 # name -> (restype, argtypes); every entry point of include/nrqcd_b200.h
 SIGNATURES = {
@@ -84,6 +85,15 @@ SIGNATURES = {
     "nrq_heavy_update_cn": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,
                                            ctypes.POINTER(CnStats)]),
     "nrq_cn_apply": (ctypes.c_int, [_vp, _vp, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int, _vp, _vp]),
+    "nrq_cn_batch_create": (ctypes.c_int, [_vp, ctypes.c_int, _pp, _dp, ctypes.c_double, _pp]),
+    "nrq_cn_batch_destroy": (ctypes.c_int, [_vp]),
+    "nrq_cn_batch_update": (ctypes.c_int, [_vp, _vp, _dp, ctypes.c_double, ctypes.c_int,
+                                           ctypes.POINTER(CnStats)]),
+    "nrq_cn_batch_residuals": (ctypes.c_int, [_vp, _dp]),
+    "nrq_cn_batch_info": (ctypes.c_int, [_vp, _ip, _ip, _dp, _ip, _ip]),
+    "nrq_ensemble_create": (ctypes.c_int, [ctypes.c_int, _pp, _pp, _pp]),
+    "nrq_ensemble_destroy": (ctypes.c_int, [_vp]),
+    "nrq_ensemble_step": (ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CnStats)]),
     "nrq_gauge_energy_noalloc": (ctypes.c_int, [_i64p, _dp, _vp, _vp, _vp, _vp]),
 }
 

@@ -1,0 +1,123 @@
+"""Batching form of the Crank-Nicolson step: many heavy fields in one gauge
+field per launch (``CNBatch``), and ensembles of independent members of
+different lattice sizes stepped by one CUDA graph launch (``Ensemble``).
+
+The reference advances one ``NRQCDField`` per ``Update`` call
+(src/nrqcd.f90:1053), field after field where the driver evolves several
+(src/main.f90:983-985).  A ``CNBatch`` gives every field the result of
+``NRQCDField.Update`` with the precision form (form 1) at the same
+tolerance; an ``Ensemble`` step is the driver's coupled step
+(src/main.f90:346-348: heavy fields, then the leapfrog) for every member.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi, lattice
+from .gaugeconfiguration_su3 import GaugeConfiguration
+from .nrqcd import NRQCDField
+
+
+class CNBatch:
+    def __init__(self, fields, masses, kspTol: float, lat=None):
+        ctx, _, self._open = lattice._resolve(lat)
+        self._ctx = ctx
+        self.fields = list(fields)
+        masses = np.ascontiguousarray(masses, dtype=np.float64).reshape(len(self.fields))
+        arr = (ctypes.c_void_p * len(self.fields))(*[f.handle.value for f in self.fields])
+        self._h = ctypes.c_void_p()
+        rc = _capi.load().nrq_cn_batch_create(ctx, len(self.fields), ctypes.cast(arr, _capi._pp),
+                                              _capi.dptr(masses), float(kspTol), ctypes.byref(self._h))
+        _capi.check(rc, ctx, "nrq_cn_batch_create")
+        self.masses = masses.copy()
+        self.last_stats = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def Destructor(self):
+        if self._h:
+            _capi.load().nrq_cn_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            if self._open():
+                self.Destructor()
+        except Exception:
+            pass
+
+    def Update(self, GaugeConf: GaugeConfiguration, WilsonCoeffs, StepWidth: float = 1.0, use_graph: bool = True,
+               raise_on_nonconvergence: bool = True) -> dict:
+        """One CN step of every field (each with its own mass)."""
+        st = _capi.CnStats()
+        c = _capi.coeffs(WilsonCoeffs)
+        rc = _capi.load().nrq_cn_batch_update(self._h, GaugeConf.handle, _capi.dptr(c), float(StepWidth),
+                                              int(bool(use_graph)), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if rc == _capi.NRQ_ERR_NOT_CONVERGED and not raise_on_nonconvergence:
+            return self.last_stats
+        _capi.check(rc, self._ctx, "nrq_cn_batch_update")
+        return self.last_stats
+
+    def residuals(self) -> np.ndarray:
+        out = np.zeros(len(self.fields))
+        _capi.check(_capi.load().nrq_cn_batch_residuals(self._h, _capi.dptr(out)), self._ctx, "residuals")
+        return out
+
+    def info(self) -> dict:
+        nf, order, npass = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = np.zeros(4)
+        steps = (ctypes.c_int * 16)()
+        _capi.check(_capi.load().nrq_cn_batch_info(self._h, ctypes.byref(nf), ctypes.byref(order), _capi.dptr(ms),
+                                                   ctypes.byref(npass), steps), self._ctx, "info")
+        return {"fields_per_tile": nf.value, "block_order": order.value,
+                "candidate_ms": {"tile1_order0": ms[0], "tile1_order1": ms[1], "tile2_order0": ms[2],
+                                 "tile2_order1": ms[3]},
+                "schedule": [int(steps[k]) for k in range(npass.value)]}
+
+
+class Ensemble:
+    """Members (batch, gauge) stepped together; with use_graph every step
+    after the calibration is one CUDA graph launch."""
+
+    def __init__(self, batches, gauges):
+        self.batches = list(batches)
+        self.gauges = list(gauges)
+        n = len(self.batches)
+        bh = (ctypes.c_void_p * n)(*[b.handle.value for b in self.batches])
+        gh = (ctypes.c_void_p * n)(*[g.handle.value for g in self.gauges])
+        self._h = ctypes.c_void_p()
+        rc = _capi.load().nrq_ensemble_create(n, ctypes.cast(bh, _capi._pp), ctypes.cast(gh, _capi._pp),
+                                              ctypes.byref(self._h))
+        _capi.check(rc, None, "nrq_ensemble_create")
+        self.last_stats = None
+
+    def Destructor(self):
+        if self._h:
+            _capi.load().nrq_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.Destructor()
+        except Exception:
+            pass
+
+    def Step(self, WilsonCoeffs, StepWidth: float, use_graph: bool = True,
+             raise_on_nonconvergence: bool = True) -> dict:
+        st = _capi.CnStats()
+        c = _capi.coeffs(WilsonCoeffs)
+        rc = _capi.load().nrq_ensemble_step(self._h, _capi.dptr(c), float(StepWidth), int(bool(use_graph)),
+                                            ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if rc == _capi.NRQ_ERR_NOT_CONVERGED and not raise_on_nonconvergence:
+            return self.last_stats
+        _capi.check(rc, self.batches[0]._ctx, "nrq_ensemble_step")
+        return self.last_stats
+
+
+__all__ = ["CNBatch", "Ensemble", "NRQCDField", "GaugeConfiguration"]

@@ -15,6 +15,9 @@
 #include "nrq_kernels.cuh"
 
 using nrq::cplx;
+using nrqh::check_launch;
+using nrqh::make_coef;
+using nrqh::set_device;
 
 namespace {
 
@@ -114,6 +117,43 @@ int ensure_red(nrq_ctx *ctx, int64_t doubles) {
   return NRQ_OK;
 }
 
+// final reduction of nq values over nb partial blocks into h_res[0..nq)
+int reduce_to_host(nrq_ctx *ctx, int64_t nb, int nq, unsigned maxmask) {
+  nrq::k_reduce_final<<<1, 256, 0, ctx->stream>>>(ctx->d_red, nb, nq, maxmask, ctx->d_res);
+  int rc = check_launch(ctx, "k_reduce_final");
+  if (rc) return rc;
+  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(double) * nq, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return NRQ_OK;
+}
+
+}  // namespace
+
+namespace nrqh {
+// Chebyshev parameters for A^H = 1 + i tau H with spec(H) in [lo, hi]:
+// theta (centre), delta (half-length), sigma = theta/delta
+ChebSeg cheb_segment(double tau, double lo, double hi) {
+  ChebSeg s;
+  s.theta = std::complex<double>(1.0, tau * 0.5 * (lo + hi));
+  double half = std::fabs(tau) * 0.5 * (hi - lo);
+  if (half < 1e-14) half = 1e-14;
+  s.delta = std::complex<double>(0.0, half);
+  s.sigma = s.theta / s.delta;
+  return s;
+}
+// |T_m(sigma)| via the recurrence T_{k+1} = 2 sigma T_k - T_{k-1}
+double cheb_gain(std::complex<double> sigma, int m) {
+  std::complex<double> t0(1.0, 0.0), t1 = sigma;
+  if (m == 0) return 1.0;
+  for (int k = 1; k < m; ++k) {
+    std::complex<double> t2 = 2.0 * sigma * t1 - t0;
+    t0 = t1;
+    t1 = t2;
+  }
+  return std::abs(t1);
+}
+
 int set_device(nrq_ctx *ctx) {
   NRQ_CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   return NRQ_OK;
@@ -125,17 +165,6 @@ int check_launch(nrq_ctx *ctx, const char *what) {
     ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
     return NRQ_ERR_CUDA;
   }
-  return NRQ_OK;
-}
-
-// final reduction of nq values over nb partial blocks into h_res[0..nq)
-int reduce_to_host(nrq_ctx *ctx, int64_t nb, int nq, unsigned maxmask) {
-  nrq::k_reduce_final<<<1, 256, 0, ctx->stream>>>(ctx->d_red, nb, nq, maxmask, ctx->d_res);
-  int rc = check_launch(ctx, "k_reduce_final");
-  if (rc) return rc;
-  NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_res, ctx->d_res, sizeof(double) * nq, cudaMemcpyDeviceToHost,
-                                    ctx->stream));
-  NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   return NRQ_OK;
 }
 
@@ -170,7 +199,7 @@ nrq::CnCoef make_coef(const nrq_ctx *ctx, double mass, const double c_[8], doubl
   return C;
 }
 
-}  // namespace
+}  // namespace nrqh
 
 // ====================================================================== context
 extern "C" const char *nrq_status_string(int s) {
@@ -716,7 +745,7 @@ namespace {
 // algorithmic bytes of one 12-column stencil launch: vector streams of
 // 12 x 6 complex per site plus the gauge inputs U and E read once
 double mv_bytes(const nrq_ctx *ctx, int mode) {
-  const int streams[5] = {2, 3, 5, 3, 3};
+  const int streams[6] = {2, 3, 5, 3, 3, 3};  // PLAIN, RHS, RES, V, T, RESC
   return (double)ctx->lat.V * (1152.0 * streams[mode] + 432.0 + 192.0);
 }
 void mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq::MvArgs &a) {
@@ -760,33 +789,10 @@ extern "C" int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const d
 }
 
 
+using nrqh::ChebSeg;
+using nrqh::cheb_gain;
+using nrqh::cheb_segment;
 namespace {
-// Chebyshev parameters for A^H = 1 + i tau H with spec(H) in [lo, hi]:
-// theta (centre), delta (half-length), sigma = theta/delta
-struct ChebSeg {
-  std::complex<double> theta, delta, sigma;
-};
-ChebSeg cheb_segment(double tau, double lo, double hi) {
-  ChebSeg s;
-  s.theta = std::complex<double>(1.0, tau * 0.5 * (lo + hi));
-  double half = std::fabs(tau) * 0.5 * (hi - lo);
-  if (half < 1e-14) half = 1e-14;
-  s.delta = std::complex<double>(0.0, half);
-  s.sigma = s.theta / s.delta;
-  return s;
-}
-// |T_m(sigma)| via the recurrence T_{k+1} = 2 sigma T_k - T_{k-1}
-double cheb_gain(std::complex<double> sigma, int m) {
-  std::complex<double> t0(1.0, 0.0), t1 = sigma;
-  if (m == 0) return 1.0;
-  for (int k = 1; k < m; ++k) {
-    std::complex<double> t2 = 2.0 * sigma * t1 - t0;
-    t0 = t1;
-    t1 = t2;
-  }
-  return std::abs(t1);
-}
-
 // Precision form: FP64 refinement around FP32 Chebyshev inner solves.
 int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass, const double c[8], double dt,
                         nrq_cn_stats *stats) {

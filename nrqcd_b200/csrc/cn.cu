@@ -467,6 +467,70 @@ void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, doub
   k_cn_finalize<<<CN_COLS, 256, 0, st>>>(stage, nblocks, partials, scal, tol);
 }
 
+// ------------------------------------------------------------ batched scalars
+// Chebyshev coefficients of every field of a batch from the spectral
+// enclosure of its mass (the device-side counterpart of the host recurrence
+// of the single-field precision form): theta = 1 + i tau (lo+hi)/2,
+// delta = i |tau| (hi-lo)/2, sigma = theta/delta, rho_0 = 1/sigma,
+// rho_{k+1} = 1/(2 sigma - rho_k), c1 = rho_{k+1} rho_k, c2 = 2 rho_{k+1}/delta.
+__global__ void k_batch_coef(BatchField *__restrict__ tab, int nfields, int *__restrict__ flags) {
+  const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (fi >= nfields) return;
+  BatchField &f = tab[fi];
+  int bad = 0;
+  for (int sp = 0; sp < 2; ++sp) {
+    double lo = f.bounds[2 * sp], hi = f.bounds[2 * sp + 1];
+    if (!(isfinite(lo) && isfinite(hi) && hi >= lo)) {
+      bad = 1;
+      lo = hi = 0.0;
+    }
+    const cplx one = {1.0, 0.0};
+    const cplx theta = {1.0, f.tau * 0.5 * (lo + hi)};
+    const cplx delta = {0.0, fmax(fabs(f.tau) * 0.5 * (hi - lo), 1e-14)};
+    const cplx sigma = cdiv(theta, delta);
+    f.inv_theta[sp] = cdiv(one, theta);
+    cplx rho = cdiv(one, sigma);
+    for (int k = 0; k < BATCH_MAX_CHEB; ++k) {
+      const cplx rn = cdiv(one, 2.0 * sigma - rho);
+      f.cheb[k].c1[sp] = rn * rho;
+      f.cheb[k].c2[sp] = cdiv(2.0 * rn, delta);
+      rho = rn;
+    }
+  }
+  flags[fi] = bad;
+}
+void launch_batch_coef(BatchField *tab, int nfields, int *flags, cudaStream_t st) {
+  k_batch_coef<<<(unsigned)((nfields + 63) / 64), 64, 0, st>>>(tab, nfields, flags);
+}
+
+// (r.r, b.b) of every column of every field from the residual stencil's
+// partial rows; sets the convergence and non-finite flags of each column.
+__global__ void k_batch_finalize(const BatchField *__restrict__ tab, int64_t nrows, double tol) {
+  const int col = blockIdx.x;
+  const BatchField &f = tab[blockIdx.y];
+  __shared__ double sh[2][256];
+  double acc[2] = {0.0, 0.0};
+  for (int64_t b = threadIdx.x; b < nrows; b += blockDim.x)
+    for (int k = 0; k < 2; ++k) acc[k] += f.partials[(b * CN_COLS + col) * 2 + k];
+  for (int k = 0; k < 2; ++k) sh[k][threadIdx.x] = acc[k];
+  __syncthreads();
+  for (int wd = blockDim.x / 2; wd > 0; wd >>= 1) {
+    if (threadIdx.x < wd)
+      for (int k = 0; k < 2; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + wd];
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  double *sc = f.scal + col * SC_STRIDE;
+  const double q0 = sh[0][0], q1 = sh[1][0];
+  sc[SC_RR] = q0;
+  sc[SC_BB] = q1;
+  sc[SC_CONV] = (q0 <= tol * tol * q1 || q1 == 0.0) ? 1.0 : 0.0;
+  sc[SC_NONFIN] = (isfinite(q0) && isfinite(q1)) ? 0.0 : 1.0;
+}
+void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, double tol, cudaStream_t st) {
+  k_batch_finalize<<<dim3(CN_COLS, (unsigned)nfields), 256, 0, st>>>(tab, nrows, tol);
+}
+
 // ------------------------------------------------------------ propagator I/O, norms, correlators
 // Fortran prop(6,6,V): (site*6 + col)*6 + row ; f holds quark then antiquark (2*V*36)
 __global__ void k_prop_f2soa(const double2 *__restrict__ f, double2 *__restrict__ P, int64_t V) {

@@ -19,6 +19,7 @@
 // Stencil layout as cn_mv.cu (32 sites x 6 warps per block; a thread owns
 // the rows (c, s) of the 6 columns of its species) in FP32 on FP32 copies of
 // the per-step gauge-derived matrices.
+#include <algorithm>
 #include <type_traits>
 
 #include "nrq_kernels.cuh"
@@ -209,27 +210,30 @@ __global__ void k_cn_bounds_final(const double *__restrict__ partials, int64_t n
 // ------------------------------------------------------------------ FP32 Chebyshev step
 // t = A^H d (FP32, all 12 columns), then per site and row:
 //   r <- r - t ; e <- e + d ; d' = c1 d + c2 r      (c1, c2 per species)
-template <bool FIRST>
-__global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2 *__restrict__ U,
-                                                   const float2 *__restrict__ Dsum, const float *__restrict__ Bsum,
-                                                   const float2 *__restrict__ DE, const float2 *__restrict__ D,
-                                                   float2 *__restrict__ Dn, float2 *__restrict__ R,
-                                                   float2 *__restrict__ Ev, ChebCoef K) {
+// One 32-site tile of one Chebyshev step for NF fields that share the same
+// operator (same mass): the gauge-derived weights are loaded and assembled
+// once per neighbour and applied to every field of the tile.
+template <bool FIRST, int NF>
+__device__ __forceinline__ void cheb32_tile(const Lat &L, const CnCoef &C, const float2 *__restrict__ U,
+                                            const float2 *__restrict__ Dsum, const float *__restrict__ Bsum,
+                                            const float2 *__restrict__ DE, const float2 *const (&D)[NF],
+                                            float2 *const (&Dn)[NF], float2 *const (&R)[NF],
+                                            float2 *const (&Ev)[NF], const ChebCoef &K, int64_t block) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int sp = warp / 3, c = warp % 3;
   const int64_t V = L.V;
-  const int64_t x0 = (int64_t)blockIdx.x * 32 + lane;
+  const int64_t x0 = block * 32 + lane;
   const bool active = x0 < V;
   const int64_t x = active ? x0 : 0;
   const int64_t pb = (int64_t)(sp * 36) * V;
-  auto load_w = [&](int64_t y, int col, cf w[6]) {
-    const float2 *p = D + pb + (int64_t)(col * 6) * V + y;
+  auto load_w = [&](const float2 *Df, int64_t y, int col, cf w[6]) {
+    const float2 *p = Df + pb + (int64_t)(col * 6) * V + y;
 #pragma unroll
     for (int r = 0; r < 6; ++r) w[r] = ldf(p + (int64_t)r * V);
   };
   const cf ak = tof(C.kin[sp]), am = tof(C.mag[sp]), ad = tof(C.dar[sp]), aso = tof(C.so[sp]);
-  cf acc[6][2];
+  cf acc[NF][6][2];
   {
     cf Cd[3];
 #pragma unroll
@@ -240,17 +244,19 @@ __global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2
     }
     Cd[c] = Cd[c] + (float)C.dkin * ak + cf{1.f, 0.f};
 #pragma unroll
-    for (int col = 0; col < 6; ++col) {
-      cf w[6];
-      load_w(x, col, w);
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        cf a_ = Cd[0] * w[s];
-        cmacf(a_, Cd[1], w[2 + s]);
-        cmacf(a_, Cd[2], w[4 + s]);
-        acc[col][s] = a_;
+      for (int col = 0; col < 6; ++col) {
+        cf w[6];
+        load_w(D[f], x, col, w);
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          cf a_ = Cd[0] * w[s];
+          cmacf(a_, Cd[1], w[2 + s]);
+          cmacf(a_, Cd[2], w[4 + s]);
+          acc[f][col][s] = a_;
+        }
       }
-    }
   }
   const cf cs0 = timesi(aso), cs1 = -timesi(aso);
   auto neighbour = [&](auto Ic, auto DIRc) {
@@ -285,17 +291,19 @@ __global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2
         }
     }
 #pragma unroll
-    for (int col = 0; col < 6; ++col) {
-      cf w[6];
-      load_w(y, col, w);
+    for (int f = 0; f < NF; ++f)
 #pragma unroll
-      for (int s = 0; s < 2; ++s)
+      for (int col = 0; col < 6; ++col) {
+        cf w[6];
+        load_w(D[f], y, col, w);
 #pragma unroll
-        for (int cp = 0; cp < 3; ++cp) {
-          cmacf(acc[col][s], Wm[s][cp][0], w[2 * cp]);
-          cmacf(acc[col][s], Wm[s][cp][1], w[2 * cp + 1]);
-        }
-    }
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+          for (int cp = 0; cp < 3; ++cp) {
+            cmacf(acc[f][col][s], Wm[s][cp][0], w[2 * cp]);
+            cmacf(acc[f][col][s], Wm[s][cp][1], w[2 * cp + 1]);
+          }
+      }
   };
   using I0 = std::integral_constant<int, 0>;
   using I1 = std::integral_constant<int, 1>;
@@ -310,16 +318,105 @@ __global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2
   if (!active) return;
   const cf c1 = tof(K.c1[sp]), c2 = tof(K.c2[sp]);
 #pragma unroll
-  for (int col = 0; col < 6; ++col)
+  for (int f = 0; f < NF; ++f)
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const int64_t o = pb + (int64_t)(col * 6 + 2 * c + s) * V + x;
-      const cf d = ldf(D + o);
-      const cf r = ldf(R + o) - acc[col][s];
-      stf(R + o, r);
-      stf(Ev + o, FIRST ? d : ldf(Ev + o) + d);
-      stf(Dn + o, c1 * d + c2 * r);
-    }
+    for (int col = 0; col < 6; ++col)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int64_t o = pb + (int64_t)(col * 6 + 2 * c + s) * V + x;
+        const cf d = ldf(D[f] + o);
+        const cf r = ldf(R[f] + o) - acc[f][col][s];
+        stf(R[f] + o, r);
+        stf(Ev[f] + o, FIRST ? d : ldf(Ev[f] + o) + d);
+        stf(Dn[f] + o, c1 * d + c2 * r);
+      }
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2 *__restrict__ U,
+                                                   const float2 *__restrict__ Dsum, const float *__restrict__ Bsum,
+                                                   const float2 *__restrict__ DE, const float2 *__restrict__ D,
+                                                   float2 *__restrict__ Dn, float2 *__restrict__ R,
+                                                   float2 *__restrict__ Ev, ChebCoef K) {
+  const float2 *const d[1] = {D};
+  float2 *const dn[1] = {Dn};
+  float2 *const r[1] = {R};
+  float2 *const e[1] = {Ev};
+  cheb32_tile<FIRST, 1>(L, C, U, Dsum, Bsum, DE, d, dn, r, e, K, blockIdx.x);
+}
+
+// ------------------------------------------------------------------ batched
+// Step `step` of the inner Chebyshev solve for every field of a batch in one
+// launch.  The table holds the fields grouped by mass in tiles of NF fields;
+// the flattened block index is split into (tile, site block) with the tile
+// fastest (ORDER 0: consecutive blocks share the gauge-derived tiles in L2)
+// or the site block fastest (ORDER 1).
+// one resident block per SM for two-field tiles (their accumulators double)
+template <bool FIRST, int NF, int ORDER>
+__global__ void __launch_bounds__(192, NF == 1 ? 2 : 1) k_batch_cheb32(Lat L, const float2 *__restrict__ U,
+                                                         const float2 *__restrict__ Dsum,
+                                                         const float *__restrict__ Bsum,
+                                                         const float2 *__restrict__ DE,
+                                                         const BatchField *__restrict__ tab, int ntiles,
+                                                         int64_t nsb, int step) {
+  const int64_t bid = blockIdx.x;
+  const int tile = ORDER == 0 ? (int)(bid % ntiles) : (int)(bid / nsb);
+  const int64_t sb = ORDER == 0 ? bid / ntiles : bid % nsb;
+  const float2 *d[NF];
+  float2 *dn[NF], *r[NF], *e[NF];
+#pragma unroll
+  for (int j = 0; j < NF; ++j) {
+    const BatchField &f = tab[tile * NF + j];
+    d[j] = (step & 1) ? f.dB : f.dA;
+    dn[j] = (step & 1) ? f.dA : f.dB;
+    r[j] = f.r32;
+    e[j] = f.e32;
+  }
+  const BatchField &f0 = tab[tile * NF];
+  cheb32_tile<FIRST, NF>(L, f0.CH, U, Dsum, Bsum, DE, d, dn, r, e, f0.cheb[step], sb);
+}
+
+// x += e for every field (blockIdx.y = field)
+__global__ void k_batch_add_e(int64_t n, const BatchField *__restrict__ tab) {
+  const BatchField &f = tab[blockIdx.y];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 e = f.e32[i];
+    const double2 x = f.x[i];
+    f.x[i] = make_double2(x.x + (double)e.x, x.y + (double)e.y);
+  }
+}
+
+template <bool FIRST, int NF>
+static void batch_cheb_nf(int order, dim3 grid, Lat L, const float2 *U, const float2 *Dsum, const float *Bsum,
+                          const float2 *DE, const BatchField *tab, int ntiles, int64_t nsb, int step,
+                          cudaStream_t st) {
+  if (order == 0)
+    k_batch_cheb32<FIRST, NF, 0><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step);
+  else
+    k_batch_cheb32<FIRST, NF, 1><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step);
+}
+
+int launch_batch_cheb(int step, int nf_tile, int order, Lat L, const float2 *U, const float2 *Dsum,
+                      const float *Bsum, const float2 *DE, const BatchField *tab, int nfields, cudaStream_t st) {
+  if (nf_tile <= 0 || nfields % nf_tile != 0 || step < 0 || step >= BATCH_MAX_CHEB) return 1;
+  const int ntiles = nfields / nf_tile;
+  const int64_t nsb = (L.V + 31) / 32;
+  const dim3 grid((unsigned)(nsb * ntiles));
+  const bool first = step == 0;
+  if (nf_tile == 1) {
+    if (first) batch_cheb_nf<true, 1>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+    else batch_cheb_nf<false, 1>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+  } else if (nf_tile == 2) {
+    if (first) batch_cheb_nf<true, 2>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+    else batch_cheb_nf<false, 2>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+  } else {
+    return 1;
+  }
+  return 0;
+}
+void launch_batch_add_e(int64_t n, const BatchField *tab, int nfields, cudaStream_t st) {
+  const dim3 grid((unsigned)std::min<int64_t>((n + 255) / 256, 2048), (unsigned)nfields);
+  k_batch_add_e<<<grid, 256, 0, st>>>(n, tab);
 }
 
 // x += e (FP64 += FP32), 72 planes

@@ -51,14 +51,15 @@ __device__ __forceinline__ cplx scal_col(const double *sc, int col12, int slot) 
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, const double2 *__restrict__ U,
-                                                   const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
-                                                   const double2 *__restrict__ DE, MvArgs A) {
+__device__ __forceinline__ void cn_mv2_body(const Lat &L, const CnCoef &C, const double2 *__restrict__ U,
+                                            const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
+                                            const double2 *__restrict__ DE, const MvArgs &A, int64_t block,
+                                            int64_t partial_row) {
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;  // 0..5
   const int sp = warp / 3, c = warp % 3;
   const int64_t V = L.V;
-  const int64_t x0 = (int64_t)blockIdx.x * 32 + lane;
+  const int64_t x0 = block * 32 + lane;
   const bool active = x0 < V;
   const int64_t x = active ? x0 : 0;
   const int64_t pb = (int64_t)(sp * 36) * V;
@@ -227,9 +228,70 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, co
       const int col12 = threadIdx.x / NQ, k = threadIdx.x % NQ;
       const int spp = col12 / 6, col = col12 % 6;
       const double v = sh[spp * 3 + 0][col][k] + sh[spp * 3 + 1][col][k] + sh[spp * 3 + 2][col][k];
-      A.partials[((int64_t)blockIdx.x * CN_COLS + col12) * NQ + k] = v;
+      A.partials[(partial_row * CN_COLS + col12) * NQ + k] = v;
     }
   }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(192, NRQ_MV_MINB) k_cn_mv2(Lat L, CnCoef C, const double2 *__restrict__ U,
+                                                   const double2 *__restrict__ Dsum, const double *__restrict__ Bsum,
+                                                   const double2 *__restrict__ DE, MvArgs A) {
+  cn_mv2_body<MODE>(L, C, U, Dsum, Bsum, DE, A, blockIdx.x, blockIdx.x);
+}
+
+// ------------------------------------------------------------------ batched
+// One launch over every field of a batch.  The flattened block index splits
+// into (field, site block), field fastest (ORDER 0) or site block fastest
+// (ORDER 1); pointers and mass-dependent coefficients come from the device
+// table.  MV_RHS: b = A psi, x = 2b - psi.  MV_RESC: r32 = f32(b - A^H x),
+// d32 = r32 / theta, with the per-column (r.r, b.b) partials of the field.
+template <int MODE, int ORDER>
+__global__ void __launch_bounds__(192, NRQ_MV_MINB) k_batch_mv2(Lat L, const double2 *__restrict__ U,
+                                                      const double2 *__restrict__ Dsum,
+                                                      const double *__restrict__ Bsum,
+                                                      const double2 *__restrict__ DE,
+                                                      const BatchField *__restrict__ tab, int nfields,
+                                                      int64_t nsb) {
+  const int64_t bid = blockIdx.x;
+  const int fi = ORDER == 0 ? (int)(bid % nfields) : (int)(bid / nsb);
+  const int64_t sb = ORDER == 0 ? bid / nfields : bid % nsb;
+  const BatchField &f = tab[fi];
+  MvArgs a{};
+  if (MODE == MV_RHS) {
+    a.in = f.psi;
+    a.out = f.b;
+    a.out2 = f.x;
+    cn_mv2_body<MV_RHS>(L, f.CA, U, Dsum, Bsum, DE, a, sb, sb);
+  } else {
+    a.in = f.x;
+    a.bvec = f.b;
+    a.r32 = f.r32;
+    a.d32 = f.dA;
+    a.partials = f.partials;
+    a.inv_theta[0] = f.inv_theta[0];
+    a.inv_theta[1] = f.inv_theta[1];
+    cn_mv2_body<MV_RESC>(L, f.CH, U, Dsum, Bsum, DE, a, sb, sb);
+  }
+}
+
+template <int MODE>
+static void batch_mv_mode(int order, dim3 grid, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
+                          const double2 *DE, const BatchField *tab, int nfields, int64_t nsb, cudaStream_t st) {
+  if (order == 0)
+    k_batch_mv2<MODE, 0><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, nfields, nsb);
+  else
+    k_batch_mv2<MODE, 1><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, nfields, nsb);
+}
+
+void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
+                     const double2 *DE, const BatchField *tab, int nfields, cudaStream_t st) {
+  const int64_t nsb = (L.V + 31) / 32;
+  const dim3 grid((unsigned)(nsb * nfields));
+  if (mode == MV_RHS)
+    batch_mv_mode<MV_RHS>(order, grid, L, U, Dsum, Bsum, DE, tab, nfields, nsb, st);
+  else
+    batch_mv_mode<MV_RESC>(order, grid, L, U, Dsum, Bsum, DE, tab, nfields, nsb, st);
 }
 
 void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,

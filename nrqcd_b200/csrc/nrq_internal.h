@@ -3,10 +3,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <complex>
 #include <string>
 #include <vector>
 
-#include "nrq_common.cuh"
+#include "nrq_kernels.cuh"
 
 struct nrq_ctx {
   int device = 0;
@@ -127,3 +128,19 @@ struct nrq_cn {
       return NRQ_ERR_CUDA;                                                   \
     }                                                                        \
   } while (0)
+
+// host helpers shared by the C-ABI translation units (capi.cu, batch.cu)
+namespace nrqh {
+int set_device(nrq_ctx *ctx);
+// NRQ_ERR_CUDA with ctx->last_error set when the last launch failed
+int check_launch(nrq_ctx *ctx, const char *what);
+// per-species, per-term coefficients of A (herm = false) or A^H (herm = true)
+nrq::CnCoef make_coef(const nrq_ctx *ctx, double mass, const double c[8], double dt, bool herm);
+// Chebyshev segment of A^H = 1 + i tau H for spec(H) in [lo, hi]
+struct ChebSeg {
+  std::complex<double> theta, delta, sigma;
+};
+ChebSeg cheb_segment(double tau, double lo, double hi);
+// |T_m(sigma)|: error reduction guaranteed by m Chebyshev steps
+double cheb_gain(std::complex<double> sigma, int m);
+}  // namespace nrqh

@@ -89,6 +89,30 @@ int launch_cn_mv3(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
 // finalize stages: 0 = after RES (rr, bb), 1 = alpha (rh.v), 2 = omega (t.s, t.t), 3 = beta (rh.r, r.r)
 void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
                         cudaStream_t st);
+// one field of a batched Crank-Nicolson step (device table entry)
+constexpr int BATCH_MAX_CHEB = 32;
+struct BatchField {
+  CnCoef CA, CH;                 // operator A and A^H coefficients at this field's mass
+  double2 *psi, *b, *x;          // FP64 propagator, right-hand side, iterate (72 planes)
+  float2 *r32, *dA, *dB, *e32;   // FP32 Chebyshev vectors (72 planes)
+  double *partials;              // residual (r.r, b.b) partials of this field
+  double *scal;                  // per-column scalars of this field (CN_COLS x SC_STRIDE)
+  const double *bounds;          // spectral enclosure of this field's mass (lo0, hi0, lo1, hi1)
+  double tau;                    // dt a0 / 2 (signed)
+  cplx inv_theta[2];             // 1/theta per species (written on the device)
+  ChebCoef cheb[BATCH_MAX_CHEB]; // Chebyshev steps (written on the device)
+};
+void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
+                     const double2 *DE, const BatchField *tab, int nfields, cudaStream_t st);
+// returns nonzero for an unsupported tile (nf_tile must divide nfields)
+int launch_batch_cheb(int step, int nf_tile, int order, Lat L, const float2 *U, const float2 *Dsum,
+                      const float *Bsum, const float2 *DE, const BatchField *tab, int nfields, cudaStream_t st);
+void launch_batch_add_e(int64_t n, const BatchField *tab, int nfields, cudaStream_t st);
+// Chebyshev coefficients of every field from its mass's bounds; sets
+// flags[f] = 1 for non-finite bounds
+void launch_batch_coef(BatchField *tab, int nfields, int *flags, cudaStream_t st);
+// stage-0 reduction of every field's residual partials (nrows rows per field)
+void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, double tol, cudaStream_t st);
 void launch_cn_to_f32(int64_t V, const double2 *U, const double2 *DE, const double2 *D, const double *B, float2 *U32,
                       float2 *DE32, float2 *D32, float *B32, cudaStream_t st);
 void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, const double2 *Dsum, const double *Bsum,

@@ -19,13 +19,13 @@ modulename = "gaugeconfiguration_su3"
 
 
 class GaugeConfiguration:
-    def __init__(self):
-        self._ctx = lattice.context()
+    def __init__(self, lat=None):
+        """lat: a lattice.Lattice (ensemble member); default the module context."""
+        self._ctx, self.V, self._open = lattice._resolve(lat)
         self._h = ctypes.c_void_p()
         lib = _capi.load()
         _capi.check(lib.nrq_gauge_create(self._ctx, ctypes.byref(self._h)), self._ctx,
                     f"Error in Allocate of {modulename}")
-        self.V = lattice.GetLatticeSize()
 
     # --------------------------------------------------------------- lifetime
     def Deallocate(self):
@@ -35,7 +35,7 @@ class GaugeConfiguration:
 
     def __del__(self):
         try:
-            if lattice.IsModuleInitialised():
+            if self._open():
                 self.Deallocate()
         except Exception:
             pass

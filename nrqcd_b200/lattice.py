@@ -72,3 +72,42 @@ def GetVolume() -> float:
 
 def synchronize():
     _capi.check(_capi.load().nrq_synchronize(context()), context(), "synchronize")
+
+
+class Lattice:
+    """A standalone lattice context beside the module's own, for ensembles
+    whose members have different extents (nrq_init per member size).  Pass
+    it as ``lat=`` to GaugeConfiguration and NRQCDField."""
+
+    def __init__(self, LatticeExtensions, LatticeSpacings, device: int = 0):
+        ext = np.ascontiguousarray(LatticeExtensions, dtype=np.int64).reshape(3)
+        sp = np.ascontiguousarray(LatticeSpacings, dtype=np.float64).reshape(4)
+        h = ctypes.c_void_p()
+        rc = _capi.load().nrq_init(ext.ctypes.data_as(_capi._i64p), _capi.dptr(sp), int(device), ctypes.byref(h))
+        _capi.check(rc, None, f"Error in init of {modulename}")
+        self.ctx = h
+        self.extents = ext.copy()
+        self.spacings = sp.copy()
+        self.V = int(np.prod(ext))
+
+    @property
+    def is_open(self) -> bool:
+        return bool(self.ctx)
+
+    def close(self):
+        if self.ctx:
+            _capi.load().nrq_finalize(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _resolve(lat):
+    """(ctx, V, is_open) of a standalone Lattice, or of the module context."""
+    if lat is None:
+        return context(), GetLatticeSize(), IsModuleInitialised
+    return lat.ctx, lat.V, lambda: lat.is_open

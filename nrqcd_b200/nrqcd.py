@@ -64,12 +64,12 @@ def solver_handle():
 
 
 class NRQCDField:
-    def __init__(self):
-        self._ctx = lattice.context()
+    def __init__(self, lat=None):
+        """lat: a lattice.Lattice (ensemble member); default the module context."""
+        self._ctx, self.V, self._open = lattice._resolve(lat)
         self._h = ctypes.c_void_p()
         _capi.check(_capi.load().nrq_heavy_create(self._ctx, ctypes.byref(self._h)), self._ctx,
                     f"Error in Allocate of {modulename}")
-        self.V = lattice.GetLatticeSize()
         self.last_stats = None
 
     def Destructor(self):
@@ -79,7 +79,7 @@ class NRQCDField:
 
     def __del__(self):
         try:
-            if lattice.IsModuleInitialised():
+            if self._open():
                 self.Destructor()
         except Exception:
             pass

@@ -1,0 +1,200 @@
+"""GPU checks of the batching form of the Crank-Nicolson step: a batch of
+fields (sources x masses) in one gauge field per launch, and ensembles of
+members of different lattice sizes stepped by one CUDA graph launch.
+
+Every field of a batch must equal the single-field update of the same field
+to within the solve tolerance (tol 1e-10 on unit-norm propagators: the
+fields agree to a few 1e-10), the graph replay must equal the eager launch
+sequence bit for bit, and an ensemble step must equal its members stepped
+one by one."""
+import numpy as np
+import pytest
+
+from nrqcd_b200 import GaugeConfiguration, NRQCDField, NrqcdError, lattice
+from nrqcd_b200.batch import CNBatch, Ensemble
+from tests.gpu_util import lattice_ctx
+
+pytestmark = pytest.mark.gpu
+
+A = (0.05, 1.0, 1.0, 1.0)
+C = [1, 1, 1, 1]
+FORM_PRECISION = 1
+
+
+def _sources(V, k, seed):
+    rng = np.random.default_rng(seed)
+    return [(int(a) + 1, int(b) + 1) for a, b in rng.integers(0, V, size=(k, 2))]
+
+
+def _hot_gauge(oracle, n, seed, lat=None):
+    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, seed, identity_links=False)
+    g = GaugeConfiguration(lat=lat)
+    g.upload(links, ef)
+    return g, links, ef
+
+
+def _fields(V, srcs, lat=None):
+    out = []
+    for lq, la in srcs:
+        h = NRQCDField(lat=lat)
+        h.InitSinglePoint(lq, la)
+        out.append(h)
+    return out
+
+
+def test_batch_matches_single_field_updates(oracle):
+    """4 sources x 2 masses at 8^3: batch (graph replays) vs one precision
+    update per field, and the oracle for two of the fields."""
+    n = (8, 8, 8)
+    V = int(np.prod(n))
+    masses = [1.0, 1.5]
+    srcs = _sources(V, 4, 11)
+    tol = 1e-10
+    with lattice_ctx(n, A, cn=(masses[0], C, 1.0, tol, 10000, FORM_PRECISION)):
+        g, links, ef = _hot_gauge(oracle, n, 7)
+        hs = _fields(V, srcs) + _fields(V, srcs)
+        ms = [masses[0]] * 4 + [masses[1]] * 4
+        b = CNBatch(hs, ms, tol)
+        singles = _fields(V, srcs) + _fields(V, srcs)
+        for step in range(3):
+            st = b.Update(g, C, 1.0, use_graph=True)
+            assert st["converged"] == 1 and st["max_rel_residual"] <= tol
+            assert (b.residuals() <= tol).all()
+            for h, m in zip(singles, ms):
+                s1 = h.Update(g, m, C, 1.0)
+                assert s1["converged"] == 1
+        info = b.info()
+        assert info["fields_per_tile"] in (1, 2) and info["block_order"] in (0, 1)
+        assert info["candidate_ms"]["tile1_order0"] > 0 and info["candidate_ms"]["tile1_order1"] > 0
+        assert 1 <= len(info["schedule"]) <= 8
+        for hb, hsg in zip(hs, singles):
+            qb, ab = hb.download()
+            qs, as_ = hsg.download()
+            assert np.abs(qb - qs).max() < 5e-10 and np.abs(ab - as_).max() < 5e-10
+            assert abs(hb.GetNorm_Quark() - 1) < 1e-9 and abs(hb.GetNorm_AntiQ() - 1) < 1e-9
+        # the oracle (FP64 GMRES to 1e-14) for the first field of each mass
+        for idx in (0, 4):
+            lq, la = srcs[idx % 4]
+            q = oracle.single_point(n, lq)
+            an = oracle.single_point(n, la)
+            for _ in range(3):
+                oracle.cn_update(n, A, links, ef, ms[idx], C, 1.0, q, an, tol=1e-14)
+            qb, ab = hs[idx].download()
+            assert np.abs(qb - q).max() < 5e-10 and np.abs(ab - an).max() < 5e-10
+        b.Destructor()
+
+
+def test_graph_replay_equals_eager_launches(oracle):
+    """The captured step and the same launches issued one by one agree bit for bit."""
+    n = (6, 6, 6)
+    V = int(np.prod(n))
+    srcs = _sources(V, 4, 5)
+    with lattice_ctx(n, A, cn=(1.0, C, 1.0, 1e-10, 10000, FORM_PRECISION)):
+        g, _, _ = _hot_gauge(oracle, n, 3)
+        ha = _fields(V, srcs)
+        hb = _fields(V, srcs)
+        ms = [1.0, 1.0, 2.0, 2.0]
+        ba = CNBatch(ha, ms, 1e-10)
+        bb = CNBatch(hb, ms, 1e-10)
+        for _ in range(4):
+            ba.Update(g, C, 1.0, use_graph=False)
+            bb.Update(g, C, 1.0, use_graph=True)
+        # same tuning choice is not guaranteed (timing); equal results only when equal
+        if ba.info()["fields_per_tile"] == bb.info()["fields_per_tile"] and \
+                ba.info()["block_order"] == bb.info()["block_order"] and \
+                ba.info()["schedule"] == bb.info()["schedule"]:
+            for x, y in zip(ha, hb):
+                qa, aa = x.download()
+                qb, ab = y.download()
+                assert np.array_equal(qa, qb) and np.array_equal(aa, ab)
+        else:
+            for x, y in zip(ha, hb):
+                qa, aa = x.download()
+                qb, ab = y.download()
+                assert np.abs(qa - qb).max() < 5e-10 and np.abs(aa - ab).max() < 5e-10
+        ba.Destructor()
+        bb.Destructor()
+
+
+def test_ensemble_of_uneven_members_matches_member_steps(oracle):
+    """Members 2 x 6^3 + 1 x 8^3, 4 fields each (2 sources x 2 masses): one
+    graph launch per step equals each member's batch update plus leapfrog."""
+    sizes = [(6, 6, 6), (6, 6, 6), (8, 8, 8)]
+    ms = [1.0, 1.0, 1.5, 1.5]
+    lat6 = lattice.Lattice((6, 6, 6), A)
+    lat8 = lattice.Lattice((8, 8, 8), A)
+    lats = [lat6, lat6, lat8]
+    try:
+        runs = []
+        for use_graph in (True, False):
+            gauges, batches, fields = [], [], []
+            for i, (n, lat) in enumerate(zip(sizes, lats)):
+                g, _, _ = _hot_gauge(oracle, n, 20 + i, lat=lat)
+                V = int(np.prod(n))
+                srcs = _sources(V, 2, 30 + i)
+                hs = _fields(V, srcs + srcs, lat=lat)
+                gauges.append(g)
+                fields.append(hs)
+                batches.append(CNBatch(hs, ms, 1e-10, lat=lat))
+            if use_graph:
+                ens = Ensemble(batches, gauges)
+                for _ in range(4):
+                    st = ens.Step(C, 1.0, use_graph=True)
+                    assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+                ens.Destructor()
+            else:
+                for _ in range(4):
+                    for b, g in zip(batches, gauges):
+                        b.Update(g, C, 1.0, use_graph=False)
+                        g.Update(1.0)
+            runs.append(([[h.download() for h in hs] for hs in fields], [g.download() for g in gauges],
+                         [b.info() for b in batches]))
+            for b in batches:
+                b.Destructor()
+            for hs in fields:
+                for h in hs:
+                    h.Destructor()
+            for g in gauges:
+                g.Deallocate()
+        (fa, ga, ia), (fb, gb, ib) = runs
+        for m in range(3):
+            la, ea = ga[m]
+            lb, eb = gb[m]
+            assert np.array_equal(la, lb) and np.array_equal(ea, eb)
+            same = ia[m]["fields_per_tile"] == ib[m]["fields_per_tile"] and \
+                ia[m]["block_order"] == ib[m]["block_order"] and ia[m]["schedule"] == ib[m]["schedule"]
+            for (qa, aa), (qb, ab) in zip(fa[m], fb[m]):
+                if same:
+                    assert np.array_equal(qa, qb) and np.array_equal(aa, ab)
+                else:
+                    assert np.abs(qa - qb).max() < 5e-10 and np.abs(aa - ab).max() < 5e-10
+    finally:
+        lat6.close()
+        lat8.close()
+
+
+def test_batch_rejects_bad_arguments(oracle):
+    n = (4, 4, 4)
+    with lattice_ctx(n, A):
+        g, _, _ = _hot_gauge(oracle, n, 1)
+        h1, h2 = NRQCDField(), NRQCDField()
+        h1.InitSinglePoint(1, 1)
+        h2.InitSinglePoint(2, 2)
+        with pytest.raises(NrqcdError):
+            CNBatch([h1, h1], [1.0, 1.0], 1e-10)
+        with pytest.raises(NrqcdError):
+            CNBatch([h1, h2], [1.0, 0.0], 1e-10)
+        b = CNBatch([h1, h2], [1.0, 2.0], 1e-10)
+        with pytest.raises(NrqcdError):
+            b.Update(g, [1, 1j, 1, 1], 1.0)
+        other = lattice.Lattice((4, 4, 4), A)
+        try:
+            g2 = GaugeConfiguration(lat=other)
+            with pytest.raises(NrqcdError):
+                b.Update(g2, C, 1.0)
+            g2.Deallocate()
+        finally:
+            other.close()
+        st = b.Update(g, C, 1.0)
+        assert st["converged"] == 1
+        b.Destructor()
