@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-forms", action="store_true")
+    p.add_argument("--no-ensemble", action="store_true")
+    p.add_argument("--only-ensemble", action="store_true", help="print only the batching-ensemble JSON")
+    p.add_argument("--only-forms", action="store_true", help="print only the CN-forms JSON")
     return p.parse_args()
 
 
@@ -168,22 +171,36 @@ def cpu_baseline_sample(L):
 
 
 # ------------------------------------------------------------------ CN forms
-FORMS = {"plain_fp64_bicgstab": 0, "precision_fp32_chebyshev_fp64_refinement": 1}
+FORMS = {"plain_fp64_bicgstab": 0, "precision_fp32_chebyshev_fp64_refinement": 1,
+         "learned_guess_precision": 2}
 
 
 def measure_cn_forms(g, stream, steps, tol=1e-10):
     """CN-only seconds per step of every solver form at the same residual,
-    on the same gauge field (the headline's comparison at <= 1e-10)."""
+    on the same gauge field (the headline's comparison at <= 1e-10).  The
+    learned form's network is trained first on seeded 32^3 solves (training
+    time reported, not in the step time)."""
     import torch
     from nrqcd_b200 import NRQCDField, nrqcd
+    from nrqcd_b200.learned import LearnedGuess, train_on_seeded_configs
     out = {}
+    t0 = time.perf_counter()
+    params, train_info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=6, mass=MASS,
+                                                 WilsonCoeffs=WILSON, spacings=A, tol=tol)
+    train_info["wall_s"] = time.perf_counter() - t0
     for name, form in FORMS.items():
         if nrqcd.IsModuleInitialised():
             nrqcd.FinalizeModule()
         nrqcd.InitModule(MASS, WILSON, 1.0, tol, form=form)
+        net = None
+        if form == 2:
+            net = LearnedGuess()
+            net.params = params
+            net.set_trained(True)
+            net.attach()
         h = NRQCDField()
         h.InitSinglePoint(1, 1)
-        for _ in range(2):
+        for _ in range(3):
             h.Update(g, MASS, WILSON, 1.0)
         stats = []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -196,12 +213,139 @@ def measure_cn_forms(g, stream, steps, tol=1e-10):
         out[name] = {"s_per_step": ms / 1000.0, "tol": tol,
                      "max_rel_residual": max(st["max_rel_residual"] for st in stats),
                      "stencil_launches_per_step": float(np.mean([st["matvecs"] for st in stats])),
+                     "inner_steps_per_step": float(np.mean([st["iterations"] for st in stats])),
+                     "initial_rel_residual": float(np.mean([st["initial_rel_residual"] for st in stats])),
                      "norms": [h.GetNorm_Quark(), h.GetNorm_AntiQ()]}
+        if form == 2:
+            out[name]["training"] = train_info
+            net.detach()
+            net.Destructor()
         del h
         nrqcd.FinalizeModule()
     base = out["plain_fp64_bicgstab"]["s_per_step"]
     for v in out.values():
         v["speedup_vs_plain_fp64"] = base / v["s_per_step"]
+    return out
+
+
+# ------------------------------------------------------------------ batching ensemble
+# 8 members at 24^3, 4 at 32^3, 2 at 48^3; 16 point sources at random sites x
+# masses aM = 1.0 and 1.5 per member; precision-form CN at residual 1e-10
+ENSEMBLE = ((24, 8), (32, 4), (48, 2))
+ENS_SOURCES = 16
+ENS_MASSES = (1.0, 1.5)
+
+
+def measure_ensemble(steps, warmup, tol=1e-10):
+    """Aggregate field-site updates/s of the uneven ensemble: one CUDA graph
+    launch per coupled step, the same batched launches issued eagerly, and a
+    serial loop of single-field precision-form updates (nrq_heavy_update_cn
+    per field, then the leapfrog per member)."""
+    import torch
+    from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice
+    from nrqcd_b200.batch import CNBatch, Ensemble
+    lib = _capi.load()
+    lats = {L: lattice.Lattice((L, L, L), A) for L, _ in ENSEMBLE}
+    members = []
+    seed = 1000
+    for L, count in ENSEMBLE:
+        for _ in range(count):
+            seed += 1
+            g = GaugeConfiguration(lat=lats[L])
+            g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=seed, identity_links=True)
+            rng = np.random.default_rng(seed)
+            srcs = rng.integers(0, L ** 3, size=(ENS_SOURCES, 2)) + 1
+            fields, masses = [], []
+            for m in ENS_MASSES:
+                for lq, la in srcs:
+                    h = NRQCDField(lat=lats[L])
+                    h.InitSinglePoint(int(lq), int(la))
+                    fields.append(h)
+                    masses.append(m)
+            members.append((L, g, fields, masses))
+    per_step = sum(L ** 3 * len(f) for L, _, f, _ in members)
+    streams = [torch.cuda.ExternalStream(lib.nrq_cuda_stream(lats[L].ctx)) for L, _ in ENSEMBLE]
+    s0 = streams[0]
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        for _ in range(n):
+            fn()
+        for s in streams[1:]:
+            s0.wait_stream(s)
+        e1.record(s0)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n / 1000.0
+
+    batches = [CNBatch(f, m, tol, lat=lats[L]) for L, _, f, m in members]
+    ens = Ensemble(batches, [g for _, g, _, _ in members])
+    stats = []
+    for _ in range(max(2, warmup)):  # calibration, then graph capture
+        ens.Step(WILSON, 1.0, use_graph=True)
+    t_graph = timed(lambda: stats.append(ens.Step(WILSON, 1.0, use_graph=True)), steps)
+    # the same batched launches without the graph, with per-class kernel timing
+    for L in lats:
+        _capi.profile_enable(lats[L].ctx, True)
+    t_eager = timed(lambda: stats.append(ens.Step(WILSON, 1.0, use_graph=False)), steps)
+    prof = {L: _capi.profile_read(lats[L].ctx) for L in lats}
+    for L in lats:
+        _capi.profile_enable(lats[L].ctx, False)
+    info = {L: b.info() for (L, _, _, _), b in zip(members, batches)}
+    ens.Destructor()
+    for b in batches:
+        b.Destructor()
+    # serial loop of single-field updates (precision form, same tolerance)
+    cns = {}
+    for L in lats:
+        h = ctypes.c_void_p()
+        _capi.check(lib.nrq_cn_init(lats[L].ctx, ENS_MASSES[0], _capi.dptr(_capi.coeffs(WILSON)), 1.0, tol, 10000, 1,
+                                    ctypes.byref(h)), lats[L].ctx, "nrq_cn_init")
+        cns[L] = h
+    cw = _capi.coeffs(WILSON)
+    serial_stats = []
+
+    def serial_step():
+        for L, g, fields, masses in members:
+            for h, m in zip(fields, masses):
+                st = _capi.CnStats()
+                _capi.check(lib.nrq_heavy_update_cn(cns[L], h.handle, g.handle, m, _capi.dptr(cw), 1.0,
+                                                    ctypes.byref(st)), lats[L].ctx, "serial update")
+                serial_stats.append(st.max_rel_residual)
+            g.Update(1.0)
+
+    serial_step()  # warm-up
+    serial_steps = max(1, min(steps, 2))
+    t_serial = timed(serial_step, serial_steps)
+    for L in lats:
+        lib.nrq_cn_finalize(cns[L])
+    sten = {}
+    for L in lats:
+        c0 = prof[L]["cn_stencil"]
+        sten[f"{L}^3"] = {"launches": c0["launches"], "ms": c0["ms"],
+                          "achieved_GBps": c0["bytes"] / (c0["ms"] / 1000.0) / 1e9 if c0["ms"] > 0 else None}
+    out = {
+        "workload": "uneven ensemble 8 x 24^3 + 4 x 32^3 + 2 x 48^3, 16 point sources at random sites x aM = 1.0, "
+                    "1.5 per member, coupled step (CN of every field, then the member's leapfrog), "
+                    "precision-form CN at residual 1e-10",
+        "field_site_updates_per_step": per_step,
+        "graph": {"s_per_step": t_graph, "field_site_updates_per_s": per_step / t_graph},
+        "eager_batched": {"s_per_step": t_eager, "field_site_updates_per_s": per_step / t_eager,
+                          "stencil_kernels": sten},
+        "serial_single_field": {"s_per_step": t_serial, "field_site_updates_per_s": per_step / t_serial,
+                                "steps": serial_steps, "max_rel_residual": max(serial_stats)},
+        "speedup_graph_vs_serial": t_serial / t_graph,
+        "max_rel_residual": max(s["max_rel_residual"] for s in stats),
+        "converged": all(s["converged"] == 1 for s in stats),
+        "tuning": {f"{L}^3": v for L, v in info.items()},
+    }
+    for _, g, fields, _ in members:
+        for h in fields:
+            h.Destructor()
+        g.Deallocate()
+    for L in lats:
+        lats[L].close()
     return out
 
 
@@ -226,6 +370,13 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
+    if args.only_ensemble:
+        import torch
+        torch.cuda.set_device(local)
+        out = measure_ensemble(args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"batching_ensemble": out}), flush=True)
+        return
 
     import torch
     from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice, nrqcd
@@ -242,6 +393,14 @@ def main():
     h.InitSinglePoint(1, 1)
     lib = _capi.load()
     stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(ctx))
+    if args.only_forms:
+        nrqcd.FinalizeModule()
+        forms = measure_cn_forms(g, stream, max(2, min(args.steps, 5)))
+        if rank == 0:
+            print(json.dumps({"cn_forms_at_1e-10": forms, "lattice": [L, L, L]}), flush=True)
+        del h, g
+        lattice.FinalizeModule()
+        return
 
     iters = []
 
@@ -317,6 +476,10 @@ def main():
                "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
                        "nrq_heavy_download + nrq_gauge_download, pinned host buffers"}
 
+    ensemble = None
+    if not args.no_ensemble and world == 1:
+        ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2)
+
     forms = None
     if not args.no_forms:
         nrqcd.FinalizeModule()
@@ -350,6 +513,7 @@ def main():
                    "norms": [norm_q, norm_a]},
             "clocks": clk, "e2e": e2e, "gpu_launches": int(sum(v["launches"] for v in prof.values())),
             "cn_forms_at_1e-10": forms,
+            "batching_ensemble": ensemble,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(min(L, 64))

@@ -59,6 +59,8 @@ typedef struct {
   int64_t vector_streams;  /* 12-column vector passes (read or write)  */
   double max_rel_residual; /* max over the 12 columns of ||b-Ax||/||b|| (true residual) */
   int converged;           /* 1 when every column reached the tolerance */
+  double initial_rel_residual; /* the same maximum for the starting guess
+                                  (0 where a batch step did not read it back) */
 } nrq_cn_stats;
 
 /* ---- context: replaces lattice%InitModule (src/lattice.f90:124-228) and
@@ -200,6 +202,53 @@ int nrq_ensemble_create(int nmembers, nrq_cn_batch *const *batches, nrq_gauge *c
 int nrq_ensemble_destroy(nrq_ensemble *ens);
 int nrq_ensemble_step(nrq_ensemble *ens, const double c[8], double stepwidth, int use_graph,
                       nrq_cn_stats *stats);
+
+/* ---- learned initial guess (form 2) ----------------------------------- */
+/* No counterpart in the reference (PETSc KSP starts from the previous
+ * propagator, src/nrqcd.f90:1112-1123).  Per sample (site, species) a
+ * 16 -> 64 -> 64 -> 6 MLP (ReLU, BF16 weights and activations, FP32
+ * accumulation on the tensor cores) maps local invariants of the right-hand
+ * side b = A psi, of the field's history and of the gauge field
+ * (plaquettes, E^2) to complex (w0, w1, w2); the solve of form 2 starts from
+ *   x0 = 2 b - psi + w0 |tau| (b - psi) + w1 v1 + w2 v2,   tau = dt a0 / 2,
+ * with v1, v2 = x - (2 b - psi) of the field's previous two steps (a
+ * learned per-site linear prediction).  The FP64 residual check of the
+ * precision form decides convergence, as without the network.
+ * Parameters: W1[64][16], b1[64], W2[64][64], b2[64], W3[6][64] and the
+ * output bias b3[6][6] per group (quark with 0, 1, 2 history vectors, then
+ * the antiquark's), FP32, this order.  Training refits b3 in closed form
+ * (the loss is quadratic in it).                                          */
+#define NRQ_LEARN_NPARAMS 5668
+typedef struct nrq_learn nrq_learn;
+int nrq_learn_create(nrq_ctx *ctx, uint64_t seed, nrq_learn **net);
+int nrq_learn_destroy(nrq_learn *net);
+/* get (set = 0) or set (set = 1) the FP32 parameters; setting resets Adam */
+int nrq_learn_params(nrq_learn *net, float *params, int set);
+/* mark the network usable by form 2 (nrq_learn_train sets it)             */
+int nrq_learn_set_trained(nrq_learn *net, int trained);
+/* training data: room for max_samples samples (2 per site and step)       */
+int nrq_learn_dataset_reserve(nrq_learn *net, int64_t max_samples);
+int nrq_learn_dataset_size(const nrq_learn *net, int64_t *n);
+/* features (n x 16) and normalised Gram statistics (n x 16) of samples
+ * [first, first+count)                                                    */
+int nrq_learn_dataset_read(nrq_learn *net, int64_t first, int64_t count, float *features, float *stats);
+/* One CN step of h (cn's form, without the network) that appends the
+ * step's 2V samples to the dataset and leaves h's history for the next one. */
+int nrq_learn_record(nrq_learn *net, nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass,
+                     const double c[8], double stepwidth, nrq_cn_stats *stats);
+/* Adam on random batches of the dataset; learning rate lr with cosine decay
+ * to 5 %; the loss (mean squared guess error relative to the plain
+ * extrapolation's) of the first and last batch.                            */
+int nrq_learn_train(nrq_learn *net, int64_t iterations, int64_t batch, double lr, uint64_t seed,
+                    double *loss_first, double *loss_last);
+/* Loss and gradient (NRQ_LEARN_NPARAMS) of n samples given in host memory
+ * (features n x 16, statistics n x 16), for checks against a CPU oracle.   */
+int nrq_learn_loss_grad(nrq_learn *net, const float *features, const float *stats, int64_t n,
+                        double *loss, float *grad);
+/* Network outputs (n x 6: Re/Im of w0, w1, w2) of host features.          */
+int nrq_learn_forward(nrq_learn *net, const float *features, int64_t n, float *out);
+/* Use net for the initial guess of cn (form 2); NULL detaches.            */
+int nrq_cn_attach_learned(nrq_cn *cn, nrq_learn *net);
 
 /* ---- energy without any device allocation ---------------------------- */
 /* No counterpart in the reference.  This is for callers that cannot call

@@ -38,7 +38,7 @@ class NrqcdError(RuntimeError):
 class CnStats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int64), ("matvecs", ctypes.c_int64),
                 ("vector_streams", ctypes.c_int64), ("max_rel_residual", ctypes.c_double),
-                ("converged", ctypes.c_int)]
+                ("converged", ctypes.c_int), ("initial_rel_residual", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -49,6 +49,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 _i64p = ctypes.POINTER(ctypes.c_int64)
 _pp = ctypes.POINTER(ctypes.c_void_p)
 _ip = ctypes.POINTER(ctypes.c_int)
+_fp = ctypes.POINTER(ctypes.c_float)
 
 # name -> (restype, argtypes); every entry point of include/nrqcd_b200.h
 SIGNATURES = {
@@ -94,6 +95,20 @@ SIGNATURES = {
     "nrq_ensemble_create": (ctypes.c_int, [ctypes.c_int, _pp, _pp, _pp]),
     "nrq_ensemble_destroy": (ctypes.c_int, [_vp]),
     "nrq_ensemble_step": (ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(CnStats)]),
+    "nrq_learn_create": (ctypes.c_int, [_vp, ctypes.c_uint64, _pp]),
+    "nrq_learn_destroy": (ctypes.c_int, [_vp]),
+    "nrq_learn_params": (ctypes.c_int, [_vp, _fp, ctypes.c_int]),
+    "nrq_learn_set_trained": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "nrq_learn_dataset_reserve": (ctypes.c_int, [_vp, ctypes.c_int64]),
+    "nrq_learn_dataset_size": (ctypes.c_int, [_vp, _i64p]),
+    "nrq_learn_dataset_read": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, _fp, _fp]),
+    "nrq_learn_record": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,
+                                        ctypes.POINTER(CnStats)]),
+    "nrq_learn_train": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, ctypes.c_uint64,
+                                       _dp, _dp]),
+    "nrq_learn_loss_grad": (ctypes.c_int, [_vp, _fp, _fp, ctypes.c_int64, _dp, _fp]),
+    "nrq_learn_forward": (ctypes.c_int, [_vp, _fp, ctypes.c_int64, _fp]),
+    "nrq_cn_attach_learned": (ctypes.c_int, [_vp, _vp]),
     "nrq_gauge_energy_noalloc": (ctypes.c_int, [_i64p, _dp, _vp, _vp, _vp, _vp]),
 }
 

@@ -74,7 +74,7 @@ struct nrq_cn_batch {
   const nrq_gauge *exec_g = nullptr;
   // statistics of the last update
   int64_t last_inner = 0, last_passes = 0, last_matvecs = 0;
-  double last_maxrel = 0.0;
+  double last_maxrel = 0.0, last_initial = 0.0;
   bool last_conv = false;
 };
 
@@ -245,9 +245,12 @@ Check check(const nrq_cn_batch *b) {
 }
 
 // inner steps whose guaranteed Chebyshev gain reaches `gain` for every mass
-// and species (FP32 arithmetic caps one pass at about 1e6)
+// and species
 int steps_for(const nrq_cn_batch *b, double dt, double gain) {
-  gain = std::min(std::max(gain, 10.0), 1e6);
+  gain = std::max(gain, 10.0);
+  // FP32 arithmetic caps one pass at about 1e6; a pass that can finish the
+  // solve may aim up to 3e7 (the FP64 check decides whether it did)
+  if (gain > 3e7) gain = 1e6;
   const double tau = dt * b->ctx->a[0] / 2.0;
   int m = 1;
   for (; m < nrq::BATCH_MAX_CHEB; ++m) {
@@ -343,6 +346,7 @@ int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], dou
   if ((rc = enq_rhs(b, st)) || (rc = enq_residual(b, st)) || (rc = enq_readback(b, st))) return rc;
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   chk = check(b);
+  b->last_initial = chk.worst;
   std::vector<int> used;
   if ((rc = refine_adaptive(b, dt, st, kMaxPasses, used, chk))) return rc;
   b->schedule = used;
@@ -376,7 +380,10 @@ int finish_step(nrq_cn_batch *b, double dt, cudaStream_t st, Check &chk, bool *s
 
 int conclude(nrq_cn_batch *b, const Check &chk, int64_t inner, int64_t passes) {
   // results: the iterate becomes the field, the old field the next work buffer
-  for (int i = 0; i < b->nf; ++i) std::swap(b->fields[i]->P, b->xbuf[i]);
+  for (int i = 0; i < b->nf; ++i) {
+    std::swap(b->fields[i]->P, b->xbuf[i]);
+    b->fields[i]->hist_count = 0;
+  }
   b->last_inner = inner;
   b->last_passes = passes;
   b->last_matvecs = 1 + (passes + 1) + inner;
@@ -400,6 +407,7 @@ void fill_stats(const nrq_cn_batch *b, nrq_cn_stats *s) {
   s->vector_streams = 1 + 3 * (b->last_passes + 1) + 3 * b->last_passes;
   s->max_rel_residual = b->last_maxrel;
   s->converged = b->last_conv ? 1 : 0;
+  s->initial_rel_residual = b->last_initial;
 }
 
 int64_t sum(const std::vector<int> &v) {
@@ -593,6 +601,7 @@ int batch_update(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double 
     if ((rc = enq_scheduled(b, g, c, dt, st))) return rc;
   }
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  b->last_initial = 0.0;  // not read back by scheduled steps
   const int64_t planned = sum(b->schedule), planned_passes = (int64_t)b->schedule.size();
   bool changed = false;
   if ((rc = finish_step(b, dt, st, chk, &changed))) return rc;
@@ -754,6 +763,7 @@ extern "C" int nrq_ensemble_step(nrq_ensemble *e, const double c[8], double dt, 
       stats->matvecs += b->last_matvecs * b->nf;
       stats->vector_streams += (1 + 3 * (b->last_passes + 1) + 3 * b->last_passes) * b->nf;
       stats->max_rel_residual = std::max(stats->max_rel_residual, b->last_maxrel);
+      stats->initial_rel_residual = std::max(stats->initial_rel_residual, b->last_initial);
       stats->converged = stats->converged && b->last_conv;
     }
   }

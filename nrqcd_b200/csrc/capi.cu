@@ -578,6 +578,8 @@ extern "C" int nrq_heavy_destroy(nrq_heavy *h) {
   cudaSetDevice(h->ctx->device);
   cudaStreamSynchronize(h->ctx->stream);
   if (h->P) cudaFree(h->P);
+  for (float2 *q : h->hist)
+    if (q) cudaFree(q);
   delete h;
   return NRQ_OK;
 }
@@ -593,6 +595,7 @@ extern "C" int nrq_heavy_upload(nrq_heavy *h, const double *q, const double *a) 
   NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(stg, q, sizeof(double2) * 36 * V, cudaMemcpyHostToDevice, ctx->stream));
   NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(stg + 36 * V, a, sizeof(double2) * 36 * V, cudaMemcpyHostToDevice, ctx->stream));
   nrq::launch_prop_f2soa(stg, h->P, V, ctx->stream);
+  h->hist_count = 0;
   return check_launch(ctx, "k_prop_f2soa");
 }
 
@@ -619,6 +622,7 @@ extern "C" int nrq_heavy_copy(nrq_heavy *dst, const nrq_heavy *src) {
   if (rc) return rc;
   NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(dst->P, src->P, sizeof(double2) * 72 * ctx->lat.V, cudaMemcpyDeviceToDevice,
                                     ctx->stream));
+  dst->hist_count = 0;
   return NRQ_OK;
 }
 
@@ -633,6 +637,7 @@ extern "C" int nrq_heavy_init_single_point(nrq_heavy *h, int64_t lq, int64_t la)
   int rc = set_device(ctx);
   if (rc) return rc;
   nrq::launch_single_point(h->P, V, lq - 1, la - 1, ctx->stream);
+  h->hist_count = 0;
   return check_launch(ctx, "k_single_point");
 }
 
@@ -670,11 +675,11 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
                            int64_t maxits, int form, nrq_cn **out) {
   if (!ctx || !c || !out) return NRQ_ERR_BAD_ARG;
   *out = nullptr;
-  if (mass == 0.0 || !(tol > 0.0) || maxits < 1 || form < 0 || form > 1) {
+  if (mass == 0.0 || !(tol > 0.0) || maxits < 1 || form < 0 || form > 2) {
     ctx->last_error = "nrq_cn_init: invalid mass, tolerance, maxits or form";
     return NRQ_ERR_BAD_ARG;
   }
-  if (form == 1 && (c[1] != 0.0 || c[3] != 0.0 || c[5] != 0.0 || c[7] != 0.0)) {
+  if (form >= 1 && (c[1] != 0.0 || c[3] != 0.0 || c[5] != 0.0 || c[7] != 0.0)) {
     ctx->last_error = "nrq_cn_init: the precision form needs real Wilson coefficients";
     return NRQ_ERR_BAD_ARG;
   }
@@ -703,7 +708,7 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
   alloc((void **)&cn->scal, kScalBytes);
   alloc((void **)&cn->partials, sizeof(double) * 3 * cn->nblocks * nrq::CN_COLS * 3);
   if (ok && cudaMallocHost((void **)&cn->h_scal, kScalBytes) != cudaSuccess) ok = false;
-  if (form == 1) {
+  if (form >= 1) {
     alloc((void **)&cn->U32, sizeof(float2) * 27 * V);
     alloc((void **)&cn->DE32, sizeof(float2) * 54 * V);
     alloc((void **)&cn->D32, sizeof(float2) * 9 * V);
@@ -832,7 +837,18 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     matvecs += 1;
     vstreams += 1;
   }
+  // learned form: x = 2 RHS - psi + w1 u + w2 v (network), history restarted
+  // with the network's part; every refinement correction is added to it
+  const bool learned = cn->form == 2 && nrqh::learned_ready(cn->learn);
+  if (learned) {
+    if ((rc = nrqh::ensure_hist(h))) return rc;
+    ProfScope ps(ctx, 3, (double)V * (1152.0 * 4 + 576.0 * 6 + 432.0 * 3 + 128.0));
+    if ((rc = nrqh::learned_guess(cn->learn, ctx, h->P, cn->b, hist_v1(h), hist_v2(h), hist_next(h), g->U, g->E,
+                                  mass, dt, cn->x, st)))
+      return rc;
+  }
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (learned && (rc = nrqh::learned_check(cn->learn))) return rc;
   ChebSeg seg[2];
   for (int sp = 0; sp < 2; ++sp) {
     double lo = cn->h_bounds[2 * sp], hi = cn->h_bounds[2 * sp + 1];
@@ -862,9 +878,11 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
       }
   }
   // smallest inner step count whose guaranteed gain reaches `gain` on both
-  // species (FP32 inner arithmetic caps a pass at about 1e6)
+  // species.  FP32 arithmetic caps one pass at about 1e6; a pass that can
+  // finish the solve may aim up to 3e7 (the FP64 check decides whether it did)
   auto inner_steps = [&](double gain) {
-    gain = std::min(std::max(gain, 10.0), 1e6);
+    gain = std::max(gain, 10.0);
+    if (gain > 3e7) gain = 1e6;
     int m = 1;
     while (m < kMaxInner && std::min(cheb_gain(seg[0].sigma, m), cheb_gain(seg[1].sigma, m)) < gain) ++m;
     return m;
@@ -873,6 +891,7 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
   double *hs = cn->h_scal;
   int64_t outer = 0, inner = 0;
   bool conv = false;
+  double initial = 0.0;
   for (outer = 0; outer < 8; ++outer) {
     nrq::MvArgs a{};
     a.in = cn->x;
@@ -900,6 +919,8 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     for (int k = 0; k < nrq::CN_COLS; ++k) {
       all = all && hs[k * nrq::SC_STRIDE + nrq::SC_CONV] != 0.0;
       nonfin = nonfin || hs[k * nrq::SC_STRIDE + nrq::SC_NONFIN] != 0.0;
+      const double *sc = hs + k * nrq::SC_STRIDE;
+      if (outer == 0 && sc[nrq::SC_BB] > 0) initial = std::max(initial, std::sqrt(sc[nrq::SC_RR] / sc[nrq::SC_BB]));
     }
     if (nonfin) {
       ctx->last_error = "CN solve: non-finite residual";
@@ -927,7 +948,10 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
       std::swap(dcur, dnext);
     }
     inner += m;
-    {
+    if (learned) {
+      ProfScope ps(ctx, 1, (double)V * (1152.0 * 2 + 576.0 * 3));
+      nrqh::add_e_hist(72 * V, cn->x, cn->e32, hist_next(h), st);
+    } else {
       ProfScope ps(ctx, 1, (double)V * (1152.0 * 2 + 576.0));
       nrq::launch_add_e(72 * V, cn->x, cn->e32, st);
     }
@@ -936,6 +960,8 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
   }
   if (status == NRQ_OK && !conv) status = NRQ_ERR_NOT_CONVERGED;
   std::swap(h->P, cn->x);
+  if (learned && status == NRQ_OK) hist_push(h);
+  else h->hist_count = 0;
   double maxrel = 0.0;
   for (int k = 0; k < nrq::CN_COLS; ++k) {
     const double *s = hs + k * nrq::SC_STRIDE;
@@ -953,6 +979,7 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     stats->vector_streams = vstreams;
     stats->max_rel_residual = maxrel;
     stats->converged = conv ? 1 : 0;
+    stats->initial_rel_residual = initial;
   }
   return status;
 }
@@ -965,7 +992,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   if (g->ctx != ctx || h->ctx != ctx || mass == 0.0) return NRQ_ERR_BAD_ARG;
   int rc = set_device(ctx);
   if (rc) return rc;
-  if (cn->form == 1) return cn_update_precision(cn, h, g, mass, c, dt, stats);
+  if (cn->form >= 1) return cn_update_precision(cn, h, g, mass, c, dt, stats);
   cudaStream_t st = ctx->stream;
   const nrq::Lat L = ctx->lat;
   const nrq::CnCoef CA = make_coef(ctx, mass, c, dt, false);
@@ -986,6 +1013,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   int64_t its = 0;
   int status = NRQ_OK;
   double *hs = cn->h_scal;
+  double initial = -1.0;  // relative residual of the start, read after the first restart
   for (;;) {
     if (restart) {
       nrq::MvArgs a{};
@@ -1059,6 +1087,13 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, sizeof(int), st));
       break;
     }
+    if (initial < 0.0) {
+      initial = 0.0;
+      for (int k = 0; k < nrq::CN_COLS; ++k) {
+        const double *s = hs + k * nrq::SC_STRIDE;
+        if (s[nrq::SC_BB] > 0) initial = std::max(initial, std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]));
+      }
+    }
     bool all = true, brk = false, nonfin = false;
     for (int k = 0; k < nrq::CN_COLS; ++k) {
       const double *s = hs + k * nrq::SC_STRIDE;
@@ -1080,8 +1115,9 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     }
     if (brk) restart = true;
   }
-  // result -> propagator (swap buffers)
+  // result -> propagator (swap buffers); a plain step leaves no history
   std::swap(h->P, cn->x);
+  h->hist_count = 0;
   double maxrel = 0.0;
   bool conv = true;
   for (int k = 0; k < nrq::CN_COLS; ++k) {
@@ -1099,6 +1135,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     stats->vector_streams = vstreams;
     stats->max_rel_residual = maxrel;
     stats->converged = conv ? 1 : 0;
+    stats->initial_rel_residual = std::max(initial, 0.0);
   }
   return status;
 }

@@ -76,7 +76,27 @@ struct nrq_heavy {
   nrq_ctx *ctx = nullptr;
   // 72 planes of V complex: (species*36 + col*6 + row); species 0 quark, 1 antiquark
   double2 *P = nullptr;
+  // history of the learned initial guess (FP32, 72 planes each): what the
+  // extrapolation 2 RHS - psi missed in the last two steps.  hist_count
+  // vectors are valid (0..2; only after learned-form or recording updates),
+  // the newest in slot hist_head.
+  float2 *hist[2] = {nullptr, nullptr};
+  int hist_count = 0;
+  int hist_head = 0;
 };
+
+inline const float2 *hist_v1(const nrq_heavy *h) { return h->hist_count >= 1 ? h->hist[h->hist_head] : nullptr; }
+inline const float2 *hist_v2(const nrq_heavy *h) {
+  return h->hist_count >= 2 ? h->hist[1 - h->hist_head] : nullptr;
+}
+// slot the next history vector goes to (the oldest one)
+inline float2 *hist_next(nrq_heavy *h) { return h->hist[1 - h->hist_head]; }
+inline void hist_push(nrq_heavy *h) {
+  h->hist_head = 1 - h->hist_head;
+  h->hist_count = h->hist_count < 2 ? h->hist_count + 1 : 2;
+}
+
+struct nrq_learn;
 
 struct nrq_cn_stats_internal;
 
@@ -88,6 +108,7 @@ struct nrq_cn {
   double tol = 1e-12;
   int64_t maxits = 10000;
   int form = 0;
+  nrq_learn *learn = nullptr;  // learned initial guess (form 2)
   // per-step derived gauge data
   double2 *Dsum = nullptr;  // 9 planes
   double *Bsum = nullptr;   // 9 planes
@@ -143,4 +164,18 @@ struct ChebSeg {
 ChebSeg cheb_segment(double tau, double lo, double hi);
 // |T_m(sigma)|: error reduction guaranteed by m Chebyshev steps
 double cheb_gain(std::complex<double> sigma, int m);
+// learned initial guess (learned.cu)
+bool learned_ready(const nrq_learn *net);
+// x = 2b - psi + w0 u + w1 v1 + w2 v2, hnew = the learned part (v1, v2 may be
+// null; hnew may alias v2)
+int learned_guess(nrq_learn *net, const nrq_ctx *ctx, const double2 *psi, const double2 *b, const float2 *v1,
+                  const float2 *v2, float2 *hnew, const double2 *U, const double *E, double mass, double dt,
+                  double2 *x, cudaStream_t st);
+void add_e_hist(int64_t n, double2 *x, const float2 *e, float2 *hist, cudaStream_t st);
+int learned_check(nrq_learn *net);
+int learn_record(nrq_learn *net, const nrq_ctx *ctx, const double2 *psi, const double2 *b, const double2 *x,
+                 const float2 *v1, const float2 *v2, float2 *hnew, const double2 *U, const double *E, double mass,
+                 double dt);
+// both history slots of h allocated
+int ensure_hist(nrq_heavy *h);
 }  // namespace nrqh

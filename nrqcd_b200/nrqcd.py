@@ -23,6 +23,8 @@ _cn = None
 _settings = None
 
 FORM_PLAIN_FP64 = 0
+FORM_PRECISION = 1  # FP32 Chebyshev inner iterations in FP64 iterative refinement
+FORM_LEARNED = 2    # precision form started from the learned guess (nrqcd_b200.learned)
 
 
 def InitModule(Mass, WilsonCoeffs, StepWidth, kspTol, maxits=10000, form=FORM_PLAIN_FP64):
