@@ -350,6 +350,19 @@ def measure_ensemble(steps, warmup, tol=1e-10):
 
 
 # ------------------------------------------------------------------ our arm
+def max_over_ranks(x, dist=None):
+    """Max of a per-rank float over all ranks (the timed region's duration);
+    identity without a process group.  NCCL reduces a CUDA tensor, gloo a
+    CPU one."""
+    if dist is None:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -432,11 +445,7 @@ def main():
     if dist is not None:
         dist.barrier()
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     ms_per_step = ms / args.steps
     value = world * V * args.steps / (ms / 1000.0)
     norm_q, norm_a = h.GetNorm_Quark(), h.GetNorm_AntiQ()
@@ -466,11 +475,7 @@ def main():
             _capi.check(lib.nrq_gauge_download(g.handle, P(links_h), P(ef_h)), ctx, "download")
         e1.record(stream)
         e1.synchronize()
-        ems = e0.elapsed_time(e1)
-        if dist is not None:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(e0.elapsed_time(e1), dist)
         e2e = {"value": world * V * e2e_steps / (ems / 1000.0), "unit": "site-updates/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(h2d), "steps": e2e_steps,
                "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
