@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--no-ensemble", action="store_true")
     p.add_argument("--only-ensemble", action="store_true", help="print only the batching-ensemble JSON")
     p.add_argument("--only-forms", action="store_true", help="print only the CN-forms JSON")
+    p.add_argument("--forms-sizes", type=int, nargs="+", default=list(FORMS_SIZES))
     return p.parse_args()
 
 
@@ -173,59 +174,91 @@ def cpu_baseline_sample(L):
 # ------------------------------------------------------------------ CN forms
 FORMS = {"plain_fp64_bicgstab": 0, "precision_fp32_chebyshev_fp64_refinement": 1,
          "learned_guess_precision": 2}
+FORMS_SIZES = (64, 96, 128)
 
 
-def measure_cn_forms(g, stream, steps, tol=1e-10):
-    """CN-only seconds per step of every solver form at the same residual,
-    on the same gauge field (the headline's comparison at <= 1e-10).  The
-    learned form's network is trained first on seeded 32^3 solves (training
-    time reported, not in the step time)."""
-    import torch
-    from nrqcd_b200 import NRQCDField, nrqcd
-    from nrqcd_b200.learned import LearnedGuess, train_on_seeded_configs
-    out = {}
+def train_learned(tol=1e-10):
+    """The learned form's network, trained on seeded 32^3 solves (2
+    configurations x 8 steps); the parameters load into any lattice size."""
+    from nrqcd_b200.learned import train_on_seeded_configs
     t0 = time.perf_counter()
-    params, train_info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=6, mass=MASS,
-                                                 WilsonCoeffs=WILSON, spacings=A, tol=tol)
-    train_info["wall_s"] = time.perf_counter() - t0
-    for name, form in FORMS.items():
-        if nrqcd.IsModuleInitialised():
-            nrqcd.FinalizeModule()
-        nrqcd.InitModule(MASS, WILSON, 1.0, tol, form=form)
-        net = None
-        if form == 2:
-            net = LearnedGuess()
-            net.params = params
-            net.set_trained(True)
-            net.attach()
-        h = NRQCDField()
-        h.InitSinglePoint(1, 1)
-        for _ in range(3):
-            h.Update(g, MASS, WILSON, 1.0)
-        stats = []
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            stats.append(h.Update(g, MASS, WILSON, 1.0))
-        e1.record(stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        out[name] = {"s_per_step": ms / 1000.0, "tol": tol,
-                     "max_rel_residual": max(st["max_rel_residual"] for st in stats),
-                     "stencil_launches_per_step": float(np.mean([st["matvecs"] for st in stats])),
-                     "inner_steps_per_step": float(np.mean([st["iterations"] for st in stats])),
-                     "initial_rel_residual": float(np.mean([st["initial_rel_residual"] for st in stats])),
-                     "norms": [h.GetNorm_Quark(), h.GetNorm_AntiQ()]}
-        if form == 2:
-            out[name]["training"] = train_info
-            net.detach()
-            net.Destructor()
-        del h
-        nrqcd.FinalizeModule()
+    params, info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=8, mass=MASS, WilsonCoeffs=WILSON,
+                                           spacings=A, tol=tol, iterations=800)
+    info["wall_s"] = time.perf_counter() - t0
+    return params, info
+
+
+def measure_cn_forms(L, steps, params, tol=1e-10, seed=1):
+    """CN-only seconds per step of every solver form at the same residual on
+    one L^3 gauge field (the headline's comparison at <= 1e-10): a fresh point
+    source per form, 3 warm-up and `steps` timed CN steps, CUDA events on the
+    lattice's stream."""
+    import torch
+    from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice
+    from nrqcd_b200.learned import LearnedGuess
+    lib = _capi.load()
+    lat = lattice.Lattice((L, L, L), A)
+    out = {}
+    try:
+        g = GaugeConfiguration(lat=lat)
+        g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=seed, identity_links=True)
+        stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(lat.ctx))
+        cw = _capi.coeffs(WILSON)
+        for name, form in FORMS.items():
+            cn = ctypes.c_void_p()
+            _capi.check(lib.nrq_cn_init(lat.ctx, MASS, _capi.dptr(cw), 1.0, tol, 10000, form, ctypes.byref(cn)),
+                        lat.ctx, "nrq_cn_init")
+            net = None
+            if form == 2:
+                net = LearnedGuess(lat=lat)
+                net.params = params
+                net.set_trained(True)
+                net.attach(cn)
+            h = NRQCDField(lat=lat)
+            h.InitSinglePoint(1, 1)
+
+            def update():
+                st = _capi.CnStats()
+                _capi.check(lib.nrq_heavy_update_cn(cn, h.handle, g.handle, MASS, _capi.dptr(cw), 1.0,
+                                                    ctypes.byref(st)), lat.ctx, "update")
+                return st.as_dict()
+            for _ in range(3):
+                update()
+            stats = []
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                stats.append(update())
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            out[name] = {"s_per_step": ms / 1000.0, "tol": tol,
+                         "max_rel_residual": max(st["max_rel_residual"] for st in stats),
+                         "stencil_launches_per_step": float(np.mean([st["matvecs"] for st in stats])),
+                         "inner_steps_per_step": float(np.mean([st["iterations"] for st in stats])),
+                         "initial_rel_residual": float(np.mean([st["initial_rel_residual"] for st in stats])),
+                         "norms": [h.GetNorm_Quark(), h.GetNorm_AntiQ()]}
+            if net is not None:
+                net.detach(cn)
+                net.Destructor()
+            h.Destructor()
+            lib.nrq_cn_finalize(cn)
+        g.Deallocate()
+    finally:
+        lat.close()
     base = out["plain_fp64_bicgstab"]["s_per_step"]
     for v in out.values():
         v["speedup_vs_plain_fp64"] = base / v["s_per_step"]
     return out
+
+
+def measure_all_forms(steps, sizes=FORMS_SIZES):
+    params, info = train_learned()
+    res = {"learned_training": info}
+    for L in sizes:
+        res[f"{L}^3"] = measure_cn_forms(L, steps, params)
+    return res
 
 
 # ------------------------------------------------------------------ batching ensemble
@@ -407,11 +440,11 @@ def main():
     lib = _capi.load()
     stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(ctx))
     if args.only_forms:
-        nrqcd.FinalizeModule()
-        forms = measure_cn_forms(g, stream, max(2, min(args.steps, 5)))
+        forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
         if rank == 0:
-            print(json.dumps({"cn_forms_at_1e-10": forms, "lattice": [L, L, L]}), flush=True)
+            print(json.dumps({"cn_forms_at_1e-10": forms}), flush=True)
         del h, g
+        nrqcd.FinalizeModule()
         lattice.FinalizeModule()
         return
 
@@ -486,10 +519,8 @@ def main():
         ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2)
 
     forms = None
-    if not args.no_forms:
-        nrqcd.FinalizeModule()
-        forms = measure_cn_forms(g, stream, max(2, min(args.steps, 5)))
-        nrqcd.InitModule(MASS, WILSON, 1.0, TOL)
+    if not args.no_forms and world == 1:
+        forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
 
     if rank == 0:
         peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")

@@ -163,8 +163,8 @@ int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const double c[8],
  *
  * The first update (and the first after c or stepwidth change) calibrates:
  * it runs the refinement adaptively with host synchronisation, times the
- * candidate kernel tiles (fields per tile x block order) and keeps the
- * fastest, and records the per-pass inner step counts as the schedule.
+ * candidate Chebyshev kernels (tile and register variants x block order)
+ * and keeps the fastest, and records the per-pass inner step counts as the schedule.
  * Later updates replay the schedule without host synchronisation, as one
  * CUDA graph when use_graph != 0, and verify every field's FP64 residual at
  * the end; a field that missed the tolerance gets adaptive passes and
@@ -181,11 +181,13 @@ int nrq_cn_batch_update(nrq_cn_batch *batch, const nrq_gauge *g, const double c[
 /* Relative residual ||b - A^H x|| / ||b|| of every field (max over its 12
  * columns) after the last update, in the order of `fields`.                 */
 int nrq_cn_batch_residuals(const nrq_cn_batch *batch, double *rel);
-/* Tuning and schedule: the chosen fields per tile and block order, the
- * measured milliseconds per Chebyshev launch of the candidates
- * (tile 1 order 0, tile 1 order 1, tile 2 order 0, tile 2 order 1; -1 where
- * not applicable), and the inner steps of each refinement pass (up to 16). */
-int nrq_cn_batch_info(const nrq_cn_batch *batch, int *nf_tile, int *order, double candidate_ms[4],
+/* Tuning and schedule: the chosen Chebyshev kernel variant (0: one field
+ * per tile, 2 blocks per SM; 1: one field per tile, 3 blocks per SM; 2: two
+ * fields of one mass per tile) and block order (0: field fastest, 1: site
+ * block fastest), the measured milliseconds per launch of every candidate
+ * (index variant*2 + order; -1 where not applicable), and the inner steps
+ * of each refinement pass (up to 16).                                     */
+int nrq_cn_batch_info(const nrq_cn_batch *batch, int *variant, int *order, double candidate_ms[6],
                       int *npasses, int steps[16]);
 
 /* An ensemble of independent members (batch[i], gauge[i]); the members may

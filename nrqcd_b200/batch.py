@@ -69,14 +69,15 @@ class CNBatch:
         return out
 
     def info(self) -> dict:
-        nf, order, npass = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        ms = np.zeros(4)
+        var, order, npass = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = np.zeros(6)
         steps = (ctypes.c_int * 16)()
-        _capi.check(_capi.load().nrq_cn_batch_info(self._h, ctypes.byref(nf), ctypes.byref(order), _capi.dptr(ms),
+        _capi.check(_capi.load().nrq_cn_batch_info(self._h, ctypes.byref(var), ctypes.byref(order), _capi.dptr(ms),
                                                    ctypes.byref(npass), steps), self._ctx, "info")
-        return {"fields_per_tile": nf.value, "block_order": order.value,
-                "candidate_ms": {"tile1_order0": ms[0], "tile1_order1": ms[1], "tile2_order0": ms[2],
-                                 "tile2_order1": ms[3]},
+        names = ("tile1_2blocks", "tile1_3blocks", "tile2_1block")
+        return {"variant": names[var.value], "fields_per_tile": 2 if var.value == 2 else 1,
+                "block_order": order.value,
+                "candidate_ms": {f"{names[v]}_order{o}": float(ms[2 * v + o]) for v in range(3) for o in range(2)},
                 "schedule": [int(steps[k]) for k in range(npass.value)]}
 
 

@@ -63,8 +63,8 @@ struct nrq_cn_batch {
   double key_dt = 0.0, key_c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<int> schedule;
   bool tuned = false;
-  int nf_tile = 1, order = 0;
-  double cand_ms[4] = {-1, -1, -1, -1};
+  int variant = 0, order = 0;  // Chebyshev kernel variant (nrq_kernels.cuh) and block order
+  double cand_ms[2 * nrq::BATCH_CHEB_VARIANTS] = {-1, -1, -1, -1, -1, -1};
   // generation: changes with every new schedule, tuning or key
   uint64_t gen = 0;
   // graph of one scheduled step (CN only), with the generation and gauge
@@ -190,7 +190,7 @@ int enq_inner(nrq_cn_batch *b, int m, cudaStream_t st) {
   const double V = (double)ctx->lat.V;
   for (int k = 0; k < m; ++k) {
     ProfScope ps(ctx, 0, V * (b->nf * 576.0 * 6 + 756.0));
-    if (nrq::launch_batch_cheb(k, b->nf_tile, b->order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf,
+    if (nrq::launch_batch_cheb(k, b->variant, b->order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf,
                                st)) {
       ctx->last_error = "batch: unsupported Chebyshev tile";
       return NRQ_ERR_BAD_ARG;
@@ -276,18 +276,20 @@ int autotune(nrq_cn_batch *b, cudaStream_t st) {
   NRQ_CUDA_TRY(ctx, cudaEventCreate(&e0));
   NRQ_CUDA_TRY(ctx, cudaEventCreate(&e1));
   double best = 1e300;
-  int best_tile = 1, best_order = 0;
+  int best_variant = 0, best_order = 0;
   const int reps = 3;
-  for (int tile = 1; tile <= 2; ++tile)
+  for (int variant = 0; variant < nrq::BATCH_CHEB_VARIANTS; ++variant)
     for (int order = 0; order < 2; ++order) {
-      const int idx = (tile - 1) * 2 + order;
+      const int idx = variant * 2 + order;
       b->cand_ms[idx] = -1.0;
-      if (tile == 2 && !even) continue;
+      if (variant == 2 && !even) continue;
       // warm-up launch, then timed repetitions
-      int bad = nrq::launch_batch_cheb(0, tile, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf, st);
+      int bad =
+          nrq::launch_batch_cheb(0, variant, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf, st);
       cudaEventRecord(e0, st);
       for (int r = 0; r < reps && !bad; ++r)
-        bad = nrq::launch_batch_cheb(0, tile, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf, st);
+        bad = nrq::launch_batch_cheb(0, variant, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf,
+                                     st);
       cudaEventRecord(e1, st);
       if (bad) continue;
       int rc = check_launch(ctx, "batch autotune");
@@ -302,13 +304,13 @@ int autotune(nrq_cn_batch *b, cudaStream_t st) {
       b->cand_ms[idx] = ms / reps;
       if (ms / reps < best) {
         best = ms / reps;
-        best_tile = tile;
+        best_variant = variant;
         best_order = order;
       }
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  b->nf_tile = best_tile;
+  b->variant = best_variant;
   b->order = best_order;
   b->tuned = true;
   return NRQ_OK;
@@ -638,13 +640,13 @@ extern "C" int nrq_cn_batch_residuals(const nrq_cn_batch *b, double *rel) {
   return NRQ_OK;
 }
 
-extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *nf_tile, int *order, double candidate_ms[4],
+extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *variant, int *order, double candidate_ms[6],
                                  int *npasses, int steps[16]) {
   if (!b) return NRQ_ERR_BAD_ARG;
-  if (nf_tile) *nf_tile = b->nf_tile;
+  if (variant) *variant = b->variant;
   if (order) *order = b->order;
   if (candidate_ms)
-    for (int k = 0; k < 4; ++k) candidate_ms[k] = b->cand_ms[k];
+    for (int k = 0; k < 2 * nrq::BATCH_CHEB_VARIANTS; ++k) candidate_ms[k] = b->cand_ms[k];
   if (npasses) *npasses = (int)b->schedule.size();
   if (steps)
     for (int k = 0; k < 16; ++k) steps[k] = k < (int)b->schedule.size() ? b->schedule[k] : 0;

@@ -351,9 +351,10 @@ __global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2
 // the flattened block index is split into (tile, site block) with the tile
 // fastest (ORDER 0: consecutive blocks share the gauge-derived tiles in L2)
 // or the site block fastest (ORDER 1).
-// one resident block per SM for two-field tiles (their accumulators double)
-template <bool FIRST, int NF, int ORDER>
-__global__ void __launch_bounds__(192, NF == 1 ? 2 : 1) k_batch_cheb32(Lat L, const float2 *__restrict__ U,
+// MINB resident blocks per SM (the register budget: 2 -> 168, 3 -> 113);
+// two-field tiles double the accumulators and run one block per SM
+template <bool FIRST, int NF, int ORDER, int MINB>
+__global__ void __launch_bounds__(192, MINB) k_batch_cheb32(Lat L, const float2 *__restrict__ U,
                                                          const float2 *__restrict__ Dsum,
                                                          const float *__restrict__ Bsum,
                                                          const float2 *__restrict__ DE,
@@ -386,31 +387,35 @@ __global__ void k_batch_add_e(int64_t n, const BatchField *__restrict__ tab) {
   }
 }
 
-template <bool FIRST, int NF>
+template <bool FIRST, int NF, int MINB>
 static void batch_cheb_nf(int order, dim3 grid, Lat L, const float2 *U, const float2 *Dsum, const float *Bsum,
                           const float2 *DE, const BatchField *tab, int ntiles, int64_t nsb, int step,
                           cudaStream_t st) {
   if (order == 0)
-    k_batch_cheb32<FIRST, NF, 0><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step);
+    k_batch_cheb32<FIRST, NF, 0, MINB><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step);
   else
-    k_batch_cheb32<FIRST, NF, 1><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step);
+    k_batch_cheb32<FIRST, NF, 1, MINB><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step);
 }
 
-int launch_batch_cheb(int step, int nf_tile, int order, Lat L, const float2 *U, const float2 *Dsum,
+int launch_batch_cheb(int step, int variant, int order, Lat L, const float2 *U, const float2 *Dsum,
                       const float *Bsum, const float2 *DE, const BatchField *tab, int nfields, cudaStream_t st) {
-  if (nf_tile <= 0 || nfields % nf_tile != 0 || step < 0 || step >= BATCH_MAX_CHEB) return 1;
+  const int nf_tile = variant == 2 ? 2 : 1;
+  if (variant < 0 || variant >= BATCH_CHEB_VARIANTS || nfields % nf_tile != 0 || step < 0 ||
+      step >= BATCH_MAX_CHEB)
+    return 1;
   const int ntiles = nfields / nf_tile;
   const int64_t nsb = (L.V + 31) / 32;
   const dim3 grid((unsigned)(nsb * ntiles));
   const bool first = step == 0;
-  if (nf_tile == 1) {
-    if (first) batch_cheb_nf<true, 1>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
-    else batch_cheb_nf<false, 1>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
-  } else if (nf_tile == 2) {
-    if (first) batch_cheb_nf<true, 2>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
-    else batch_cheb_nf<false, 2>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+  if (variant == 0) {
+    if (first) batch_cheb_nf<true, 1, 2>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+    else batch_cheb_nf<false, 1, 2>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+  } else if (variant == 1) {
+    if (first) batch_cheb_nf<true, 1, 3>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+    else batch_cheb_nf<false, 1, 3>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
   } else {
-    return 1;
+    if (first) batch_cheb_nf<true, 2, 1>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
+    else batch_cheb_nf<false, 2, 1>(order, grid, L, U, Dsum, Bsum, DE, tab, ntiles, nsb, step, st);
   }
   return 0;
 }

@@ -104,8 +104,12 @@ struct BatchField {
 };
 void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
                      const double2 *DE, const BatchField *tab, int nfields, cudaStream_t st);
-// returns nonzero for an unsupported tile (nf_tile must divide nfields)
-int launch_batch_cheb(int step, int nf_tile, int order, Lat L, const float2 *U, const float2 *Dsum,
+// Chebyshev kernel variants: 0 = one field per tile, 2 blocks/SM (168
+// registers); 1 = one field per tile, 3 blocks/SM (113 registers); 2 = two
+// fields of one mass per tile, 1 block/SM.  Returns nonzero for an
+// unsupported variant (a two-field tile needs an even count per mass).
+constexpr int BATCH_CHEB_VARIANTS = 3;
+int launch_batch_cheb(int step, int variant, int order, Lat L, const float2 *U, const float2 *Dsum,
                       const float *Bsum, const float2 *DE, const BatchField *tab, int nfields, cudaStream_t st);
 void launch_batch_add_e(int64_t n, const BatchField *tab, int nfields, cudaStream_t st);
 // Chebyshev coefficients of every field from its mass's bounds; sets

@@ -65,7 +65,7 @@ def test_batch_matches_single_field_updates(oracle):
                 assert s1["converged"] == 1
         info = b.info()
         assert info["fields_per_tile"] in (1, 2) and info["block_order"] in (0, 1)
-        assert info["candidate_ms"]["tile1_order0"] > 0 and info["candidate_ms"]["tile1_order1"] > 0
+        assert info["candidate_ms"]["tile1_2blocks_order0"] > 0 and info["candidate_ms"]["tile1_3blocks_order1"] > 0
         assert 1 <= len(info["schedule"]) <= 8
         for hb, hsg in zip(hs, singles):
             qb, ab = hb.download()
@@ -100,7 +100,7 @@ def test_graph_replay_equals_eager_launches(oracle):
             ba.Update(g, C, 1.0, use_graph=False)
             bb.Update(g, C, 1.0, use_graph=True)
         # same tuning choice is not guaranteed (timing); equal results only when equal
-        if ba.info()["fields_per_tile"] == bb.info()["fields_per_tile"] and \
+        if ba.info()["variant"] == bb.info()["variant"] and \
                 ba.info()["block_order"] == bb.info()["block_order"] and \
                 ba.info()["schedule"] == bb.info()["schedule"]:
             for x, y in zip(ha, hb):
@@ -161,7 +161,7 @@ def test_ensemble_of_uneven_members_matches_member_steps(oracle):
             la, ea = ga[m]
             lb, eb = gb[m]
             assert np.array_equal(la, lb) and np.array_equal(ea, eb)
-            same = ia[m]["fields_per_tile"] == ib[m]["fields_per_tile"] and \
+            same = ia[m]["variant"] == ib[m]["variant"] and \
                 ia[m]["block_order"] == ib[m]["block_order"] and ia[m]["schedule"] == ib[m]["schedule"]
             for (qa, aa), (qb, ab) in zip(fa[m], fb[m]):
                 if same:
