@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--only-ensemble", action="store_true", help="print only the batching-ensemble JSON")
     p.add_argument("--only-forms", action="store_true", help="print only the CN-forms JSON")
     p.add_argument("--forms-sizes", type=int, nargs="+", default=list(FORMS_SIZES))
+    p.add_argument("--no-drift", action="store_true")
+    p.add_argument("--only-drift", action="store_true", help="print only the precision-drift JSON")
     return p.parse_args()
 
 
@@ -261,6 +263,76 @@ def measure_all_forms(steps, sizes=FORMS_SIZES):
     return res
 
 
+# ------------------------------------------------------------------ precision drift
+def measure_precision_drift(L, n0, steps, seed=1):
+    """The precision form end to end (FP32-link leapfrog with FP64
+    reunitarisation every 10 steps, FP32 Chebyshev CN with FP64 refinement
+    at 1e-10) against the FP64 path (FP64 leapfrog, plain FP64 CN at 1e-12)
+    from the same seeded fields: the drift of every observable after `steps`
+    coupled steps, and the s/step of both paths (CUDA events)."""
+    import torch
+    from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice
+    lib = _capi.load()
+    lat = lattice.Lattice((L, L, L), A)
+    cw = _capi.coeffs(WILSON)
+    out = {"lattice": [L, L, L], "n0": n0, "steps": steps}
+    try:
+        stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(lat.ctx))
+        paths = {}
+        for name, form, tol, prec in (("fp64", 0, 1e-12, 0), ("precision", 1, 1e-10, 1)):
+            g = GaugeConfiguration(lat=lat)
+            g.TransversePolarisedOccupiedInit_Box(0.5, n0, 0.0, RandomSeed=seed, identity_links=True)
+            if prec:
+                g.SetPrecision(1, 10)
+            h = NRQCDField(lat=lat)
+            h.InitSinglePoint(1, 1)
+            cn = ctypes.c_void_p()
+            _capi.check(lib.nrq_cn_init(lat.ctx, MASS, _capi.dptr(cw), 1.0, tol, 10000, form, ctypes.byref(cn)),
+                        lat.ctx, "nrq_cn_init")
+            e_start = g.GetEnergy()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                st = _capi.CnStats()
+                _capi.check(lib.nrq_heavy_update_cn(cn, h.handle, g.handle, MASS, _capi.dptr(cw), 1.0,
+                                                    ctypes.byref(st)), lat.ctx, "update")
+                g.Update(1.0)
+            e1.record(stream)
+            e1.synchronize()
+            paths[name] = {"g": g, "h": h, "cn": cn, "ms": e0.elapsed_time(e1) / steps, "e_start": e_start}
+        res = {}
+        for name, p in paths.items():
+            g, h = p["g"], p["h"]
+            en = g.GetEnergy()
+            gref, gmax = g._gauss()
+            res[name] = {"s_per_step": p["ms"] / 1000.0, "energy": en,
+                         "energy_drift_rel": abs(en - p["e_start"]) / abs(p["e_start"]),
+                         "gauss_max_norm": gmax, "norm_quark_minus_1": h.GetNorm_Quark() - 1.0,
+                         "norm_antiq_minus_1": h.GetNorm_AntiQ() - 1.0,
+                         "unitarity_max_dev": g.GetUnitarityDeviation()[0]}
+        la, ea = paths["fp64"]["g"].download()
+        lb, eb = paths["precision"]["g"].download()
+        qa, aa = paths["fp64"]["h"].download()
+        qb, ab = paths["precision"]["h"].download()
+        out["fp64"] = res["fp64"]
+        out["precision"] = res["precision"]
+        out["drift_vs_fp64"] = {
+            "energy_rel": abs(res["precision"]["energy"] - res["fp64"]["energy"]) / abs(res["fp64"]["energy"]),
+            "gauss_max_norm_abs": abs(res["precision"]["gauss_max_norm"] - res["fp64"]["gauss_max_norm"]),
+            "links_max_abs": float(np.abs(lb - la).max()), "efield_max_abs": float(np.abs(eb - ea).max()),
+            "propagator_max_abs": float(max(np.abs(qb - qa).max(), np.abs(ab - aa).max())),
+            "norm_abs": abs(res["precision"]["norm_quark_minus_1"] - res["fp64"]["norm_quark_minus_1"])}
+        out["speedup_coupled_step"] = res["fp64"]["s_per_step"] / res["precision"]["s_per_step"]
+        for p in paths.values():
+            lib.nrq_cn_finalize(p["cn"])
+            p["h"].Destructor()
+            p["g"].Deallocate()
+    finally:
+        lat.close()
+    return out
+
+
 # ------------------------------------------------------------------ batching ensemble
 # 8 members at 24^3, 4 at 32^3, 2 at 48^3; 16 point sources at random sites x
 # masses aM = 1.0 and 1.5 per member; precision-form CN at residual 1e-10
@@ -416,6 +488,13 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
+    if args.only_drift:
+        import torch
+        torch.cuda.set_device(local)
+        out = [measure_precision_drift(args.size, n0, 20) for n0 in (0.5, 1.0, 2.0)]
+        if rank == 0:
+            print(json.dumps({"precision_drift": out}), flush=True)
+        return
     if args.only_ensemble:
         import torch
         torch.cuda.set_device(local)
@@ -518,6 +597,10 @@ def main():
     if not args.no_ensemble and world == 1:
         ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2)
 
+    drift = None
+    if not args.no_drift and world == 1:
+        drift = [measure_precision_drift(L, n0, 20) for n0 in (0.5, 1.0, 2.0)]
+
     forms = None
     if not args.no_forms and world == 1:
         forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
@@ -550,6 +633,7 @@ def main():
             "clocks": clk, "e2e": e2e, "gpu_launches": int(sum(v["launches"] for v in prof.values())),
             "cn_forms_at_1e-10": forms,
             "batching_ensemble": ensemble,
+            "precision_drift": drift,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(min(L, 64))

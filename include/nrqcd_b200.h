@@ -103,6 +103,16 @@ int nrq_gauge_transverse_box_init(nrq_gauge *g, double saturation_scale, double 
                                   double coupling, int64_t seed, int identity_links);
 /* Update_Leapfrog(StepWidth), src/gaugeconfiguration_su3.f90:2082-2111 */
 int nrq_gauge_update(nrq_gauge *g, double stepwidth);
+/* Precision form of the leapfrog (no reference counterpart; the reference
+ * is FP64 throughout, src/precision.f90:20).  prec = 1: the links evolve in
+ * FP32 storage (staple products in FP32, staple sums, force projection and
+ * Ẽ in FP64, group exponential in FP64), with an FP64 reunitarisation onto
+ * SU(3) every reunit_every steps.  Energy, Gauss law, downloads and the CN
+ * step read the FP64 view of the links, refreshed on demand.  prec = 0 (the
+ * default) is the FP64 leapfrog.  Ensemble members must stay at prec 0.    */
+int nrq_gauge_set_precision(nrq_gauge *g, int prec, int reunit_every);
+/* max over sites and directions of |(U U^+ - 1)_ij| and of |det U - 1|     */
+int nrq_gauge_unitarity(nrq_gauge *g, double *max_dev, double *max_det_dev);
 /* GetEnergy, src/gaugeconfiguration_su3.f90:1769-1817 */
 int nrq_gauge_energy(nrq_gauge *g, double *energy);
 /* GetDeviationFromGaussLaw (:1480-1531) -> ref_measure, and the max-norm

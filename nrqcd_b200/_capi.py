@@ -70,6 +70,8 @@ SIGNATURES = {
     "nrq_gauge_transverse_box_init": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                                       ctypes.c_int64, ctypes.c_int]),
     "nrq_gauge_update": (ctypes.c_int, [_vp, ctypes.c_double]),
+    "nrq_gauge_set_precision": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "nrq_gauge_unitarity": (ctypes.c_int, [_vp, _dp, _dp]),
     "nrq_gauge_energy": (ctypes.c_int, [_vp, _dp]),
     "nrq_gauge_gauss": (ctypes.c_int, [_vp, _dp, _dp]),
     "nrq_heavy_create": (ctypes.c_int, [_vp, _pp]),

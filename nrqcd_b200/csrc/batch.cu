@@ -569,6 +569,14 @@ int check_inputs(nrq_cn_batch *b, const nrq_gauge *g, const double c[8]) {
     if (b->fields[i]->ctx != b->ctx || !b->fields[i]->P) return NRQ_ERR_BAD_ARG;
   return NRQ_OK;
 }
+// ensemble members step inside one graph: their leapfrog must be the FP64 one
+int check_member_gauge(nrq_cn_batch *b, const nrq_gauge *g) {
+  if (g->prec != 0) {
+    b->ctx->last_error = "ensemble: gauge fields in the FP32-link precision form are not supported";
+    return NRQ_ERR_BAD_ARG;
+  }
+  return NRQ_OK;
+}
 
 // one batch update (CN only), eager or as the batch's own graph
 int batch_update(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double dt, bool use_graph) {
@@ -620,7 +628,7 @@ extern "C" int nrq_cn_batch_update(nrq_cn_batch *b, const nrq_gauge *g, const do
                                    nrq_cn_stats *stats) {
   int rc = check_inputs(b, g, c);
   if (rc) return rc;
-  if ((rc = set_device(b->ctx))) return rc;
+  if ((rc = set_device(b->ctx)) || (rc = nrqh::gauge_sync64(g))) return rc;
   rc = batch_update(b, g, c, dt, use_graph != 0);
   fill_stats(b, stats);
   return rc;
@@ -686,6 +694,7 @@ extern "C" int nrq_ensemble_step(nrq_ensemble *e, const double c[8], double dt, 
   const int n = (int)e->batches.size();
   for (int i = 0; i < n; ++i) {
     int rc = check_inputs(e->batches[i], e->gauges[i], c);
+    if (!rc) rc = check_member_gauge(e->batches[i], e->gauges[i]);
     if (rc) return rc;
   }
   nrq_ctx *ctx0 = e->batches[0]->ctx;

@@ -199,7 +199,29 @@ nrq::CnCoef make_coef(const nrq_ctx *ctx, double mass, const double c_[8], doubl
   return C;
 }
 
+int gauge_sync64(const nrq_gauge *gc) {
+  nrq_gauge *g = const_cast<nrq_gauge *>(gc);
+  if (g->prec != 1 || !g->stale64) return NRQ_OK;
+  const int64_t n = 27 * g->ctx->lat.V;
+  nrq::k_links_widen<<<(unsigned)((n + 255) / 256), 256, 0, g->ctx->stream>>>(n, g->U32, g->U);
+  int rc = check_launch(g->ctx, "k_links_widen");
+  if (!rc) g->stale64 = false;
+  return rc;
+}
 }  // namespace nrqh
+
+namespace {
+// after the FP64 links were written: refresh the FP32 links of the precision form
+int gauge_written64(nrq_gauge *g) {
+  if (g->prec != 1) return NRQ_OK;
+  const int64_t n = 27 * g->ctx->lat.V;
+  nrq::k_links_narrow<<<(unsigned)((n + 255) / 256), 256, 0, g->ctx->stream>>>(n, g->U, g->U32);
+  g->stale64 = false;
+  g->since_reunit = 0;
+  return check_launch(g->ctx, "k_links_narrow");
+}
+}  // namespace
+using nrqh::gauge_sync64;
 
 // ====================================================================== context
 extern "C" const char *nrq_status_string(int s) {
@@ -355,6 +377,7 @@ extern "C" int nrq_gauge_destroy(nrq_gauge *g) {
   cudaStreamSynchronize(g->ctx->stream);
   if (g->U) cudaFree(g->U);
   if (g->E) cudaFree(g->E);
+  if (g->U32) cudaFree(g->U32);
   delete g;
   return NRQ_OK;
 }
@@ -373,7 +396,8 @@ extern "C" int nrq_gauge_upload(nrq_gauge *g, const double *links, const double 
   NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_stage, efield, sizeof(double) * 24 * V, cudaMemcpyHostToDevice,
                                     ctx->stream));
   nrq::k_efield_f2soa<<<nblk(V, 128), 128, 0, ctx->stream>>>((const double *)ctx->d_stage, g->E, V);
-  return check_launch(ctx, "k_efield_f2soa");
+  if ((rc = check_launch(ctx, "k_efield_f2soa"))) return rc;
+  return gauge_written64(g);
 }
 
 extern "C" int nrq_gauge_download(const nrq_gauge *g, double *links, double *efield) {
@@ -382,6 +406,7 @@ extern "C" int nrq_gauge_download(const nrq_gauge *g, double *links, double *efi
   const int64_t V = ctx->lat.V;
   int rc = set_device(ctx);
   if (!rc) rc = ensure_stage(ctx, sizeof(double2) * 27 * V);
+  if (!rc) rc = gauge_sync64(g);
   if (rc) return rc;
   nrq::k_links_soa2f<<<nblk(V, 128), 128, 0, ctx->stream>>>(g->U, (double2 *)ctx->d_stage, V);
   if ((rc = check_launch(ctx, "k_links_soa2f"))) return rc;
@@ -401,10 +426,11 @@ extern "C" int nrq_gauge_copy(nrq_gauge *dst, const nrq_gauge *src) {
   nrq_ctx *ctx = dst->ctx;
   const int64_t V = ctx->lat.V;
   int rc = set_device(ctx);
+  if (!rc) rc = gauge_sync64(src);
   if (rc) return rc;
   NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(dst->U, src->U, sizeof(double2) * 27 * V, cudaMemcpyDeviceToDevice, ctx->stream));
   NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(dst->E, src->E, sizeof(double) * 24 * V, cudaMemcpyDeviceToDevice, ctx->stream));
-  return NRQ_OK;
+  return gauge_written64(dst);
 }
 
 extern "C" int nrq_gauge_cold_init(nrq_gauge *g) {
@@ -413,7 +439,8 @@ extern "C" int nrq_gauge_cold_init(nrq_gauge *g) {
   int rc = set_device(ctx);
   if (rc) return rc;
   nrq::k_cold<<<nblk(ctx->lat.V, 256), 256, 0, ctx->stream>>>(g->U, g->E, ctx->lat.V);
-  return check_launch(ctx, "k_cold");
+  if ((rc = check_launch(ctx, "k_cold"))) return rc;
+  return gauge_written64(g);
 }
 
 extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, double coupling, int64_t seed,
@@ -495,7 +522,7 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
     ctx->last_error = "transverse_box_init: FFT or kernel failure";
     return NRQ_ERR_CUDA;
   }
-  return NRQ_OK;
+  return gauge_written64(g);
 }
 
 extern "C" int nrq_gauge_update(nrq_gauge *g, double dt) {
@@ -505,13 +532,24 @@ extern "C" int nrq_gauge_update(nrq_gauge *g, double dt) {
   if (rc) return rc;
   const unsigned nb_ = nblk(ctx->lat.V, 128);
   const double V = (double)ctx->lat.V;
+  const bool p32 = g->prec == 1;
   auto links = [&]() {
-    ProfScope ps(ctx, 4, V * (192.0 + 432.0 + 432.0));
-    nrq::k_update_links<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+    if (p32) {
+      ProfScope ps(ctx, 4, V * (192.0 + 216.0 + 216.0));
+      nrq::k_update_links32<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U32, g->E, dt);
+    } else {
+      ProfScope ps(ctx, 4, V * (192.0 + 432.0 + 432.0));
+      nrq::k_update_links<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+    }
   };
   auto efield = [&]() {
-    ProfScope ps(ctx, 5, V * (432.0 + 192.0 + 192.0));
-    nrq::k_update_efield<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+    if (p32) {
+      ProfScope ps(ctx, 5, V * (216.0 + 192.0 + 192.0));
+      nrq::k_update_efield32<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U32, g->E, dt);
+    } else {
+      ProfScope ps(ctx, 5, V * (432.0 + 192.0 + 192.0));
+      nrq::k_update_efield<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+    }
   };
   // Update_Leapfrog ordering (gauge:2100-2110)
   if (dt > 0) {
@@ -521,7 +559,55 @@ extern "C" int nrq_gauge_update(nrq_gauge *g, double dt) {
     efield();
     links();
   }
-  return check_launch(ctx, "leapfrog");
+  if ((rc = check_launch(ctx, "leapfrog"))) return rc;
+  if (p32) {
+    g->stale64 = true;
+    if (++g->since_reunit >= g->reunit_every) {  // FP64 reunitarisation
+      ProfScope ps(ctx, 4, V * (216.0 + 432.0 + 216.0));
+      nrq::k_reunitarise<<<nblk(ctx->lat.V, 128), 128, 0, ctx->stream>>>(ctx->lat.V, g->U32, g->U);
+      g->since_reunit = 0;
+      g->stale64 = false;
+      rc = check_launch(ctx, "k_reunitarise");
+    }
+  }
+  return rc;
+}
+
+extern "C" int nrq_gauge_set_precision(nrq_gauge *g, int prec, int reunit_every) {
+  if (!g || prec < 0 || prec > 1 || (prec == 1 && reunit_every < 1)) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  if (prec == g->prec) {
+    if (prec == 1) g->reunit_every = reunit_every;
+    return NRQ_OK;
+  }
+  if (prec == 1) {
+    if (!g->U32) NRQ_CUDA_TRY(ctx, cudaMalloc(&g->U32, sizeof(float2) * 27 * ctx->lat.V));
+    g->prec = 1;
+    g->reunit_every = reunit_every;
+    return gauge_written64(g);
+  }
+  if ((rc = gauge_sync64(g))) return rc;  // back to FP64: the FP64 view becomes the state
+  g->prec = 0;
+  g->stale64 = false;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_gauge_unitarity(nrq_gauge *g, double *max_dev, double *max_det_dev) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  int rc = set_device(ctx);
+  if (!rc) rc = gauge_sync64(g);
+  if (rc) return rc;
+  const int64_t nb_ = nblk(ctx->lat.V, 256);
+  if ((rc = ensure_red(ctx, nb_ * 2))) return rc;
+  nrq::k_unitarity<<<(unsigned)nb_, 256, 0, ctx->stream>>>(ctx->lat, g->U, ctx->d_red);
+  if ((rc = check_launch(ctx, "k_unitarity"))) return rc;
+  if ((rc = reduce_to_host(ctx, nb_, 2, 3u))) return rc;
+  if (max_dev) *max_dev = ctx->h_res[0];
+  if (max_det_dev) *max_det_dev = ctx->h_res[1];
+  return NRQ_OK;
 }
 
 extern "C" int nrq_gauge_energy(nrq_gauge *g, double *energy) {
@@ -531,6 +617,7 @@ extern "C" int nrq_gauge_energy(nrq_gauge *g, double *energy) {
   if (rc) return rc;
   const int64_t nb_ = nblk(ctx->lat.V, 256);
   if ((rc = ensure_red(ctx, nb_ * 2))) return rc;
+  if ((rc = gauge_sync64(g))) return rc;
   nrq::k_energy<<<(unsigned)nb_, 256, 0, ctx->stream>>>(ctx->lat, g->U, g->E, ctx->d_red);
   if ((rc = check_launch(ctx, "k_energy"))) return rc;
   if ((rc = reduce_to_host(ctx, nb_, 1, 0u))) return rc;
@@ -545,6 +632,7 @@ extern "C" int nrq_gauge_gauss(nrq_gauge *g, double *ref_measure, double *max_no
   if (rc) return rc;
   const int64_t nb_ = nblk(ctx->lat.V, 256);
   if ((rc = ensure_red(ctx, nb_ * 2))) return rc;
+  if ((rc = gauge_sync64(g))) return rc;
   nrq::k_gauss<<<(unsigned)nb_, 256, 0, ctx->stream>>>(ctx->lat, g->U, g->E, ctx->d_red);
   if ((rc = check_launch(ctx, "k_gauss"))) return rc;
   if ((rc = reduce_to_host(ctx, nb_, 2, 2u))) return rc;
@@ -771,6 +859,8 @@ void fin(nrq_cn *cn, int stage) {
 }
 int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
   nrq_ctx *ctx = cn->ctx;
+  int rc = gauge_sync64(g);
+  if (rc) return rc;
   ProfScope ps(ctx, 3, (double)ctx->lat.V * (432.0 + 192.0));
   nrq::launch_cn_prepare(ctx->lat, g->U, g->E, cn->Dsum, cn->Bsum, cn->DE, ctx->stream);
   return check_launch(ctx, "k_cn_prepare");

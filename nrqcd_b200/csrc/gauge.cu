@@ -114,6 +114,199 @@ __global__ void __launch_bounds__(128) k_update_efield(Lat L, const double2 *__r
   }
 }
 
+// ------------------------------------------------------------ FP32 links
+// Precision form of the leapfrog: links stored in FP32 (27 float2 planes,
+// the same plane order), Ẽ kept in FP64.  Staple products run in FP32; their
+// sum over k, the force projection and Ẽ accumulate in FP64; the group
+// exponential is FP64 and the product exp(iẼdt)·U FP32.  FP64
+// reunitarisation (k_reunitarise) restores det U = 1 and U U^+ = 1.
+struct m3f {
+  float2 e[9];
+};
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ void cmacf_(float2 &acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, fmaf(-a.y, b.y, acc.x));
+  acc.y = fmaf(a.x, b.y, fmaf(a.y, b.x, acc.y));
+}
+// acc += a * conj(b)
+__device__ __forceinline__ void cmacf_nc(float2 &acc, float2 a, float2 b) {
+  acc.x = fmaf(a.x, b.x, fmaf(a.y, b.y, acc.x));
+  acc.y = fmaf(a.y, b.x, fmaf(-a.x, b.y, acc.y));
+}
+__device__ __forceinline__ m3f load_link32(const float2 *__restrict__ U, int64_t V, int64_t s, int d) {
+  m3f m;
+  const float2 *p = U + (int64_t)d * 9 * V + s;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) m.e[k] = __ldg(p + k * V);
+  return m;
+}
+__device__ __forceinline__ m3f mulf(const m3f &a, const m3f &b) {
+  m3f r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float2 acc = cmulf(a.e[i * 3], b.e[j]);
+      cmacf_(acc, a.e[i * 3 + 1], b.e[3 + j]);
+      cmacf_(acc, a.e[i * 3 + 2], b.e[6 + j]);
+      r.e[i * 3 + j] = acc;
+    }
+  return r;
+}
+// a * b^+
+__device__ __forceinline__ m3f mulf_nd(const m3f &a, const m3f &b) {
+  m3f r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) cmacf_nc(acc, a.e[i * 3 + k], b.e[j * 3 + k]);
+      r.e[i * 3 + j] = acc;
+    }
+  return r;
+}
+// a^+ * b
+__device__ __forceinline__ m3f mulf_dn(const m3f &a, const m3f &b) {
+  m3f r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        // conj(a[k][i]) * b[k][j]
+        const float2 x = a.e[k * 3 + i], y = b.e[k * 3 + j];
+        acc.x = fmaf(x.x, y.x, fmaf(x.y, y.y, acc.x));
+        acc.y = fmaf(x.x, y.y, fmaf(-x.y, y.x, acc.y));
+      }
+      r.e[i * 3 + j] = acc;
+    }
+  return r;
+}
+
+__global__ void __launch_bounds__(128) k_update_links32(Lat L, float2 *__restrict__ U, const double *__restrict__ E,
+                                                        double dt) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= L.V) return;
+  const int64_t V = L.V;
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) {
+    double al[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) al[a] = __ldg(E + (int64_t)(d * 8 + a) * V + s) * dt;
+    const m3 G = expi_herm(algebra_matrix(al));
+    m3f g;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g.e[k] = make_float2((float)G.e[k].re, (float)G.e[k].im);
+    const m3f r = mulf(g, load_link32(U, V, s, d));
+    float2 *p = U + (int64_t)d * 9 * V + s;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) p[k * V] = r.e[k];
+  }
+}
+
+__global__ void __launch_bounds__(128) k_update_efield32(Lat L, const float2 *__restrict__ U,
+                                                         double *__restrict__ E, double dt) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= L.V) return;
+  const int64_t V = L.V;
+#pragma unroll 1
+  for (int i = 0; i < 3; ++i) {
+    m3 sum = m3_zero();
+    const int64_t xpi = nb(L, s, i, +1);
+#pragma unroll 1
+    for (int k = 0; k < 3; ++k) {
+      if (k == i) continue;
+      const double r = L.a0 / L.a[k];
+      const double coef = dt * (r * r);
+      const int64_t xpk = nb(L, s, k, +1), xmk = nb(L, s, k, -1);
+      const int64_t xpimk = nb(L, xmk, i, +1);
+      // U staple  U_k(x+i) U_i(x+k)^+ U_k(x)^+ ; D staple  U_k(x+i-k)^+ U_i(x-k)^+ U_k(x-k)
+      const m3f su = mulf_nd(mulf_nd(load_link32(U, V, xpi, k), load_link32(U, V, xpk, i)), load_link32(U, V, s, k));
+      const m3f sd = mulf_dn(mulf(load_link32(U, V, xmk, i), load_link32(U, V, xpimk, k)), load_link32(U, V, xmk, k));
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        sum.e[m].re += coef * ((double)su.e[m].x + (double)sd.e[m].x);
+        sum.e[m].im += coef * ((double)su.e[m].y + (double)sd.e[m].y);
+      }
+    }
+    const m3f ui = load_link32(U, V, s, i);
+    m3 u;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) u.e[k] = {(double)ui.e[k].x, (double)ui.e[k].y};
+    const m3 ls = mul(u, sum);
+    cplx tr[8];
+    traces_with_generators(ls, tr);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      double *e = E + (int64_t)(i * 8 + a) * V + s;
+      *e = *e - 2.0 * tr[a].im;
+    }
+  }
+}
+
+// FP64 projection of every link onto SU(3): rows 0 and 1 orthonormalised
+// (Gram-Schmidt), row 2 = conj(row0 x row1).  Reads the FP32 links, writes
+// the FP64 links and their FP32 rounding.
+__global__ void k_reunitarise(int64_t V, float2 *__restrict__ U32, double2 *__restrict__ U64) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= V) return;
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) {
+    cplx m[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float2 v = U32[(int64_t)(d * 9 + k) * V + s];
+      m[k] = {(double)v.x, (double)v.y};
+    }
+    double n0 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) n0 += norm2(m[c]);
+    n0 = 1.0 / sqrt(n0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m[c] = n0 * m[c];
+    cplx p = {0.0, 0.0};  // <row0, row1>
+#pragma unroll
+    for (int c = 0; c < 3; ++c) cmac_cj(p, m[c], m[3 + c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m[3 + c] = m[3 + c] - p * m[c];
+    double n1 = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) n1 += norm2(m[3 + c]);
+    n1 = 1.0 / sqrt(n1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m[3 + c] = n1 * m[3 + c];
+    // row2 = conj(row0 x row1)
+    m[6] = conj(m[1] * m[5] - m[2] * m[4]);
+    m[7] = conj(m[2] * m[3] - m[0] * m[5]);
+    m[8] = conj(m[0] * m[4] - m[1] * m[3]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int64_t o = (int64_t)(d * 9 + k) * V + s;
+      U64[o] = make_double2(m[k].re, m[k].im);
+      U32[o] = make_float2((float)m[k].re, (float)m[k].im);
+    }
+  }
+}
+
+__global__ void k_links_widen(int64_t n, const float2 *__restrict__ U32, double2 *__restrict__ U64) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float2 v = U32[i];
+  U64[i] = make_double2((double)v.x, (double)v.y);
+}
+__global__ void k_links_narrow(int64_t n, const double2 *__restrict__ U64, float2 *__restrict__ U32) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double2 v = U64[i];
+  U32[i] = make_float2((float)v.x, (float)v.y);
+}
+
 // ------------------------------------------------------------ reductions
 // Block-level sum of nq values per thread into partials[block*nq + q].
 template <int NQ>
@@ -335,6 +528,52 @@ __global__ void k_ic_write(Lat L, const double2 *__restrict__ A, const double2 *
     }
     m3 G = identity_links ? m3_id() : expi_herm(algebra_matrix(as));
     store_link(U, V, s, i, G);
+  }
+}
+
+// max over sites and directions of max_ij |(U U^+ - 1)_ij| and of |det U - 1|
+// (partials[block*2 + q], both maxima)
+__global__ void __launch_bounds__(256) k_unitarity(Lat L, const double2 *__restrict__ U, double *partials) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (s < L.V) {
+    for (int d = 0; d < 3; ++d) {
+      const m3 u = load_link(U, L.V, s, d);
+      const m3 p = mul_nd(u, u);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          const cplx e = p.e[i * 3 + j] - cplx{i == j ? 1.0 : 0.0, 0.0};
+          v[0] = fmax(v[0], hypot(e.re, e.im));
+        }
+      const cplx det = u.e[0] * (u.e[4] * u.e[8] - u.e[5] * u.e[7]) - u.e[1] * (u.e[3] * u.e[8] - u.e[5] * u.e[6]) +
+                       u.e[2] * (u.e[3] * u.e[7] - u.e[4] * u.e[6]);
+      v[1] = fmax(v[1], hypot(det.re - 1.0, det.im));
+    }
+  }
+  __shared__ double sh[32][2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v[0] = fmax(v[0], __shfl_down_sync(0xffffffffu, v[0], o));
+    v[1] = fmax(v[1], __shfl_down_sync(0xffffffffu, v[1], o));
+  }
+  if (lane == 0) {
+    sh[warp][0] = v[0];
+    sh[warp][1] = v[1];
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    double t0 = (lane < nw) ? sh[lane][0] : 0.0, t1 = (lane < nw) ? sh[lane][1] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t0 = fmax(t0, __shfl_down_sync(0xffffffffu, t0, o));
+      t1 = fmax(t1, __shfl_down_sync(0xffffffffu, t1, o));
+    }
+    if (lane == 0) {
+      partials[blockIdx.x * 2] = t0;
+      partials[blockIdx.x * 2 + 1] = t1;
+    }
   }
 }
 

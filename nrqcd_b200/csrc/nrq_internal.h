@@ -70,6 +70,14 @@ struct nrq_gauge {
   nrq_ctx *ctx = nullptr;
   double2 *U = nullptr;  // 27 planes of V complex: (dir*9 + row*3 + col)
   double *E = nullptr;   // 24 planes of V reals  : (dir*8 + a)
+  // precision form of the leapfrog (prec 1): the links evolve in U32 (FP32,
+  // same planes); U is their FP64 view, refreshed on demand (stale64) and
+  // replaced by the FP64 reunitarised links every reunit_every steps
+  float2 *U32 = nullptr;
+  int prec = 0;
+  int reunit_every = 10;
+  int since_reunit = 0;
+  bool stale64 = false;
 };
 
 struct nrq_heavy {
@@ -164,6 +172,8 @@ struct ChebSeg {
 ChebSeg cheb_segment(double tau, double lo, double hi);
 // |T_m(sigma)|: error reduction guaranteed by m Chebyshev steps
 double cheb_gain(std::complex<double> sigma, int m);
+// FP64 view of the links of g current (precision form: widen the FP32 links)
+int gauge_sync64(const nrq_gauge *g);
 // learned initial guess (learned.cu)
 bool learned_ready(const nrq_learn *net);
 // x = 2b - psi + w0 u + w1 v1 + w2 v2, hnew = the learned part (v1, v2 may be

@@ -13,6 +13,13 @@ __global__ void k_efield_soa2f(const double *__restrict__ E, double *__restrict_
 __global__ void k_cold(double2 *__restrict__ U, double *__restrict__ E, int64_t V);
 __global__ void k_update_links(Lat L, double2 *__restrict__ U, const double *__restrict__ E, double dt);
 __global__ void k_update_efield(Lat L, const double2 *__restrict__ U, double *__restrict__ E, double dt);
+// precision form of the leapfrog: FP32 links, FP64 Ẽ (gauge.cu)
+__global__ void k_update_links32(Lat L, float2 *__restrict__ U, const double *__restrict__ E, double dt);
+__global__ void k_update_efield32(Lat L, const float2 *__restrict__ U, double *__restrict__ E, double dt);
+__global__ void k_reunitarise(int64_t V, float2 *__restrict__ U32, double2 *__restrict__ U64);
+__global__ void k_links_widen(int64_t n, const float2 *__restrict__ U32, double2 *__restrict__ U64);
+__global__ void k_links_narrow(int64_t n, const double2 *__restrict__ U64, float2 *__restrict__ U32);
+__global__ void k_unitarity(Lat L, const double2 *__restrict__ U, double *partials);
 __global__ void k_energy(Lat L, const double2 *__restrict__ U, const double *__restrict__ E, double *partials);
 __global__ void k_gauss(Lat L, const double2 *__restrict__ U, const double *__restrict__ E, double *partials);
 __global__ void k_reduce_final(const double *__restrict__ partials, int64_t nblk, int nq, unsigned maxmask,

@@ -89,6 +89,17 @@ class GaugeConfiguration:
         self._call("nrq_gauge_update", float(StepWidth_))
 
     # --------------------------------------------------------------- observables
+    def SetPrecision(self, prec: int = 1, reunit_every: int = 10):
+        """prec 1: FP32 links in the leapfrog with FP64 reunitarisation every
+        reunit_every steps; prec 0: FP64 (the reference's precision)."""
+        self._call("nrq_gauge_set_precision", int(prec), int(reunit_every))
+
+    def GetUnitarityDeviation(self):
+        """(max |U U^+ - 1|, max |det U - 1|) over all links."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        self._call("nrq_gauge_unitarity", ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
     def GetEnergy(self) -> float:
         e = ctypes.c_double()
         self._call("nrq_gauge_energy", ctypes.byref(e))

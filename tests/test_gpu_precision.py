@@ -72,3 +72,68 @@ def test_precision_form_reversible(oracle):
             h.Update(g, 1.0, [1, 1, 1, 1], -1.0)
         q, an = h.download()
     assert np.abs(q - q0).max() < 1e-10 and np.abs(an - a0).max() < 1e-10
+
+
+def test_fp32_leapfrog_tracks_fp64_and_reunitarises(oracle):
+    """Precision form of the leapfrog (FP32 links, FP64 reunitarisation
+    every 10 steps) against the FP64 oracle on a hot 10^3 field."""
+    n = (10, 10, 10)
+    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 6, identity_links=False)
+    l0, e0 = links.copy(), ef.copy()
+    e_ref0 = oracle.energy(n, A, links, ef)
+    with lattice_ctx(n, A):
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        g.SetPrecision(1, 10)
+        dev = []
+        for step in range(1, 26):
+            g.Update(1.0)
+            oracle.gauge_update(n, A, links, ef, 1.0)
+            if step in (20, 25):
+                dev.append(g.GetUnitarityDeviation())
+        gl, ge = g.download()
+        en = g.GetEnergy()
+        gref, gmax = g._gauss()
+        g.SetPrecision(0)
+    # 25 steps: the FP32 rounding of the links propagates at ~1e-7 per step
+    assert np.abs(gl - links).max() < 2e-5 and np.abs(ge - ef).max() < 2e-5
+    e_ref = oracle.energy(n, A, links, ef)
+    assert abs(en - e_ref) <= 1e-5 * abs(e_ref)
+    assert abs(e_ref - e_ref0) <= 1e-3 * abs(e_ref0)  # the FP64 leapfrog's own drift, for scale
+    assert abs(gmax - oracle.gauss_maxnorm(n, A, links, ef)) < 1e-4
+    # right after the reunitarisation (step 20) the links are unitary to FP64
+    # rounding; five FP32 steps later to FP32 rounding
+    assert dev[0][0] < 1e-13 and dev[0][1] < 1e-13
+    assert dev[1][0] < 1e-5 and dev[1][1] < 1e-5
+    del l0, e0
+
+
+@pytest.mark.parametrize("n0", [0.5, 1.0, 2.0])
+def test_precision_form_drift_against_fp64_oracle(oracle, n0):
+    """Coupled steps of the whole precision form (FP32-link leapfrog, FP32
+    Chebyshev CN with FP64 refinement at 1e-10) against the FP64 oracle (GMRES
+    to 1e-14, FP64 leapfrog): the drift of every observable stays small."""
+    n = (8, 8, 8)
+    M, c = 1.0, [1, 1, 1, 1]
+    links, ef = oracle.transverse_box(n, A, 0.5, n0, 0.0, 2, identity_links=True)
+    q = oracle.single_point(n, 1)
+    an = oracle.single_point(n, 1)
+    with lattice_ctx(n, A, cn=(M, c, 1.0, 1e-10, 10000, FORM_PRECISION)):
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        g.SetPrecision(1, 10)
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        for _ in range(12):
+            st = h.Update(g, M, c, 1.0)
+            assert st["converged"] == 1
+            g.Update(1.0)
+            oracle.cn_update(n, A, links, ef, M, c, 1.0, q, an, tol=1e-14)
+            oracle.gauge_update(n, A, links, ef, 1.0)
+        gq, ga = h.download()
+        en = g.GetEnergy()
+        nq, na = h.GetNorm_Quark(), h.GetNorm_AntiQ()
+    e_ref = oracle.energy(n, A, links, ef)
+    assert abs(en - e_ref) <= 1e-5 * max(abs(e_ref), 1e-12)
+    assert np.abs(gq - q).max() < 1e-6 and np.abs(ga - an).max() < 1e-6
+    assert abs(nq - 1) < 1e-9 and abs(na - 1) < 1e-9
