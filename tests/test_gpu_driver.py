@@ -1,0 +1,61 @@
+"""GPU runs of the drop-in driver (modes 2 and 32 of the reference's
+`program simulation`), checked line by line against the FP64 oracle and the
+reference's output formats."""
+import re
+
+import numpy as np
+import pytest
+
+from nrqcd_b200 import driver
+
+pytestmark = pytest.mark.gpu
+
+E16 = r"[+-]0\.\d{9}E[+-]\d\d "
+E13 = r"[+-]0\.\d{6}E[+-]\d\d "
+
+
+def test_mode32_free_correlators_match_oracle(oracle, tmp_path):
+    n, a, M = (6, 6, 6), (0.05, 1.0, 1.0, 1.0), 1.0
+    fc, fn = tmp_path / "mesoncorrelators.txt", tmp_path / "norm.txt"
+    args = ["32", "6", "6", "6", "0.05", "1.0", "1.0", "1.0", "0.25", "1", "1e-12", "1.0",
+            "1.0", "0.0", "1.0", "0.0", "1.0", "0.0", "1.0", "0.0", str(fc), str(fn)]
+    driver.main(args)
+    corr = fc.read_text().splitlines()
+    norm = fn.read_text().splitlines()
+    assert corr[0] == driver.CORRELATOR_HEADER and norm[0] == driver.NORM_HEADER
+    assert len(corr) == 7 and len(norm) == 7  # s = 0 and 5 steps
+    for ln in corr[1:]:
+        assert re.fullmatch(f"(?:{E16}){{9}}", ln), ln
+    for ln in norm[1:]:
+        assert re.fullmatch(f"(?:{E16}){{3}}", ln), ln
+    links, ef = oracle.cold(n, a)
+    q, an = oracle.single_point(n, 1), oracle.single_point(n, 1)
+    for step in range(6):
+        if step > 0:
+            oracle.cn_update(n, a, links, ef, M, [1, 1, 1, 1], 1.0, q, an, tol=1e-14)
+            oracle.gauge_update(n, a, links, ef, 1.0)
+        ref = oracle.meson_correlators(n, q, an)
+        vals = [float(v) for v in corr[1 + step].split()]
+        assert abs(vals[0] - 0.05 * step) < 1e-9
+        got = [complex(vals[1 + 2 * k], vals[2 + 2 * k]) for k in range(4)]
+        for g_, key in zip(got, ("o1_1s0", "o1_3s1", "o8_1s0", "o8_3s1")):
+            assert abs(g_ - ref[key]) <= 1e-8 * max(1.0, abs(ref[key]))
+        nv = [float(v) for v in norm[1 + step].split()]
+        assert abs(nv[1] - oracle.heavy_norm(n, q)) < 1e-8 and abs(nv[2] - oracle.heavy_norm(n, an)) < 1e-8
+
+
+def test_mode2_energy_gauss_matches_oracle(oracle, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
+    n, a = (6, 6, 6), (0.05, 1.0, 1.0, 1.0)
+    driver.main(["2", "6", "6", "6", "0.05", "1.0", "1.0", "1.0", "0.0", "0.25", "3", "0.8", "1.0", "0.0"])
+    lines = (tmp_path / "energy_gauss.txt").read_text().splitlines()
+    assert len(lines) == 6
+    links, ef = oracle.transverse_box(n, a, 0.8, 1.0, 0.0, 3, identity_links=False)
+    for step, ln in enumerate(lines):
+        assert re.fullmatch(f"(?:{E13}){{3}}", ln), ln
+        t, en, gauss = (float(v) for v in ln.split())
+        e_ref = oracle.energy(n, a, links, ef)
+        assert abs(t - 0.05 * step) < 1e-9
+        assert abs(en - e_ref) <= 1e-6 * abs(e_ref)
+        assert abs(gauss - oracle.gauss_ref(n, a, links, ef)) <= 1e-6 * max(1.0, abs(e_ref))
+        oracle.gauge_update(n, a, links, ef, 1.0)
