@@ -561,6 +561,12 @@ def main():
     ms_per_step = ms / args.steps
     value = world * V * args.steps / (ms / 1000.0)
     norm_q, norm_a = h.GetNorm_Quark(), h.GetNorm_AntiQ()
+    tma = ctypes.c_int()
+    tune_ms = np.zeros(2)
+    _capi.check(lib.nrq_cn_stencil_info(nrqcd.solver_handle(), ctypes.byref(tma), _capi.dptr(tune_ms)), ctx,
+                "stencil_info")
+    stencil = {"in_use": "k_cn_mv3 (TMA-staged)" if tma.value else "k_cn_mv2 (register-tiled)",
+               "tuning_ms_per_launch": {"k_cn_mv2": float(tune_ms[0]), "k_cn_mv3_with_vec_s": float(tune_ms[1])}}
 
     # ---------------- end-to-end through the C ABI with host buffers
     e2e = None
@@ -619,13 +625,14 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(L, world),
-            "roofline": {"bound": "hbm", "kernel": "k_cn_mv (CN 12-column stencil)",
+            "roofline": {"bound": "hbm", "kernel": "CN 12-column stencil: " + stencil["in_use"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
                          "traffic": None,
                          "launches": sten["launches"], "avg_launch_ms": sten["ms"] / max(1, sten["launches"]),
                          "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9},
             "kernel_classes": prof,
+            "stencil": stencil,
             "cn": {"iterations_per_step": float(np.mean(its)) if its else None,
                    "matvecs_per_step": float(np.mean([s["matvecs"] for s in iters])) if iters else None,
                    "max_rel_residual": max(s["max_rel_residual"] for s in iters) if iters else None,

@@ -145,6 +145,10 @@ int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, 
                 int64_t maxits, int form, nrq_cn **cn);
 /* FinalizeModule, src/nrqcd.f90:199-212 */
 int nrq_cn_finalize(nrq_cn *cn);
+/* The stencil the solver uses (tma_staged = 1: TMA-staged, 0: register-
+ * tiled) and the per-launch milliseconds of both measured on its first
+ * update (-1 before it, or where only one applies).                      */
+int nrq_cn_stencil_info(const nrq_cn *cn, int *tma_staged, double ms[2]);
 /* NRQCDField%Update(GaugeConf, Mass, WilsonCoeffs, StepWidth) =
  * Update_CrankNicholson, src/nrqcd.f90:1053-1168: quark (+M, c) and
  * antiquark (-M, conj c); per column RHS = A psi, solve A^H psi' = RHS with

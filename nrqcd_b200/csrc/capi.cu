@@ -815,7 +815,19 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
     return NRQ_ERR_OOM;
   }
   NRQ_CUDA_TRY(ctx, cudaMemsetAsync(cn->scal, 0, kScalBytes, ctx->stream));
+  for (double2 *p : {cn->r, cn->v, cn->s})
+    NRQ_CUDA_TRY(ctx, cudaMemsetAsync(p, 0, sizeof(double2) * 72 * V, ctx->stream));
   *out = cn;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_stencil_info(const nrq_cn *cn, int *tma_staged, double ms[2]) {
+  if (!cn) return NRQ_ERR_BAD_ARG;
+  if (tma_staged) *tma_staged = cn->use_tma ? 1 : 0;
+  if (ms) {
+    ms[0] = cn->tune_ms[0];
+    ms[1] = cn->tune_ms[1];
+  }
   return NRQ_OK;
 }
 
@@ -857,6 +869,75 @@ void fin(nrq_cn *cn, int stage) {
   ProfScope ps(ctx, 2, (double)rows * 12 * 3 * 8);
   nrq::launch_cn_finalize(stage, rows, cn->partials, cn->scal, cn->tol, ctx->stream);
 }
+// Choose between the register-tiled and the TMA-staged stencil by timing,
+// on this lattice and field, the work each does in the solve: for the plain
+// form t = A^H (r - alpha v) (the register-tiled stencil forms s on the fly,
+// the TMA-staged one needs s materialised first); for the precision forms the
+// FP64 refinement residual.  Every buffer written here (s, t, the partials,
+// r32, d32) is rewritten by the solve before it is read.
+int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
+  nrq_ctx *ctx = cn->ctx;
+  cn->stencil_tuned = true;
+  if (!cn->use_tma) return NRQ_OK;  // only the register-tiled stencil applies
+  cudaStream_t st = ctx->stream;
+  const nrq::Lat L = ctx->lat;
+  const bool prof = ctx->prof;
+  ctx->prof = false;
+  cudaEvent_t e[3];
+  for (auto &x : e) NRQ_CUDA_TRY(ctx, cudaEventCreate(&x));
+  const int reps = 3;
+  auto run = [&](bool tma) {
+    for (int r = 0; r < reps + 1; ++r) {
+      if (r == 1) cudaEventRecord(tma ? e[1] : e[0], st);
+      nrq::MvArgs a{};
+      a.partials = cn->partials;
+      a.scal = cn->scal;
+      if (cn->form == 0) {
+        a.out = cn->t;
+        if (tma) {
+          nrq::launch_vec_s(L, cn->s, cn->r, cn->v, cn->scal, st);
+          a.in = cn->s;
+          nrq::launch_cn_mv3(nrq::MV_T, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, scal_err(cn->scal),
+                             ctx->sm_count, st);
+        } else {
+          a.in = cn->r;
+          a.in2 = cn->v;
+          nrq::launch_cn_mv(nrq::MV_T, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, st);
+        }
+      } else {
+        a.in = cn->x;
+        a.bvec = cn->b;
+        a.r32 = cn->r32;
+        a.d32 = cn->dA32;
+        if (tma)
+          nrq::launch_cn_mv3(nrq::MV_RESC, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, scal_err(cn->scal),
+                             ctx->sm_count, st);
+        else
+          nrq::launch_cn_mv(nrq::MV_RESC, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, st);
+      }
+    }
+  };
+  run(false);
+  cudaEventRecord(e[2], st);
+  run(true);
+  cudaEvent_t done;
+  cudaEventCreate(&done);
+  cudaEventRecord(done, st);
+  cudaEventSynchronize(done);
+  float ms_v2 = 0.f, ms_v3 = 0.f;
+  cudaEventElapsedTime(&ms_v2, e[0], e[2]);
+  cudaEventElapsedTime(&ms_v3, e[1], done);
+  for (auto &x : e) cudaEventDestroy(x);
+  cudaEventDestroy(done);
+  ctx->prof = prof;
+  int rc = check_launch(ctx, "stencil tuning");
+  if (rc) return rc;
+  cn->tune_ms[0] = ms_v2 / reps;
+  cn->tune_ms[1] = ms_v3 / reps;
+  cn->use_tma = cn->tune_ms[1] < cn->tune_ms[0];
+  return NRQ_OK;
+}
+
 int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
   nrq_ctx *ctx = cn->ctx;
   int rc = gauge_sync64(g);
@@ -939,6 +1020,7 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
   }
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (learned && (rc = nrqh::learned_check(cn->learn))) return rc;
+  if (!cn->stencil_tuned && (rc = tune_stencil(cn, CH, g))) return rc;
   ChebSeg seg[2];
   for (int sp = 0; sp < 2; ++sp) {
     double lo = cn->h_bounds[2 * sp], hi = cn->h_bounds[2 * sp + 1];
@@ -1088,6 +1170,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   const nrq::CnCoef CA = make_coef(ctx, mass, c, dt, false);
   const nrq::CnCoef CH = make_coef(ctx, mass, c, dt, true);
   if ((rc = cn_prepare(cn, g))) return rc;
+  if (!cn->stencil_tuned && (rc = tune_stencil(cn, CH, g))) return rc;
   int64_t matvecs = 0, vstreams = 0;
   // RHS = A psi ; extrapolated start x0 = 2 RHS - psi
   {

@@ -124,8 +124,11 @@ struct nrq_cn {
   // Krylov vectors, 72 planes each
   double2 *b = nullptr, *x = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr,
           *t = nullptr, *s = nullptr;
-  // TMA-staged stencil usable for this lattice (else the register-tiled one)
+  // TMA-staged stencil in use (else the register-tiled one); chosen by timing
+  // both on the first update (tune_ms: register-tiled, TMA-staged)
   bool use_tma = false;
+  bool stencil_tuned = false;
+  double tune_ms[2] = {-1.0, -1.0};
   // precision form (form 1): FP32 copies of the per-step matrices and the
   // FP32 Chebyshev vectors; spectral bounds of the hermitian part
   float2 *U32 = nullptr, *DE32 = nullptr, *D32 = nullptr;
