@@ -565,6 +565,8 @@ def main():
     tune_ms = np.zeros(2)
     _capi.check(lib.nrq_cn_stencil_info(nrqcd.solver_handle(), ctypes.byref(tma), _capi.dptr(tune_ms)), ctx,
                 "stencil_info")
+    p64, p32 = ctypes.c_double(), ctypes.c_double()
+    _capi.check(lib.nrq_measure_peaks(ctx, ctypes.byref(p64), ctypes.byref(p32)), ctx, "measure_peaks")
     stencil = {"in_use": "k_cn_mv3 (TMA-staged)" if tma.value else "k_cn_mv2 (register-tiled)",
                "tuning_ms_per_launch": {"k_cn_mv2": float(tune_ms[0]), "k_cn_mv3_with_vec_s": float(tune_ms[1])}}
 
@@ -618,6 +620,11 @@ def main():
             peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
         sten = prof["cn_stencil"]
         achieved = sten["bytes"] / (sten["ms"] / 1000.0) / 1e9 if sten["ms"] > 0 else None
+        # FP64 arithmetic of one 12-column stencil launch per site: 2 species x
+        # (6 neighbours x 6 columns x 36 + 6 columns x 18) complex FMAs (4 DFMA
+        # each, 2 flops per DFMA) plus the block assembly (~270 complex FMAs)
+        flops_site = 2 * (6 * 6 * 36 + 6 * 18 + 270) * 4 * 2
+        fp64_achieved = flops_site * V * sten["launches"] / (sten["ms"] / 1000.0) / 1e12 if sten["ms"] > 0 else None
         step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
         its = [s["iterations"] for s in iters]
         line = {
@@ -630,7 +637,11 @@ def main():
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
                          "traffic": None,
                          "launches": sten["launches"], "avg_launch_ms": sten["ms"] / max(1, sten["launches"]),
-                         "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9},
+                         "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9,
+                         "fp64": {"flops_per_site_per_launch": flops_site, "achieved_tflops": fp64_achieved,
+                                  "peak_tflops": p64.value, "peak_source": "measured (FP64 FMA probe)",
+                                  "frac": fp64_achieved / p64.value if fp64_achieved else None,
+                                  "fp32_packed_peak_tflops": p32.value}},
             "kernel_classes": prof,
             "stencil": stencil,
             "cn": {"iterations_per_step": float(np.mean(its)) if its else None,

@@ -87,6 +87,10 @@ void *nrq_cuda_stream(nrq_ctx *ctx);
 enum { NRQ_PROF_CLASSES = 6 };
 int nrq_profile_enable(nrq_ctx *ctx, int enable);
 int nrq_profile_read(nrq_ctx *ctx, int64_t launches[6], double milliseconds[6], double bytes[6]);
+/* Measured arithmetic peaks of this device (TFLOP/s): FP64 FMA and packed
+ * FP32 FMA throughput of issue-bound probe kernels (compute-side roofline
+ * denominators of the benchmark).                                         */
+int nrq_measure_peaks(nrq_ctx *ctx, double *fp64_tflops, double *fp32_tflops);
 
 /* ---- gauge configuration: src/gaugeconfiguration_su3.f90:33-116 -------- */
 int nrq_gauge_create(nrq_ctx *ctx, nrq_gauge **g);      /* Allocate (:124-140)   */
