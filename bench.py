@@ -181,11 +181,12 @@ FORMS_SIZES = (64, 96, 128)
 
 def train_learned(tol=1e-10):
     """The learned form's network, trained on seeded 32^3 solves (2
-    configurations x 8 steps); the parameters load into any lattice size."""
+    configurations x masses aM = 1.0 and 1.5 (the ensemble's) x 8 steps); the
+    parameters load into any lattice size."""
     from nrqcd_b200.learned import train_on_seeded_configs
     t0 = time.perf_counter()
-    params, info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=8, mass=MASS, WilsonCoeffs=WILSON,
-                                           spacings=A, tol=tol, iterations=800)
+    params, info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=8, masses=(MASS, 1.5),
+                                           WilsonCoeffs=WILSON, spacings=A, tol=tol, iterations=1000)
     info["wall_s"] = time.perf_counter() - t0
     return params, info
 
@@ -255,8 +256,8 @@ def measure_cn_forms(L, steps, params, tol=1e-10, seed=1):
     return out
 
 
-def measure_all_forms(steps, sizes=FORMS_SIZES):
-    params, info = train_learned()
+def measure_all_forms(steps, sizes=FORMS_SIZES, learned=None):
+    params, info = train_learned() if learned is None else learned
     res = {"learned_training": info}
     for L in sizes:
         res[f"{L}^3"] = measure_cn_forms(L, steps, params)
@@ -341,7 +342,7 @@ ENS_SOURCES = 16
 ENS_MASSES = (1.0, 1.5)
 
 
-def measure_ensemble(steps, warmup, tol=1e-10):
+def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
     """Aggregate field-site updates/s of the uneven ensemble: one CUDA graph
     launch per coupled step, the same batched launches issued eagerly, and a
     serial loop of single-field precision-form updates (nrq_heavy_update_cn
@@ -398,6 +399,25 @@ def measure_ensemble(steps, warmup, tol=1e-10):
     for L in lats:
         _capi.profile_enable(lats[L].ctx, False)
     info = {L: b.info() for (L, _, _, _), b in zip(members, batches)}
+    # forms combined: every batch starts its solves from the learned guess
+    t_learned, info_learned, learned_stats = None, None, []
+    if learned_params is not None:
+        from nrqcd_b200.learned import LearnedGuess
+        nets = {}
+        for L in lats:
+            nets[L] = LearnedGuess(lat=lats[L])
+            nets[L].params = learned_params
+            nets[L].set_trained(True)
+        for (L, _, _, _), b in zip(members, batches):
+            b.attach_learned(nets[L])
+        for _ in range(max(4, warmup + 2)):  # history fills (depth 0, 1, 2), then calibration and capture
+            ens.Step(WILSON, 1.0, use_graph=True)
+        t_learned = timed(lambda: learned_stats.append(ens.Step(WILSON, 1.0, use_graph=True)), steps)
+        info_learned = {L: b.info() for (L, _, _, _), b in zip(members, batches)}
+        for b in batches:
+            b.attach_learned(None)
+        for net in nets.values():
+            net.Destructor()
     ens.Destructor()
     for b in batches:
         b.Destructor()
@@ -441,6 +461,11 @@ def measure_ensemble(steps, warmup, tol=1e-10):
         "serial_single_field": {"s_per_step": t_serial, "field_site_updates_per_s": per_step / t_serial,
                                 "steps": serial_steps, "max_rel_residual": max(serial_stats)},
         "speedup_graph_vs_serial": t_serial / t_graph,
+        "graph_learned_guess": None if t_learned is None else {
+            "s_per_step": t_learned, "field_site_updates_per_s": per_step / t_learned,
+            "speedup_vs_serial": t_serial / t_learned,
+            "max_rel_residual": max(st["max_rel_residual"] for st in learned_stats),
+            "schedules": {f"{L}^3": v["schedule"] for L, v in info_learned.items()}},
         "max_rel_residual": max(s["max_rel_residual"] for s in stats),
         "converged": all(s["converged"] == 1 for s in stats),
         "tuning": {f"{L}^3": v for L, v in info.items()},
@@ -498,7 +523,7 @@ def main():
     if args.only_ensemble:
         import torch
         torch.cuda.set_device(local)
-        out = measure_ensemble(args.steps, args.warmup)
+        out = measure_ensemble(args.steps, args.warmup, learned_params=train_learned()[0])
         if rank == 0:
             print(json.dumps({"batching_ensemble": out}), flush=True)
         return
@@ -601,9 +626,10 @@ def main():
                "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
                        "nrq_heavy_download + nrq_gauge_download, pinned host buffers"}
 
+    learned = train_learned() if world == 1 and not (args.no_ensemble and args.no_forms) else None
     ensemble = None
     if not args.no_ensemble and world == 1:
-        ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2)
+        ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2, learned_params=learned[0])
 
     drift = None
     if not args.no_drift and world == 1:
@@ -611,7 +637,7 @@ def main():
 
     forms = None
     if not args.no_forms and world == 1:
-        forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
+        forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes), learned=learned)
 
     if rank == 0:
         peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")

@@ -196,6 +196,13 @@ int nrq_cn_batch_destroy(nrq_cn_batch *batch);
  * field, max_rel_residual = max over fields and columns.                    */
 int nrq_cn_batch_update(nrq_cn_batch *batch, const nrq_gauge *g, const double c[8], double stepwidth,
                         int use_graph, nrq_cn_stats *stats);
+/* Start every field's solve from the learned guess of `net` (a network of
+ * the same context, see nrq_learn_*; NULL detaches).  The fields keep their
+ * two-step history as with nrq_heavy_update_cn in form 2; the schedule is
+ * recalibrated while the history fills (depth 0, 1, 2).  Declared in the
+ * learned-guess section below.                                            */
+struct nrq_learn;
+int nrq_cn_batch_attach_learned(nrq_cn_batch *batch, struct nrq_learn *net);
 /* Relative residual ||b - A^H x|| / ||b|| of every field (max over its 12
  * columns) after the last update, in the order of `fields`.                 */
 int nrq_cn_batch_residuals(const nrq_cn_batch *batch, double *rel);

@@ -95,6 +95,7 @@ SIGNATURES = {
     "nrq_cn_batch_update": (ctypes.c_int, [_vp, _vp, _dp, ctypes.c_double, ctypes.c_int,
                                            ctypes.POINTER(CnStats)]),
     "nrq_cn_batch_residuals": (ctypes.c_int, [_vp, _dp]),
+    "nrq_cn_batch_attach_learned": (ctypes.c_int, [_vp, _vp]),
     "nrq_cn_batch_info": (ctypes.c_int, [_vp, _ip, _ip, _dp, _ip, _ip]),
     "nrq_ensemble_create": (ctypes.c_int, [ctypes.c_int, _pp, _pp, _pp]),
     "nrq_ensemble_destroy": (ctypes.c_int, [_vp]),

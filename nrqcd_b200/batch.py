@@ -63,6 +63,13 @@ class CNBatch:
         _capi.check(rc, self._ctx, "nrq_cn_batch_update")
         return self.last_stats
 
+    def attach_learned(self, net):
+        """Start every field's solve from the learned guess of ``net`` (a
+        trained nrqcd_b200.learned.LearnedGuess of the same lattice; None
+        detaches)."""
+        handle = net.handle if net is not None else None
+        _capi.check(_capi.load().nrq_cn_batch_attach_learned(self._h, handle), self._ctx, "attach_learned")
+
     def residuals(self) -> np.ndarray:
         out = np.zeros(len(self.fields))
         _capi.check(_capi.load().nrq_cn_batch_residuals(self._h, _capi.dptr(out)), self._ctx, "residuals")

@@ -72,6 +72,12 @@ struct nrq_cn_batch {
   cudaGraphExec_t exec = nullptr;
   uint64_t exec_gen = 0;
   const nrq_gauge *exec_g = nullptr;
+  // learned initial guess (attached network, per-batch scratch) and the
+  // history depth the schedule was calibrated for
+  nrq_learn *learn = nullptr;
+  float4 *lgf = nullptr, *lomega = nullptr;
+  float *lfeat = nullptr;
+  int key_depth = -1;
   // statistics of the last update
   int64_t last_inner = 0, last_passes = 0, last_matvecs = 0;
   double last_maxrel = 0.0, last_initial = 0.0;
@@ -97,8 +103,18 @@ void free_graph(cudaGraphExec_t &g) {
   g = nullptr;
 }
 
+bool learned_on(const nrq_cn_batch *b) { return b->learn && nrqh::learned_ready(b->learn); }
+
+// history depth of the learned guess (every field's count, capped at 2), -1 without it
+int depth_of(const nrq_cn_batch *b) {
+  if (!learned_on(b)) return -1;
+  int d = 2;
+  for (const nrq_heavy *h : b->fields) d = std::min(d, h->hist_count);
+  return d;
+}
+
 bool same_key(const nrq_cn_batch *b, const double c[8], double dt) {
-  if (!b->have_key || b->key_dt != dt) return false;
+  if (!b->have_key || b->key_dt != dt || b->key_depth != depth_of(b)) return false;
   for (int k = 0; k < 8; ++k)
     if (b->key_c[k] != c[k]) return false;
   return true;
@@ -126,6 +142,13 @@ void fill_table(nrq_cn_batch *b, const double c[8], double dt) {
     f.scal = b->scal_all + (int64_t)i * kFieldScal;
     f.bounds = b->bounds + 4 * b->mass_of[i];
     f.tau = dt * ctx->a[0] / 2.0;
+    f.mass = m;
+    if (learned_on(b)) {
+      nrq_heavy *h = b->fields[i];
+      f.h1 = hist_v1(h);
+      f.h2 = hist_v2(h);
+      f.hnew = hist_next(h);
+    }
   }
 }
 
@@ -162,11 +185,19 @@ int enq_prepare(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double d
   return check_launch(ctx, "batch prepare");
 }
 
-int enq_rhs(nrq_cn_batch *b, cudaStream_t st) {
+// b = A psi and the start x (2b - psi, or the learned guess)
+int enq_rhs(nrq_cn_batch *b, const nrq_gauge *g, cudaStream_t st) {
   nrq_ctx *ctx = b->ctx;
-  ProfScope ps(ctx, 0, (double)ctx->lat.V * (b->nf * 1152.0 * 3 + 432.0 + 192.0));
-  nrq::launch_batch_mv(nrq::MV_RHS, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, st);
-  return check_launch(ctx, "batch rhs");
+  {
+    ProfScope ps(ctx, 0, (double)ctx->lat.V * (b->nf * 1152.0 * 3 + 432.0 + 192.0));
+    nrq::launch_batch_mv(nrq::MV_RHS, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, st);
+  }
+  int rc = check_launch(ctx, "batch rhs");
+  if (!rc && learned_on(b)) {
+    ProfScope ps(ctx, 3, (double)ctx->lat.V * b->nf * (1152.0 * 4 + 576.0 * 5 + 128.0));
+    rc = nrqh::learned_guess_batch(b->learn, ctx, b->d_tab, b->nf, b->U64, g->E, b->lgf, b->lfeat, b->lomega, st);
+  }
+  return rc;
 }
 
 // r = b - A^H x (FP64) of every field, FP32 copies r32 and d = r/theta, and
@@ -214,7 +245,7 @@ int enq_readback(nrq_cn_batch *b, cudaStream_t st) {
 // check and its read-back
 int enq_scheduled(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double dt, cudaStream_t st) {
   int rc = enq_prepare(b, g, c, dt, st);
-  if (!rc) rc = enq_rhs(b, st);
+  if (!rc) rc = enq_rhs(b, g, st);
   for (size_t p = 0; !rc && p < b->schedule.size(); ++p) {
     rc = enq_residual(b, st);
     if (!rc) rc = enq_inner(b, b->schedule[p], st);
@@ -345,7 +376,7 @@ int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], dou
                                     cudaMemcpyDeviceToHost, st));
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (!b->tuned && (rc = autotune(b, st))) return rc;
-  if ((rc = enq_rhs(b, st)) || (rc = enq_residual(b, st)) || (rc = enq_readback(b, st))) return rc;
+  if ((rc = enq_rhs(b, g, st)) || (rc = enq_residual(b, st)) || (rc = enq_readback(b, st))) return rc;
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   chk = check(b);
   b->last_initial = chk.worst;
@@ -353,6 +384,7 @@ int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], dou
   if ((rc = refine_adaptive(b, dt, st, kMaxPasses, used, chk))) return rc;
   b->schedule = used;
   b->have_key = true;
+  b->key_depth = depth_of(b);
   b->key_dt = dt;
   std::memcpy(b->key_c, c, sizeof(b->key_c));
   b->gen++;
@@ -381,10 +413,13 @@ int finish_step(nrq_cn_batch *b, double dt, cudaStream_t st, Check &chk, bool *s
 }
 
 int conclude(nrq_cn_batch *b, const Check &chk, int64_t inner, int64_t passes) {
-  // results: the iterate becomes the field, the old field the next work buffer
+  // results: the iterate becomes the field, the old field the next work
+  // buffer; a learned step leaves the new history in the field
+  const bool keep = learned_on(b) && chk.conv && !chk.nonfin && !chk.badbounds;
   for (int i = 0; i < b->nf; ++i) {
     std::swap(b->fields[i]->P, b->xbuf[i]);
-    b->fields[i]->hist_count = 0;
+    if (keep) hist_push(b->fields[i]);
+    else b->fields[i]->hist_count = 0;
   }
   b->last_inner = inner;
   b->last_passes = passes;
@@ -547,7 +582,8 @@ extern "C" int nrq_cn_batch_destroy(nrq_cn_batch *b) {
   for (void *p : {(void *)b->U64, (void *)b->Dsum, (void *)b->Bsum, (void *)b->DE, (void *)b->U32, (void *)b->DE32,
                   (void *)b->D32, (void *)b->B32, (void *)b->bpart, (void *)b->bounds, (void *)b->b_all,
                   (void *)b->r32_all, (void *)b->dA_all, (void *)b->dB_all, (void *)b->e32_all, (void *)b->part_all,
-                  (void *)b->scal_all, (void *)b->flags, (void *)b->d_tab})
+                  (void *)b->scal_all, (void *)b->flags, (void *)b->d_tab, (void *)b->lgf, (void *)b->lfeat,
+                  (void *)b->lomega})
     if (p) cudaFree(p);
   for (double2 *p : b->xbuf)
     if (p) cudaFree(p);
@@ -611,6 +647,7 @@ int batch_update(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double 
     if ((rc = enq_scheduled(b, g, c, dt, st))) return rc;
   }
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (learned_on(b) && (rc = nrqh::learned_check(b->learn))) return rc;
   b->last_initial = 0.0;  // not read back by scheduled steps
   const int64_t planned = sum(b->schedule), planned_passes = (int64_t)b->schedule.size();
   bool changed = false;
@@ -632,6 +669,25 @@ extern "C" int nrq_cn_batch_update(nrq_cn_batch *b, const nrq_gauge *g, const do
   rc = batch_update(b, g, c, dt, use_graph != 0);
   fill_stats(b, stats);
   return rc;
+}
+
+extern "C" int nrq_cn_batch_attach_learned(nrq_cn_batch *b, nrq_learn *net) {
+  if (!b || (net && nrqh::learned_ctx(net) != b->ctx)) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = b->ctx;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  if (net) {
+    const int64_t V = ctx->lat.V, ns = 2 * V * b->nf;
+    if (!b->lgf) NRQ_CUDA_TRY(ctx, cudaMalloc(&b->lgf, sizeof(float4) * V));
+    if (!b->lfeat) NRQ_CUDA_TRY(ctx, cudaMalloc(&b->lfeat, sizeof(float) * 16 * ns));
+    if (!b->lomega) NRQ_CUDA_TRY(ctx, cudaMalloc(&b->lomega, sizeof(float4) * 2 * ns));
+    for (nrq_heavy *h : b->fields)
+      if ((rc = nrqh::ensure_hist(h))) return rc;
+  }
+  b->learn = net;
+  b->have_key = false;  // recalibrate (and recapture) with or without the guess
+  b->gen++;
+  return NRQ_OK;
 }
 
 extern "C" int nrq_cn_batch_residuals(const nrq_cn_batch *b, double *rel) {
@@ -757,6 +813,8 @@ extern "C" int nrq_ensemble_step(nrq_ensemble *e, const double c[8], double dt, 
     }
     NRQ_CUDA_TRY(ctx0, cudaGraphLaunch(e->exec, st0));
     NRQ_CUDA_TRY(ctx0, cudaStreamSynchronize(st0));
+    for (nrq_cn_batch *b : e->batches)
+      if (learned_on(b) && (rc = nrqh::learned_check(b->learn))) return rc;
     for (nrq_cn_batch *b : e->batches) {
       Check chk;
       bool changed = false;

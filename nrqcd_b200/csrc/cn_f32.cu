@@ -377,13 +377,19 @@ __global__ void __launch_bounds__(192, MINB) k_batch_cheb32(Lat L, const float2 
   cheb32_tile<FIRST, NF>(L, f0.CH, U, Dsum, Bsum, DE, d, dn, r, e, f0.cheb[step], sb);
 }
 
-// x += e for every field (blockIdx.y = field)
+// x += e for every field (blockIdx.y = field); with a learned guess the
+// field's new history collects every correction as well
 __global__ void k_batch_add_e(int64_t n, const BatchField *__restrict__ tab) {
   const BatchField &f = tab[blockIdx.y];
+  float2 *hn = f.hnew;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float2 e = f.e32[i];
     const double2 x = f.x[i];
     f.x[i] = make_double2(x.x + (double)e.x, x.y + (double)e.y);
+    if (hn) {
+      const float2 h = hn[i];
+      hn[i] = make_float2(h.x + e.x, h.y + e.y);
+    }
   }
 }
 

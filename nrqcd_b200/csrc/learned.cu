@@ -198,6 +198,47 @@ __global__ void k_learn_apply(int64_t V, const double2 *__restrict__ psi, const 
   hnew[i] = make_float2((float)d.re, (float)d.im);
 }
 
+// batched guess over the fields of a batch table: sample q of field f is
+// row f*2V + q of feat / omega
+__global__ void __launch_bounds__(256) k_batch_learn_features(Lat L, const BatchField *__restrict__ tab,
+                                                              const float4 *__restrict__ gf,
+                                                              float *__restrict__ feat) {
+  const int64_t V = L.V;
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= 2 * V) return;
+  const BatchField &f = tab[blockIdx.y];
+  float v[NIN];
+  sample_features(L, f.psi, f.b, f.h1, f.h2, gf, f.mass, f.tau, q % V, (int)(q / V), v);
+  float4 *o = reinterpret_cast<float4 *>(feat + ((int64_t)blockIdx.y * 2 * V + q) * NIN);
+#pragma unroll
+  for (int k = 0; k < NIN / 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+__global__ void k_batch_learn_apply(int64_t V, const BatchField *__restrict__ tab,
+                                    const float4 *__restrict__ omega) {
+  const BatchField &f = tab[blockIdx.y];
+  const float4 *om = omega + (int64_t)blockIdx.y * 2 * V * 2;
+  const double s0 = fabs(f.tau);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < 72 * V; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t plane = i / V, s = i - plane * V;
+    const int sp = plane >= 36;
+    const float4 wa = __ldg(om + 2 * (sp * V + s)), wb = __ldg(om + 2 * (sp * V + s) + 1);
+    const cplx p = ldg(f.psi + i), bb = ldg(f.b + i);
+    cplx d = (s0 * cplx{wa.x, wa.y}) * (bb - p);
+    if (f.h1) {
+      const float2 h = f.h1[i];
+      d = d + cplx{wa.z, wa.w} * cplx{(double)h.x, (double)h.y};
+    }
+    if (f.h2) {
+      const float2 h = f.h2[i];
+      d = d + cplx{wb.x, wb.y} * cplx{(double)h.x, (double)h.y};
+    }
+    const cplx x0 = 2.0 * bb - p + d;
+    f.x[i] = make_double2(x0.re, x0.im);
+    f.hnew[i] = make_float2((float)d.re, (float)d.im);
+  }
+}
+
 // ------------------------------------------------------------ shared staging
 __device__ __forceinline__ void st_bf16(uint8_t *tile, int r, int k, int R, float x) {
   *reinterpret_cast<__nv_bfloat16 *>(tile + tc::kmajor_offset(r, k, R)) = __float2bfloat16_rn(x);
@@ -979,6 +1020,24 @@ int learned_guess(nrq_learn *net, const nrq_ctx *ctx, const double2 *psi, const 
                                                                               std::fabs(tau), hnew, x);
   return check_launch(c, "learned guess");
 }
+// learned guess of every field of a batch (table on the device): gauge
+// features of the member (U, E), features, the MLP, x and the new history
+int learned_guess_batch(nrq_learn *net, const nrq_ctx *ctx, const nrq::BatchField *tab, int nfields,
+                        const double2 *U, const double *E, float4 *gf, float *fbuf, float4 *omega,
+                        cudaStream_t st) {
+  nrq_ctx *c = const_cast<nrq_ctx *>(ctx);
+  const int64_t V = ctx->lat.V;
+  nrq::learn::k_learn_gauge_features<<<(unsigned)((V + 127) / 128), 128, 0, st>>>(ctx->lat, U, E, gf);
+  nrq::learn::k_batch_learn_features<<<dim3((unsigned)((2 * V + 255) / 256), (unsigned)nfields), 256, 0, st>>>(
+      ctx->lat, tab, gf, fbuf);
+  const int64_t n = 2 * V * nfields;
+  const int64_t ntiles = (n + TILE - 1) / TILE;
+  nrq::learn::k_learn_forward<<<(unsigned)std::min<int64_t>(ntiles, (int64_t)ctx->sm_count * 4), TILE, 0, st>>>(
+      model_of(net), fbuf, n, reinterpret_cast<float *>(omega), 8, net->err);
+  nrq::learn::k_batch_learn_apply<<<dim3((unsigned)std::min<int64_t>((72 * V + 255) / 256, 2048), (unsigned)nfields),
+                                    256, 0, st>>>(V, tab, omega);
+  return check_launch(c, "batched learned guess");
+}
 int ensure_hist(nrq_heavy *h) {
   for (int k = 0; k < 2; ++k)
     if (!h->hist[k]) NRQ_CUDA_TRY(h->ctx, cudaMalloc(&h->hist[k], sizeof(float2) * 72 * h->ctx->lat.V));
@@ -988,6 +1047,7 @@ void add_e_hist(int64_t n, double2 *x, const float2 *e, float2 *hist, cudaStream
   nrq::learn::k_add_e_hist<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, x, e, hist);
 }
 int learned_check(nrq_learn *net) { return learn_err(net); }
+const nrq_ctx *learned_ctx(const nrq_learn *net) { return net ? net->ctx : nullptr; }
 bool learned_ready(const nrq_learn *net) { return net && net->trained; }
 }  // namespace nrqh
 

@@ -186,9 +186,14 @@ int learned_guess(nrq_learn *net, const nrq_ctx *ctx, const double2 *psi, const 
                   double2 *x, cudaStream_t st);
 void add_e_hist(int64_t n, double2 *x, const float2 *e, float2 *hist, cudaStream_t st);
 int learned_check(nrq_learn *net);
+const nrq_ctx *learned_ctx(const nrq_learn *net);
 int learn_record(nrq_learn *net, const nrq_ctx *ctx, const double2 *psi, const double2 *b, const double2 *x,
                  const float2 *v1, const float2 *v2, float2 *hnew, const double2 *U, const double *E, double mass,
                  double dt);
 // both history slots of h allocated
 int ensure_hist(nrq_heavy *h);
+// learned guess of every field of a batch table (learned.cu)
+int learned_guess_batch(nrq_learn *net, const nrq_ctx *ctx, const nrq::BatchField *tab, int nfields,
+                        const double2 *U, const double *E, float4 *gf, float *fbuf, float4 *omega,
+                        cudaStream_t st);
 }  // namespace nrqh

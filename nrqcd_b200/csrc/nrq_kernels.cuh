@@ -106,6 +106,11 @@ struct BatchField {
   double *scal;                  // per-column scalars of this field (CN_COLS x SC_STRIDE)
   const double *bounds;          // spectral enclosure of this field's mass (lo0, hi0, lo1, hi1)
   double tau;                    // dt a0 / 2 (signed)
+  double mass;                   // heavy mass of this field
+  // learned initial guess: the field's history (v1 newest, v2 older; null
+  // when absent) and the slot the new history goes to (null: no learned guess)
+  const float2 *h1, *h2;
+  float2 *hnew;
   cplx inv_theta[2];             // 1/theta per species (written on the device)
   ChebCoef cheb[BATCH_MAX_CHEB]; // Chebyshev steps (written on the device)
 };

@@ -130,14 +130,16 @@ class LearnedGuess:
 
 def train_on_seeded_configs(extent=32, configs=(1, 2), steps=6, mass=1.0, WilsonCoeffs=(1, 1, 1, 1),
                             spacings=(0.05, 1.0, 1.0, 1.0), tol=1e-10, iterations=600, batch=8192, lr=2e-3,
-                            init_seed=5, train_seed=7, device=0, Q=0.5, n0=1.0):
+                            init_seed=5, train_seed=7, device=0, Q=0.5, n0=1.0, masses=None):
     """Train the guess on the method's own solves: for every seed in
-    ``configs`` a transverse-polarised occupation field (saturation Q,
-    amplitude n0, identity links) on an ``extent``^3 lattice and one point
-    source at a seeded random site evolve ``steps`` coupled steps (precision
-    form at ``tol``, then the leapfrog), every CN step recording 2 V samples.
+    ``configs`` and every heavy mass in ``masses`` (default: ``mass``) a
+    transverse-polarised occupation field (saturation Q, amplitude n0,
+    identity links) on an ``extent``^3 lattice and one point source at a
+    seeded random site evolve ``steps`` coupled steps (precision form at
+    ``tol``, then the leapfrog), every CN step recording 2 V samples.
     Returns (params, info); the parameters load into a LearnedGuess of any
     lattice size."""
+    masses = tuple(masses) if masses is not None else (mass,)
     from .gaugeconfiguration_su3 import GaugeConfiguration
     from .nrqcd import NRQCDField
     lat = lattice.Lattice((extent, extent, extent), spacings, device=device)
@@ -149,18 +151,19 @@ def train_on_seeded_configs(extent=32, configs=(1, 2), steps=6, mass=1.0, Wilson
                                     ctypes.byref(cn)), lat.ctx, "nrq_cn_init")
         net = LearnedGuess(seed=init_seed, lat=lat)
         V = extent ** 3
-        net.reserve(len(configs) * steps * 2 * V)
+        net.reserve(len(configs) * len(masses) * steps * 2 * V)
         for seed in configs:
-            g = GaugeConfiguration(lat=lat)
-            g.TransversePolarisedOccupiedInit_Box(Q, n0, 0.0, RandomSeed=int(seed), identity_links=True)
-            h = NRQCDField(lat=lat)
-            src = np.random.default_rng(int(seed)).integers(0, V, size=2) + 1
-            h.InitSinglePoint(int(src[0]), int(src[1]))
-            for _ in range(steps):
-                net.record(h, g, mass, WilsonCoeffs, 1.0, cn=cn)
-                g.Update(1.0)
-            h.Destructor()
-            g.Deallocate()
+            for m in masses:
+                g = GaugeConfiguration(lat=lat)
+                g.TransversePolarisedOccupiedInit_Box(Q, n0, 0.0, RandomSeed=int(seed), identity_links=True)
+                h = NRQCDField(lat=lat)
+                src = np.random.default_rng(int(seed)).integers(0, V, size=2) + 1
+                h.InitSinglePoint(int(src[0]), int(src[1]))
+                for _ in range(steps):
+                    net.record(h, g, m, WilsonCoeffs, 1.0, cn=cn)
+                    g.Update(1.0)
+                h.Destructor()
+                g.Deallocate()
         nsamples = net.size()
         l0, l1 = net.train(iterations, batch=batch, lr=lr, seed=train_seed)
         params = net.params
@@ -168,6 +171,7 @@ def train_on_seeded_configs(extent=32, configs=(1, 2), steps=6, mass=1.0, Wilson
         lib.nrq_cn_finalize(cn)
     finally:
         lat.close()
-    return params, {"lattice": [extent] * 3, "configs": list(configs), "steps_per_config": steps,
+    return params, {"lattice": [extent] * 3, "configs": list(configs), "masses": list(masses),
+                    "steps_per_config": steps,
                     "samples": nsamples, "iterations": iterations, "batch": batch,
                     "loss_first_batch": l0, "loss_last_batch": l1}

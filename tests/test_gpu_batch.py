@@ -198,3 +198,54 @@ def test_batch_rejects_bad_arguments(oracle):
         st = b.Update(g, C, 1.0)
         assert st["converged"] == 1
         b.Destructor()
+
+
+def test_batch_with_learned_guess_matches_single_updates(oracle):
+    """Forms combined: a batch whose solves start from the learned guess
+    (network trained on recorded 8^3 steps) gives every field the result of
+    its own precision-form update, and needs no more inner steps per step
+    than the batch without the guess once the history is full."""
+    from nrqcd_b200 import nrqcd
+    from nrqcd_b200.learned import LearnedGuess
+    n = (8, 8, 8)
+    V = int(np.prod(n))
+    tol = 1e-10
+    with lattice_ctx(n, A, cn=(1.0, C, 1.0, tol, 10000, FORM_PRECISION)):
+        net = LearnedGuess(seed=5)
+        net.reserve(16 * 2 * V)
+        for seed in (41, 42):
+            g0, _, _ = _hot_gauge(oracle, n, seed)
+            h0 = NRQCDField()
+            h0.InitSinglePoint(3 + seed, 7 + seed)
+            for _ in range(8):
+                net.record(h0, g0, 1.0, C, 1.0)
+                g0.Update(1.0)
+        net.train(400, batch=2048, lr=2e-3, seed=7)
+        g, _, _ = _hot_gauge(oracle, n, 43)
+        srcs = _sources(V, 2, 17)
+        ms = [1.0, 1.0, 1.5, 1.5]
+        hl = _fields(V, srcs + srcs)
+        hp = _fields(V, srcs + srcs)
+        singles = _fields(V, srcs + srcs)
+        bl = CNBatch(hl, ms, tol)
+        bl.attach_learned(net)
+        bp = CNBatch(hp, ms, tol)
+        inner_l, inner_p = [], []
+        for step in range(6):
+            sl = bl.Update(g, C, 1.0, use_graph=True)
+            sp_ = bp.Update(g, C, 1.0, use_graph=True)
+            assert sl["converged"] == 1 and sl["max_rel_residual"] <= tol
+            inner_l.append(sl["iterations"])
+            inner_p.append(sp_["iterations"])
+            for h, m in zip(singles, ms):
+                assert nrqcd.solver_handle() is not None
+                h.Update(g, m, C, 1.0)
+        assert sum(inner_l[3:]) <= sum(inner_p[3:])
+        for a_, b_ in zip(hl, singles):
+            qa, aa = a_.download()
+            qb, ab = b_.download()
+            assert np.abs(qa - qb).max() < 5e-10 and np.abs(aa - ab).max() < 5e-10
+        bl.attach_learned(None)
+        bl.Destructor()
+        bp.Destructor()
+        net.Destructor()
