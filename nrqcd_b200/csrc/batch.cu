@@ -190,7 +190,7 @@ int enq_rhs(nrq_cn_batch *b, const nrq_gauge *g, cudaStream_t st) {
   nrq_ctx *ctx = b->ctx;
   {
     ProfScope ps(ctx, 0, (double)ctx->lat.V * (b->nf * 1152.0 * 3 + 432.0 + 192.0));
-    nrq::launch_batch_mv(nrq::MV_RHS, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, st);
+    nrq::launch_batch_mv(nrq::MV_RHS, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, 0, st);
   }
   int rc = check_launch(ctx, "batch rhs");
   if (!rc && learned_on(b)) {
@@ -201,12 +201,14 @@ int enq_rhs(nrq_cn_batch *b, const nrq_gauge *g, cudaStream_t st) {
 }
 
 // r = b - A^H x (FP64) of every field, FP32 copies r32 and d = r/theta, and
-// the per-column (r.r, b.b) reduction
-int enq_residual(nrq_cn_batch *b, cudaStream_t st) {
+// the per-column (r.r, b.b) reduction.  After the first check of a step
+// (first = false) fields that already converged are skipped.
+int enq_residual(nrq_cn_batch *b, cudaStream_t st, bool first) {
   nrq_ctx *ctx = b->ctx;
   {
     ProfScope ps(ctx, 0, (double)ctx->lat.V * (b->nf * (1152.0 * 2 + 576.0 * 2) + 432.0 + 192.0));
-    nrq::launch_batch_mv(nrq::MV_RESC, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, st);
+    nrq::launch_batch_mv(nrq::MV_RESC, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf,
+                         first ? 0 : 1, st);
   }
   {
     ProfScope ps(ctx, 2, (double)b->nf * b->nsb * nrq::CN_COLS * 2 * 8);
@@ -247,10 +249,10 @@ int enq_scheduled(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double
   int rc = enq_prepare(b, g, c, dt, st);
   if (!rc) rc = enq_rhs(b, g, st);
   for (size_t p = 0; !rc && p < b->schedule.size(); ++p) {
-    rc = enq_residual(b, st);
+    rc = enq_residual(b, st, p == 0);
     if (!rc) rc = enq_inner(b, b->schedule[p], st);
   }
-  if (!rc) rc = enq_residual(b, st);
+  if (!rc) rc = enq_residual(b, st, b->schedule.empty());
   if (!rc) rc = enq_readback(b, st);
   return rc;
 }
@@ -309,6 +311,9 @@ int autotune(nrq_cn_batch *b, cudaStream_t st) {
   double best = 1e300;
   int best_variant = 0, best_order = 0;
   const int reps = 3;
+  // no field may count as converged while the candidates are timed (the
+  // residual check of the solve rewrites these flags before they matter)
+  NRQ_CUDA_TRY(ctx, cudaMemsetAsync(b->scal_all, 0, sizeof(double) * kFieldScal * b->nf, st));
   for (int variant = 0; variant < nrq::BATCH_CHEB_VARIANTS; ++variant)
     for (int order = 0; order < 2; ++order) {
       const int idx = variant * 2 + order;
@@ -355,7 +360,7 @@ int refine_adaptive(nrq_cn_batch *b, double dt, cudaStream_t st, int budget, std
   for (int p = 0; p < budget && !chk.conv && !chk.nonfin && !chk.badbounds; ++p) {
     const int m = steps_for(b, dt, chk.worst / (0.3 * b->tol));
     int rc = enq_inner(b, m, st);
-    if (!rc) rc = enq_residual(b, st);
+    if (!rc) rc = enq_residual(b, st, false);
     if (!rc) rc = enq_readback(b, st);
     if (rc) return rc;
     NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -376,7 +381,7 @@ int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], dou
                                     cudaMemcpyDeviceToHost, st));
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (!b->tuned && (rc = autotune(b, st))) return rc;
-  if ((rc = enq_rhs(b, g, st)) || (rc = enq_residual(b, st)) || (rc = enq_readback(b, st))) return rc;
+  if ((rc = enq_rhs(b, g, st)) || (rc = enq_residual(b, st, true)) || (rc = enq_readback(b, st))) return rc;
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   chk = check(b);
   b->last_initial = chk.worst;
@@ -566,9 +571,11 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
   if ((e = cudaMallocHost(&b->h_scal, sizeof(double) * kFieldScal * nfields)) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&b->h_flags, sizeof(int) * nfields)) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&b->h_bounds, sizeof(double) * 4 * b->masses.size())) != cudaSuccess) return fail(e);
-  // defined contents for the FP32 vectors the tuner's first launches read
+  // defined contents for the FP32 vectors and flags the tuner's first launches read
   for (float2 *p : {b->r32_all, b->dA_all, b->dB_all, b->e32_all})
     if ((e = cudaMemsetAsync(p, 0, sizeof(float2) * P * nfields, ctx->stream)) != cudaSuccess) return fail(e);
+  if ((e = cudaMemsetAsync(b->scal_all, 0, sizeof(double) * kFieldScal * nfields, ctx->stream)) != cudaSuccess)
+    return fail(e);
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e);
   *out = b;
   return NRQ_OK;

@@ -363,6 +363,11 @@ __global__ void __launch_bounds__(192, MINB) k_batch_cheb32(Lat L, const float2 
   const int64_t bid = blockIdx.x;
   const int tile = ORDER == 0 ? (int)(bid % ntiles) : (int)(bid / nsb);
   const int64_t sb = ORDER == 0 ? bid / ntiles : bid % nsb;
+  // fields that passed their last residual check sit out (uniform per block)
+  bool all_done = true;
+#pragma unroll
+  for (int j = 0; j < NF; ++j) all_done = all_done && batch_field_done(tab[tile * NF + j]);
+  if (all_done) return;
   const float2 *d[NF];
   float2 *dn[NF], *r[NF], *e[NF];
 #pragma unroll
@@ -381,6 +386,7 @@ __global__ void __launch_bounds__(192, MINB) k_batch_cheb32(Lat L, const float2 
 // field's new history collects every correction as well
 __global__ void k_batch_add_e(int64_t n, const BatchField *__restrict__ tab) {
   const BatchField &f = tab[blockIdx.y];
+  if (batch_field_done(f)) return;  // its Chebyshev steps were skipped too
   float2 *hn = f.hnew;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float2 e = f.e32[i];

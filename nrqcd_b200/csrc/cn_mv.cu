@@ -252,11 +252,12 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_batch_mv2(Lat L, const dou
                                                       const double *__restrict__ Bsum,
                                                       const double2 *__restrict__ DE,
                                                       const BatchField *__restrict__ tab, int nfields,
-                                                      int64_t nsb) {
+                                                      int64_t nsb, int skip_done) {
   const int64_t bid = blockIdx.x;
   const int fi = ORDER == 0 ? (int)(bid % nfields) : (int)(bid / nsb);
   const int64_t sb = ORDER == 0 ? bid / nfields : bid % nsb;
   const BatchField &f = tab[fi];
+  if (MODE == MV_RESC && skip_done && batch_field_done(f)) return;  // uniform per block
   MvArgs a{};
   if (MODE == MV_RHS) {
     a.in = f.psi;
@@ -277,21 +278,22 @@ __global__ void __launch_bounds__(192, NRQ_MV_MINB) k_batch_mv2(Lat L, const dou
 
 template <int MODE>
 static void batch_mv_mode(int order, dim3 grid, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
-                          const double2 *DE, const BatchField *tab, int nfields, int64_t nsb, cudaStream_t st) {
+                          const double2 *DE, const BatchField *tab, int nfields, int64_t nsb, int skip_done,
+                          cudaStream_t st) {
   if (order == 0)
-    k_batch_mv2<MODE, 0><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, nfields, nsb);
+    k_batch_mv2<MODE, 0><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, nfields, nsb, skip_done);
   else
-    k_batch_mv2<MODE, 1><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, nfields, nsb);
+    k_batch_mv2<MODE, 1><<<grid, 192, 0, st>>>(L, U, Dsum, Bsum, DE, tab, nfields, nsb, skip_done);
 }
 
 void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
-                     const double2 *DE, const BatchField *tab, int nfields, cudaStream_t st) {
+                     const double2 *DE, const BatchField *tab, int nfields, int skip_done, cudaStream_t st) {
   const int64_t nsb = (L.V + 31) / 32;
   const dim3 grid((unsigned)(nsb * nfields));
   if (mode == MV_RHS)
-    batch_mv_mode<MV_RHS>(order, grid, L, U, Dsum, Bsum, DE, tab, nfields, nsb, st);
+    batch_mv_mode<MV_RHS>(order, grid, L, U, Dsum, Bsum, DE, tab, nfields, nsb, 0, st);
   else
-    batch_mv_mode<MV_RESC>(order, grid, L, U, Dsum, Bsum, DE, tab, nfields, nsb, st);
+    batch_mv_mode<MV_RESC>(order, grid, L, U, Dsum, Bsum, DE, tab, nfields, nsb, skip_done, st);
 }
 
 void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,

@@ -114,8 +114,17 @@ struct BatchField {
   cplx inv_theta[2];             // 1/theta per species (written on the device)
   ChebCoef cheb[BATCH_MAX_CHEB]; // Chebyshev steps (written on the device)
 };
+// every column of the field converged at its last residual check
+__device__ __forceinline__ bool batch_field_done(const BatchField &f) {
+  bool d = true;
+#pragma unroll
+  for (int k = 0; k < CN_COLS; ++k) d = d && f.scal[k * SC_STRIDE + SC_CONV] != 0.0;
+  return d;
+}
+// skip_done: residual launches after the first of a step leave converged
+// fields alone (their iterate did not change since their last check)
 void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
-                     const double2 *DE, const BatchField *tab, int nfields, cudaStream_t st);
+                     const double2 *DE, const BatchField *tab, int nfields, int skip_done, cudaStream_t st);
 // Chebyshev kernel variants: 0 = one field per tile, 2 blocks/SM (168
 // registers); 1 = one field per tile, 3 blocks/SM (113 registers); 2 = two
 // fields of one mass per tile, 1 block/SM.  Returns nonzero for an
