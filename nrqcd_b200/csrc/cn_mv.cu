@@ -14,15 +14,14 @@
 // the 6 columns: 36 complex multiply-adds per column per neighbour, the
 // minimum for a dense 6x6 block.  The three colour warps of a species read
 // the same neighbour spinors; those reads hit L1.
+#include <type_traits>
+
 #include "nrq_kernels.cuh"
 
 // tuning parameters of the stencil kernel (blocks per SM for the register
-// budget, unroll depth of the direction and column loops)
+// budget, unroll depth of the column loop)
 #ifndef NRQ_MV_MINB
 #define NRQ_MV_MINB 2
-#endif
-#ifndef NRQ_MV_UNROLL_DIR
-#define NRQ_MV_UNROLL_DIR 1
 #endif
 #ifndef NRQ_MV_UNROLL_COL
 #define NRQ_MV_UNROLL_COL 2
@@ -30,20 +29,21 @@
 
 namespace nrq {
 
-constexpr int kMvUnrollDir = NRQ_MV_UNROLL_DIR;
 constexpr int kMvUnrollCol = NRQ_MV_UNROLL_COL;
 
-// entry (s, sp) of the transposed reference Pauli matrix s_k^T
-// (src/su2.f90:68-79 holds s_2 transposed, so s_2^T = [[0,-i],[i,0]])
-__device__ __forceinline__ cplx sigT(int k, int s, int t) {
-  if (k == 0) return (s != t) ? cplx{1.0, 0.0} : cplx{0.0, 0.0};
-  if (k == 1) {
-    if (s == 0 && t == 1) return {0.0, -1.0};
-    if (s == 1 && t == 0) return {0.0, 1.0};
+// v times entry (s, t) of the transposed reference Pauli matrix s_K^T
+// (src/su2.f90:68-79 holds s_2 transposed, so s_2^T = [[0,-i],[i,0]]); with
+// K, s and t known at compile time this is a sign flip or a swap
+template <int K>
+__device__ __forceinline__ cplx sig_mul(int s, int t, cplx v) {
+  if (K == 0) return (s != t) ? v : cplx{0.0, 0.0};
+  if (K == 1) {
+    if (s == 0 && t == 1) return -times_i(v);
+    if (s == 1 && t == 0) return times_i(v);
     return {0.0, 0.0};
   }
   if (s != t) return {0.0, 0.0};
-  return (s == 0) ? cplx{1.0, 0.0} : cplx{-1.0, 0.0};
+  return (s == 0) ? v : -v;
 }
 
 __device__ __forceinline__ cplx scal_col(const double *sc, int col12, int slot) {
@@ -108,57 +108,63 @@ __device__ __forceinline__ void cn_mv2_body(const Lat &L, const CnCoef &C, const
   }
   const cplx cs0 = times_i(aso);   // eps = +1 permutation (j,k) = (i+1, i+2)
   const cplx cs1 = -times_i(aso);  // eps = -1 permutation (j,k) = (i+2, i+1)
-#pragma unroll kMvUnrollDir
-  for (int i = 0; i < 3; ++i) {
-    const cplx ck = (-0.5 * C.inva2[i]) * ak;
-    const int k0 = (i + 2) % 3, k1 = (i + 1) % 3;
-#pragma unroll kMvUnrollDir
-    for (int dir = 0; dir < 2; ++dir) {
-      // dir 0: neighbour x+i, blocks from site x (transposed)
-      // dir 1: neighbour x-i, blocks from site x-i (complex conjugated)
-      const int64_t y = nb(L, x, i, dir == 0 ? +1 : -1);
-      const int64_t ms = dir == 0 ? x : y;
-      const double2 *Up = U + (int64_t)(i * 9) * V + ms;
-      const double2 *D0 = DE + (int64_t)((i * 2 + 0) * 9) * V + ms;
-      const double2 *D1 = DE + (int64_t)((i * 2 + 1) * 9) * V + ms;
-      const cplx s0 = dir == 0 ? cs0 : -cs0, s1 = dir == 0 ? cs1 : -cs1;
-      cplx Wm[2][3][2];
+  // one neighbour, direction I and side DIR known at compile time, so the
+  // Pauli factors of the block fold to sign flips and swaps
+  // (DIR 0: neighbour x+I, blocks from site x, transposed;
+  //  DIR 1: neighbour x-I, blocks from site x-I, complex conjugated)
+  auto neighbour = [&](auto Ic, auto DIRc) {
+    constexpr int I = decltype(Ic)::value, DIR = decltype(DIRc)::value;
+    constexpr int K0 = (I + 2) % 3, K1 = (I + 1) % 3;
+    const cplx ck = (-0.5 * C.inva2[I]) * ak;
+    const int64_t y = nb(L, x, I, DIR == 0 ? +1 : -1);
+    const int64_t ms = DIR == 0 ? x : y;
+    const double2 *Up = U + (int64_t)(I * 9) * V + ms;
+    const double2 *D0 = DE + (int64_t)((I * 2 + 0) * 9) * V + ms;
+    const double2 *D1 = DE + (int64_t)((I * 2 + 1) * 9) * V + ms;
+    const cplx s0 = DIR == 0 ? cs0 : -cs0, s1 = DIR == 0 ? cs1 : -cs1;
+    cplx Wm[2][3][2];
 #pragma unroll
-      for (int cp = 0; cp < 3; ++cp) {
-        cplx u, d0, d1;
-        if (dir == 0) {  // M^T[c][cp] = M[cp][c]
-          u = ldg(Up + (int64_t)(cp * 3 + c) * V);
-          d0 = ldg(D0 + (int64_t)(cp * 3 + c) * V);
-          d1 = ldg(D1 + (int64_t)(cp * 3 + c) * V);
-        } else {         // M^*[c][cp]
-          u = conj(ldg(Up + (int64_t)(c * 3 + cp) * V));
-          d0 = conj(ldg(D0 + (int64_t)(c * 3 + cp) * V));
-          d1 = conj(ldg(D1 + (int64_t)(c * 3 + cp) * V));
+    for (int cp = 0; cp < 3; ++cp) {
+      const int e = DIR == 0 ? (cp * 3 + c) : (c * 3 + cp);  // M^T[c][cp] = M[cp][c] ; M^*[c][cp]
+      cplx u = ldg(Up + (int64_t)e * V), d0 = ldg(D0 + (int64_t)e * V), d1 = ldg(D1 + (int64_t)e * V);
+      if (DIR == 1) {
+        u = conj(u);
+        d0 = conj(d0);
+        d1 = conj(d1);
+      }
+      const cplx ku = ck * u, e0 = s0 * d0, e1 = s1 * d1;
+#pragma unroll
+      for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          cplx v = (s == t) ? ku : cplx{0.0, 0.0};
+          v = v + sig_mul<K0>(s, t, e0);
+          v = v + sig_mul<K1>(s, t, e1);
+          Wm[s][cp][t] = v;
         }
-        const cplx ku = ck * u, e0 = s0 * d0, e1 = s1 * d1;
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-          for (int t = 0; t < 2; ++t) {
-            cplx v = sigT(k0, s, t) * e0 + sigT(k1, s, t) * e1;
-            if (s == t) v = v + ku;
-            Wm[s][cp][t] = v;
-          }
-      }
-#pragma unroll kMvUnrollCol
-      for (int col = 0; col < 6; ++col) {
-        cplx w[6];
-        load_w(y, col, w);
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-          for (int cp = 0; cp < 3; ++cp) {
-            cmac(acc[col][s], Wm[s][cp][0], w[2 * cp]);
-            cmac(acc[col][s], Wm[s][cp][1], w[2 * cp + 1]);
-          }
-      }
     }
-  }
+#pragma unroll kMvUnrollCol
+    for (int col = 0; col < 6; ++col) {
+      cplx w[6];
+      load_w(y, col, w);
+#pragma unroll
+      for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int cp = 0; cp < 3; ++cp) {
+          cmac(acc[col][s], Wm[s][cp][0], w[2 * cp]);
+          cmac(acc[col][s], Wm[s][cp][1], w[2 * cp + 1]);
+        }
+    }
+  };
+  using I0 = std::integral_constant<int, 0>;
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  neighbour(I0{}, I0{});
+  neighbour(I0{}, I1{});
+  neighbour(I1{}, I0{});
+  neighbour(I1{}, I1{});
+  neighbour(I2{}, I0{});
+  neighbour(I2{}, I1{});
 
   // ---------------- epilogue by mode; rows (c, s) of the 6 columns
   constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
