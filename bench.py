@@ -179,14 +179,17 @@ FORMS = {"plain_fp64_bicgstab": 0, "precision_fp32_chebyshev_fp64_refinement": 1
 FORMS_SIZES = (64, 96, 128)
 
 
-def train_learned(tol=1e-10):
+def train_learned(tol=1e-10, masses=(MASS,)):
     """The learned form's network, trained on seeded 32^3 solves (2
-    configurations x masses aM = 1.0 and 1.5 (the ensemble's) x 8 steps); the
-    parameters load into any lattice size."""
+    configurations x the given heavy masses x 8 steps); the parameters load
+    into any lattice size.  The FP32 output bias is per species and history
+    depth, not per mass, so a network serves best at the masses it was
+    trained on: the forms use aM = 1.0, the ensemble aM = 1.0 and 1.5."""
     from nrqcd_b200.learned import train_on_seeded_configs
     t0 = time.perf_counter()
-    params, info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=8, masses=(MASS, 1.5),
-                                           WilsonCoeffs=WILSON, spacings=A, tol=tol, iterations=1000)
+    params, info = train_on_seeded_configs(extent=32, configs=(11, 12), steps=8, masses=tuple(masses),
+                                           WilsonCoeffs=WILSON, spacings=A, tol=tol,
+                                           iterations=800 if len(masses) == 1 else 1000)
     info["wall_s"] = time.perf_counter() - t0
     return params, info
 
@@ -523,7 +526,7 @@ def main():
     if args.only_ensemble:
         import torch
         torch.cuda.set_device(local)
-        out = measure_ensemble(args.steps, args.warmup, learned_params=train_learned()[0])
+        out = measure_ensemble(args.steps, args.warmup, learned_params=train_learned(masses=ENS_MASSES)[0])
         if rank == 0:
             print(json.dumps({"batching_ensemble": out}), flush=True)
         return
@@ -626,10 +629,10 @@ def main():
                "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
                        "nrq_heavy_download + nrq_gauge_download, pinned host buffers"}
 
-    learned = train_learned() if world == 1 and not (args.no_ensemble and args.no_forms) else None
     ensemble = None
     if not args.no_ensemble and world == 1:
-        ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2, learned_params=learned[0])
+        ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2,
+                                    learned_params=train_learned(masses=ENS_MASSES)[0])
 
     drift = None
     if not args.no_drift and world == 1:
@@ -637,7 +640,7 @@ def main():
 
     forms = None
     if not args.no_forms and world == 1:
-        forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes), learned=learned)
+        forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
 
     if rank == 0:
         peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
