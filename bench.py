@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--only-forms", action="store_true", help="print only the CN-forms JSON")
     p.add_argument("--forms-sizes", type=int, nargs="+", default=list(FORMS_SIZES))
     p.add_argument("--no-drift", action="store_true")
+    p.add_argument("--stencil", default="timed", choices=["timed", "register", "tma", "tensor"],
+                   help="FP64 stencil of the headline step (default: the solver's timed choice)")
     p.add_argument("--only-drift", action="store_true", help="print only the precision-drift JSON")
     return p.parse_args()
 
@@ -540,6 +542,9 @@ def main():
     lattice.InitModule([L, L, L], list(A), device=local)
     ctx = lattice.context()
     nrqcd.InitModule(MASS, WILSON, 1.0, TOL)
+    if args.stencil != "timed":
+        nrqcd.SetStencil({"register": nrqcd.STENCIL_REGISTER, "tma": nrqcd.STENCIL_TMA,
+                          "tensor": nrqcd.STENCIL_TENSOR}[args.stencil])
     g = GaugeConfiguration()
     g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=1 + rank, identity_links=True)
     h = NRQCDField()
@@ -589,14 +594,12 @@ def main():
     ms_per_step = ms / args.steps
     value = world * V * args.steps / (ms / 1000.0)
     norm_q, norm_a = h.GetNorm_Quark(), h.GetNorm_AntiQ()
-    tma = ctypes.c_int()
-    tune_ms = np.zeros(2)
-    _capi.check(lib.nrq_cn_stencil_info(nrqcd.solver_handle(), ctypes.byref(tma), _capi.dptr(tune_ms)), ctx,
-                "stencil_info")
+    which, tune_ms = nrqcd.StencilInfo()
     p64, p32 = ctypes.c_double(), ctypes.c_double()
     _capi.check(lib.nrq_measure_peaks(ctx, ctypes.byref(p64), ctypes.byref(p32)), ctx, "measure_peaks")
-    stencil = {"in_use": "k_cn_mv3 (TMA-staged)" if tma.value else "k_cn_mv2 (register-tiled)",
-               "tuning_ms_per_launch": {"k_cn_mv2": float(tune_ms[0]), "k_cn_mv3_with_vec_s": float(tune_ms[1])}}
+    stencil = {"in_use": nrqcd.STENCIL_NAMES[which],
+               "tuning_ms_per_launch": {"k_cn_mv2": float(tune_ms[0]), "k_cn_mv3_with_vec_s": float(tune_ms[1]),
+                                        "k_cn_mv4_with_vec_s": float(tune_ms[2])}}
 
     # ---------------- end-to-end through the C ABI with host buffers
     e2e = None
@@ -652,7 +655,10 @@ def main():
         # FP64 arithmetic of one 12-column stencil launch per site: 2 species x
         # (6 neighbours x 6 columns x 36 + 6 columns x 18) complex FMAs (4 DFMA
         # each, 2 flops per DFMA) plus the block assembly (~270 complex FMAs)
-        flops_site = 2 * (6 * 6 * 36 + 6 * 18 + 270) * 4 * 2
+        # (the tensor-core stencil reads the blocks assembled once per update,
+        # and its MMA tiles carry 16/12 x 8/6 of these products with padding)
+        tensor = which == nrqcd.STENCIL_TENSOR
+        flops_site = 2 * (6 * 6 * 36 + 6 * 18 + (0 if tensor else 270)) * 4 * 2
         fp64_achieved = flops_site * V * sten["launches"] / (sten["ms"] / 1000.0) / 1e12 if sten["ms"] > 0 else None
         step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
         its = [s["iterations"] for s in iters]

@@ -149,10 +149,21 @@ int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, 
                 int64_t maxits, int form, nrq_cn **cn);
 /* FinalizeModule, src/nrqcd.f90:199-212 */
 int nrq_cn_finalize(nrq_cn *cn);
-/* The stencil the solver uses (tma_staged = 1: TMA-staged, 0: register-
- * tiled) and the per-launch milliseconds of both measured on its first
- * update (-1 before it, or where only one applies).                      */
-int nrq_cn_stencil_info(const nrq_cn *cn, int *tma_staged, double ms[2]);
+/* FP64 stencils of the solver (no reference counterpart: PETSc applies its
+ * assembled matrix; these apply the same operator matrix-free).
+ * REGISTER: register-tiled; TMA: TMA-staged; TENSOR: FP64 tensor-core MMAs
+ * on per-update 6x6 blocks (real Wilson coefficients; otherwise the TMA or
+ * register-tiled stencil runs).                                           */
+#define NRQ_STENCIL_REGISTER 0
+#define NRQ_STENCIL_TMA 1
+#define NRQ_STENCIL_TENSOR 2
+/* The stencil the solver uses and the per-launch milliseconds of each one
+ * measured on its first update (index = NRQ_STENCIL_*; -1 before it, or for
+ * one that does not apply to the lattice or coefficients).               */
+int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[3]);
+/* Force a stencil (NRQ_STENCIL_*) or restore the timed choice (-1).
+ * NRQ_ERR_BAD_ARG if the stencil cannot describe this lattice.            */
+int nrq_cn_set_stencil(nrq_cn *cn, int stencil);
 /* NRQCDField%Update(GaugeConf, Mass, WilsonCoeffs, StepWidth) =
  * Update_CrankNicholson, src/nrqcd.f90:1053-1168: quark (+M, c) and
  * antiquark (-M, conj c); per column RHS = A psi, solve A^H psi' = RHS with

@@ -807,7 +807,8 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
   }
   // the TMA-staged stencil needs 16-byte plane strides for the real-valued
   // magnetic planes (V even) and tiles no wider than the lattice
-  cn->use_tma = (V % 2 == 0) && V >= 64;
+  cn->tma_ok = (V % 2 == 0) && V >= 64;
+  cn->stencil = cn->tma_ok ? NRQ_STENCIL_TMA : NRQ_STENCIL_REGISTER;
   if (!ok) {
     cudaGetLastError();
     nrq_cn_finalize(cn);
@@ -821,13 +822,23 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
   return NRQ_OK;
 }
 
-extern "C" int nrq_cn_stencil_info(const nrq_cn *cn, int *tma_staged, double ms[2]) {
+extern "C" int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[3]) {
   if (!cn) return NRQ_ERR_BAD_ARG;
-  if (tma_staged) *tma_staged = cn->use_tma ? 1 : 0;
-  if (ms) {
-    ms[0] = cn->tune_ms[0];
-    ms[1] = cn->tune_ms[1];
+  if (stencil) *stencil = cn->stencil;
+  if (ms)
+    for (int k = 0; k < 3; ++k) ms[k] = cn->tune_ms[k];
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_set_stencil(nrq_cn *cn, int stencil) {
+  if (!cn || stencil < -1 || stencil > NRQ_STENCIL_TENSOR) return NRQ_ERR_BAD_ARG;
+  if (stencil > NRQ_STENCIL_REGISTER && !cn->tma_ok) {
+    cn->ctx->last_error = "nrq_cn_set_stencil: tensor maps cannot describe this lattice";
+    return NRQ_ERR_BAD_ARG;
   }
+  cn->forced_stencil = stencil;
+  cn->stencil_tuned = false;
+  cn->stencil = stencil >= 0 ? stencil : (cn->tma_ok ? NRQ_STENCIL_TMA : NRQ_STENCIL_REGISTER);
   return NRQ_OK;
 }
 
@@ -838,7 +849,8 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
   for (void *p : {(void *)cn->Dsum, (void *)cn->Bsum, (void *)cn->DE, (void *)cn->b, (void *)cn->x, (void *)cn->r,
                   (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->s, (void *)cn->scal,
                   (void *)cn->partials, (void *)cn->U32, (void *)cn->DE32, (void *)cn->D32, (void *)cn->B32,
-                  (void *)cn->r32, (void *)cn->dA32, (void *)cn->dB32, (void *)cn->e32, (void *)cn->bounds})
+                  (void *)cn->r32, (void *)cn->dA32, (void *)cn->dB32, (void *)cn->e32, (void *)cn->bounds,
+                  (void *)cn->Wblk})
     if (p) cudaFree(p);
   if (cn->h_scal) cudaFreeHost(cn->h_scal);
   if (cn->h_bounds) cudaFreeHost(cn->h_bounds);
@@ -848,102 +860,170 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
 
 namespace {
 // algorithmic bytes of one 12-column stencil launch: vector streams of
-// 12 x 6 complex per site plus the gauge inputs U and E read once
-double mv_bytes(const nrq_ctx *ctx, int mode) {
+// 12 x 6 complex per site plus the gauge inputs U and E read once, or for
+// the tensor-core stencil its 6x6 blocks (6 x 576 B) and the diagonal
+// colour matrices (216 B) read once
+double mv_bytes(const nrq_ctx *ctx, int mode, bool tensor = false) {
   const int streams[6] = {2, 3, 5, 3, 3, 3};  // PLAIN, RHS, RES, V, T, RESC
-  return (double)ctx->lat.V * (1152.0 * streams[mode] + 432.0 + 192.0);
+  return (double)ctx->lat.V * (1152.0 * streams[mode] + (tensor ? 3456.0 + 216.0 : 432.0 + 192.0));
 }
-void mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq::MvArgs &a) {
+// the tensor-core stencil's backward blocks are -W^H of the forward ones,
+// which holds when every off-diagonal coefficient is imaginary (real
+// Wilson coefficients)
+bool offdiag_imaginary(const nrq::CnCoef &C) {
+  for (int sp = 0; sp < 2; ++sp)
+    if (C.kin[sp].re != 0.0 || C.so[sp].re != 0.0) return false;
+  return true;
+}
+// +1 / -1 when the current blocks were built for C / for the coefficients
+// whose off-diagonal terms are those of C negated (A vs A^H), 0 otherwise
+double blocks_sign(const nrq_cn *cn, const nrq::CnCoef &C) {
+  if (!cn->w_valid) return 0.0;
+  const nrq::CnCoef &w = cn->w_coef;
+  bool same = true, neg = true;
+  for (int sp = 0; sp < 2; ++sp) {
+    same = same && C.kin[sp].im == w.kin[sp].im && C.so[sp].im == w.so[sp].im;
+    neg = neg && C.kin[sp].im == -w.kin[sp].im && C.so[sp].im == -w.so[sp].im;
+  }
+  return same ? 1.0 : (neg ? -1.0 : 0.0);
+}
+int ensure_blocks(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *sign) {
   nrq_ctx *ctx = cn->ctx;
+  *sign = blocks_sign(cn, C);
+  if (*sign != 0.0) return NRQ_OK;
+  const int64_t V = ctx->lat.V;
+  if (!cn->Wblk) NRQ_CUDA_TRY(ctx, cudaMalloc((void **)&cn->Wblk, sizeof(double2) * 216 * V));
+  {
+    ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 3456.0));
+    nrq::launch_cn_blocks(ctx->lat, C, g->U, cn->DE, cn->Wblk, ctx->stream);
+  }
+  cn->w_coef = C;
+  cn->w_valid = true;
+  *sign = 1.0;
+  return check_launch(ctx, "k_cn_blocks");
+}
+// The stencil launch of one 12-column application.  The tensor-core stencil
+// needs imaginary off-diagonal coefficients and tensor maps; otherwise the
+// TMA-staged stencil runs, and without tensor maps the register-tiled one.
+// cn->last_stencil records which ran (the partial rows it left).
+int mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq::MvArgs &a) {
+  nrq_ctx *ctx = cn->ctx;
+  if (cn->stencil == NRQ_STENCIL_TENSOR && offdiag_imaginary(C)) {
+    double sign = 0.0;
+    int rc = ensure_blocks(cn, C, g, &sign);
+    if (rc) return rc;
+    ProfScope ps(ctx, 0, mv_bytes(ctx, mode, true));
+    if (nrq::launch_cn_mv4(mode, ctx->lat, C, sign, cn->Wblk, cn->Dsum, cn->Bsum, a, scal_err(cn->scal),
+                           ctx->sm_count, ctx->stream) == 0) {
+      cn->last_stencil = NRQ_STENCIL_TENSOR;
+      return NRQ_OK;
+    }
+  }
   ProfScope ps(ctx, 0, mv_bytes(ctx, mode));
-  if (cn->use_tma && nrq::launch_cn_mv3(mode, ctx->lat, C, g->U, cn->Dsum, cn->Bsum, cn->DE, a,
-                                        scal_err(cn->scal), ctx->sm_count, ctx->stream) == 0)
-    return;
-  cn->use_tma = false;  // tensor maps unavailable: register-tiled stencil from here on
+  if (cn->tma_ok && cn->stencil != NRQ_STENCIL_REGISTER &&
+      nrq::launch_cn_mv3(mode, ctx->lat, C, g->U, cn->Dsum, cn->Bsum, cn->DE, a, scal_err(cn->scal),
+                         ctx->sm_count, ctx->stream) == 0) {
+    cn->last_stencil = NRQ_STENCIL_TMA;
+    return NRQ_OK;
+  }
+  if (cn->stencil != NRQ_STENCIL_REGISTER) {  // tensor maps unavailable
+    cn->tma_ok = false;
+    cn->stencil = NRQ_STENCIL_REGISTER;
+  }
   nrq::launch_cn_mv(mode, ctx->lat, C, g->U, cn->Dsum, cn->Bsum, cn->DE, a, ctx->stream);
+  cn->last_stencil = NRQ_STENCIL_REGISTER;
+  return NRQ_OK;
+}
+// the MV_T input: the register-tiled stencil forms s = r - alpha v on the
+// fly, the staged ones read a materialised s
+bool mv_t_needs_s(const nrq_cn *cn, const nrq::CnCoef &CH) {
+  if (cn->stencil == NRQ_STENCIL_TENSOR && offdiag_imaginary(CH)) return true;
+  return cn->tma_ok && cn->stencil != NRQ_STENCIL_REGISTER;
 }
 void fin(nrq_cn *cn, int stage) {
   nrq_ctx *ctx = cn->ctx;
-  // the TMA-staged stencil leaves one partial row per (unit, colour warp)
-  const int64_t rows = (stage <= 2 && cn->use_tma) ? 3 * cn->nblocks : cn->nblocks;
+  // partial rows: one per 32-site block (register-tiled), per (unit, colour
+  // warp) (TMA-staged), per CTA (tensor-core)
+  int64_t rows = cn->nblocks;
+  if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TMA) rows = 3 * cn->nblocks;
+  if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TENSOR) rows = nrq::cn_mv4_rows(ctx->lat.V, ctx->sm_count);
   ProfScope ps(ctx, 2, (double)rows * 12 * 3 * 8);
   nrq::launch_cn_finalize(stage, rows, cn->partials, cn->scal, cn->tol, ctx->stream);
 }
-// Choose between the register-tiled and the TMA-staged stencil by timing,
-// on this lattice and field, the work each does in the solve: for the plain
-// form t = A^H (r - alpha v) (the register-tiled stencil forms s on the fly,
-// the TMA-staged one needs s materialised first); for the precision forms the
-// FP64 refinement residual.  Every buffer written here (s, t, the partials,
-// r32, d32) is rewritten by the solve before it is read.
+// Choose the stencil by timing, on this lattice and field, the work each
+// does in the solve: for the plain form t = A^H (r - alpha v) (the
+// register-tiled stencil forms s on the fly, the staged ones need s
+// materialised first); for the precision forms the FP64 refinement
+// residual.  Every buffer written here (s, t, the partials, r32, d32) is
+// rewritten by the solve before it is read.  A forced stencil skips this.
 int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
   nrq_ctx *ctx = cn->ctx;
   cn->stencil_tuned = true;
-  if (!cn->use_tma) return NRQ_OK;  // only the register-tiled stencil applies
+  if (cn->forced_stencil >= 0) {
+    cn->stencil = cn->forced_stencil;
+    return NRQ_OK;
+  }
+  if (!cn->tma_ok) return NRQ_OK;  // only the register-tiled stencil applies
   cudaStream_t st = ctx->stream;
-  const nrq::Lat L = ctx->lat;
   const bool prof = ctx->prof;
   ctx->prof = false;
-  cudaEvent_t e[3];
-  for (auto &x : e) NRQ_CUDA_TRY(ctx, cudaEventCreate(&x));
   const int reps = 3;
-  auto run = [&](bool tma) {
-    for (int r = 0; r < reps + 1; ++r) {
-      if (r == 1) cudaEventRecord(tma ? e[1] : e[0], st);
+  const bool tensor = offdiag_imaginary(CH);
+  cudaEvent_t e0, e1;
+  NRQ_CUDA_TRY(ctx, cudaEventCreate(&e0));
+  NRQ_CUDA_TRY(ctx, cudaEventCreate(&e1));
+  int rc = NRQ_OK;
+  for (int which = 0; which < 3 && !rc; ++which) {
+    cn->tune_ms[which] = -1.0;
+    if (which == NRQ_STENCIL_TENSOR && !tensor) continue;
+    cn->stencil = which;
+    for (int r = 0; r < reps + 1 && !rc; ++r) {
+      if (r == 1) cudaEventRecord(e0, st);
       nrq::MvArgs a{};
       a.partials = cn->partials;
       a.scal = cn->scal;
       if (cn->form == 0) {
         a.out = cn->t;
-        if (tma) {
-          nrq::launch_vec_s(L, cn->s, cn->r, cn->v, cn->scal, st);
+        if (mv_t_needs_s(cn, CH)) {
+          nrq::launch_vec_s(ctx->lat, cn->s, cn->r, cn->v, cn->scal, st);
           a.in = cn->s;
-          nrq::launch_cn_mv3(nrq::MV_T, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, scal_err(cn->scal),
-                             ctx->sm_count, st);
         } else {
           a.in = cn->r;
           a.in2 = cn->v;
-          nrq::launch_cn_mv(nrq::MV_T, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, st);
         }
+        rc = mv(cn, nrq::MV_T, CH, g, a);
       } else {
         a.in = cn->x;
         a.bvec = cn->b;
         a.r32 = cn->r32;
         a.d32 = cn->dA32;
-        if (tma)
-          nrq::launch_cn_mv3(nrq::MV_RESC, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, scal_err(cn->scal),
-                             ctx->sm_count, st);
-        else
-          nrq::launch_cn_mv(nrq::MV_RESC, L, CH, g->U, cn->Dsum, cn->Bsum, cn->DE, a, st);
+        rc = mv(cn, nrq::MV_RESC, CH, g, a);
       }
     }
-  };
-  run(false);
-  cudaEventRecord(e[2], st);
-  run(true);
-  cudaEvent_t done;
-  cudaEventCreate(&done);
-  cudaEventRecord(done, st);
-  cudaEventSynchronize(done);
-  float ms_v2 = 0.f, ms_v3 = 0.f;
-  cudaEventElapsedTime(&ms_v2, e[0], e[2]);
-  cudaEventElapsedTime(&ms_v3, e[1], done);
-  for (auto &x : e) cudaEventDestroy(x);
-  cudaEventDestroy(done);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (cn->last_stencil == which) cn->tune_ms[which] = ms / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   ctx->prof = prof;
-  int rc = check_launch(ctx, "stencil tuning");
   if (rc) return rc;
-  cn->tune_ms[0] = ms_v2 / reps;
-  cn->tune_ms[1] = ms_v3 / reps;
-  cn->use_tma = cn->tune_ms[1] < cn->tune_ms[0];
+  if ((rc = check_launch(ctx, "stencil tuning"))) return rc;
+  int best = NRQ_STENCIL_REGISTER;
+  for (int which = 1; which < 3; ++which)
+    if (cn->tune_ms[which] > 0.0 && cn->tune_ms[which] < cn->tune_ms[best]) best = which;
+  cn->stencil = best;
   return NRQ_OK;
 }
-
 int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
   nrq_ctx *ctx = cn->ctx;
   int rc = gauge_sync64(g);
   if (rc) return rc;
   ProfScope ps(ctx, 3, (double)ctx->lat.V * (432.0 + 192.0));
   nrq::launch_cn_prepare(ctx->lat, g->U, g->E, cn->Dsum, cn->Bsum, cn->DE, ctx->stream);
+  cn->w_valid = false;  // the tensor-core blocks follow the new gauge field on demand
   return check_launch(ctx, "k_cn_prepare");
 }
 }  // namespace
@@ -960,7 +1040,7 @@ extern "C" int nrq_cn_apply(nrq_cn *cn, const nrq_gauge *g, double mass, const d
   nrq::MvArgs a{};
   a.in = in->P;
   a.out = out->P;
-  mv(cn, nrq::MV_PLAIN, C, g, a);
+  if ((rc = mv(cn, nrq::MV_PLAIN, C, g, a))) return rc;
   return check_launch(ctx, "k_cn_mv");
 }
 
@@ -1004,7 +1084,7 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     a.in = h->P;
     a.out = cn->b;
     a.out2 = cn->x;
-    mv(cn, nrq::MV_RHS, CA, g, a);
+    if ((rc = mv(cn, nrq::MV_RHS, CA, g, a))) return rc;
     matvecs += 1;
     vstreams += 1;
   }
@@ -1075,7 +1155,7 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
       std::complex<double> it = 1.0 / seg[sp].theta;
       a.inv_theta[sp] = {it.real(), it.imag()};
     }
-    mv(cn, nrq::MV_RESC, CH, g, a);
+    if ((rc = mv(cn, nrq::MV_RESC, CH, g, a))) return rc;
     fin(cn, 0);
     matvecs += 1;
     vstreams += 3;
@@ -1178,7 +1258,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     a.in = h->P;
     a.out = cn->b;
     a.out2 = cn->x;
-    mv(cn, nrq::MV_RHS, CA, g, a);
+    if ((rc = mv(cn, nrq::MV_RHS, CA, g, a))) return rc;
     matvecs += 1;
     vstreams += 1;  // extra write of x0
   }
@@ -1196,7 +1276,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       a.out2 = cn->rh;
       a.out3 = cn->p;
       a.partials = cn->partials;
-      mv(cn, nrq::MV_RES, CH, g, a);
+      if ((rc = mv(cn, nrq::MV_RES, CH, g, a))) return rc;
       fin(cn, 0);
       matvecs += 1;
       vstreams += 3;  // b read, rh and p writes
@@ -1214,9 +1294,9 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       a.out = cn->v;
       a.partials = cn->partials;
       a.scal = cn->scal;
-      mv(cn, nrq::MV_V, CH, g, a);
+      if ((rc = mv(cn, nrq::MV_V, CH, g, a))) return rc;
       fin(cn, 1);
-      const bool tma = cn->use_tma;
+      const bool tma = mv_t_needs_s(cn, CH);
       nrq::MvArgs b{};
       if (tma) {  // s = r - alpha v materialised, then t = A^H s
         {
@@ -1232,7 +1312,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       b.out = cn->t;
       b.partials = cn->partials;
       b.scal = cn->scal;
-      mv(cn, nrq::MV_T, CH, g, b);
+      if ((rc = mv(cn, nrq::MV_T, CH, g, b))) return rc;
       fin(cn, 2);
       if (tma) {
         ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 7);

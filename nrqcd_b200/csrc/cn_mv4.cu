@@ -1,0 +1,605 @@
+// Tensor-core FP64 stencil of the assembled Crank-Nicolson operator
+// (src/nrqcd.f90:1175-1387 with PETSc's block transposition; the operator
+// is described in cn.cu).  out = D in + sum over the 6 neighbours of the
+// 6x6 spin-colour blocks applied to the 6 propagator columns, both species.
+//
+// Blocks.  Once per update, k_cn_blocks writes the forward block of every
+// site, direction and species (the operator's coefficients folded in):
+//   W_I(x) = ck (U_I(x)^T x 1) + cs0 (DE_I0(x)^T x s_K0^T) + cs1 (DE_I1(x)^T x s_K1^T)
+// With real Wilson coefficients every alpha_t is imaginary and every G_t
+// hermitian, so the backward block is W_back(x) = -W_I(x-I)^H; the kernel
+// reads it from the forward block of x-I (index transposed, signs flipped)
+// and needs no second copy.  A^H differs from A only by conj(alpha_t) =
+// -alpha_t: one set of blocks serves both with a sign on the neighbour sum.
+//
+// Products.  Per site, species and neighbour, out(6 x 6 cols) += W(6x6) in:
+// as a real GEMM, M = 16 (re rows 0-5, im rows 8-13 of the 6 output rows),
+// N = 8 (6 columns), K = 12 (re/im of the 6 input rows), three
+// mma.sync.m16n8k4 FP64 steps.  A lane's A fragment is one complex entry of
+// W (x1 or xi), its B fragment the real or imaginary part of one spinor
+// entry, its C fragment two complex outputs.  The FP64 tensor pipe has the
+// DFMA peak on B200 but one instruction carries 512 FMAs, which frees issue
+// slots for the loads the register-tiled stencils stall on.
+//
+// Pipeline.  Persistent, one CTA (8 warps) per SM.  A work unit is 16 sites
+// (x0 = 16u); five stages per unit stream through five shared-memory buffers
+// (TMA tiles for the spinors, bulk copies for the blocks, completion on
+// mbarriers): stage 0 = diagonal, +x, -x; 1 = +y; 2 = -y; 3 = +z; 4 = -z.
+// Thread 0 issues the copies four stages ahead.  A warp owns two sites of
+// the unit.  A site whose neighbour (periodic wrap) or neighbour block lies
+// outside the stage's tiles reads it from global memory (warp-uniform).
+//
+// Every mbarrier wait is bounded (about two seconds); on expiry the thread
+// records NRQ_ERR_TIMEOUT in *err, skips the remaining work without leaving
+// a barrier unmatched, and thread 0 waits (bounded) for its copies in flight
+// before the CTA exits.  Single-GPU code: no load uses cluster multicast.
+#include <algorithm>
+#include <type_traits>
+
+#include "../../include/nrqcd_b200.h"
+#include "nrq_kernels.cuh"
+#include "stage.cuh"
+
+namespace nrq {
+
+namespace mv4 {
+constexpr int kUnit = 16;                 // sites per work unit
+constexpr int kTileS = 19;                // spinor tile width in sites (odd stride in 16-byte words)
+constexpr int kStages = 5;                // stages per unit
+constexpr int kBufs = 5;                  // shared-memory buffers
+constexpr int kWarps = kUnit;             // one site per warp
+constexpr int kThreads = kWarps * 32;
+constexpr int kBlk = 36;                  // complex entries of one 6x6 block
+constexpr int kBlkBytes = kBlk * 16;      // 576
+constexpr int kWMax = kUnit + 1;          // blocks per species and stage (stage 0: x0-1 .. x0+15)
+// byte offsets inside one buffer (TMA destinations 128-byte aligned)
+constexpr int kOffSpin = 0;                            // 72 x 19 x 16 = 21888
+constexpr int kOffW = 21888;                           // 2 x 17 x 576 = 19584
+constexpr int kWSpecies = kWMax * kBlkBytes;           // 9792
+constexpr int kOffD = kOffW + 2 * kWSpecies;           // 9 x 16 x 16 = 2304
+constexpr int kOffB = kOffD + 2304;                    // 9 x 16 x 8 = 1152
+constexpr int kBufBytes = kOffB + 1152;                // 44928
+constexpr uint32_t kSpinBytes = 72 * kTileS * 16;
+constexpr int kSmemBytes = kBufs * kBufBytes + 128;    // + alignment slack
+static_assert(kOffW % 128 == 0 && kOffD % 128 == 0 && kOffB % 128 == 0 && kBufBytes % 128 == 0, "TMA alignment");
+}  // namespace mv4
+
+struct Mv4Maps {
+  CUtensorMap spin;  // 72 planes x 2V doubles, box {38, 72}
+  CUtensorMap D;     // 9 planes x 2V doubles, box {32, 9}
+  CUtensorMap B;     // 9 planes x V doubles, box {16, 9}
+};
+
+// entry (s, t) of s_k^T for the reference Pauli matrices (src/su2.f90:68-79
+// holds s_2 transposed, so s_2^T = [[0,-i],[i,0]])
+__device__ __forceinline__ cplx pauli_t(int k, int s, int t) {
+  if (k == 0) return (s != t) ? cplx{1.0, 0.0} : cplx{0.0, 0.0};
+  if (k == 1) {
+    if (s == 0 && t == 1) return {0.0, -1.0};
+    if (s == 1 && t == 0) return {0.0, 1.0};
+    return {0.0, 0.0};
+  }
+  if (s != t) return {0.0, 0.0};
+  return (s == 0) ? cplx{1.0, 0.0} : cplx{-1.0, 0.0};
+}
+
+// storage slot of entry (row g, column q) inside a 6x6 block: the entries a
+// lane group reads in one MMA step (q in {2j, 2j+1}, all rows) are adjacent
+__host__ __device__ __forceinline__ int blk_slot(int g, int q) { return ((q >> 1) * 6 + g) * 2 + (q & 1); }
+
+// One thread per (direction I, species, site, output row g): row g of the
+// forward block W_I(x) of that species.  Layout: block (I*2 + sp)*V + x.
+__global__ void __launch_bounds__(256) k_cn_blocks(Lat L, CnCoef C, const double2 *__restrict__ U,
+                                                   const double2 *__restrict__ DE, double2 *__restrict__ W) {
+  const int64_t V = L.V;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= 36 * V) return;
+  const int g = (int)(tid % 6);
+  const int64_t r = tid / 6;  // (I*2 + sp)*V + x
+  const int64_t x = r % V;
+  const int isp = (int)(r / V);
+  const int I = isp >> 1, sp = isp & 1;
+  const int c = g >> 1, s = g & 1;
+  const int K0 = (I + 2) % 3, K1 = (I + 1) % 3;
+  const cplx ck = (-0.5 * C.inva2[I]) * C.kin[sp];
+  const cplx cs0 = times_i(C.so[sp]), cs1 = -times_i(C.so[sp]);
+  double2 *blk = W + r * mv4::kBlk;
+#pragma unroll
+  for (int cp = 0; cp < 3; ++cp) {
+    const int e = cp * 3 + c;  // M^T[c][cp] = M[cp][c]
+    const cplx u = ldg(U + (int64_t)(I * 9 + e) * V + x);
+    const cplx d0 = ldg(DE + (int64_t)((I * 2 + 0) * 9 + e) * V + x);
+    const cplx d1 = ldg(DE + (int64_t)((I * 2 + 1) * 9 + e) * V + x);
+    const cplx ku = ck * u, e0 = cs0 * d0, e1 = cs1 * d1;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      cplx v = (s == t) ? ku : cplx{0.0, 0.0};
+      v = v + pauli_t(K0, s, t) * e0 + pauli_t(K1, s, t) * e1;
+      st(blk + blk_slot(g, 2 * cp + t), v);
+    }
+  }
+}
+
+// D(16x8) += A(16x4) B(4x8), FP64 tensor cores
+__device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, double b0) {
+  asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+// sign flip by an XOR on the high word (m = 0 or the sign bit)
+__device__ __forceinline__ double flip(double v, unsigned m) {
+  return __hiloint2double(__double2hiint(v) ^ (int)m, __double2loint(v));
+}
+constexpr unsigned kSign = 0x80000000u;
+// shared-memory load at a register address plus a compile-time offset
+template <int OFF>
+__device__ __forceinline__ double lds_at(uint32_t a) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1+%2];" : "=d"(v) : "r"(a), "n"(OFF));
+  return v;
+}
+
+// 32-bit coordinates and neighbours (the stencil runs for V < 2^31 only)
+__device__ __forceinline__ void coords32(const Lat &L, uint32_t s, uint32_t &x, uint32_t &y, uint32_t &z) {
+  const uint32_t nx = (uint32_t)L.nx, ny = (uint32_t)L.ny;
+  const uint32_t t = s / nx;
+  x = s - t * nx;
+  z = t / ny;
+  y = t - z * ny;
+}
+__device__ __forceinline__ int nb32(const Lat &L, uint32_t s, int d, int sgn) {
+  uint32_t x, y, z;
+  coords32(L, s, x, y, z);
+  const uint32_t nx = (uint32_t)L.nx, ny = (uint32_t)L.ny, nz = (uint32_t)L.nz;
+  if (d == 0) x = sgn > 0 ? (x + 1 == nx ? 0 : x + 1) : (x == 0 ? nx - 1 : x - 1);
+  else if (d == 1) y = sgn > 0 ? (y + 1 == ny ? 0 : y + 1) : (y == 0 ? ny - 1 : y - 1);
+  else z = sgn > 0 ? (z + 1 == nz ? 0 : z + 1) : (z == 0 ? nz - 1 : z - 1);
+  return (int)((z * ny + y) * nx + x);
+}
+// first sites of the spinor tiles of the five stages of the unit at x0
+// (stage 0: x0 - 1; stages 1-4: the +y, -y, +z, -z neighbours of x0), from
+// one coordinate decomposition
+__device__ __forceinline__ void mv4_spin_starts(const Lat &L, int x0, int ss[5]) {
+  uint32_t cx, cy, cz;
+  coords32(L, (uint32_t)x0, cx, cy, cz);
+  (void)cx;
+  const int ny = (int)L.ny, nz = (int)L.nz, row = (int)L.nx, plane = (int)(L.nx * L.ny);
+  ss[0] = x0 - 1;
+  ss[1] = (int)cy + 1 < ny ? x0 + row : x0 - (ny - 1) * row;
+  ss[2] = cy > 0 ? x0 - row : x0 + (ny - 1) * row;
+  ss[3] = (int)cz + 1 < nz ? x0 + plane : x0 - (nz - 1) * plane;
+  ss[4] = cz > 0 ? x0 - plane : x0 + (nz - 1) * plane;
+}
+// first block of the block tiles of stage st (forward stages: the unit
+// itself; backward stages: the unit's neighbours; stage 0 covers both)
+__device__ __forceinline__ int mv4_blk_start(int x0, int spin_start, int st) {
+  if (st == 0) return x0 > 0 ? x0 - 1 : 0;
+  if (st == 1 || st == 3) return x0;
+  return spin_start;
+}
+__device__ __forceinline__ int mv4_blk_count(int V, int start, int st) {
+  const int want = st == 0 ? mv4::kWMax : mv4::kUnit;
+  return min(want, V - start);
+}
+
+// Operands of step J of a neighbour with every operand in the stage's
+// shared tiles: wa0/wa1 = the lane's A-fragment addresses (block of species
+// 0), sb = its B-fragment address (species 0); the step and the species add
+// compile-time offsets.
+template <bool BWD, int J>
+__device__ __forceinline__ void nb_fast_load(double (&a0)[2], double (&a1)[2], double (&b0)[2], uint32_t wa0,
+                                             uint32_t wa1, uint32_t sb) {
+  constexpr int oA = J * (BWD ? 64 : 192), sA = mv4::kWSpecies;
+  constexpr int oB = J * 2 * mv4::kTileS * 16, sB = 36 * mv4::kTileS * 16;
+  a0[0] = lds_at<oA>(wa0);
+  a0[1] = lds_at<oA + sA>(wa0);
+  a1[0] = lds_at<oA>(wa1);
+  a1[1] = lds_at<oA + sA>(wa1);
+  b0[0] = lds_at<oB>(sb);
+  b0[1] = lds_at<oB + sB>(sb);
+}
+// a whole neighbour of the warp's site: all operands loaded, then 6 MMAs in
+// two independent chains (species)
+template <bool BWD>
+__device__ __forceinline__ void nb_fast(double (&acc)[2][4], uint32_t wa0, uint32_t wa1, uint32_t sb, unsigned m0,
+                                        unsigned m1) {
+  double a0[3][2], a1[3][2], b0[3][2];
+  nb_fast_load<BWD, 0>(a0[0], a1[0], b0[0], wa0, wa1, sb);
+  nb_fast_load<BWD, 1>(a0[1], a1[1], b0[1], wa0, wa1, sb);
+  nb_fast_load<BWD, 2>(a0[2], a1[2], b0[2], wa0, wa1, sb);
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) dmma(acc[sp], flip(a0[j][sp], m0), flip(a1[j][sp], m1), b0[j][sp]);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(mv4::kThreads, 1)
+    k_cn_mv4(Lat L, CnCoef C, double nb_sign, const __grid_constant__ Mv4Maps maps, const double2 *__restrict__ W,
+             const double2 *__restrict__ Dsum, const double *__restrict__ Bsum, MvArgs A, int64_t nunits, int *err) {
+  using namespace mv4;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kBufs], empty_bar[kBufs];
+  // per-warp partial sums of the CTA (one partial row per CTA, at the end)
+  __shared__ double red[kWarps][CN_COLS][3];
+  // per warp and unit: neighbours (+x,-x,+y,-y,+z,-z) of its site (entries
+  // 0-5) and the spinor tile starts of stages 1-4 (6-9)
+  __shared__ int nbt[kWarps][10];
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t V = L.V;
+
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kBufs; ++b) {
+      mbar_init(&full_bar[b], 1);
+      mbar_init(&empty_bar[b], kWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  // ---- producer role of thread 0: issues the stages of this CTA's units in
+  // order, kBufs - 1 ahead of the consumers (incremental 32-bit counters)
+  const int V32 = (int)V;  // the launcher admits V < 2^31 only
+  const int nu = (int)nunits;
+  const int my_units = (nu - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int total = my_units * kStages;
+  int issued = 0;
+  int p_unit = (int)blockIdx.x, p_stg = 0, p_buf = 0;  // next stage to issue
+  uint32_t p_par = 0;                                   // empty-barrier parity of p_buf's previous use
+  int pss[5] = {0, 0, 0, 0, 0};                         // tile starts of p_unit
+  auto issue = [&]() {
+    if (issued >= kBufs && !mbar_wait(&empty_bar[p_buf], p_par)) return false;
+    const int x0 = p_unit * kUnit;
+    if (p_stg == 0) mv4_spin_starts(L, x0, pss);
+    unsigned char *bb = smem + p_buf * kBufBytes;
+    const int stg = p_stg;
+    const int I = (stg == 0) ? 0 : (stg + 1) / 2;
+    // stage start without a dynamically indexed (local-memory) array
+    const int sst = stg == 0 ? pss[0] : stg == 1 ? pss[1] : stg == 2 ? pss[2] : stg == 3 ? pss[3] : pss[4];
+    const int ws = mv4_blk_start(x0, sst, stg);
+    const int wn = mv4_blk_count(V32, ws, stg);
+    uint32_t tx = kSpinBytes + 2u * (uint32_t)wn * kBlkBytes;
+    if (stg == 0) tx += 2304 + 1152;
+    mbar_expect_tx(&full_bar[p_buf], tx);
+    tma_2d(bb + kOffSpin, &maps.spin, 2 * sst, 0, &full_bar[p_buf]);
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp)
+      bulk_1d(bb + kOffW + sp * kWSpecies, W + ((int64_t)(I * 2 + sp) * V + ws) * kBlk, (uint32_t)wn * kBlkBytes,
+              &full_bar[p_buf]);
+    if (stg == 0) {
+      tma_2d(bb + kOffD, &maps.D, 2 * x0, 0, &full_bar[p_buf]);
+      tma_2d(bb + kOffB, &maps.B, x0, 0, &full_bar[p_buf]);
+    }
+    if (++p_stg == kStages) {
+      p_stg = 0;
+      p_unit += (int)gridDim.x;
+    }
+    if (++p_buf == kBufs) {
+      p_buf = 0;
+      if (issued >= kBufs) p_par ^= 1u;
+    }
+    return true;
+  };
+  bool prod_dead = false, dead = false;
+  if (threadIdx.x == 0)
+    for (; issued < total && issued < kBufs - 1; ++issued) issue();
+  int c_buf = 0;       // consumers: buffer of the current stage
+  uint32_t c_par = 0;  // its full-barrier parity
+  int consumed = 0;
+  auto stage_begin = [&]() -> const unsigned char * {
+    if (threadIdx.x == 0 && !prod_dead && issued < total) {
+      if (issue()) ++issued;
+      else {
+        prod_dead = true;
+        atomicExch(err, NRQ_ERR_TIMEOUT);
+      }
+    }
+    if (!dead && !mbar_wait(&full_bar[c_buf], c_par)) {
+      dead = true;
+      atomicExch(err, NRQ_ERR_TIMEOUT);
+    }
+    return smem + c_buf * kBufBytes;
+  };
+  auto stage_end = [&]() {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty_bar[c_buf]);
+    ++consumed;
+    if (++c_buf == kBufs) {
+      c_buf = 0;
+      c_par ^= 1u;
+    }
+  };
+
+  // ---- lane roles in the MMA fragments
+  const int g = lane >> 2, kq = lane & 3;
+  const int gc = g < 6 ? g : 5;       // rows 6, 7 are padding (any finite data)
+  const int part = kq & 1, h = kq >> 1;
+  const bool out_lane = g < 6 && kq < 3;  // owns output rows g, columns 2kq, 2kq+1
+  const unsigned nbm = nb_sign < 0.0 ? kSign : 0u;
+  // A fragments: component byte offsets and sign masks (forward, backward)
+  const uint32_t ca0 = (uint32_t)part * 8u, ca1 = (uint32_t)(1 - part) * 8u;
+  const unsigned mf0 = (part ? kSign : 0u) ^ nbm, mf1 = nbm;
+  const unsigned mb0 = kSign ^ nbm, mb1 = (part ? kSign : 0u) ^ nbm;
+  // lane byte offsets of step 0, species 0: A inside a block (forward and
+  // backward = transposed entry), B inside a spinor tile column
+  const uint32_t offAf = (uint32_t)(2 * gc + h) * 16u, offAb = (uint32_t)((gc >> 1) * 12 + 2 * h + (gc & 1)) * 16u;
+  const uint32_t offB = (uint32_t)((gc * 6 + h) * kTileS * 16) + (uint32_t)part * 8u;
+
+  double acc[2][4];  // [species][C fragment] of the warp's site
+
+  // general path of one neighbour: block and spinor each in the stage's
+  // shared tiles or in global memory (periodic wraps, tile edges)
+  auto nb_general = [&](bool bwd, bool wsh, uint32_t wsa, const double2 *wg, bool ssh, uint32_t ssa,
+                        const double2 *sg) {
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) {
+      double a0[3], a1[3], b0[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int q = 2 * j + h;
+        const int sl = bwd ? blk_slot(q, gc) : blk_slot(gc, q);
+        const int pl = gc * 6 + q;  // spinor plane in the species: column n = gc, row q
+        if (wsh) {
+          const uint32_t ea = wsa + (uint32_t)(sp * kWSpecies + sl * 16);
+          a0[j] = lds1(ea + ca0);
+          a1[j] = lds1(ea + ca1);
+        } else {
+          const double *ep = (const double *)(wg + (int64_t)sp * V * kBlk + sl);
+          a0[j] = __ldg(ep + part);
+          a1[j] = __ldg(ep + 1 - part);
+        }
+        if (ssh)
+          b0[j] = lds1(ssa + (uint32_t)(((sp * 36 + pl) * kTileS) * 16) + (uint32_t)part * 8u);
+        else
+          b0[j] = __ldg((const double *)(sg + (int64_t)(sp * 36 + pl) * V) + part);
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        dmma(acc[sp], flip(a0[j], bwd ? mb0 : mf0), flip(a1[j], bwd ? mb1 : mf1), b0[j]);
+    }
+  };
+  // one neighbour (direction I, forward or backward): m = site of the
+  // forward block, y = neighbour site; the tiles start at block ws (wn
+  // blocks) and spinor site ss
+  auto neighbour = [&](auto BWDc, int I, uint32_t sw, uint32_t sspin, int ws, int wn, int ss, int m, int y) {
+    constexpr bool BWD = decltype(BWDc)::value;
+    const int wi = m - ws, si = y - ss;
+    const bool wsh = (unsigned)wi < (unsigned)wn, ssh = (unsigned)si < (unsigned)kTileS;
+    if (wsh && ssh) {
+      const uint32_t blk = sw + (uint32_t)wi * kBlkBytes + (BWD ? offAb : offAf);
+      nb_fast<BWD>(acc, blk + ca0, blk + ca1, sspin + (uint32_t)si * 16u + offB, BWD ? mb0 : mf0, BWD ? mb1 : mf1);
+    } else {
+      nb_general(BWD, wsh, sw + (uint32_t)((wsh ? wi : 0) * kBlkBytes), W + ((int64_t)(I * 2) * V + m) * kBlk, ssh,
+                 sspin + (uint32_t)((ssh ? si : 0) * 16), A.in + y);
+    }
+  };
+  using F = std::integral_constant<bool, false>;
+  using T = std::integral_constant<bool, true>;
+
+  constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
+  // the lane's partial sums over every unit of this CTA: [species][column e][quantity]
+  double qs[2][2][3];
+#pragma unroll
+  for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) qs[sp][e][0] = qs[sp][e][1] = qs[sp][e][2] = 0.0;
+
+  for (int u = (int)blockIdx.x; u < nu; u += (int)gridDim.x) {
+    const int x0 = u * kUnit;
+    const int x = x0 + warp;
+    const bool act = x < V32;
+    // neighbour table, one entry per lane (the previous unit's reads ended
+    // at its last stage_end): lanes 0-5 the site's neighbours, lanes 6-9
+    // the tile starts of stages 1-4
+    if (lane < 10) {
+      int v = 0;
+      if (lane < 6) {
+        if (act) v = nb32(L, (uint32_t)x, lane >> 1, (lane & 1) ? -1 : +1);
+      } else {
+        const int st = lane - 5;  // 1..4
+        v = nb32(L, (uint32_t)x0, (st + 1) >> 1, (st & 1) ? +1 : -1);
+      }
+      nbt[warp][lane] = v;
+    }
+    __syncwarp();
+    const int *nbw = nbt[warp];
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[sp][e] = 0.0;
+    // epilogue operand of the lane's outputs (b, rh or the centre spinor)
+    cplx pre[2][2];
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) pre[sp][0] = pre[sp][1] = cplx{0.0, 0.0};
+
+    // ---------------------------------------------------------- stage 0
+    {
+      const unsigned char *b = stage_begin();
+      if (!dead && act) {
+        const int ss = x0 - 1, ws = mv4_blk_start(x0, ss, 0);
+        const int wn = mv4_blk_count(V32, ws, 0);
+        const uint32_t sspin = smem_u32(b + kOffSpin), sw = smem_u32(b + kOffW);
+        const uint32_t sD = smem_u32(b + kOffD), sB = smem_u32(b + kOffB);
+        const int l = warp;
+        if (out_lane) {
+#pragma unroll
+          for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int pl = sp * 36 + (2 * kq + e) * 6 + g;
+              if (MODE == MV_T || MODE == MV_RHS)
+                pre[sp][e] = lds2(sspin + (uint32_t)((pl * kTileS + l + 1) * 16));
+              else if (MODE == MV_RES || MODE == MV_RESC)
+                pre[sp][e] = ldg(A.bvec + (int64_t)pl * V + x);
+              else if (MODE == MV_V)
+                pre[sp][e] = ldg(A.in2 + (int64_t)pl * V + x);
+            }
+        }
+        // diagonal block (colour only): A = delta_st Cd_c[cp], centre spinor
+        {
+          const int c = gc >> 1, s = gc & 1;
+          cplx dv[3];
+          double bv[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {  // j = cp, input spin t = h
+            const int e = j * 3 + c;
+            dv[j] = lds2(sD + (uint32_t)((e * kUnit + l) * 16));
+            bv[j] = lds1(sB + (uint32_t)((e * kUnit + l) * 8));
+          }
+          const uint32_t sbc = sspin + (uint32_t)(l + 1) * 16u + offB;
+#pragma unroll
+          for (int sp = 0; sp < 2; ++sp) {
+            const cplx ak = C.kin[sp], am = C.mag[sp], ad = C.dar[sp];
+            const cplx dg = C.dkin * ak + cplx{1.0, 0.0};
+            const uint32_t sbs = sbc + (uint32_t)(sp * 36 * kTileS * 16);
+            double b0[3];
+            b0[0] = lds_at<0>(sbs);
+            b0[1] = lds_at<2 * kTileS * 16>(sbs);
+            b0[2] = lds_at<4 * kTileS * 16>(sbs);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              cplx cd = ad * dv[j] + bv[j] * am;
+              if (j == c) cd = cd + dg;
+              if (s != h) cd = cplx{0.0, 0.0};
+              dmma(acc[sp], part ? -cd.im : cd.re, part ? cd.re : cd.im, b0[j]);
+            }
+          }
+        }
+        // +x: block at x (forward), spinor at x+1; -x: block and spinor at x-1
+        neighbour(F{}, 0, sw, sspin, ws, wn, ss, x, nbw[0]);
+        neighbour(T{}, 0, sw, sspin, ws, wn, ss, nbw[1], nbw[1]);
+      }
+      stage_end();
+    }
+    // ------------------------------------------------------- stages 1-4
+#pragma unroll
+    for (int stg = 1; stg < kStages; ++stg) {
+      const unsigned char *b = stage_begin();
+      if (!dead && act) {
+        const int I = (stg + 1) / 2;
+        const int ss = nbw[5 + stg], ws = mv4_blk_start(x0, ss, stg);
+        const int wn = mv4_blk_count(V32, ws, stg);
+        const uint32_t sspin = smem_u32(b + kOffSpin), sw = smem_u32(b + kOffW);
+        const int y = nbw[2 * I + ((stg & 1) ? 0 : 1)];
+        if (stg & 1)
+          neighbour(F{}, I, sw, sspin, ws, wn, ss, x, y);
+        else
+          neighbour(T{}, I, sw, sspin, ws, wn, ss, y, y);
+      }
+      if (stg < kStages - 1) stage_end();
+    }
+
+    // ------------------------------------------------------------ epilogue
+    if (!dead && act && out_lane) {
+#pragma unroll
+      for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int64_t o = (int64_t)(sp * 36 + (2 * kq + e) * 6 + g) * V + x;
+          const cplx y_ = {acc[sp][e], acc[sp][2 + e]};
+          const cplx pv = pre[sp][e];
+          if (MODE == MV_PLAIN) {
+            st(A.out + o, y_);
+          } else if (MODE == MV_RHS) {
+            st(A.out + o, y_);
+            st(A.out2 + o, 2.0 * y_ - pv);
+          } else if (MODE == MV_RES) {
+            const cplx r = pv - y_;
+            st(A.out + o, r);
+            st(A.out2 + o, r);
+            st(A.out3 + o, r);
+            qs[sp][e][0] += norm2(r);
+            qs[sp][e][1] += norm2(pv);
+          } else if (MODE == MV_V) {
+            st(A.out + o, y_);
+            cplx dd = {0.0, 0.0};
+            cmac_cj(dd, pv, y_);
+            qs[sp][e][0] += dd.re;
+            qs[sp][e][1] += dd.im;
+          } else if (MODE == MV_RESC) {
+            const cplx r = pv - y_;
+            const cplx dd = r * A.inv_theta[sp];
+            A.r32[o] = make_float2((float)r.re, (float)r.im);
+            A.d32[o] = make_float2((float)dd.re, (float)dd.im);
+            qs[sp][e][0] += norm2(r);
+            qs[sp][e][1] += norm2(pv);
+          } else {  // MV_T: in = s
+            st(A.out + o, y_);
+            cplx dd = {0.0, 0.0};
+            cmac_cj(dd, y_, pv);
+            qs[sp][e][0] += dd.re;
+            qs[sp][e][1] += dd.im;
+            qs[sp][e][2] += norm2(y_);
+          }
+        }
+    }
+    stage_end();
+  }
+  // error path: copies issued ahead of the consumers must land before exit
+  if (threadIdx.x == 0 && (dead || prod_dead))
+    for (int kk = consumed; kk < issued; ++kk)
+      if (!mbar_wait(&full_bar[kk % kBufs], (uint32_t)((kk / kBufs) & 1))) atomicExch(err, NRQ_ERR_TIMEOUT);
+  // one partial row per CTA: sum over the rows g (lane bits 2-4), then over
+  // the warps in a fixed order
+  if constexpr (NQ > 0) {
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+      for (int e = 0; e < 2; ++e)
+#pragma unroll
+        for (int kk = 0; kk < NQ; ++kk) {
+          double v = qs[sp][e][kk];
+          v += __shfl_xor_sync(0xffffffffu, v, 4);
+          v += __shfl_xor_sync(0xffffffffu, v, 8);
+          v += __shfl_xor_sync(0xffffffffu, v, 16);
+          if (lane < 3) red[warp][sp * 6 + 2 * lane + e][kk] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < CN_COLS * NQ) {
+      const int col12 = threadIdx.x / NQ, kk = threadIdx.x % NQ;
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) v += red[w][col12][kk];
+      A.partials[((int64_t)blockIdx.x * CN_COLS + col12) * NQ + kk] = v;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host
+void launch_cn_blocks(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, cudaStream_t st) {
+  const int64_t n = 36 * L.V;
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  k_cn_blocks<<<grid, 256, 0, st>>>(L, C, U, DE, W);
+}
+
+int64_t cn_mv4_units(int64_t V) { return (V + mv4::kUnit - 1) / mv4::kUnit; }
+int64_t cn_mv4_rows(int64_t V, int sm_count) { return std::min<int64_t>(cn_mv4_units(V), sm_count); }
+
+int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double2 *W, const double2 *Dsum,
+                  const double *Bsum, const MvArgs &a, int *err, int sm_count, cudaStream_t st) {
+  using namespace mv4;
+  const uint64_t V = (uint64_t)L.V;
+  if (L.V < kWMax || L.V > 0x7fffffffLL) return -1;
+  Mv4Maps maps;
+  if (!stage::encode(&maps.spin, a.in, 2 * V, 72, 2 * kTileS, 72) ||
+      !stage::encode(&maps.D, Dsum, 2 * V, 9, 2 * kUnit, 9) || !stage::encode(&maps.B, Bsum, V, 9, kUnit, 9))
+    return -1;
+  const int64_t nunits = cn_mv4_units(L.V);
+  const unsigned grid = (unsigned)cn_mv4_rows(L.V, sm_count);
+  auto go = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    kern<<<grid, kThreads, kSmemBytes, st>>>(L, C, nb_sign, maps, W, Dsum, Bsum, a, nunits, err);
+  };
+  switch (mode) {
+    case MV_PLAIN: go(k_cn_mv4<MV_PLAIN>); break;
+    case MV_RHS: go(k_cn_mv4<MV_RHS>); break;
+    case MV_RES: go(k_cn_mv4<MV_RES>); break;
+    case MV_V: go(k_cn_mv4<MV_V>); break;
+    case MV_RESC: go(k_cn_mv4<MV_RESC>); break;
+    default: go(k_cn_mv4<MV_T>); break;
+  }
+  return 0;
+}
+
+}  // namespace nrq

@@ -124,11 +124,22 @@ struct nrq_cn {
   // Krylov vectors, 72 planes each
   double2 *b = nullptr, *x = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr,
           *t = nullptr, *s = nullptr;
-  // TMA-staged stencil in use (else the register-tiled one); chosen by timing
-  // both on the first update (tune_ms: register-tiled, TMA-staged)
-  bool use_tma = false;
+  // FP64 stencil (NRQ_STENCIL_*): register-tiled, TMA-staged or tensor-core.
+  // Chosen by timing the applicable ones on the first update (tune_ms, per
+  // launch) unless forced; tma_ok: tensor maps can describe the lattice.
+  // last_stencil: the stencil of the latest launch (its partial-row count).
+  int stencil = 0;
+  int forced_stencil = -1;
+  int last_stencil = 0;
+  bool tma_ok = false;
   bool stencil_tuned = false;
-  double tune_ms[2] = {-1.0, -1.0};
+  double tune_ms[3] = {-1.0, -1.0, -1.0};
+  // tensor-core stencil: forward 6x6 blocks (6 per site: direction x
+  // species, 36 complex each) built for the coefficients w_coef from the
+  // current gauge field (w_valid cleared by every preparation)
+  double2 *Wblk = nullptr;
+  bool w_valid = false;
+  nrq::CnCoef w_coef{};
   // precision form (form 1): FP32 copies of the per-step matrices and the
   // FP32 Chebyshev vectors; spectral bounds of the hermitian part
   float2 *U32 = nullptr, *DE32 = nullptr, *D32 = nullptr;

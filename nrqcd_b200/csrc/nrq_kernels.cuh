@@ -93,6 +93,17 @@ void launch_vec_xr_s(Lat L, double2 *x, double2 *r, const double2 *p, const doub
 // input is the materialised s = r - alpha v.
 int launch_cn_mv3(int mode, Lat L, const CnCoef &C, const double2 *U, const double2 *Dsum, const double *Bsum,
                   const double2 *DE, const MvArgs &a, int *err, int sm_count, cudaStream_t st);
+// Tensor-core stencil (cn_mv4.cu): forward 6x6 blocks of every site,
+// direction and species for coefficients C (216 complex per site), then the
+// stencil over them; nb_sign = -1 applies the operator whose off-diagonal
+// coefficients are those of C negated.  Needs imaginary off-diagonal
+// coefficients.  Returns nonzero if the tensor maps cannot describe this
+// lattice.  One partial row per CTA (cn_mv4_rows).
+void launch_cn_blocks(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, cudaStream_t st);
+int64_t cn_mv4_units(int64_t V);
+int64_t cn_mv4_rows(int64_t V, int sm_count);
+int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double2 *W, const double2 *Dsum,
+                  const double *Bsum, const MvArgs &a, int *err, int sm_count, cudaStream_t st);
 // finalize stages: 0 = after RES (rr, bb), 1 = alpha (rh.v), 2 = omega (t.s, t.t), 3 = beta (rh.r, r.r)
 void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
                         cudaStream_t st);

@@ -65,6 +65,31 @@ def solver_handle():
     return _cn
 
 
+STENCIL_REGISTER = 0  # register-tiled FP64 stencil (k_cn_mv2)
+STENCIL_TMA = 1       # TMA-staged FP64 stencil (k_cn_mv3)
+STENCIL_TENSOR = 2    # FP64 tensor-core stencil on per-update 6x6 blocks (k_cn_mv4)
+STENCIL_NAMES = {STENCIL_REGISTER: "k_cn_mv2 (register-tiled)", STENCIL_TMA: "k_cn_mv3 (TMA-staged)",
+                 STENCIL_TENSOR: "k_cn_mv4 (FP64 tensor cores)"}
+
+
+def SetStencil(stencil=None):
+    """Force the solver's FP64 stencil (STENCIL_*); None restores the choice
+    timed on the next update."""
+    ctx = lattice.context()
+    _capi.check(_capi.load().nrq_cn_set_stencil(solver_handle(), -1 if stencil is None else int(stencil)), ctx,
+                f"Error in {modulename}: stencil")
+
+
+def StencilInfo():
+    """(stencil in use, per-launch ms of each stencil timed on the first
+    update; -1 where not timed)."""
+    which = ctypes.c_int()
+    ms = np.zeros(3)
+    _capi.check(_capi.load().nrq_cn_stencil_info(solver_handle(), ctypes.byref(which), _capi.dptr(ms)),
+                lattice.context(), f"Error in {modulename}: stencil info")
+    return int(which.value), ms
+
+
 class NRQCDField:
     def __init__(self, lat=None):
         """lat: a lattice.Lattice (ensemble member); default the module context."""
