@@ -21,19 +21,26 @@
 // DFMA peak on B200 but one instruction carries 512 FMAs, which frees issue
 // slots for the loads the register-tiled stencils stall on.
 //
-// Pipeline.  Persistent, one CTA (8 warps) per SM.  A work unit is 16 sites
-// (x0 = 16u); five stages per unit stream through five shared-memory buffers
-// (TMA tiles for the spinors, bulk copies for the blocks, completion on
-// mbarriers): stage 0 = diagonal, +x, -x; 1 = +y; 2 = -y; 3 = +z; 4 = -z.
-// Thread 0 issues the copies four stages ahead.  A warp owns two sites of
-// the unit.  A site whose neighbour (periodic wrap) or neighbour block lies
-// outside the stage's tiles reads it from global memory (warp-uniform).
+// Pipeline.  Persistent, one CTA per SM: 16 consumer warps (one site of the
+// unit each) and one producer warp.  A work unit is 16 sites (x0 = 16u);
+// five stages per unit, stage s in shared-memory buffer s (TMA tiles for the
+// spinors, bulk copies for the blocks, completion on mbarriers): stage 0 =
+// diagonal, +x, -x; 1 = +y; 2 = -y; 3 = +z; 4 = -z.  The producer issues
+// each buffer's next stage as soon as every consumer released it.  A site
+// whose neighbour (periodic wrap) or neighbour block lies outside the stage's
+// tiles reads it from global memory (warp-uniform).  Results go through an
+// epilogue tile in buffer 4 (128-byte swizzle): each warp writes its site's
+// column, the producer stores the tile with TMA once all warps released the
+// buffer.  The residual and dot-product partial sums stay in registers over
+// all units of the CTA: one partial row per CTA.
 //
 // Every mbarrier wait is bounded (about two seconds); on expiry the thread
-// records NRQ_ERR_TIMEOUT in *err, skips the remaining work without leaving
-// a barrier unmatched, and thread 0 waits (bounded) for its copies in flight
-// before the CTA exits.  Single-GPU code: no load uses cluster multicast.
+// records NRQ_ERR_TIMEOUT in *err and skips the remaining work without
+// leaving a barrier unmatched; the producer waits (bounded) for its copies in
+// flight before the CTA exits.  Single-GPU code: no load uses cluster
+// multicast.
 #include <algorithm>
+#include <cstring>
 #include <type_traits>
 
 #include "../../include/nrqcd_b200.h"
@@ -45,29 +52,46 @@ namespace nrq {
 namespace mv4 {
 constexpr int kUnit = 16;                 // sites per work unit
 constexpr int kTileS = 19;                // spinor tile width in sites (odd stride in 16-byte words)
-constexpr int kStages = 5;                // stages per unit
-constexpr int kBufs = 5;                  // shared-memory buffers
-constexpr int kWarps = kUnit;             // one site per warp
-constexpr int kThreads = kWarps * 32;
+constexpr int kStages = 5;                // stages per unit; stage s always uses buffer s
+constexpr int kWarps = kUnit;             // consumer warps, one site each
+constexpr int kThreads = (kWarps + 1) * 32;  // + one producer warp
 constexpr int kBlk = 36;                  // complex entries of one 6x6 block
 constexpr int kBlkBytes = kBlk * 16;      // 576
 constexpr int kWMax = kUnit + 1;          // blocks per species and stage (stage 0: x0-1 .. x0+15)
-// byte offsets inside one buffer (TMA destinations 128-byte aligned)
-constexpr int kOffSpin = 0;                            // 72 x 19 x 16 = 21888
-constexpr int kOffW = 21888;                           // 2 x 17 x 576 = 19584
-constexpr int kWSpecies = kWMax * kBlkBytes;           // 9792
-constexpr int kOffD = kOffW + 2 * kWSpecies;           // 9 x 16 x 16 = 2304
-constexpr int kOffB = kOffD + 2304;                    // 9 x 16 x 8 = 1152
-constexpr int kBufBytes = kOffB + 1152;                // 44928
-constexpr uint32_t kSpinBytes = 72 * kTileS * 16;
-constexpr int kSmemBytes = kBufs * kBufBytes + 128;    // + alignment slack
-static_assert(kOffW % 128 == 0 && kOffD % 128 == 0 && kOffB % 128 == 0 && kBufBytes % 128 == 0, "TMA alignment");
+constexpr int kWSpecies0 = kWMax * kBlkBytes;  // 9792: species stride of stage 0's block tile
+constexpr int kWSpecies = kUnit * kBlkBytes;   // 9216: species stride of stages 1-4
+constexpr uint32_t kSpinBytes = 72 * kTileS * 16;  // 21888
+// Buffer layout (byte offsets from the 1024-aligned base).  Buffer 4 first:
+// spinors, blocks, then the epilogue tile (operand b or rh in, the result
+// out; two 128-byte-swizzled halves of 8 sites x 72 planes, 1024-aligned).
+// Buffer 0: spinors, blocks, Darwin and magnetic matrices.  Buffers 1-3:
+// spinors and blocks.
+constexpr int kEpiHalf = 72 * 128;                     // 9216
+constexpr int kBuf4 = 0, kOffEpi = 40960;              // buffer 4: spin 0, blocks 22528, epilogue 40960
+constexpr int kBuf0 = kOffEpi + 2 * kEpiHalf;          // 59392
+constexpr int kOffD = kSpinBytes + 2 * kWSpecies0;     // buffer 0: 41472 (9 x 16 x 16 = 2304)
+constexpr int kOffB = kOffD + 2304;                    // 43776 (9 x 16 x 8 = 1152)
+constexpr int kBuf1 = kBuf0 + kOffB + 1152;            // 104320
+constexpr int kBufPlain = kSpinBytes + 2 * kUnit * kBlkBytes;  // 40320: buffers 1-3
+constexpr int kSmemBytes = kBuf1 + 3 * kBufPlain + 1024;       // 226304 + alignment slack
+__host__ __device__ constexpr int buf_off(int s) {
+  return s == 4 ? kBuf4 : s == 0 ? kBuf0 : kBuf1 + (s - 1) * kBufPlain;
+}
+__host__ __device__ constexpr int w_off(int s) { return s == 4 ? 22528 : (int)kSpinBytes; }
+__host__ __device__ constexpr int w_species(int s) { return s == 0 ? kWSpecies0 : kWSpecies; }
+static_assert(kBuf0 % 128 == 0 && kBuf1 % 128 == 0 && kBufPlain % 128 == 0 && kOffD % 128 == 0 &&
+                  kOffB % 128 == 0 && kOffEpi % 1024 == 0 && 22528 >= (int)kSpinBytes &&
+                  22528 + 2 * kWSpecies <= kOffEpi && kBufPlain == (int)kSpinBytes + 2 * kWSpecies &&
+                  kBuf0 + kOffB + 1152 <= kBuf1 && kBuf1 + 3 * kBufPlain + 1024 <= kSmemBytes,
+              "buffer layout");
 }  // namespace mv4
 
 struct Mv4Maps {
-  CUtensorMap spin;  // 72 planes x 2V doubles, box {38, 72}
-  CUtensorMap D;     // 9 planes x 2V doubles, box {32, 9}
-  CUtensorMap B;     // 9 planes x V doubles, box {16, 9}
+  CUtensorMap spin;    // 72 planes x 2V doubles, box {38, 72}
+  CUtensorMap D;       // 9 planes x 2V doubles, box {32, 9}
+  CUtensorMap B;       // 9 planes x V doubles, box {16, 9}
+  CUtensorMap epi_in;  // epilogue operand (b or rh), box {16, 72}, 128-byte swizzle
+  CUtensorMap out[3];  // results stored from the epilogue tile, same boxes
 };
 
 // entry (s, t) of s_k^T for the reference Pauli matrices (src/su2.f90:68-79
@@ -186,10 +210,10 @@ __device__ __forceinline__ int mv4_blk_count(int V, int start, int st) {
 // shared tiles: wa0/wa1 = the lane's A-fragment addresses (block of species
 // 0), sb = its B-fragment address (species 0); the step and the species add
 // compile-time offsets.
-template <bool BWD, int J>
+template <bool BWD, int SA, int J>
 __device__ __forceinline__ void nb_fast_load(double (&a0)[2], double (&a1)[2], double (&b0)[2], uint32_t wa0,
                                              uint32_t wa1, uint32_t sb) {
-  constexpr int oA = J * (BWD ? 64 : 192), sA = mv4::kWSpecies;
+  constexpr int oA = J * (BWD ? 64 : 192), sA = SA;
   constexpr int oB = J * 2 * mv4::kTileS * 16, sB = 36 * mv4::kTileS * 16;
   a0[0] = lds_at<oA>(wa0);
   a0[1] = lds_at<oA + sA>(wa0);
@@ -199,38 +223,56 @@ __device__ __forceinline__ void nb_fast_load(double (&a0)[2], double (&a1)[2], d
   b0[1] = lds_at<oB + sB>(sb);
 }
 // a whole neighbour of the warp's site: all operands loaded, then 6 MMAs in
-// two independent chains (species)
-template <bool BWD>
+// two independent chains (species); SA = species stride of the block tile
+template <bool BWD, int SA>
 __device__ __forceinline__ void nb_fast(double (&acc)[2][4], uint32_t wa0, uint32_t wa1, uint32_t sb, unsigned m0,
                                         unsigned m1) {
   double a0[3][2], a1[3][2], b0[3][2];
-  nb_fast_load<BWD, 0>(a0[0], a1[0], b0[0], wa0, wa1, sb);
-  nb_fast_load<BWD, 1>(a0[1], a1[1], b0[1], wa0, wa1, sb);
-  nb_fast_load<BWD, 2>(a0[2], a1[2], b0[2], wa0, wa1, sb);
+  nb_fast_load<BWD, SA, 0>(a0[0], a1[0], b0[0], wa0, wa1, sb);
+  nb_fast_load<BWD, SA, 1>(a0[1], a1[1], b0[1], wa0, wa1, sb);
+  nb_fast_load<BWD, SA, 2>(a0[2], a1[2], b0[2], wa0, wa1, sb);
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp) dmma(acc[sp], flip(a0[j][sp], m0), flip(a1[j][sp], m1), b0[j][sp]);
 }
 
+// results of a mode stored from the epilogue tile (RES: r, rh and p are the
+// same values) and whether the epilogue operand arrives in it (b or rh)
+__host__ __device__ constexpr int mv4_tile_outputs(int mode) {
+  return mode == MV_RES ? 3 : (mode == MV_RESC ? 0 : 1);
+}
+__host__ __device__ constexpr bool mv4_tile_input(int mode) {
+  return mode == MV_RES || mode == MV_RESC || mode == MV_V;
+}
+// byte offset of (plane p, site l) in the epilogue tile: two halves of 8
+// sites, rows of 128 bytes, 16-byte chunks swizzled with the row (the
+// 128-byte swizzle of the tensor maps; the tile is 1024-aligned)
+__device__ __forceinline__ uint32_t epi_off(int p, int l) {
+  return (uint32_t)((l >> 3) * mv4::kEpiHalf + p * 128 + (((l & 7) ^ (p & 7)) << 4));
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(mv4::kThreads, 1)
+__global__ void __maxnreg__(96)
     k_cn_mv4(Lat L, CnCoef C, double nb_sign, const __grid_constant__ Mv4Maps maps, const double2 *__restrict__ W,
              const double2 *__restrict__ Dsum, const double *__restrict__ Bsum, MvArgs A, int64_t nunits, int *err) {
   using namespace mv4;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kBufs], empty_bar[kBufs];
+  constexpr int kNOut = mv4_tile_outputs(MODE);
+  constexpr bool kIn = mv4_tile_input(MODE);
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
   // per-warp partial sums of the CTA (one partial row per CTA, at the end)
   __shared__ double red[kWarps][CN_COLS][3];
   // per warp and unit: neighbours (+x,-x,+y,-y,+z,-z) of its site (entries
   // 0-5) and the spinor tile starts of stages 1-4 (6-9)
   __shared__ int nbt[kWarps][10];
-  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t V = L.V;
+  const int V32 = (int)V;  // the launcher admits V < 2^31 only
 
   if (threadIdx.x == 0) {
-    for (int b = 0; b < kBufs; ++b) {
+    for (int b = 0; b < kStages; ++b) {
       mbar_init(&full_bar[b], 1);
       mbar_init(&empty_bar[b], kWarps);
     }
@@ -238,22 +280,35 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
   }
   __syncthreads();
 
-  // ---- producer role of thread 0: issues the stages of this CTA's units in
-  // order, kBufs - 1 ahead of the consumers (incremental 32-bit counters)
-  const int V32 = (int)V;  // the launcher admits V < 2^31 only
+  // ---- producer: lane 0 of warp kWarps issues the stages of this CTA's
+  // units in order, as far ahead as the buffers allow.  Before refilling
+  // buffer 4 it stores the previous unit's results from the epilogue tile.
   const int nu = (int)nunits;
   const int my_units = (nu - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   const int total = my_units * kStages;
   int issued = 0;
-  int p_unit = (int)blockIdx.x, p_stg = 0, p_buf = 0;  // next stage to issue
-  uint32_t p_par = 0;                                   // empty-barrier parity of p_buf's previous use
-  int pss[5] = {0, 0, 0, 0, 0};                         // tile starts of p_unit
+  int p_unit = (int)blockIdx.x, p_stg = 0;
+  uint32_t p_par = 0;                // empty-barrier parity of the previous use of a buffer
+  int pss[5] = {0, 0, 0, 0, 0};      // tile starts of p_unit
+  auto store_results = [&](int x0) {
+#pragma unroll
+    for (int o = 0; o < kNOut; ++o)
+#pragma unroll
+      for (int hf = 0; hf < 2; ++hf)
+        tma_store_2d(&maps.out[o], 2 * x0 + 16 * hf, 0, smem + kBuf4 + kOffEpi + hf * kEpiHalf);
+    bulk_commit();
+  };
   auto issue = [&]() {
-    if (issued >= kBufs && !mbar_wait(&empty_bar[p_buf], p_par)) return false;
-    const int x0 = p_unit * kUnit;
-    if (p_stg == 0) mv4_spin_starts(L, x0, pss);
-    unsigned char *bb = smem + p_buf * kBufBytes;
     const int stg = p_stg;
+    if (issued >= kStages && !mbar_wait(&empty_bar[stg], p_par)) return false;
+    const int x0 = p_unit * kUnit;
+    if (stg == 0) mv4_spin_starts(L, x0, pss);
+    unsigned char *bb = smem + buf_off(stg);
+    if (stg == kStages - 1 && kNOut > 0 && issued >= kStages) {
+      // the previous unit's results must leave the tile before new operands land in it
+      store_results(x0 - (int)gridDim.x * kUnit);
+      bulk_wait_read_all();
+    }
     const int I = (stg == 0) ? 0 : (stg + 1) / 2;
     // stage start without a dynamically indexed (local-memory) array
     const int sst = stg == 0 ? pss[0] : stg == 1 ? pss[1] : stg == 2 ? pss[2] : stg == 3 ? pss[3] : pss[4];
@@ -261,54 +316,58 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
     const int wn = mv4_blk_count(V32, ws, stg);
     uint32_t tx = kSpinBytes + 2u * (uint32_t)wn * kBlkBytes;
     if (stg == 0) tx += 2304 + 1152;
-    mbar_expect_tx(&full_bar[p_buf], tx);
-    tma_2d(bb + kOffSpin, &maps.spin, 2 * sst, 0, &full_bar[p_buf]);
+    if (stg == kStages - 1 && kIn) tx += 2 * kEpiHalf;
+    mbar_expect_tx(&full_bar[stg], tx);
+    tma_2d(bb, &maps.spin, 2 * sst, 0, &full_bar[stg]);
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp)
-      bulk_1d(bb + kOffW + sp * kWSpecies, W + ((int64_t)(I * 2 + sp) * V + ws) * kBlk, (uint32_t)wn * kBlkBytes,
-              &full_bar[p_buf]);
+      bulk_1d(bb + w_off(stg) + sp * w_species(stg), W + ((int64_t)(I * 2 + sp) * V + ws) * kBlk,
+              (uint32_t)wn * kBlkBytes, &full_bar[stg]);
     if (stg == 0) {
-      tma_2d(bb + kOffD, &maps.D, 2 * x0, 0, &full_bar[p_buf]);
-      tma_2d(bb + kOffB, &maps.B, x0, 0, &full_bar[p_buf]);
+      tma_2d(bb + kOffD, &maps.D, 2 * x0, 0, &full_bar[stg]);
+      tma_2d(bb + kOffB, &maps.B, x0, 0, &full_bar[stg]);
+    }
+    if (stg == kStages - 1 && kIn) {
+      tma_2d(bb + kOffEpi, &maps.epi_in, 2 * x0, 0, &full_bar[stg]);
+      tma_2d(bb + kOffEpi + kEpiHalf, &maps.epi_in, 2 * x0 + 16, 0, &full_bar[stg]);
     }
     if (++p_stg == kStages) {
       p_stg = 0;
       p_unit += (int)gridDim.x;
-    }
-    if (++p_buf == kBufs) {
-      p_buf = 0;
-      if (issued >= kBufs) p_par ^= 1u;
+      if (issued >= kStages) p_par ^= 1u;
     }
     return true;
   };
-  bool prod_dead = false, dead = false;
-  if (threadIdx.x == 0)
-    for (; issued < total && issued < kBufs - 1; ++issued) issue();
-  int c_buf = 0;       // consumers: buffer of the current stage
-  uint32_t c_par = 0;  // its full-barrier parity
-  int consumed = 0;
-  auto stage_begin = [&]() -> const unsigned char * {
-    if (threadIdx.x == 0 && !prod_dead && issued < total) {
-      if (issue()) ++issued;
-      else {
-        prod_dead = true;
-        atomicExch(err, NRQ_ERR_TIMEOUT);
+  bool dead = false;
+  if (warp == kWarps) {
+    if (lane == 0) {
+      bool ok = true;
+      for (; issued < total && ok; ++issued) ok = issue();
+      if (ok && kNOut > 0 && my_units > 0) {
+        // the last unit's results: every warp released buffer 4 after its epilogue
+        ok = mbar_wait(&empty_bar[kStages - 1], (uint32_t)((my_units - 1) & 1));
+        if (ok) store_results(((int)blockIdx.x + (my_units - 1) * (int)gridDim.x) * kUnit);
       }
+      if (!ok) atomicExch(err, NRQ_ERR_TIMEOUT);
+      bulk_wait_all();
+      // error path: copies issued ahead of the consumers must land before
+      // exit (the last use of each buffer; earlier uses were consumed)
+      if (!ok)
+        for (int kk = issued > kStages ? issued - kStages : 0; kk < issued; ++kk)
+          if (!mbar_wait(&full_bar[kk % kStages], (uint32_t)((kk / kStages) & 1))) break;
     }
-    if (!dead && !mbar_wait(&full_bar[c_buf], c_par)) {
+  }
+  uint32_t c_par = 0;  // consumers: full-barrier parity of the current unit
+  auto stage_begin = [&](int stg) -> const unsigned char * {
+    if (!dead && !mbar_wait(&full_bar[stg], c_par)) {
       dead = true;
       atomicExch(err, NRQ_ERR_TIMEOUT);
     }
-    return smem + c_buf * kBufBytes;
+    return smem + buf_off(stg);
   };
-  auto stage_end = [&]() {
+  auto stage_end = [&](int stg) {
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty_bar[c_buf]);
-    ++consumed;
-    if (++c_buf == kBufs) {
-      c_buf = 0;
-      c_par ^= 1u;
-    }
+    if (lane == 0) mbar_arrive(&empty_bar[stg]);
   };
 
   // ---- lane roles in the MMA fragments
@@ -330,7 +389,7 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
 
   // general path of one neighbour: block and spinor each in the stage's
   // shared tiles or in global memory (periodic wraps, tile edges)
-  auto nb_general = [&](bool bwd, bool wsh, uint32_t wsa, const double2 *wg, bool ssh, uint32_t ssa,
+  auto nb_general = [&](bool bwd, int wspec, bool wsh, uint32_t wsa, const double2 *wg, bool ssh, uint32_t ssa,
                         const double2 *sg) {
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp) {
@@ -341,7 +400,7 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
         const int sl = bwd ? blk_slot(q, gc) : blk_slot(gc, q);
         const int pl = gc * 6 + q;  // spinor plane in the species: column n = gc, row q
         if (wsh) {
-          const uint32_t ea = wsa + (uint32_t)(sp * kWSpecies + sl * 16);
+          const uint32_t ea = wsa + (uint32_t)(sp * wspec + sl * 16);
           a0[j] = lds1(ea + ca0);
           a1[j] = lds1(ea + ca1);
         } else {
@@ -362,18 +421,23 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
   // one neighbour (direction I, forward or backward): m = site of the
   // forward block, y = neighbour site; the tiles start at block ws (wn
   // blocks) and spinor site ss
-  auto neighbour = [&](auto BWDc, int I, uint32_t sw, uint32_t sspin, int ws, int wn, int ss, int m, int y) {
+  auto neighbour = [&](auto BWDc, auto SAc, int I, uint32_t sw, uint32_t sspin, int ws, int wn, int ss, int m,
+                       int y) {
     constexpr bool BWD = decltype(BWDc)::value;
+    constexpr int SA = decltype(SAc)::value;
     const int wi = m - ws, si = y - ss;
     const bool wsh = (unsigned)wi < (unsigned)wn, ssh = (unsigned)si < (unsigned)kTileS;
     if (wsh && ssh) {
       const uint32_t blk = sw + (uint32_t)wi * kBlkBytes + (BWD ? offAb : offAf);
-      nb_fast<BWD>(acc, blk + ca0, blk + ca1, sspin + (uint32_t)si * 16u + offB, BWD ? mb0 : mf0, BWD ? mb1 : mf1);
+      nb_fast<BWD, SA>(acc, blk + ca0, blk + ca1, sspin + (uint32_t)si * 16u + offB, BWD ? mb0 : mf0,
+                       BWD ? mb1 : mf1);
     } else {
-      nb_general(BWD, wsh, sw + (uint32_t)((wsh ? wi : 0) * kBlkBytes), W + ((int64_t)(I * 2) * V + m) * kBlk, ssh,
-                 sspin + (uint32_t)((ssh ? si : 0) * 16), A.in + y);
+      nb_general(BWD, SA, wsh, sw + (uint32_t)((wsh ? wi : 0) * kBlkBytes), W + ((int64_t)(I * 2) * V + m) * kBlk,
+                 ssh, sspin + (uint32_t)((ssh ? si : 0) * 16), A.in + y);
     }
   };
+  using S0 = std::integral_constant<int, kWSpecies0>;
+  using S1 = std::integral_constant<int, kWSpecies>;
   using F = std::integral_constant<bool, false>;
   using T = std::integral_constant<bool, true>;
 
@@ -385,7 +449,7 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
 #pragma unroll
     for (int e = 0; e < 2; ++e) qs[sp][e][0] = qs[sp][e][1] = qs[sp][e][2] = 0.0;
 
-  for (int u = (int)blockIdx.x; u < nu; u += (int)gridDim.x) {
+  for (int u = (int)blockIdx.x; u < nu && warp < kWarps; u += (int)gridDim.x) {
     const int x0 = u * kUnit;
     const int x = x0 + warp;
     const bool act = x < V32;
@@ -408,33 +472,26 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
     for (int sp = 0; sp < 2; ++sp)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[sp][e] = 0.0;
-    // epilogue operand of the lane's outputs (b, rh or the centre spinor)
-    cplx pre[2][2];
+    // the centre spinor of the lane's outputs (RHS: psi, T: s)
+    cplx ctr[2][2];
 #pragma unroll
-    for (int sp = 0; sp < 2; ++sp) pre[sp][0] = pre[sp][1] = cplx{0.0, 0.0};
+    for (int sp = 0; sp < 2; ++sp) ctr[sp][0] = ctr[sp][1] = cplx{0.0, 0.0};
 
     // ---------------------------------------------------------- stage 0
     {
-      const unsigned char *b = stage_begin();
+      const unsigned char *b = stage_begin(0);
       if (!dead && act) {
         const int ss = x0 - 1, ws = mv4_blk_start(x0, ss, 0);
         const int wn = mv4_blk_count(V32, ws, 0);
-        const uint32_t sspin = smem_u32(b + kOffSpin), sw = smem_u32(b + kOffW);
+        const uint32_t sspin = smem_u32(b), sw = smem_u32(b + w_off(0));
         const uint32_t sD = smem_u32(b + kOffD), sB = smem_u32(b + kOffB);
         const int l = warp;
-        if (out_lane) {
+        if ((MODE == MV_T || MODE == MV_RHS) && out_lane) {
 #pragma unroll
           for (int sp = 0; sp < 2; ++sp)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int pl = sp * 36 + (2 * kq + e) * 6 + g;
-              if (MODE == MV_T || MODE == MV_RHS)
-                pre[sp][e] = lds2(sspin + (uint32_t)((pl * kTileS + l + 1) * 16));
-              else if (MODE == MV_RES || MODE == MV_RESC)
-                pre[sp][e] = ldg(A.bvec + (int64_t)pl * V + x);
-              else if (MODE == MV_V)
-                pre[sp][e] = ldg(A.in2 + (int64_t)pl * V + x);
-            }
+            for (int e = 0; e < 2; ++e)
+              ctr[sp][e] = lds2(sspin + (uint32_t)(((sp * 36 + (2 * kq + e) * 6 + g) * kTileS + l + 1) * 16));
         }
         // diagonal block (colour only): A = delta_st Cd_c[cp], centre spinor
         {
@@ -467,57 +524,60 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
           }
         }
         // +x: block at x (forward), spinor at x+1; -x: block and spinor at x-1
-        neighbour(F{}, 0, sw, sspin, ws, wn, ss, x, nbw[0]);
-        neighbour(T{}, 0, sw, sspin, ws, wn, ss, nbw[1], nbw[1]);
+        neighbour(F{}, S0{}, 0, sw, sspin, ws, wn, ss, x, nbw[0]);
+        neighbour(T{}, S0{}, 0, sw, sspin, ws, wn, ss, nbw[1], nbw[1]);
       }
-      stage_end();
+      stage_end(0);
     }
     // ------------------------------------------------------- stages 1-4
 #pragma unroll
     for (int stg = 1; stg < kStages; ++stg) {
-      const unsigned char *b = stage_begin();
+      const unsigned char *b = stage_begin(stg);
       if (!dead && act) {
         const int I = (stg + 1) / 2;
         const int ss = nbw[5 + stg], ws = mv4_blk_start(x0, ss, stg);
         const int wn = mv4_blk_count(V32, ws, stg);
-        const uint32_t sspin = smem_u32(b + kOffSpin), sw = smem_u32(b + kOffW);
+        const uint32_t sspin = smem_u32(b), sw = smem_u32(b + w_off(stg));
         const int y = nbw[2 * I + ((stg & 1) ? 0 : 1)];
         if (stg & 1)
-          neighbour(F{}, I, sw, sspin, ws, wn, ss, x, y);
+          neighbour(F{}, S1{}, I, sw, sspin, ws, wn, ss, x, y);
         else
-          neighbour(T{}, I, sw, sspin, ws, wn, ss, y, y);
+          neighbour(T{}, S1{}, I, sw, sspin, ws, wn, ss, y, y);
       }
-      if (stg < kStages - 1) stage_end();
+      if (stg < kStages - 1) stage_end(stg);
     }
 
     // ------------------------------------------------------------ epilogue
+    // (buffer 4 is released after it: the producer then stores the tile)
     if (!dead && act && out_lane) {
+      const uint32_t epi = smem_u32(smem + kBuf4 + kOffEpi);
 #pragma unroll
       for (int sp = 0; sp < 2; ++sp)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int64_t o = (int64_t)(sp * 36 + (2 * kq + e) * 6 + g) * V + x;
+          const int pl = sp * 36 + (2 * kq + e) * 6 + g;
+          const uint32_t ea = epi + epi_off(pl, warp);
           const cplx y_ = {acc[sp][e], acc[sp][2 + e]};
-          const cplx pv = pre[sp][e];
+          cplx pv = ctr[sp][e];
+          if (kIn) pv = lds2(ea);
           if (MODE == MV_PLAIN) {
-            st(A.out + o, y_);
+            sts2(ea, y_.re, y_.im);
           } else if (MODE == MV_RHS) {
-            st(A.out + o, y_);
-            st(A.out2 + o, 2.0 * y_ - pv);
+            sts2(ea, y_.re, y_.im);
+            st(A.out2 + (int64_t)pl * V + x, 2.0 * y_ - pv);
           } else if (MODE == MV_RES) {
             const cplx r = pv - y_;
-            st(A.out + o, r);
-            st(A.out2 + o, r);
-            st(A.out3 + o, r);
+            sts2(ea, r.re, r.im);
             qs[sp][e][0] += norm2(r);
             qs[sp][e][1] += norm2(pv);
           } else if (MODE == MV_V) {
-            st(A.out + o, y_);
+            sts2(ea, y_.re, y_.im);
             cplx dd = {0.0, 0.0};
             cmac_cj(dd, pv, y_);
             qs[sp][e][0] += dd.re;
             qs[sp][e][1] += dd.im;
           } else if (MODE == MV_RESC) {
+            const int64_t o = (int64_t)pl * V + x;
             const cplx r = pv - y_;
             const cplx dd = r * A.inv_theta[sp];
             A.r32[o] = make_float2((float)r.re, (float)r.im);
@@ -525,7 +585,7 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
             qs[sp][e][0] += norm2(r);
             qs[sp][e][1] += norm2(pv);
           } else {  // MV_T: in = s
-            st(A.out + o, y_);
+            sts2(ea, y_.re, y_.im);
             cplx dd = {0.0, 0.0};
             cmac_cj(dd, y_, pv);
             qs[sp][e][0] += dd.re;
@@ -534,27 +594,27 @@ __global__ void __launch_bounds__(mv4::kThreads, 1)
           }
         }
     }
-    stage_end();
+    if (kNOut > 0) fence_proxy_async_smem();
+    stage_end(kStages - 1);
+    c_par ^= 1u;
   }
-  // error path: copies issued ahead of the consumers must land before exit
-  if (threadIdx.x == 0 && (dead || prod_dead))
-    for (int kk = consumed; kk < issued; ++kk)
-      if (!mbar_wait(&full_bar[kk % kBufs], (uint32_t)((kk / kBufs) & 1))) atomicExch(err, NRQ_ERR_TIMEOUT);
   // one partial row per CTA: sum over the rows g (lane bits 2-4), then over
   // the warps in a fixed order
   if constexpr (NQ > 0) {
+    if (warp < kWarps) {
 #pragma unroll
-    for (int sp = 0; sp < 2; ++sp)
+      for (int sp = 0; sp < 2; ++sp)
 #pragma unroll
-      for (int e = 0; e < 2; ++e)
+        for (int e = 0; e < 2; ++e)
 #pragma unroll
-        for (int kk = 0; kk < NQ; ++kk) {
-          double v = qs[sp][e][kk];
-          v += __shfl_xor_sync(0xffffffffu, v, 4);
-          v += __shfl_xor_sync(0xffffffffu, v, 8);
-          v += __shfl_xor_sync(0xffffffffu, v, 16);
-          if (lane < 3) red[warp][sp * 6 + 2 * lane + e][kk] = v;
-        }
+          for (int kk = 0; kk < NQ; ++kk) {
+            double v = qs[sp][e][kk];
+            v += __shfl_xor_sync(0xffffffffu, v, 4);
+            v += __shfl_xor_sync(0xffffffffu, v, 8);
+            v += __shfl_xor_sync(0xffffffffu, v, 16);
+            if (lane < 3) red[warp][sp * 6 + 2 * lane + e][kk] = v;
+          }
+    }
     __syncthreads();
     if (threadIdx.x < CN_COLS * NQ) {
       const int col12 = threadIdx.x / NQ, kk = threadIdx.x % NQ;
@@ -582,9 +642,18 @@ int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double
   const uint64_t V = (uint64_t)L.V;
   if (L.V < kWMax || L.V > 0x7fffffffLL) return -1;
   Mv4Maps maps;
+  memset(&maps, 0, sizeof(maps));
   if (!stage::encode(&maps.spin, a.in, 2 * V, 72, 2 * kTileS, 72) ||
       !stage::encode(&maps.D, Dsum, 2 * V, 9, 2 * kUnit, 9) || !stage::encode(&maps.B, Bsum, V, 9, kUnit, 9))
     return -1;
+  // epilogue tile: operand in, results out (halves of 8 sites, 128-byte swizzle)
+  const auto sw128 = CU_TENSOR_MAP_SWIZZLE_128B;
+  if (mv4_tile_input(mode) &&
+      !stage::encode(&maps.epi_in, mode == MV_V ? (const void *)a.in2 : (const void *)a.bvec, 2 * V, 72, 16, 72, sw128))
+    return -1;
+  const void *outs[3] = {a.out, a.out2, a.out3};
+  for (int o = 0; o < mv4_tile_outputs(mode); ++o)
+    if (!stage::encode(&maps.out[o], outs[o], 2 * V, 72, 16, 72, sw128)) return -1;
   const int64_t nunits = cn_mv4_units(L.V);
   const unsigned grid = (unsigned)cn_mv4_rows(L.V, sm_count);
   auto go = [&](auto kern) {

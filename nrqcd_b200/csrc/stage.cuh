@@ -1,8 +1,9 @@
 // Shared-memory staging helpers of the persistent stencil kernels
 // (cn_mv3.cu, cn_mv4.cu): mbarriers with bounded waits, 2D tensor-map copies
 // (cp.async.bulk.tensor) and 1D bulk copies (cp.async.bulk) into shared
-// memory that complete on an mbarrier, explicit shared-memory loads, and the
-// host-side encoder of 2D FP64 tensor maps.
+// memory that complete on an mbarrier, 2D tensor-map stores from shared
+// memory (bulk async-groups), explicit shared-memory loads and stores, and
+// the host-side encoder of 2D FP64 tensor maps.
 //
 // Single-GPU code: every copy reads this GPU's own memory and no copy uses
 // cluster multicast.
@@ -66,6 +67,27 @@ __device__ __forceinline__ void tma_2d(void *dst, const CUtensorMap *map, int c0
       "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(smem_u32(bar))
       : "memory");
 }
+// 2D tile from shared memory to a tensor map at (c0, c1) (bulk async-group
+// of the issuing thread; c0, c1 >= 0; elements outside the tensor are not
+// written)
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int c0, int c1, const void *src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"((uint64_t)map),
+               "r"(c0), "r"(c1), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the issuing thread's committed bulk stores have read their shared memory
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// ... and completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// this thread's shared-memory writes become visible to later bulk copies
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void sts2(uint32_t a, double re, double im) {
+  asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(re), "d"(im) : "memory");
+}
+
 // contiguous copy of `bytes` (multiple of 16; both addresses 16-byte aligned)
 __device__ __forceinline__ void bulk_1d(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
@@ -90,7 +112,7 @@ inline PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
 
 // 2D map over `planes` planes of `elems_per_plane` doubles (plane stride = elems)
 inline bool encode(CUtensorMap *m, const void *base, uint64_t elems_per_plane, uint64_t planes, uint32_t box0,
-                   uint32_t box1) {
+                   uint32_t box1, CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
   auto fn = get_encoder();
   if (!fn) return false;
   cuuint64_t dims[2] = {elems_per_plane, planes};
@@ -98,7 +120,7 @@ inline bool encode(CUtensorMap *m, const void *base, uint64_t elems_per_plane, u
   cuuint32_t box[2] = {box0, box1};
   cuuint32_t es[2] = {1, 1};
   CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims, strides, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
