@@ -37,6 +37,8 @@ MASS = 1.0
 WILSON = [1.0, 1.0, 1.0, 1.0]
 A = (0.05, 1.0, 1.0, 1.0)
 TOL = 1e-12
+# FP64 stencils of the solver, by NRQ_STENCIL_* index
+STENCIL_NAMES = {0: "k_cn_mv2 (register-tiled)", 1: "k_cn_mv3 (TMA-staged)", 2: "k_cn_mv4 (FP64 tensor cores)"}
 
 
 def parse():
@@ -241,8 +243,13 @@ def measure_cn_forms(L, steps, params, tol=1e-10, seed=1):
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1) / steps
+            which = ctypes.c_int()
+            tune = np.zeros(3)
+            _capi.check(lib.nrq_cn_stencil_info(cn, ctypes.byref(which), _capi.dptr(tune)), lat.ctx, "stencil_info")
             out[name] = {"s_per_step": ms / 1000.0, "tol": tol,
                          "max_rel_residual": max(st["max_rel_residual"] for st in stats),
+                         "fp64_stencil": STENCIL_NAMES[which.value],
+                         "fp64_stencil_tuning_ms": [float(t) for t in tune],
                          "stencil_launches_per_step": float(np.mean([st["matvecs"] for st in stats])),
                          "inner_steps_per_step": float(np.mean([st["iterations"] for st in stats])),
                          "initial_rel_residual": float(np.mean([st["initial_rel_residual"] for st in stats])),

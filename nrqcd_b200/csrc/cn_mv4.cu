@@ -238,13 +238,12 @@ __device__ __forceinline__ void nb_fast(double (&acc)[2][4], uint32_t wa0, uint3
 }
 
 // results of a mode stored from the epilogue tile (RES: r, rh and p are the
-// same values) and whether the epilogue operand arrives in it (b or rh)
+// same values) and whether an epilogue operand arrives in it (b for RES and
+// RESC, rh for V, the input itself for T and RHS)
 __host__ __device__ constexpr int mv4_tile_outputs(int mode) {
   return mode == MV_RES ? 3 : (mode == MV_RESC ? 0 : 1);
 }
-__host__ __device__ constexpr bool mv4_tile_input(int mode) {
-  return mode == MV_RES || mode == MV_RESC || mode == MV_V;
-}
+__host__ __device__ constexpr bool mv4_tile_input(int mode) { return mode != MV_PLAIN; }
 // byte offset of (plane p, site l) in the epilogue tile: two halves of 8
 // sites, rows of 128 bytes, 16-byte chunks swizzled with the row (the
 // 128-byte swizzle of the tensor maps; the tile is 1024-aligned)
@@ -472,10 +471,6 @@ __global__ void __maxnreg__(96)
     for (int sp = 0; sp < 2; ++sp)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[sp][e] = 0.0;
-    // the centre spinor of the lane's outputs (RHS: psi, T: s)
-    cplx ctr[2][2];
-#pragma unroll
-    for (int sp = 0; sp < 2; ++sp) ctr[sp][0] = ctr[sp][1] = cplx{0.0, 0.0};
 
     // ---------------------------------------------------------- stage 0
     {
@@ -486,13 +481,6 @@ __global__ void __maxnreg__(96)
         const uint32_t sspin = smem_u32(b), sw = smem_u32(b + w_off(0));
         const uint32_t sD = smem_u32(b + kOffD), sB = smem_u32(b + kOffB);
         const int l = warp;
-        if ((MODE == MV_T || MODE == MV_RHS) && out_lane) {
-#pragma unroll
-          for (int sp = 0; sp < 2; ++sp)
-#pragma unroll
-            for (int e = 0; e < 2; ++e)
-              ctr[sp][e] = lds2(sspin + (uint32_t)(((sp * 36 + (2 * kq + e) * 6 + g) * kTileS + l + 1) * 16));
-        }
         // diagonal block (colour only): A = delta_st Cd_c[cp], centre spinor
         {
           const int c = gc >> 1, s = gc & 1;
@@ -558,8 +546,7 @@ __global__ void __maxnreg__(96)
           const int pl = sp * 36 + (2 * kq + e) * 6 + g;
           const uint32_t ea = epi + epi_off(pl, warp);
           const cplx y_ = {acc[sp][e], acc[sp][2 + e]};
-          cplx pv = ctr[sp][e];
-          if (kIn) pv = lds2(ea);
+          const cplx pv = kIn ? lds2(ea) : cplx{0.0, 0.0};
           if (MODE == MV_PLAIN) {
             sts2(ea, y_.re, y_.im);
           } else if (MODE == MV_RHS) {
@@ -648,9 +635,9 @@ int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double
     return -1;
   // epilogue tile: operand in, results out (halves of 8 sites, 128-byte swizzle)
   const auto sw128 = CU_TENSOR_MAP_SWIZZLE_128B;
-  if (mv4_tile_input(mode) &&
-      !stage::encode(&maps.epi_in, mode == MV_V ? (const void *)a.in2 : (const void *)a.bvec, 2 * V, 72, 16, 72, sw128))
-    return -1;
+  const void *epi_src = (mode == MV_V) ? (const void *)a.in2
+                        : (mode == MV_RES || mode == MV_RESC) ? (const void *)a.bvec : (const void *)a.in;
+  if (mv4_tile_input(mode) && !stage::encode(&maps.epi_in, epi_src, 2 * V, 72, 16, 72, sw128)) return -1;
   const void *outs[3] = {a.out, a.out2, a.out3};
   for (int o = 0; o < mv4_tile_outputs(mode); ++o)
     if (!stage::encode(&maps.out[o], outs[o], 2 * V, 72, 16, 72, sw128)) return -1;
