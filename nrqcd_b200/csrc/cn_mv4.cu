@@ -47,14 +47,25 @@
 #include "nrq_kernels.cuh"
 #include "stage.cuh"
 
+// sites per consumer warp of the tensor-core stencil (1: 16 consumer warps
+// with two MMA chains each; 2: 8 consumer warps with four)
+#ifndef NRQ_MV4_SPW
+#define NRQ_MV4_SPW 1
+#endif
+
 namespace nrq {
 
 namespace mv4 {
 constexpr int kUnit = 16;                 // sites per work unit
 constexpr int kTileS = 19;                // spinor tile width in sites (odd stride in 16-byte words)
 constexpr int kStages = 5;                // stages per unit; stage s always uses buffer s
-constexpr int kWarps = kUnit;             // consumer warps, one site each
+constexpr int kSPW = NRQ_MV4_SPW;         // sites per consumer warp
+constexpr int kWarps = kUnit / kSPW;      // consumer warps
 constexpr int kThreads = (kWarps + 1) * 32;  // + one producer warp
+// registers per thread: the SM quarter that hosts the most warps of the CTA
+// (ceil((kWarps + 1) / 4)) holds 16384 registers
+constexpr int kMaxReg = kSPW == 1 ? 96 : 168;
+static_assert(kUnit % kSPW == 0 && ((kWarps + 4) / 4) * 32 * kMaxReg <= 16384, "warp layout");
 constexpr int kBlk = 36;                  // complex entries of one 6x6 block
 constexpr int kBlkBytes = kBlk * 16;      // 576
 constexpr int kWMax = kUnit + 1;          // blocks per species and stage (stage 0: x0-1 .. x0+15)
@@ -222,19 +233,26 @@ __device__ __forceinline__ void nb_fast_load(double (&a0)[2], double (&a1)[2], d
   b0[0] = lds_at<oB>(sb);
   b0[1] = lds_at<oB + sB>(sb);
 }
-// a whole neighbour of the warp's site: all operands loaded, then 6 MMAs in
-// two independent chains (species); SA = species stride of the block tile
-template <bool BWD, int SA>
-__device__ __forceinline__ void nb_fast(double (&acc)[2][4], uint32_t wa0, uint32_t wa1, uint32_t sb, unsigned m0,
-                                        unsigned m1) {
-  double a0[3][2], a1[3][2], b0[3][2];
-  nb_fast_load<BWD, SA, 0>(a0[0], a1[0], b0[0], wa0, wa1, sb);
-  nb_fast_load<BWD, SA, 1>(a0[1], a1[1], b0[1], wa0, wa1, sb);
-  nb_fast_load<BWD, SA, 2>(a0[2], a1[2], b0[2], wa0, wa1, sb);
+// a whole neighbour of the warp's N sites: all operands loaded, then 6N
+// MMAs in 2N independent chains (site x species); SA = species stride of the
+// block tile
+template <bool BWD, int SA, int N>
+__device__ __forceinline__ void nb_fast(double (&acc)[N][2][4], const uint32_t (&wa0)[N], const uint32_t (&wa1)[N],
+                                        const uint32_t (&sb)[N], unsigned m0, unsigned m1) {
+  double a0[3][N][2], a1[3][N][2], b0[3][N][2];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    nb_fast_load<BWD, SA, 0>(a0[0][i], a1[0][i], b0[0][i], wa0[i], wa1[i], sb[i]);
+    nb_fast_load<BWD, SA, 1>(a0[1][i], a1[1][i], b0[1][i], wa0[i], wa1[i], sb[i]);
+    nb_fast_load<BWD, SA, 2>(a0[2][i], a1[2][i], b0[2][i], wa0[i], wa1[i], sb[i]);
+  }
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
-    for (int sp = 0; sp < 2; ++sp) dmma(acc[sp], flip(a0[j][sp], m0), flip(a1[j][sp], m1), b0[j][sp]);
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+      for (int sp = 0; sp < 2; ++sp)
+        dmma(acc[i][sp], flip(a0[j][i][sp], m0), flip(a1[j][i][sp], m1), b0[j][i][sp]);
 }
 
 // results of a mode stored from the epilogue tile (RES: r, rh and p are the
@@ -252,7 +270,7 @@ __device__ __forceinline__ uint32_t epi_off(int p, int l) {
 }
 
 template <int MODE>
-__global__ void __maxnreg__(96)
+__global__ void __maxnreg__(mv4::kMaxReg)
     k_cn_mv4(Lat L, CnCoef C, double nb_sign, const __grid_constant__ Mv4Maps maps, const double2 *__restrict__ W,
              const double2 *__restrict__ Dsum, const double *__restrict__ Bsum, MvArgs A, int64_t nunits, int *err) {
   using namespace mv4;
@@ -262,9 +280,10 @@ __global__ void __maxnreg__(96)
   __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages];
   // per-warp partial sums of the CTA (one partial row per CTA, at the end)
   __shared__ double red[kWarps][CN_COLS][3];
-  // per warp and unit: neighbours (+x,-x,+y,-y,+z,-z) of its site (entries
-  // 0-5) and the spinor tile starts of stages 1-4 (6-9)
-  __shared__ int nbt[kWarps][10];
+  // per warp and unit: neighbours (+x,-x,+y,-y,+z,-z) of its sites (entries
+  // 6i .. 6i+5 for site i) and the spinor tile starts of stages 1-4 (last 4)
+  constexpr int kNbt = 6 * kSPW + 4;
+  __shared__ int nbt[kWarps][kNbt];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t V = L.V;
@@ -384,12 +403,12 @@ __global__ void __maxnreg__(96)
   const uint32_t offAf = (uint32_t)(2 * gc + h) * 16u, offAb = (uint32_t)((gc >> 1) * 12 + 2 * h + (gc & 1)) * 16u;
   const uint32_t offB = (uint32_t)((gc * 6 + h) * kTileS * 16) + (uint32_t)part * 8u;
 
-  double acc[2][4];  // [species][C fragment] of the warp's site
+  double acc[kSPW][2][4];  // [site][species][C fragment] of the warp's sites
 
-  // general path of one neighbour: block and spinor each in the stage's
-  // shared tiles or in global memory (periodic wraps, tile edges)
-  auto nb_general = [&](bool bwd, int wspec, bool wsh, uint32_t wsa, const double2 *wg, bool ssh, uint32_t ssa,
-                        const double2 *sg) {
+  // general path of one neighbour of one site: block and spinor each in the
+  // stage's shared tiles or in global memory (periodic wraps, tile edges)
+  auto nb_general = [&](double (&ac)[2][4], bool bwd, int wspec, bool wsh, uint32_t wsa, const double2 *wg, bool ssh,
+                        uint32_t ssa, const double2 *sg) {
 #pragma unroll
     for (int sp = 0; sp < 2; ++sp) {
       double a0[3], a1[3], b0[3];
@@ -414,25 +433,44 @@ __global__ void __maxnreg__(96)
       }
 #pragma unroll
       for (int j = 0; j < 3; ++j)
-        dmma(acc[sp], flip(a0[j], bwd ? mb0 : mf0), flip(a1[j], bwd ? mb1 : mf1), b0[j]);
+        dmma(ac[sp], flip(a0[j], bwd ? mb0 : mf0), flip(a1[j], bwd ? mb1 : mf1), b0[j]);
     }
   };
-  // one neighbour (direction I, forward or backward): m = site of the
-  // forward block, y = neighbour site; the tiles start at block ws (wn
-  // blocks) and spinor site ss
-  auto neighbour = [&](auto BWDc, auto SAc, int I, uint32_t sw, uint32_t sspin, int ws, int wn, int ss, int m,
-                       int y) {
+  // one neighbour (direction I, forward or backward) of the warp's sites:
+  // m[i] = site of the forward block, y[i] = neighbour site; the tiles start
+  // at block ws (wn blocks) and spinor site ss.  All operands in the tiles:
+  // the fast path for every site at once; otherwise site by site.
+  auto neighbour = [&](auto BWDc, auto SAc, int I, uint32_t sw, uint32_t sspin, int ws, int wn, int ss,
+                       const int (&m)[kSPW], const int (&y)[kSPW], const bool (&act)[kSPW]) {
     constexpr bool BWD = decltype(BWDc)::value;
     constexpr int SA = decltype(SAc)::value;
-    const int wi = m - ws, si = y - ss;
-    const bool wsh = (unsigned)wi < (unsigned)wn, ssh = (unsigned)si < (unsigned)kTileS;
-    if (wsh && ssh) {
-      const uint32_t blk = sw + (uint32_t)wi * kBlkBytes + (BWD ? offAb : offAf);
-      nb_fast<BWD, SA>(acc, blk + ca0, blk + ca1, sspin + (uint32_t)si * 16u + offB, BWD ? mb0 : mf0,
-                       BWD ? mb1 : mf1);
+    int wi[kSPW], si[kSPW];
+    bool fast = true;
+#pragma unroll
+    for (int i = 0; i < kSPW; ++i) {
+      wi[i] = m[i] - ws;
+      si[i] = y[i] - ss;
+      fast = fast && act[i] && (unsigned)wi[i] < (unsigned)wn && (unsigned)si[i] < (unsigned)kTileS;
+    }
+    if (fast) {
+      uint32_t wa0[kSPW], wa1[kSPW], sb[kSPW];
+#pragma unroll
+      for (int i = 0; i < kSPW; ++i) {
+        const uint32_t blk = sw + (uint32_t)wi[i] * kBlkBytes + (BWD ? offAb : offAf);
+        wa0[i] = blk + ca0;
+        wa1[i] = blk + ca1;
+        sb[i] = sspin + (uint32_t)si[i] * 16u + offB;
+      }
+      nb_fast<BWD, SA, kSPW>(acc, wa0, wa1, sb, BWD ? mb0 : mf0, BWD ? mb1 : mf1);
     } else {
-      nb_general(BWD, SA, wsh, sw + (uint32_t)((wsh ? wi : 0) * kBlkBytes), W + ((int64_t)(I * 2) * V + m) * kBlk,
-                 ssh, sspin + (uint32_t)((ssh ? si : 0) * 16), A.in + y);
+#pragma unroll
+      for (int i = 0; i < kSPW; ++i) {
+        if (!act[i]) continue;
+        const bool wsh = (unsigned)wi[i] < (unsigned)wn, ssh = (unsigned)si[i] < (unsigned)kTileS;
+        nb_general(acc[i], BWD, SA, wsh, sw + (uint32_t)((wsh ? wi[i] : 0) * kBlkBytes),
+                   W + ((int64_t)(I * 2) * V + m[i]) * kBlk, ssh, sspin + (uint32_t)((ssh ? si[i] : 0) * 16),
+                   A.in + y[i]);
+      }
     }
   };
   using S0 = std::integral_constant<int, kWSpecies0>;
@@ -450,17 +488,23 @@ __global__ void __maxnreg__(96)
 
   for (int u = (int)blockIdx.x; u < nu && warp < kWarps; u += (int)gridDim.x) {
     const int x0 = u * kUnit;
-    const int x = x0 + warp;
-    const bool act = x < V32;
+    int xs[kSPW];
+    bool act[kSPW];
+#pragma unroll
+    for (int i = 0; i < kSPW; ++i) {
+      xs[i] = x0 + warp * kSPW + i;
+      act[i] = xs[i] < V32;
+    }
     // neighbour table, one entry per lane (the previous unit's reads ended
-    // at its last stage_end): lanes 0-5 the site's neighbours, lanes 6-9
-    // the tile starts of stages 1-4
-    if (lane < 10) {
+    // at its last stage_end): lanes 0 .. 6 kSPW - 1 the sites' neighbours,
+    // the next 4 lanes the tile starts of stages 1-4
+    if (lane < kNbt) {
       int v = 0;
-      if (lane < 6) {
-        if (act) v = nb32(L, (uint32_t)x, lane >> 1, (lane & 1) ? -1 : +1);
+      if (lane < 6 * kSPW) {
+        const int xi = x0 + warp * kSPW + lane / 6, d = lane % 6;
+        if (xi < V32) v = nb32(L, (uint32_t)xi, d >> 1, (d & 1) ? -1 : +1);
       } else {
-        const int st = lane - 5;  // 1..4
+        const int st = lane - 6 * kSPW + 1;  // 1..4
         v = nb32(L, (uint32_t)x0, (st + 1) >> 1, (st & 1) ? +1 : -1);
       }
       nbt[warp][lane] = v;
@@ -468,21 +512,25 @@ __global__ void __maxnreg__(96)
     __syncwarp();
     const int *nbw = nbt[warp];
 #pragma unroll
-    for (int sp = 0; sp < 2; ++sp)
+    for (int i = 0; i < kSPW; ++i)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc[sp][e] = 0.0;
+      for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[i][sp][e] = 0.0;
 
     // ---------------------------------------------------------- stage 0
     {
       const unsigned char *b = stage_begin(0);
-      if (!dead && act) {
+      if (!dead && act[0]) {
         const int ss = x0 - 1, ws = mv4_blk_start(x0, ss, 0);
         const int wn = mv4_blk_count(V32, ws, 0);
         const uint32_t sspin = smem_u32(b), sw = smem_u32(b + w_off(0));
         const uint32_t sD = smem_u32(b + kOffD), sB = smem_u32(b + kOffB);
-        const int l = warp;
         // diagonal block (colour only): A = delta_st Cd_c[cp], centre spinor
-        {
+#pragma unroll
+        for (int i = 0; i < kSPW; ++i) {
+          if (!act[i]) continue;
+          const int l = warp * kSPW + i;
           const int c = gc >> 1, s = gc & 1;
           cplx dv[3];
           double bv[3];
@@ -507,13 +555,19 @@ __global__ void __maxnreg__(96)
               cplx cd = ad * dv[j] + bv[j] * am;
               if (j == c) cd = cd + dg;
               if (s != h) cd = cplx{0.0, 0.0};
-              dmma(acc[sp], part ? -cd.im : cd.re, part ? cd.re : cd.im, b0[j]);
+              dmma(acc[i][sp], part ? -cd.im : cd.re, part ? cd.re : cd.im, b0[j]);
             }
           }
         }
         // +x: block at x (forward), spinor at x+1; -x: block and spinor at x-1
-        neighbour(F{}, S0{}, 0, sw, sspin, ws, wn, ss, x, nbw[0]);
-        neighbour(T{}, S0{}, 0, sw, sspin, ws, wn, ss, nbw[1], nbw[1]);
+        int yp[kSPW], ym[kSPW];
+#pragma unroll
+        for (int i = 0; i < kSPW; ++i) {
+          yp[i] = nbw[6 * i + 0];
+          ym[i] = nbw[6 * i + 1];
+        }
+        neighbour(F{}, S0{}, 0, sw, sspin, ws, wn, ss, xs, yp, act);
+        neighbour(T{}, S0{}, 0, sw, sspin, ws, wn, ss, ym, ym, act);
       }
       stage_end(0);
     }
@@ -521,65 +575,72 @@ __global__ void __maxnreg__(96)
 #pragma unroll
     for (int stg = 1; stg < kStages; ++stg) {
       const unsigned char *b = stage_begin(stg);
-      if (!dead && act) {
+      if (!dead && act[0]) {
         const int I = (stg + 1) / 2;
-        const int ss = nbw[5 + stg], ws = mv4_blk_start(x0, ss, stg);
+        const int ss = nbw[6 * kSPW - 1 + stg], ws = mv4_blk_start(x0, ss, stg);
         const int wn = mv4_blk_count(V32, ws, stg);
         const uint32_t sspin = smem_u32(b), sw = smem_u32(b + w_off(stg));
-        const int y = nbw[2 * I + ((stg & 1) ? 0 : 1)];
+        int y[kSPW];
+#pragma unroll
+        for (int i = 0; i < kSPW; ++i) y[i] = nbw[6 * i + 2 * I + ((stg & 1) ? 0 : 1)];
         if (stg & 1)
-          neighbour(F{}, S1{}, I, sw, sspin, ws, wn, ss, x, y);
+          neighbour(F{}, S1{}, I, sw, sspin, ws, wn, ss, xs, y, act);
         else
-          neighbour(T{}, S1{}, I, sw, sspin, ws, wn, ss, y, y);
+          neighbour(T{}, S1{}, I, sw, sspin, ws, wn, ss, y, y, act);
       }
       if (stg < kStages - 1) stage_end(stg);
     }
 
     // ------------------------------------------------------------ epilogue
     // (buffer 4 is released after it: the producer then stores the tile)
-    if (!dead && act && out_lane) {
+    if (!dead && out_lane) {
       const uint32_t epi = smem_u32(smem + kBuf4 + kOffEpi);
 #pragma unroll
-      for (int sp = 0; sp < 2; ++sp)
+      for (int i = 0; i < kSPW; ++i) {
+        if (!act[i]) continue;
+        const int x = xs[i];
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int pl = sp * 36 + (2 * kq + e) * 6 + g;
-          const uint32_t ea = epi + epi_off(pl, warp);
-          const cplx y_ = {acc[sp][e], acc[sp][2 + e]};
-          const cplx pv = kIn ? lds2(ea) : cplx{0.0, 0.0};
-          if (MODE == MV_PLAIN) {
-            sts2(ea, y_.re, y_.im);
-          } else if (MODE == MV_RHS) {
-            sts2(ea, y_.re, y_.im);
-            st(A.out2 + (int64_t)pl * V + x, 2.0 * y_ - pv);
-          } else if (MODE == MV_RES) {
-            const cplx r = pv - y_;
-            sts2(ea, r.re, r.im);
-            qs[sp][e][0] += norm2(r);
-            qs[sp][e][1] += norm2(pv);
-          } else if (MODE == MV_V) {
-            sts2(ea, y_.re, y_.im);
-            cplx dd = {0.0, 0.0};
-            cmac_cj(dd, pv, y_);
-            qs[sp][e][0] += dd.re;
-            qs[sp][e][1] += dd.im;
-          } else if (MODE == MV_RESC) {
-            const int64_t o = (int64_t)pl * V + x;
-            const cplx r = pv - y_;
-            const cplx dd = r * A.inv_theta[sp];
-            A.r32[o] = make_float2((float)r.re, (float)r.im);
-            A.d32[o] = make_float2((float)dd.re, (float)dd.im);
-            qs[sp][e][0] += norm2(r);
-            qs[sp][e][1] += norm2(pv);
-          } else {  // MV_T: in = s
-            sts2(ea, y_.re, y_.im);
-            cplx dd = {0.0, 0.0};
-            cmac_cj(dd, y_, pv);
-            qs[sp][e][0] += dd.re;
-            qs[sp][e][1] += dd.im;
-            qs[sp][e][2] += norm2(y_);
+        for (int sp = 0; sp < 2; ++sp)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int pl = sp * 36 + (2 * kq + e) * 6 + g;
+            const uint32_t ea = epi + epi_off(pl, warp * kSPW + i);
+            const cplx y_ = {acc[i][sp][e], acc[i][sp][2 + e]};
+            const cplx pv = kIn ? lds2(ea) : cplx{0.0, 0.0};
+            if (MODE == MV_PLAIN) {
+              sts2(ea, y_.re, y_.im);
+            } else if (MODE == MV_RHS) {
+              sts2(ea, y_.re, y_.im);
+              st(A.out2 + (int64_t)pl * V + x, 2.0 * y_ - pv);
+            } else if (MODE == MV_RES) {
+              const cplx r = pv - y_;
+              sts2(ea, r.re, r.im);
+              qs[sp][e][0] += norm2(r);
+              qs[sp][e][1] += norm2(pv);
+            } else if (MODE == MV_V) {
+              sts2(ea, y_.re, y_.im);
+              cplx dd = {0.0, 0.0};
+              cmac_cj(dd, pv, y_);
+              qs[sp][e][0] += dd.re;
+              qs[sp][e][1] += dd.im;
+            } else if (MODE == MV_RESC) {
+              const int64_t o = (int64_t)pl * V + x;
+              const cplx r = pv - y_;
+              const cplx dd = r * A.inv_theta[sp];
+              A.r32[o] = make_float2((float)r.re, (float)r.im);
+              A.d32[o] = make_float2((float)dd.re, (float)dd.im);
+              qs[sp][e][0] += norm2(r);
+              qs[sp][e][1] += norm2(pv);
+            } else {  // MV_T: in = s
+              sts2(ea, y_.re, y_.im);
+              cplx dd = {0.0, 0.0};
+              cmac_cj(dd, y_, pv);
+              qs[sp][e][0] += dd.re;
+              qs[sp][e][1] += dd.im;
+              qs[sp][e][2] += norm2(y_);
+            }
           }
-        }
+      }
     }
     if (kNOut > 0) fence_proxy_async_smem();
     stage_end(kStages - 1);
