@@ -306,20 +306,28 @@ def measure_precision_drift(L, n0, steps, seed=1):
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
+            its, mvs = [], []
             for _ in range(steps):
                 st = _capi.CnStats()
                 _capi.check(lib.nrq_heavy_update_cn(cn, h.handle, g.handle, MASS, _capi.dptr(cw), 1.0,
                                                     ctypes.byref(st)), lat.ctx, "update")
+                its.append(st.iterations)
+                mvs.append(st.matvecs)
                 g.Update(1.0)
             e1.record(stream)
             e1.synchronize()
-            paths[name] = {"g": g, "h": h, "cn": cn, "ms": e0.elapsed_time(e1) / steps, "e_start": e_start}
+            which = ctypes.c_int()
+            _capi.check(lib.nrq_cn_stencil_info(cn, ctypes.byref(which), None), lat.ctx, "stencil_info")
+            paths[name] = {"g": g, "h": h, "cn": cn, "ms": e0.elapsed_time(e1) / steps, "e_start": e_start,
+                           "solve": {"fp64_stencil": STENCIL_NAMES[which.value],
+                                     "iterations_per_step": float(np.mean(its)),
+                                     "stencil_launches_per_step": float(np.mean(mvs))}}
         res = {}
         for name, p in paths.items():
             g, h = p["g"], p["h"]
             en = g.GetEnergy()
             gref, gmax = g._gauss()
-            res[name] = {"s_per_step": p["ms"] / 1000.0, "energy": en,
+            res[name] = {"s_per_step": p["ms"] / 1000.0, **p["solve"], "energy": en,
                          "energy_drift_rel": abs(en - p["e_start"]) / abs(p["e_start"]),
                          "gauss_max_norm": gmax, "norm_quark_minus_1": h.GetNorm_Quark() - 1.0,
                          "norm_antiq_minus_1": h.GetNorm_AntiQ() - 1.0,

@@ -955,7 +955,10 @@ void fin(nrq_cn *cn, int stage) {
 // register-tiled stencil forms s on the fly, the staged ones need s
 // materialised first); for the precision forms the FP64 refinement
 // residual.  Every buffer written here (s, t, the partials, r32, d32) is
-// rewritten by the solve before it is read.  A forced stencil skips this.
+// rewritten by the solve before it is read.  The choice minimises the time
+// of an update's stencil work (launches per update x time per launch, plus
+// the per-update block build of the tensor-core stencil).  A forced stencil
+// skips this.
 int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
   nrq_ctx *ctx = cn->ctx;
   cn->stencil_tuned = true;
@@ -1006,14 +1009,34 @@ int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
     cudaEventElapsedTime(&ms, e0, e1);
     if (cn->last_stencil == which) cn->tune_ms[which] = ms / reps;
   }
+  // the tensor-core stencil also builds its blocks once per update: charge
+  // that against the launches an update makes (about 10 for the plain
+  // BiCGStab solve, 3 for the precision forms: right-hand side and
+  // refinement residuals)
+  double build_ms = 0.0;
+  if (!rc && cn->tune_ms[NRQ_STENCIL_TENSOR] > 0.0) {
+    cn->w_valid = false;
+    double sign = 0.0;
+    cudaEventRecord(e0, st);
+    rc = ensure_blocks(cn, CH, g, &sign);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    build_ms = ms;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   ctx->prof = prof;
   if (rc) return rc;
   if ((rc = check_launch(ctx, "stencil tuning"))) return rc;
+  const double per_update = cn->form == 0 ? 10.0 : 3.0;
+  auto cost = [&](int which) {
+    return per_update * cn->tune_ms[which] + (which == NRQ_STENCIL_TENSOR ? build_ms : 0.0);
+  };
   int best = NRQ_STENCIL_REGISTER;
   for (int which = 1; which < 3; ++which)
-    if (cn->tune_ms[which] > 0.0 && cn->tune_ms[which] < cn->tune_ms[best]) best = which;
+    if (cn->tune_ms[which] > 0.0 && cost(which) < cost(best)) best = which;
   cn->stencil = best;
   return NRQ_OK;
 }

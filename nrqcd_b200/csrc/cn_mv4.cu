@@ -255,11 +255,12 @@ __device__ __forceinline__ void nb_fast(double (&acc)[N][2][4], const uint32_t (
         dmma(acc[i][sp], flip(a0[j][i][sp], m0), flip(a1[j][i][sp], m1), b0[j][i][sp]);
 }
 
-// results of a mode stored from the epilogue tile (RES: r, rh and p are the
-// same values) and whether an epilogue operand arrives in it (b for RES and
-// RESC, rh for V, the input itself for T and RHS)
+// results of a mode stored from the epilogue tiles (RES: r, rh and p are the
+// same values; RESC: the FP32 r and r/theta, two FP32 tiles in buffer 4's
+// block region) and whether an epilogue operand arrives in the FP64 tile (b
+// for RES and RESC, rh for V, the input itself for T and RHS)
 __host__ __device__ constexpr int mv4_tile_outputs(int mode) {
-  return mode == MV_RES ? 3 : (mode == MV_RESC ? 0 : 1);
+  return mode == MV_RES ? 3 : (mode == MV_RESC ? 2 : 1);
 }
 __host__ __device__ constexpr bool mv4_tile_input(int mode) { return mode != MV_PLAIN; }
 // byte offset of (plane p, site l) in the epilogue tile: two halves of 8
@@ -268,6 +269,12 @@ __host__ __device__ constexpr bool mv4_tile_input(int mode) { return mode != MV_
 __device__ __forceinline__ uint32_t epi_off(int p, int l) {
   return (uint32_t)((l >> 3) * mv4::kEpiHalf + p * 128 + (((l & 7) ^ (p & 7)) << 4));
 }
+// byte offset of (plane p, site l) in an FP32 result tile: rows of 16 sites
+// x 8 bytes, 16-byte chunks swizzled with the row (1024-aligned tile)
+__device__ __forceinline__ uint32_t epi32_off(int p, int l) {
+  return (uint32_t)(p * 128 + ((((l >> 1) ^ (p & 7))) << 4) + ((l & 1) << 3));
+}
+constexpr int kOffF32 = 22528;  // FP32 result tiles of RESC in buffer 4 (its block region, after stage 4)
 
 template <int MODE>
 __global__ void __maxnreg__(mv4::kMaxReg)
@@ -309,11 +316,16 @@ __global__ void __maxnreg__(mv4::kMaxReg)
   uint32_t p_par = 0;                // empty-barrier parity of the previous use of a buffer
   int pss[5] = {0, 0, 0, 0, 0};      // tile starts of p_unit
   auto store_results = [&](int x0) {
+    if (MODE == MV_RESC) {
 #pragma unroll
-    for (int o = 0; o < kNOut; ++o)
+      for (int o = 0; o < 2; ++o) tma_store_2d(&maps.out[o], 2 * x0, 0, smem + kBuf4 + kOffF32 + o * kEpiHalf);
+    } else {
 #pragma unroll
-      for (int hf = 0; hf < 2; ++hf)
-        tma_store_2d(&maps.out[o], 2 * x0 + 16 * hf, 0, smem + kBuf4 + kOffEpi + hf * kEpiHalf);
+      for (int o = 0; o < kNOut; ++o)
+#pragma unroll
+        for (int hf = 0; hf < 2; ++hf)
+          tma_store_2d(&maps.out[o], 2 * x0 + 16 * hf, 0, smem + kBuf4 + kOffEpi + hf * kEpiHalf);
+    }
     bulk_commit();
   };
   auto issue = [&]() {
@@ -592,7 +604,10 @@ __global__ void __maxnreg__(mv4::kMaxReg)
     }
 
     // ------------------------------------------------------------ epilogue
-    // (buffer 4 is released after it: the producer then stores the tile)
+    // (buffer 4 is released after it: the producer then stores the tiles).
+    // RESC writes into buffer 4's block region: every consumer warp must have
+    // finished stage 4's products first.
+    if (MODE == MV_RESC) named_bar_sync(1, kWarps * 32);
     if (!dead && out_lane) {
       const uint32_t epi = smem_u32(smem + kBuf4 + kOffEpi);
 #pragma unroll
@@ -624,11 +639,11 @@ __global__ void __maxnreg__(mv4::kMaxReg)
               qs[sp][e][0] += dd.re;
               qs[sp][e][1] += dd.im;
             } else if (MODE == MV_RESC) {
-              const int64_t o = (int64_t)pl * V + x;
+              const uint32_t fa = smem_u32(smem + kBuf4 + kOffF32) + epi32_off(pl, warp * kSPW + i);
               const cplx r = pv - y_;
               const cplx dd = r * A.inv_theta[sp];
-              A.r32[o] = make_float2((float)r.re, (float)r.im);
-              A.d32[o] = make_float2((float)dd.re, (float)dd.im);
+              sts2f(fa, (float)r.re, (float)r.im);
+              sts2f(fa + kEpiHalf, (float)dd.re, (float)dd.im);
               qs[sp][e][0] += norm2(r);
               qs[sp][e][1] += norm2(pv);
             } else {  // MV_T: in = s
@@ -699,9 +714,15 @@ int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double
   const void *epi_src = (mode == MV_V) ? (const void *)a.in2
                         : (mode == MV_RES || mode == MV_RESC) ? (const void *)a.bvec : (const void *)a.in;
   if (mv4_tile_input(mode) && !stage::encode(&maps.epi_in, epi_src, 2 * V, 72, 16, 72, sw128)) return -1;
-  const void *outs[3] = {a.out, a.out2, a.out3};
-  for (int o = 0; o < mv4_tile_outputs(mode); ++o)
-    if (!stage::encode(&maps.out[o], outs[o], 2 * V, 72, 16, 72, sw128)) return -1;
+  if (mode == MV_RESC) {  // FP32 tiles: 16 sites x 2 floats per row
+    const void *outs[2] = {a.r32, a.d32};
+    for (int o = 0; o < 2; ++o)
+      if (!stage::encode(&maps.out[o], outs[o], 2 * V, 72, 32, 72, sw128, CU_TENSOR_MAP_DATA_TYPE_FLOAT32)) return -1;
+  } else {
+    const void *outs[3] = {a.out, a.out2, a.out3};
+    for (int o = 0; o < mv4_tile_outputs(mode); ++o)
+      if (!stage::encode(&maps.out[o], outs[o], 2 * V, 72, 16, 72, sw128)) return -1;
+  }
   const int64_t nunits = cn_mv4_units(L.V);
   const unsigned grid = (unsigned)cn_mv4_rows(L.V, sm_count);
   auto go = [&](auto kern) {

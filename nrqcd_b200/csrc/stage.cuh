@@ -87,6 +87,13 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 __device__ __forceinline__ void sts2(uint32_t a, double re, double im) {
   asm volatile("st.shared.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(re), "d"(im) : "memory");
 }
+__device__ __forceinline__ void sts2f(uint32_t a, float re, float im) {
+  asm volatile("st.shared.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(re), "f"(im) : "memory");
+}
+// barrier `id` (1-15) among the first `nthreads` threads of the CTA (whole warps)
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
 
 // contiguous copy of `bytes` (multiple of 16; both addresses 16-byte aligned)
 __device__ __forceinline__ void bulk_1d(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
@@ -110,16 +117,19 @@ inline PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
   return fn;
 }
 
-// 2D map over `planes` planes of `elems_per_plane` doubles (plane stride = elems)
+// 2D map over `planes` planes of `elems_per_plane` elements (FP64 unless
+// dt says FP32; plane stride = elems)
 inline bool encode(CUtensorMap *m, const void *base, uint64_t elems_per_plane, uint64_t planes, uint32_t box0,
-                   uint32_t box1, CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
+                   uint32_t box1, CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_FLOAT64) {
   auto fn = get_encoder();
   if (!fn) return false;
+  const uint64_t esize = dt == CU_TENSOR_MAP_DATA_TYPE_FLOAT32 ? 4 : 8;
   cuuint64_t dims[2] = {elems_per_plane, planes};
-  cuuint64_t strides[1] = {elems_per_plane * sizeof(double)};
+  cuuint64_t strides[1] = {elems_per_plane * esize};
   cuuint32_t box[2] = {box0, box1};
   cuuint32_t es[2] = {1, 1};
-  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void *>(base), dims, strides, box, es,
+  CUresult r = fn(m, dt, 2, const_cast<void *>(base), dims, strides, box, es,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
