@@ -16,25 +16,42 @@ Modes (the reference's `program simulation`, src/main.f90:3301-3340):
   correlator file (s, Re/Im of O1(1S0), O1(3S1), O8(1S0), O8(3S1)) and the
   norm file (s, quark, antiquark), '(n(SP,E16.9,1X))', with the reference's
   header lines.
+- **3**, MeasureHeavyQuarkoniumCorrelators, the (t,s)-grid correlator
+  (src/main.f90:2169-2565).  Arguments: Nx Ny Nz ds ax ay az tmin tmax smax
+  Seed Qs Amplitude Coupling kspTol M Re(c1) Im(c1) ... Re(c4) Im(c4)
+  FileMesonCorrelator FileNorm, with a0 = ds/2.  Transverse-polarised box
+  initial condition and a point source at t = 0; the configuration is
+  evolved to t1min = tmin - smax/2, and from every t1 a copy of the
+  configuration and of the (never evolved) point source runs coupled steps
+  to t2 = t1 + a0 .. t1 + smax.  Points with t = (t1+t2)/2 and s = t2 - t1 on
+  the ds grid inside [tmin, tmax] record O1(3S1) and the norms.  Writes the
+  correlator file (one row per s, Re/Im per t) and the norm file (Q/A per
+  t), NaN where the grid has no sample, '(SP,E16.9,1X)' with the
+  reference's F-formatted header.
 
 `--form` selects the CN solver form (0 plain FP64, the reference's
 precision; 1 precision form).  Progress goes to stdout as in the reference.
+Records follow Fortran's rule that a trailing X edit descriptor transmits
+no characters: values are separated by one blank and no record ends in one.
 The modes whose initial state needs the thermal EquilibriumInit (33, 51, 52)
-and the analysis modes (1, 11, 3, 4, 5) are outside the hot path.
+and the analysis modes (1, 11, 4, 5) are outside the hot path.
 """
 from __future__ import annotations
 
 import math
 import sys
 
+import numpy as np
+
 from . import lattice, nrqcd
 from .gaugeconfiguration_su3 import GaugeConfiguration
 from .nrqcd import NRQCDField
 
 
-def fortran_e(x: float, w: int, d: int) -> str:
-    """Fortran 'SP,Ew.d' edit descriptor: sign, 0., d digits, exponent."""
-    sign = "-" if (x < 0 or (x == 0 and math.copysign(1.0, x) < 0)) else "+"
+def fortran_e(x: float, w: int, d: int, plus: bool = True) -> str:
+    """Fortran 'SP,Ew.d' edit descriptor: sign, 0., d digits, exponent
+    ('Ew.d' without SP when plus is False: no sign for positive values)."""
+    sign = "-" if (x < 0 or (x == 0 and math.copysign(1.0, x) < 0)) else ("+" if plus else "")
     ax = abs(float(x))
     if ax == 0.0:
         body = "0." + "0" * d + "E+00"
@@ -54,8 +71,22 @@ def fortran_e(x: float, w: int, d: int) -> str:
     return s.rjust(w) if len(s) <= w else "*" * w
 
 
+def fortran_f(x: float, w: int, d: int) -> str:
+    """Fortran 'Fw.d' edit descriptor: d decimals right-justified in w
+    characters; the optional leading zero of |x| < 1 is dropped when the
+    width needs it, and a value that does not fit prints w asterisks."""
+    s = f"{abs(float(x)):.{d}f}" + ("." if d == 0 else "")
+    neg = x < 0 and float(s.rstrip(".")) != 0.0
+    if neg:
+        s = "-" + s
+    if len(s) > w and (s.startswith("0.") or s.startswith("-0.")):
+        s = s.replace("0.", ".", 1)
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
 def _line(values, w: int, d: int) -> str:
-    return "".join(fortran_e(v, w, d) + " " for v in values)
+    """One record of n(SP,Ew.d,1X): values separated by one blank."""
+    return " ".join(fortran_e(v, w, d) for v in values)
 
 
 def _nint(x: float) -> int:
@@ -137,6 +168,143 @@ def mode_correlators_free(args, form=0, device=0):
     del seed
 
 
+ZERO_TOL = 1e-12  # GetZeroTol() of the FP64 build, src/tolerances.f90:21-26
+
+
+def ts_grid_schedule(a0: float, ds: float, tmin: float, tmax: float, smax: float):
+    """The (t,s)-grid loop structure of mode 3 (src/main.f90:2244-2362),
+    host arithmetic only.
+
+    Returns (pre_sign, n_pre, rows): n_pre leapfrog steps of width pre_sign
+    bring the configuration from t = 0 to t1min = tmin - smax/2; each row
+    (it1, steps) starts from the configuration at t1 = it1*a0, and each entry
+    (it2, point) of steps is one coupled step ending at t2 = it2*a0, with
+    point = (is, it) where the reference records the sample and None
+    otherwise.  As in the reference, the step that leaves [., tmax] is still
+    taken before the row ends, and every entry counts as one unit of
+    progress.
+    """
+    t1min = tmin - smax / 2
+    t1max = tmax
+    n_pre = _nint(abs(t1min) / a0)
+    pre_sign = math.copysign(1.0, t1min)
+    it2range = _nint(smax / a0)
+    rows = []
+    for it1 in range(_nint(t1min / a0), _nint(t1max / a0) + 1):
+        t1 = it1 * a0
+        steps = []
+        for it2 in range(it1 + 1, it1 + it2range + 1):
+            t2 = it2 * a0
+            t = (t2 + t1) / 2
+            s = t2 - t1
+            itt, ist = _nint(t / ds), _nint(s / ds)
+            on_grid = abs(itt * ds - t) <= ZERO_TOL and abs(ist * ds - s) <= ZERO_TOL
+            if tmin <= t <= tmax and on_grid:
+                steps.append((it2, (ist, itt)))
+            else:
+                steps.append((it2, None))
+                if t > tmax:
+                    break
+        rows.append((it1, steps))
+    return pre_sign, n_pre, rows
+
+
+def ts_grid_bounds(ds: float, tmin: float, tmax: float, smax: float):
+    """Index ranges of the result arrays: is in [0, ismax], it in [itmin, itmax]."""
+    return 0, _nint(smax / ds), _nint(tmin / ds), _nint(tmax / ds)
+
+
+def write_ts_grid(f_corr: str, f_norm: str, ds: float, itmin: int, corr, qnorm, anorm):
+    """Output of mode 3 (src/main.f90:2366-2434).  corr, qnorm, anorm are
+    indexed [is][it - itmin].  Header: 's', then per t 'Re'/'Im' (correlator)
+    or 'Q'/'A' (norm) glued to t in F(w.d) with d = nint(-log10 ds) and
+    w = d + p + 2, p = nint(log10|t|) for |t| > 1 else 0 (the reference
+    writes w and d with I1, so both must be single digits)."""
+    nt = len(corr[0])
+    d = _nint(-math.log10(ds))
+    hc, hn = ["s"], ["s"]
+    for k in range(nt):
+        t = (itmin + k) * ds
+        p = _nint(math.log10(abs(t))) if abs(t) > 1 else 0
+        w = d + p + 2
+        if not (0 <= d <= 9 and 0 <= w <= 9):
+            raise ValueError(f"(t,s)-grid header: F{w}.{d} is outside the reference's single-digit format")
+        ft = fortran_f(t, w, d)
+        hc += ["Re" + ft, "Im" + ft]
+        hn += ["Q" + ft, "A" + ft]
+    with open(f_corr, "w") as fc, open(f_norm, "w") as fn:
+        fc.write(" ".join(hc) + "\n")
+        fn.write(" ".join(hn) + "\n")
+        for is_ in range(len(corr)):
+            s = is_ * ds
+            vc, vn = [s], [s]
+            for k in range(nt):
+                vc += [corr[is_][k].real, corr[is_][k].imag]
+                vn += [qnorm[is_][k], anorm[is_][k]]
+            fc.write(_line(vc, 16, 9) + "\n")
+            fn.write(_line(vn, 16, 9) + "\n")
+
+
+def mode_ts_grid(args, form=0, device=0):
+    ext = [int(a) for a in args[0:3]]
+    ds = float(args[3])
+    sp = [ds / 2] + [float(a) for a in args[4:7]]
+    tmin, tmax, smax = float(args[7]), float(args[8]), float(args[9])
+    seed = int(args[10])
+    qs, amp, coupling = float(args[11]), float(args[12]), float(args[13])
+    ksp_tol = float(args[14])
+    mass = float(args[15])
+    c = [complex(float(args[16 + 2 * k]), float(args[17 + 2 * k])) for k in range(4)]
+    f_corr, f_norm = args[24], args[25]
+    ismin, ismax, itmin, itmax = ts_grid_bounds(ds, tmin, tmax, smax)
+    nan = float("nan")
+    ns, nt = ismax - ismin + 1, itmax - itmin + 1
+    corr = [[complex(nan, nan)] * nt for _ in range(ns)]
+    qnorm = [[nan] * nt for _ in range(ns)]
+    corr[0] = [1j] * nt  # s = 0: the reference's preset row
+    qnorm[0] = [1.0] * nt
+    anorm = [row[:] for row in qnorm]
+    pre_sign, n_pre, rows = ts_grid_schedule(sp[0], ds, tmin, tmax, smax)
+    nprogress = sum(len(steps) for _, steps in rows)
+    lattice.InitModule(ext, sp, device=device)
+    try:
+        nrqcd.InitModule(mass, c, 1.0, ksp_tol, form=form)
+        g1, g2 = GaugeConfiguration(), GaugeConfiguration()
+        g1.TransversePolarisedOccupiedInit_Box(qs, amp, coupling, RandomSeed=seed, identity_links=False)
+        h1, h2 = NRQCDField(), NRQCDField()
+        h1.InitSinglePoint(1, 1)
+        for _ in range(n_pre):
+            g1.Update(pre_sign)
+        iprogress = 0
+        for _, steps in rows:
+            g2.assign(g1)
+            h2.Assign(h1)
+            for _, point in steps:
+                iprogress += 1
+                # '(E16.9,A1)' of real(iprogress)/nprogress*100 in default (single) precision
+                pct = np.float32(iprogress) / np.float32(nprogress) * np.float32(100)
+                print(fortran_e(float(pct), 16, 9, plus=False) + "%", flush=True)
+                h2.Update(g2, mass, c, 1.0)
+                g2.Update(1.0)
+                if point is not None:
+                    is_, it_ = point
+                    if not (ismin <= is_ <= ismax and itmin <= it_ <= itmax):
+                        raise RuntimeError(f"(t,s)-grid point ({is_}, {it_}) outside the result arrays")
+                    corr[is_][it_ - itmin] = h2.GetMesoncorrelator_O1_3S1_ZeroMomentum()
+                    qnorm[is_][it_ - itmin] = h2.GetNorm_Quark()
+                    anorm[is_][it_ - itmin] = h2.GetNorm_AntiQ()
+            g1.Update(1.0)
+        write_ts_grid(f_corr, f_norm, ds, itmin, corr, qnorm, anorm)
+        h1.Destructor()
+        h2.Destructor()
+        g1.Deallocate()
+        g2.Deallocate()
+        nrqcd.FinalizeModule()
+    finally:
+        lattice.FinalizeModule()
+    print(" Simulation completed", flush=True)
+
+
 def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
     form, device = 0, 0
@@ -153,10 +321,12 @@ def main(argv=None):
     mode = int(argv[0])
     if mode == 2:
         mode_energy_gauss(argv[1:], device=device)
+    elif mode == 3:
+        mode_ts_grid(argv[1:], form=form, device=device)
     elif mode == 32:
         mode_correlators_free(argv[1:], form=form, device=device)
     else:
-        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2 and 32): {mode}")
+        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2, 3 and 32): {mode}")
 
 
 if __name__ == "__main__":
