@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--only-forms", action="store_true", help="print only the CN-forms JSON")
     p.add_argument("--forms-sizes", type=int, nargs="+", default=list(FORMS_SIZES))
     p.add_argument("--no-drift", action="store_true")
+    p.add_argument("--no-thermal", action="store_true")
+    p.add_argument("--only-thermal", action="store_true", help="print only the thermal initial-condition JSON")
     p.add_argument("--stencil", default="timed", choices=["timed", "register", "tma", "tensor"],
                    help="FP64 stencil of the headline step (default: the solver's timed choice)")
     p.add_argument("--only-drift", action="store_true", help="print only the precision-drift JSON")
@@ -175,6 +177,56 @@ def cpu_baseline_sample(L):
     return {"value": L ** 3 / dt, "unit": "site-updates/s", "cores": oc.num_threads(), "kind": "port",
             "sample": f"1 coupled {L}^3 step ({dt:.1f} s), FP64 C restatement of the reference algorithm "
                       "(OpenMP), GMRES(30) to 1e-12"}
+
+
+# ------------------------------------------------------------------ thermal initial condition
+THERMAL_BETA = 10.0
+# algorithmic bytes per site of one Gauss projection sweep: k_gauss_g reads E
+# (192 B) and the links (432 B) and writes G (144 B); k_gauss_sweep reads G,
+# E and the links and writes E (144 + 192 + 432 + 192 B)
+THERMAL_BYTES_SITE_SWEEP = 768 + 960
+
+
+def measure_thermal_ic(L, seed=1, cpu=True, cpu_sweeps=4):
+    """EquilibriumInit (beta 10, one round, no leapfrog steps) on an L^3
+    lattice of the open module context: the Gauss projection dominates.
+    CUDA events around the call on the context's stream; the CPU leg times
+    `cpu_sweeps` sweeps of the oracle's projection on the same drawn field."""
+    import torch
+    from nrqcd_b200 import GaugeConfiguration, _capi, lattice
+    ctx = lattice.context()
+    stream = torch.cuda.ExternalStream(_capi.load().nrq_cuda_stream(ctx))
+    g = GaugeConfiguration()
+    g.EquilibriumInit(THERMAL_BETA, 1, 0, RandomSeed=seed, verbose=False)  # warm-up (allocations)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    sw, en, dev = g.EquilibriumInit(THERMAL_BETA, 1, 0, RandomSeed=seed, verbose=False)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    del g
+    V = L ** 3
+    sweeps = int(sw[0])
+    out = {"config": {"lattice": [L, L, L], "beta": THERMAL_BETA, "nefieldinit": 1, "nequilibrium": 0,
+                      "tolerance": 1e-3, "seed": seed},
+           "sweeps": sweeps, "final_deviation": float(dev[0]), "ms_total": ms,
+           "ms_per_sweep": ms / max(1, sweeps),
+           "site_sweeps_per_s": V * sweeps / (ms / 1000.0),
+           "algorithmic_GBps": THERMAL_BYTES_SITE_SWEEP * V * sweeps / (ms / 1000.0) / 1e9,
+           "note": "ms_total includes the host ranlxd draw of the thermal field and its upload"}
+    if cpu:
+        from oracle import oracle as oc
+        n = (L, L, L)
+        links, ef, _, _, _ = oc.equilibrium_init(n, A, THERMAL_BETA, 1, 0, tol=1e9, seed=seed)
+        t0 = time.perf_counter()
+        done = oc.gauss_project(n, A, links, ef, tol=1e-3, max_sweeps=cpu_sweeps)
+        dt = time.perf_counter() - t0
+        cps = V * done / dt
+        out["cpu_baseline"] = {"value": cps, "unit": "site-sweeps/s", "cores": oc.num_threads(), "kind": "port",
+                               "sample": f"{done} projection sweeps of the oracle at {L}^3 ({dt:.1f} s)"}
+        out["speedup_vs_cpu"] = out["site_sweeps_per_s"] / cps
+    return out
 
 
 # ------------------------------------------------------------------ CN forms
@@ -566,6 +618,14 @@ def main():
     h.InitSinglePoint(1, 1)
     lib = _capi.load()
     stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(ctx))
+    if args.only_thermal:
+        out = measure_thermal_ic(L, cpu=not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps({"thermal_initial_condition": out}), flush=True)
+        del h, g
+        nrqcd.FinalizeModule()
+        lattice.FinalizeModule()
+        return
     if args.only_forms:
         forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
         if rank == 0:
@@ -656,6 +716,10 @@ def main():
     if not args.no_drift and world == 1:
         drift = [measure_precision_drift(L, n0, 20) for n0 in (0.5, 1.0, 2.0)]
 
+    thermal = None
+    if not args.no_thermal and world == 1:
+        thermal = measure_thermal_ic(L, cpu=not args.no_cpu_baseline)
+
     forms = None
     if not args.no_forms and world == 1:
         forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
@@ -702,6 +766,7 @@ def main():
             "cn_forms_at_1e-10": forms,
             "batching_ensemble": ensemble,
             "precision_drift": drift,
+            "thermal_initial_condition": thermal,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(min(L, 64))

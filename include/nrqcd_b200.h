@@ -122,6 +122,25 @@ int nrq_gauge_energy(nrq_gauge *g, double *energy);
 /* GetDeviationFromGaussLaw (:1480-1531) -> ref_measure, and the max-norm
  * GetGdeviation of EquilibriumInit (:724-768) -> max_norm                   */
 int nrq_gauge_gauss(nrq_gauge *g, double *ref_measure, double *max_norm);
+/* The Gauss projection loop of EquilibriumInit,
+ * src/gaugeconfiguration_su3.f90:455-500 (no charges): Jacobi sweeps of the
+ * electric field until the max-norm deviation (:724-768) is at most tol.
+ * *sweeps gets the sweeps taken and *deviation the final deviation (either
+ * may be NULL).  max_sweeps <= 0 means no limit, as in the reference;
+ * otherwise NRQ_ERR_NOT_CONVERGED after max_sweeps sweeps.                  */
+int nrq_gauge_gauss_project(nrq_gauge *g, double tol, int64_t max_sweeps, int64_t *sweeps, double *deviation);
+/* EquilibriumInit(beta, nefieldinit, nequilibrium, tol), same file :380-814
+ * after random%InitModule(seed) (src/random.f90:126-140), without charges and
+ * without the file output of MeasureEnergy: cold links, then nefieldinit
+ * rounds of a thermal field (E^a_k(x) = Re(sqrt(4/beta) r) a0 for complex
+ * normals r drawn per site and direction, :432-444), the Gauss projection and
+ * nequilibrium leapfrog steps.  Per round (arrays of nefieldinit entries,
+ * each may be NULL): projection sweeps, energy and max-norm deviation after
+ * the steps (the values the reference writes and prints).  max_sweeps bounds
+ * each projection as in nrq_gauge_gauss_project.                            */
+int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nefieldinit, int64_t nequilibrium,
+                               double tol, int64_t seed, int64_t max_sweeps, int64_t *sweeps,
+                               double *energies, double *deviations);
 
 /* ---- heavy-quark field: src/nrqcd.f90:58-117 -------------------------- */
 int nrq_heavy_create(nrq_ctx *ctx, nrq_heavy **h);      /* NRQCDField() (:235-248) */

@@ -75,6 +75,10 @@ SIGNATURES = {
     "nrq_gauge_unitarity": (ctypes.c_int, [_vp, _dp, _dp]),
     "nrq_gauge_energy": (ctypes.c_int, [_vp, _dp]),
     "nrq_gauge_gauss": (ctypes.c_int, [_vp, _dp, _dp]),
+    "nrq_gauge_gauss_project": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int64, _i64p, _dp]),
+    "nrq_gauge_equilibrium_init": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int64, ctypes.c_int64,
+                                                  ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _i64p, _dp,
+                                                  _dp]),
     "nrq_heavy_create": (ctypes.c_int, [_vp, _pp]),
     "nrq_heavy_destroy": (ctypes.c_int, [_vp]),
     "nrq_heavy_upload": (ctypes.c_int, [_vp, _dp, _dp]),

@@ -293,6 +293,7 @@ extern "C" int nrq_finalize(nrq_ctx *ctx) {
   if (ctx->d_res) cudaFree(ctx->d_res);
   if (ctx->h_res) cudaFreeHost(ctx->h_res);
   if (ctx->d_stage) cudaFree(ctx->d_stage);
+  if (ctx->d_proj) cudaFree(ctx->d_proj);
   for (auto &r : ctx->prof_recs) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
@@ -638,6 +639,106 @@ extern "C" int nrq_gauge_gauss(nrq_gauge *g, double *ref_measure, double *max_no
   if ((rc = reduce_to_host(ctx, nb_, 2, 2u))) return rc;
   if (ref_measure) *ref_measure = ctx->h_res[0];
   if (max_norm) *max_norm = ctx->h_res[1];
+  return NRQ_OK;
+}
+
+// ---------------------------------------------------------------- thermal initial condition
+namespace {
+constexpr int64_t kProjUnbounded = INT64_MAX;
+
+// Gauss projection sweeps of EquilibriumInit (gauge:455-500) on g's FP64
+// field.  Sweeps are queued in growing batches; the kernels themselves stop
+// at the first sweep whose deviation is at most tol, so the count is exact.
+int gauss_project(nrq_gauge *g, double tol, int64_t max_sweeps, int64_t *sweeps, double *deviation) {
+  nrq_ctx *ctx = g->ctx;
+  const nrq::Lat L = ctx->lat;
+  const int64_t V = L.V;
+  const unsigned nbg = (unsigned)nblk(V, 128), nbs = (unsigned)nblk(V, 128);
+  int rc = gauge_sync64(g);
+  if (!rc) rc = ensure_stage(ctx, sizeof(double2) * 9 * V);
+  if (!rc) rc = ensure_red(ctx, nbg);
+  if (rc) return rc;
+  if (!ctx->d_proj) NRQ_CUDA_TRY(ctx, cudaMalloc(&ctx->d_proj, sizeof(nrq::GaussProjState)));
+  nrq::GaussProjState *st = (nrq::GaussProjState *)ctx->d_proj;
+  double2 *G = (double2 *)ctx->d_stage;
+  const double kdt = 0.01 * ctx->a[0];  // kappa a0, kappa = 0.01 (gauge:408)
+  NRQ_CUDA_TRY(ctx, cudaMemsetAsync(st, 0, sizeof(nrq::GaussProjState), ctx->stream));
+  nrq::k_gauss_g<<<nbg, 128, 0, ctx->stream>>>(L, g->U, g->E, G, ctx->d_red, st, tol, 0);
+  if ((rc = check_launch(ctx, "k_gauss_g"))) return rc;
+  const int64_t limit = max_sweeps > 0 ? max_sweeps : kProjUnbounded;
+  int64_t queued = 0, batch = 16;
+  nrq::GaussProjState h{};
+  for (;;) {
+    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h.done || queued >= limit) break;
+    const int64_t n = std::min(batch, limit - queued);
+    for (int64_t k = 0; k < n; ++k) {
+      nrq::k_gauss_sweep<<<nbs, 128, 0, ctx->stream>>>(L, g->U, G, g->E, st, kdt);
+      nrq::k_gauss_g<<<nbg, 128, 0, ctx->stream>>>(L, g->U, g->E, G, ctx->d_red, st, tol, 1);
+    }
+    if ((rc = check_launch(ctx, "Gauss projection sweep"))) return rc;
+    queued += n;
+    batch = std::min<int64_t>(batch * 2, 512);
+  }
+  if (sweeps) *sweeps = h.sweeps;
+  if (deviation) *deviation = h.dev;
+  if (!h.done) {
+    ctx->last_error = "Gauss projection: deviation above tolerance after max_sweeps sweeps";
+    return NRQ_ERR_NOT_CONVERGED;
+  }
+  return NRQ_OK;
+}
+}  // namespace
+
+extern "C" int nrq_gauge_gauss_project(nrq_gauge *g, double tol, int64_t max_sweeps, int64_t *sweeps,
+                                       double *deviation) {
+  if (!g || !(tol >= 0.0)) return NRQ_ERR_BAD_ARG;
+  int rc = set_device(g->ctx);
+  if (rc) return rc;
+  return gauss_project(g, tol, max_sweeps, sweeps, deviation);
+}
+
+extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nefieldinit, int64_t nequilibrium,
+                                          double tol, int64_t seed, int64_t max_sweeps, int64_t *sweeps,
+                                          double *energies, double *deviations) {
+  if (!g || !(beta > 0.0) || nefieldinit < 0 || nequilibrium < 0 || !(tol >= 0.0)) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  const int64_t V = ctx->lat.V;
+  int rc = set_device(ctx);
+  if (rc) return rc;
+  Ranlxd rng;
+  if (!rng.init(2, seed)) {
+    ctx->last_error = "equilibrium_init: seed must lie in [1, 2^31-1]";
+    return NRQ_ERR_BAD_ARG;
+  }
+  nrq::k_cold<<<nblk(V, 256), 256, 0, ctx->stream>>>(g->U, g->E, V);
+  if ((rc = check_launch(ctx, "k_cold"))) return rc;
+  if ((rc = gauge_written64(g))) return rc;
+  const double sigma = std::sqrt(4.0 / beta), a0 = ctx->a[0];
+  const double twopi = 2.0 * std::acos(-1.0);
+  std::vector<double> ef((size_t)24 * V);  // the reference's efield(8,3,V)
+  for (int64_t r = 0; r < nefieldinit; ++r) {
+    // Box-Muller pairs in the reference's order: site, direction, generator
+    // (random.f90:238-255); the real part, times sigma, times a0
+    for (size_t i = 0; i < ef.size(); ++i) {
+      const double u1 = rng.next(), u2 = rng.next();
+      ef[i] = (sigma * (std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2))) * a0;
+    }
+    if ((rc = ensure_stage(ctx, sizeof(double) * 24 * V))) return rc;
+    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_stage, ef.data(), sizeof(double) * 24 * V, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+    nrq::k_efield_f2soa<<<nblk(V, 256), 256, 0, ctx->stream>>>((const double *)ctx->d_stage, g->E, V);
+    if ((rc = check_launch(ctx, "k_efield_f2soa"))) return rc;
+    int64_t it = 0;
+    rc = gauss_project(g, tol, max_sweeps, &it, nullptr);
+    if (sweeps) sweeps[r] = it;
+    if (rc) return rc;
+    for (int64_t t = 0; t < nequilibrium; ++t)
+      if ((rc = nrq_gauge_update(g, 1.0))) return rc;
+    if (energies && (rc = nrq_gauge_energy(g, &energies[r]))) return rc;
+    if (deviations && (rc = nrq_gauge_gauss(g, nullptr, &deviations[r]))) return rc;
+  }
   return NRQ_OK;
 }
 

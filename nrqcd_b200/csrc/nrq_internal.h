@@ -23,6 +23,8 @@ struct nrq_ctx {
   // staging buffer for layout transposes (device), grown on demand
   void *d_stage = nullptr;
   size_t stage_bytes = 0;
+  // state of a Gauss projection (nrq::GaussProjState), allocated on first use
+  void *d_proj = nullptr;
   std::string last_error;
   int sm_count = 148;
   // opt-in per-class kernel timing (events recorded on `stream`)

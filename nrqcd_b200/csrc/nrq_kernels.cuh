@@ -30,6 +30,22 @@ __global__ void k_ic_write(Lat L, const double2 *__restrict__ A, const double2 *
                            double inv_volume, int identity_links, double2 *__restrict__ U,
                            double *__restrict__ E);
 
+// ---------------- gauss_proj.cu
+// device state of a Gauss projection: convergence flag, sweeps taken, last
+// deviation, and the block ticket of the deviation reduction (zero between
+// launches)
+struct GaussProjState {
+  int done;
+  unsigned ticket;
+  long long sweeps;
+  double dev;
+};
+__global__ void k_gauss_g(Lat L, const double2 *__restrict__ U, const double *__restrict__ E,
+                          double2 *__restrict__ G, double *__restrict__ partials, GaussProjState *st, double tol,
+                          int count);
+__global__ void k_gauss_sweep(Lat L, const double2 *__restrict__ U, const double2 *__restrict__ G,
+                              double *__restrict__ E, const GaussProjState *st, double kdt);
+
 // ---------------- cn.cu
 // Per-species, per-term complex coefficients of the assembled CN operator:
 //   out = in + sum_t alpha_t G_t in      (t = kinetic, magnetic, Darwin, spin-orbit)

@@ -29,12 +29,20 @@ Modes (the reference's `program simulation`, src/main.f90:3301-3340):
   t), NaN where the grid has no sample, '(SP,E16.9,1X)' with the
   reference's F-formatted header.
 
+- **33**, MeasureHeavyQuarkoniumCorrelators_Equilibrium (src/main.f90:18-280).
+  Arguments: Nx Ny Nz a0 ax ay az smax Seed Beta nefieldinit
+  nequilibriumtimesteps kspTol M Re(c1) Im(c1) ... Re(c4) Im(c4)
+  FileMesonCorrelator FileNorm MeasureEnergy [EnergyFilename].  As mode 32
+  from the thermal EquilibriumInit (Gauss projection on the device); with
+  MeasureEnergy = 1 the energy after each initialisation round goes to
+  EnergyFilename.
+
 `--form` selects the CN solver form (0 plain FP64, the reference's
 precision; 1 precision form).  Progress goes to stdout as in the reference.
 Records follow Fortran's rule that a trailing X edit descriptor transmits
 no characters: values are separated by one blank and no record ends in one.
-The modes whose initial state needs the thermal EquilibriumInit (33, 51, 52)
-and the analysis modes (1, 11, 4, 5) are outside the hot path.
+The Wilson-line modes (5, 51, 52), the one-t correlator (31) and the
+analysis modes (1, 11, 4) are outside the hot path.
 """
 from __future__ import annotations
 
@@ -125,21 +133,16 @@ CORRELATOR_HEADER = ("s Re(O1(1S0)) Im(O1(1S0)) Re(O1(3S1)) Im(O1(3S1)) Re(O8(1S
 NORM_HEADER = "s Quark Antiq"
 
 
-def mode_correlators_free(args, form=0, device=0):
-    ext = [int(a) for a in args[0:3]]
-    sp = [float(a) for a in args[3:7]]
-    smax = float(args[7])
-    seed = int(args[8])  # the free mode draws no random numbers
-    ksp_tol = float(args[9])
-    mass = float(args[10])
-    c = [complex(float(args[11 + 2 * k]), float(args[12 + 2 * k])) for k in range(4)]
-    f_corr, f_norm = args[19], args[20]
+def _correlators_run(ext, sp, smax, ksp_tol, mass, c, f_corr, f_norm, init_gauge, form=0, device=0):
+    """The time loop shared by modes 32 and 33 (src/main.f90:330-371 and
+    :66-110): point sources at the origin, nint(|smax|/a0) coupled steps
+    (CN, then leapfrog), observables after each."""
     tsteps = _nint(abs(smax) / sp[0])
     lattice.InitModule(ext, sp, device=device)
     try:
         nrqcd.InitModule(mass, c, 1.0, ksp_tol, form=form)
         g = GaugeConfiguration()
-        g.ColdInit()
+        init_gauge(g)
         h = NRQCDField()
         h.InitSinglePoint(1, 1)
         with open(f_corr, "w") as fc, open(f_norm, "w") as fn:
@@ -165,7 +168,40 @@ def mode_correlators_free(args, form=0, device=0):
     finally:
         lattice.FinalizeModule()
     print(" Simulation completed", flush=True)
-    del seed
+
+
+def mode_correlators_free(args, form=0, device=0):
+    ext = [int(a) for a in args[0:3]]
+    sp = [float(a) for a in args[3:7]]
+    smax = float(args[7])
+    int(args[8])  # Seed: read, but the free mode draws no random numbers
+    ksp_tol = float(args[9])
+    mass = float(args[10])
+    c = [complex(float(args[11 + 2 * k]), float(args[12 + 2 * k])) for k in range(4)]
+    _correlators_run(ext, sp, smax, ksp_tol, mass, c, args[19], args[20], lambda g: g.ColdInit(), form, device)
+
+
+def mode_correlators_equilibrium(args, form=0, device=0):
+    """Mode 33 (src/main.f90:18-280): as mode 32 from a thermal configuration,
+    EquilibriumInit(Beta, nefieldinit, nequilibriumtimesteps) with the
+    default projection tolerance 1e-3 after random%InitModule(Seed)."""
+    ext = [int(a) for a in args[0:3]]
+    sp = [float(a) for a in args[3:7]]
+    smax = float(args[7])
+    seed = int(args[8])
+    beta = float(args[9])
+    nefieldinit, nequilibrium = int(args[10]), int(args[11])
+    ksp_tol = float(args[12])
+    mass = float(args[13])
+    c = [complex(float(args[14 + 2 * k]), float(args[15 + 2 * k])) for k in range(4)]
+    f_corr, f_norm = args[22], args[23]
+    measure = int(args[24]) != 0
+    energy_file = args[25] if measure else None
+
+    def init(g):
+        g.EquilibriumInit(beta, nefieldinit, nequilibrium, MeasureEnergy=measure, filename=energy_file,
+                          RandomSeed=seed)
+    _correlators_run(ext, sp, smax, ksp_tol, mass, c, f_corr, f_norm, init, form, device)
 
 
 ZERO_TOL = 1e-12  # GetZeroTol() of the FP64 build, src/tolerances.f90:21-26
@@ -325,8 +361,10 @@ def main(argv=None):
         mode_ts_grid(argv[1:], form=form, device=device)
     elif mode == 32:
         mode_correlators_free(argv[1:], form=form, device=device)
+    elif mode == 33:
+        mode_correlators_equilibrium(argv[1:], form=form, device=device)
     else:
-        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2, 3 and 32): {mode}")
+        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2, 3, 32 and 33): {mode}")
 
 
 if __name__ == "__main__":

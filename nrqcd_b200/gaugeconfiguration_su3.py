@@ -18,6 +18,37 @@ from . import _capi, lattice
 modulename = "gaugeconfiguration_su3"
 
 
+def _list_real8(x: float) -> str:
+    """A real(8) item of gfortran's list-directed output: 17 significant
+    digits, fixed form for 0.1 <= |x| < 1e16 (five blanks where the exponent
+    would be), otherwise E form with a three-digit exponent; 26 characters."""
+    ax = abs(x)
+    if x != x or ax in (float("inf"),):
+        return ("NaN" if x != x else ("-" if x < 0 else "") + "Infinity").rjust(26)
+    if ax == 0.0 or 0.1 <= ax < 1e16:
+        e = 0 if ax == 0.0 else int(np.floor(np.log10(ax)))
+        body = f"{x:.{max(16 - e, 0)}f}"
+        if len(body.lstrip("-").split(".")[0]) > e + 1 and ax != 0.0:  # rounding carried into a new digit
+            body = f"{x:.{max(15 - e, 0)}f}"
+        return (body + " " * 5).rjust(26)
+    m, ex = f"{x:.16E}".split("E")
+    return f"{m}E{int(ex):+04d}".rjust(26)
+
+
+def list_directed(items) -> str:
+    """One record of gfortran list-directed output: integers as I12, reals as
+    _list_real8, character items as themselves after one blank."""
+    out = []
+    for v in items:
+        if isinstance(v, str):
+            out.append(" " + v)
+        elif isinstance(v, (int, np.integer)):
+            out.append(f"{int(v):12d}")
+        else:
+            out.append(_list_real8(float(v)))
+    return "".join(out)
+
+
 class GaugeConfiguration:
     def __init__(self, lat=None):
         """lat: a lattice.Lattice (ensemble member); default the module context."""
@@ -82,6 +113,42 @@ class GaugeConfiguration:
         """src/gaugeconfiguration_su3.f90:906-951 after random%InitModule(RandomSeed)."""
         self._call("nrq_gauge_transverse_box_init", float(SaturationScale), float(Amplitude), float(Coupling),
                    int(RandomSeed), int(bool(identity_links)))
+
+    def EquilibriumInit(self, Beta, nefieldinit, nequilibrium, tolerance_Eprojection=1e-3, MeasureEnergy=False,
+                        filename=None, RandomSeed=1, max_sweeps=0, verbose=True):
+        """EquilibriumInit, src/gaugeconfiguration_su3.f90:380-814 (no charge
+        density), after random%InitModule(RandomSeed).  With MeasureEnergy the
+        energy after each round is written to `filename` as the reference's
+        list-directed `iefieldinit, energy` records, and echoed to stdout;
+        every round prints its Gauss deviation ('G[U,E]=').  Returns per round
+        the projection sweeps, the energies and the deviations."""
+        if MeasureEnergy and not filename:
+            raise _capi.NrqcdError("Filename for energy output missing")
+        n = int(nefieldinit)
+        sweeps = np.zeros(max(n, 1), dtype=np.int64)
+        en = np.zeros(max(n, 1))
+        dev = np.zeros(max(n, 1))
+        self._call("nrq_gauge_equilibrium_init", float(Beta), n, int(nequilibrium), float(tolerance_Eprojection),
+                   int(RandomSeed), int(max_sweeps), sweeps.ctypes.data_as(_capi._i64p), _capi.dptr(en),
+                   _capi.dptr(dev))
+        if MeasureEnergy:
+            with open(filename, "w") as f:
+                for r in range(n):
+                    f.write(list_directed((r + 1, float(en[r]))) + "\n")
+        if verbose:
+            for r in range(n):
+                if MeasureEnergy:
+                    print(list_directed((r + 1, float(en[r]))), flush=True)
+                print(list_directed(("G[U,E]=", float(dev[r]))), flush=True)
+        return sweeps[:n], en[:n], dev[:n]
+
+    def GaussProjection(self, tolerance=1e-3, max_sweeps=0):
+        """The Gauss projection loop of EquilibriumInit
+        (src/gaugeconfiguration_su3.f90:455-500) on the current
+        configuration; returns (sweeps, final deviation)."""
+        sw, d = ctypes.c_int64(), ctypes.c_double()
+        self._call("nrq_gauge_gauss_project", float(tolerance), int(max_sweeps), ctypes.byref(sw), ctypes.byref(d))
+        return sw.value, d.value
 
     # --------------------------------------------------------------- evolution
     def Update(self, StepWidth_: float = 1.0):

@@ -381,3 +381,37 @@ int64_t oc_gauge_gauss_project(const oc_lattice *L, double *links, double *efiel
   free(prev);
   return it;
 }
+
+/* EquilibriumInit without charges (gauge:380-814; the measurement branches
+   after the projection are jumped over there): cold links, then nefieldinit
+   rounds of a thermal E (sigma = sqrt(4/beta); E^a_k(x) = Re(sigma r) a0 for
+   complex normals r drawn per site and direction, gauge:432-444), Gauss
+   projection to tol, nequilibrium leapfrog steps (gauge:667-672).  Per
+   round: projection sweeps, energy and max-norm deviation after the steps
+   (any output may be NULL).  Returns -1 for a bad seed, -2 when a projection
+   did not converge within max_sweeps. */
+int oc_gauge_equilibrium_init(const oc_lattice *L, double beta, int64_t nefieldinit, int64_t nequilibrium,
+                              double tol, int64_t seed, int64_t max_sweeps, double *links, double *efield,
+                              int64_t *sweeps, double *energies, double *deviations) {
+  const int64_t V = oc_volume(L);
+  oc_ranlxd_state rng;
+  memset(&rng, 0, sizeof(rng));
+  if (oc_ranlxd_init(&rng, 2, seed) != 0) return -1;
+  const double sigma = sqrt(4.0 / beta);
+  oc_gauge_cold(L, links, efield);
+  double buf[16];
+  for (int64_t r = 0; r < nefieldinit; ++r) {
+    for (int64_t s = 0; s < V; ++s)
+      for (int k = 0; k < 3; ++k) {
+        oc_random_normal_cmplx(&rng, 8, buf);
+        for (int a = 0; a < 8; ++a) efield[(s * 3 + k) * 8 + a] = (sigma * buf[2 * a]) * L->a[0];
+      }
+    int64_t it = oc_gauge_gauss_project(L, links, efield, tol, max_sweeps);
+    if (sweeps) sweeps[r] = it;
+    if (oc_gauge_gauss_maxnorm(L, links, efield) > tol) return -2;
+    for (int64_t t = 0; t < nequilibrium; ++t) oc_gauge_update(L, links, efield, 1.0);
+    if (energies) energies[r] = oc_gauge_energy(L, links, efield);
+    if (deviations) deviations[r] = oc_gauge_gauss_maxnorm(L, links, efield);
+  }
+  return 0;
+}

@@ -76,6 +76,9 @@ void   oc_field_strength(const oc_lattice *L, const double *links, const double 
 /* Gauss projection loop of EquilibriumInit (gauge:494-540); returns sweeps */
 int64_t oc_gauge_gauss_project(const oc_lattice *L, double *links, double *efield,
                                double tol, int64_t max_sweeps);
+int     oc_gauge_equilibrium_init(const oc_lattice *L, double beta, int64_t nefieldinit, int64_t nequilibrium,
+                                  double tol, int64_t seed, int64_t max_sweeps, double *links, double *efield,
+                                  int64_t *sweeps, double *energies, double *deviations);
 
 /* ---- heavy quarks (src/nrqcd.f90) -------------------------------------- */
 void   oc_heavy_init_single_point(const oc_lattice *L, int64_t lat_index_1based, double *prop);

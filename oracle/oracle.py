@@ -80,6 +80,9 @@ def lib():
                                          ctypes.c_int64, _dp]),
             "oc_gauge_gauss_project": (ctypes.c_int64, [ctypes.POINTER(Lattice), _dp, _dp, ctypes.c_double,
                                                         ctypes.c_int64]),
+            "oc_gauge_equilibrium_init": (ctypes.c_int, [ctypes.POINTER(Lattice), ctypes.c_double, ctypes.c_int64,
+                                                         ctypes.c_int64, ctypes.c_double, ctypes.c_int64,
+                                                         ctypes.c_int64, _dp, _dp, _i64p, _dp, _dp]),
             "oc_heavy_init_single_point": (None, [ctypes.POINTER(Lattice), ctypes.c_int64, _dp]),
             "oc_heavy_norm": (ctypes.c_double, [ctypes.POINTER(Lattice), _dp]),
             "oc_cn_apply": (None, [ctypes.POINTER(Lattice), _dp, _dp, ctypes.c_double, _dp, ctypes.c_double,
@@ -242,6 +245,21 @@ def gauss_maxnorm(n, a, links, efield):
 def gauss_project(n, a, links, efield, tol=1e-3, max_sweeps=1000):
     L = lattice(n, a)
     return lib().oc_gauge_gauss_project(ctypes.byref(L), _p(links), _p(efield), tol, max_sweeps)
+
+
+def equilibrium_init(n, a, beta, nefieldinit, nequilibrium, tol=1e-3, seed=1, max_sweeps=10_000_000):
+    """EquilibriumInit (gauge:380-814, no charges): returns links, efield and
+    per round the projection sweeps, energy and deviation after the steps."""
+    links, efield = alloc_gauge(n)
+    L = lattice(n, a)
+    sweeps = np.zeros(max(nefieldinit, 1), dtype=np.int64)
+    en = np.zeros(max(nefieldinit, 1))
+    dev = np.zeros(max(nefieldinit, 1))
+    rc = lib().oc_gauge_equilibrium_init(ctypes.byref(L), beta, nefieldinit, nequilibrium, tol, seed, max_sweeps,
+                                         _p(links), _p(efield), sweeps.ctypes.data_as(_i64p), _p(en), _p(dev))
+    if rc != 0:
+        raise ValueError(f"equilibrium_init failed ({rc})")
+    return links, efield, sweeps[:nefieldinit], en[:nefieldinit], dev[:nefieldinit]
 
 
 def field_strength(n, a, links, efield, i, j, site):

@@ -76,3 +76,21 @@ def test_leapfrog_reversible_and_energy_bounded(oracle):
     for _ in range(40):
         oracle.gauge_update(n, a, links, ef, -1.0)
     assert np.abs(links - l0).max() < 1e-13 and np.abs(ef - e0).max() < 1e-15
+
+
+def test_equilibrium_init_draw_order_and_projection(oracle):
+    """EquilibriumInit's thermal field (gauge:432-444): per site, per
+    direction, the real parts of eight complex normals times sigma a0, from
+    the ranlxd stream of the seed; a round with a tolerance the field meets
+    takes no projection sweep, and a finite tolerance is met after the
+    projection and kept by the leapfrog only approximately."""
+    n, a = (3, 2, 2), (0.05, 1.0, 1.0, 1.0)
+    links, ef, sw, en, dev = oracle.equilibrium_init(n, a, 4.0, 1, 0, tol=1e9, seed=11)
+    rng = oracle.Ranlxd(2, 11)
+    want = np.array([[(1.0 * rng.normal_cmplx(8)).real * 0.05 for _ in range(3)] for _ in range(12)])
+    assert sw[0] == 0 and np.array_equal(ef, want)
+    assert np.all(links[:, :, 0, 0] == 1) and np.all(links[:, :, 0, 1] == 0)
+    n = (4, 4, 4)
+    links, ef, sw, en, dev = oracle.equilibrium_init(n, a, 10.0, 2, 0, tol=1e-3, seed=5)
+    assert np.all(sw > 0) and np.all(dev <= 1e-3) and np.all(en > 0)
+    assert abs(oracle.gauss_maxnorm(n, a, links, ef) - dev[-1]) == 0.0
