@@ -693,7 +693,7 @@ int gauss_project(nrq_gauge *g, double tol, int64_t max_sweeps, int64_t *sweeps,
 
 extern "C" int nrq_gauge_gauss_project(nrq_gauge *g, double tol, int64_t max_sweeps, int64_t *sweeps,
                                        double *deviation) {
-  if (!g || !(tol >= 0.0)) return NRQ_ERR_BAD_ARG;
+  if (!g || !(tol >= 0.0) || g->ctx->lat.V > INT32_MAX) return NRQ_ERR_BAD_ARG;
   int rc = set_device(g->ctx);
   if (rc) return rc;
   return gauss_project(g, tol, max_sweeps, sweeps, deviation);
@@ -702,7 +702,8 @@ extern "C" int nrq_gauge_gauss_project(nrq_gauge *g, double tol, int64_t max_swe
 extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nefieldinit, int64_t nequilibrium,
                                           double tol, int64_t seed, int64_t max_sweeps, int64_t *sweeps,
                                           double *energies, double *deviations) {
-  if (!g || !(beta > 0.0) || nefieldinit < 0 || nequilibrium < 0 || !(tol >= 0.0)) return NRQ_ERR_BAD_ARG;
+  if (!g || !(beta > 0.0) || nefieldinit < 0 || nequilibrium < 0 || !(tol >= 0.0) || g->ctx->lat.V > INT32_MAX)
+    return NRQ_ERR_BAD_ARG;
   nrq_ctx *ctx = g->ctx;
   const int64_t V = ctx->lat.V;
   int rc = set_device(ctx);
