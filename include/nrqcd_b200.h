@@ -157,6 +157,10 @@ int nrq_heavy_norms(nrq_heavy *h, double *norm_quark, double *norm_antiq);
 /* GetMesoncorrelator_{O1_1S0,O1_3S1,O8_1S0,O8_3S1}_ZeroMomentum,
  * src/nrqcd.f90:1484-1661; out[8] = re/im of the four correlators          */
 int nrq_heavy_correlators(nrq_heavy *h, double out[8]);
+/* GetMesoncorrelator_{O1_1S0,O1_3S1,O8_1S0,O8_3S1}_ZeroMomentum_gconjg,
+ * src/nrqcd.f90:1728-1905 (conjg(AntiQProp) in place of its hermitian
+ * conjugate); out[8] as above                                              */
+int nrq_heavy_correlators_gconjg(nrq_heavy *h, double out[8]);
 
 /* ---- Crank-Nicolson solver module: src/nrqcd.f90:167-212, 619-869 ------ */
 /* InitModule(Mass, WilsonCoeffs, StepWidth, kspTol); c = 4 complex (8 doubles).

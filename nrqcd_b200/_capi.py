@@ -87,6 +87,7 @@ SIGNATURES = {
     "nrq_heavy_init_single_point": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64]),
     "nrq_heavy_norms": (ctypes.c_int, [_vp, _dp, _dp]),
     "nrq_heavy_correlators": (ctypes.c_int, [_vp, _dp]),
+    "nrq_heavy_correlators_gconjg": (ctypes.c_int, [_vp, _dp]),
     "nrq_cn_init": (ctypes.c_int, [_vp, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_int64, ctypes.c_int, _pp]),
     "nrq_cn_finalize": (ctypes.c_int, [_vp]),

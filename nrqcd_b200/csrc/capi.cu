@@ -846,19 +846,25 @@ extern "C" int nrq_heavy_norms(nrq_heavy *h, double *nq, double *na) {
   return NRQ_OK;
 }
 
-extern "C" int nrq_heavy_correlators(nrq_heavy *h, double out[8]) {
+namespace {
+int heavy_correlators(nrq_heavy *h, double out[8], bool gconjg) {
   if (!h || !out) return NRQ_ERR_BAD_ARG;
   nrq_ctx *ctx = h->ctx;
   int rc = set_device(ctx);
   if (rc) return rc;
   int64_t nb_ = nblk(ctx->lat.V, 128);
   if ((rc = ensure_red(ctx, nb_ * 8))) return rc;
-  nrq::launch_correlators(h->P, ctx->lat.V, ctx->d_red, nb_, ctx->stream);
+  nrq::launch_correlators(h->P, ctx->lat.V, ctx->d_red, nb_, ctx->stream, gconjg);
   if ((rc = check_launch(ctx, "k_correlators"))) return rc;
   if ((rc = reduce_to_host(ctx, nb_, 8, 0u))) return rc;
   for (int k = 0; k < 8; ++k) out[k] = ctx->h_res[k];
   return NRQ_OK;
 }
+}  // namespace
+
+extern "C" int nrq_heavy_correlators(nrq_heavy *h, double out[8]) { return heavy_correlators(h, out, false); }
+
+extern "C" int nrq_heavy_correlators_gconjg(nrq_heavy *h, double out[8]) { return heavy_correlators(h, out, true); }
 
 // ====================================================================== CN solver
 extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, double tol,

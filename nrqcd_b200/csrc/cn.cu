@@ -616,13 +616,18 @@ struct GamTable {
 };
 __constant__ GamTable c_gam;
 
+// GCONJ: the _gconjg variants (src/nrqcd.f90:1728-1905), conj(A) in place of
+// A^+, i.e. A's indices swapped in every product below
+template <bool GCONJ>
 __global__ void __launch_bounds__(128) k_correlators(const double2 *__restrict__ P, int64_t V, double *partials) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (s < V) {
     // Q[r][c] = quark (row r, col c), A likewise
     auto q = [&](int r, int c) { return ldg(P + (int64_t)(c * 6 + r) * V + s); };
-    auto a = [&](int r, int c) { return ldg(P + (int64_t)(36 + c * 6 + r) * V + s); };
+    auto a = [&](int r, int c) {
+      return GCONJ ? ldg(P + (int64_t)(36 + r * 6 + c) * V + s) : ldg(P + (int64_t)(36 + c * 6 + r) * V + s);
+    };
     // O1_1S0 = i Tr(A^+ Q) = i sum_{rc} conj(A[r][c]) Q[r][c]
     cplx t = {0.0, 0.0};
     for (int r = 0; r < 6; ++r)
@@ -711,7 +716,8 @@ static void build_gamma_table(GamTable &T) {
     for (int a = 0; a < 8; ++a) add_gamma(2, g++, Tre[a], Tim[a], Sre[k], Sim[k]);
 }
 
-void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st) {
+void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st,
+                        bool gconjg) {
   static GamTable T;
   static bool built = false;
   if (!built) {
@@ -720,7 +726,8 @@ void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &
   }
   cudaMemcpyToSymbolAsync(c_gam, &T, sizeof(T), 0, cudaMemcpyHostToDevice, st);
   nblk = (V + 127) / 128;
-  k_correlators<<<(unsigned)nblk, 128, 0, st>>>(P, V, partials);
+  if (gconjg) k_correlators<true><<<(unsigned)nblk, 128, 0, st>>>(P, V, partials);
+  else k_correlators<false><<<(unsigned)nblk, 128, 0, st>>>(P, V, partials);
 }
 
 }  // namespace nrq

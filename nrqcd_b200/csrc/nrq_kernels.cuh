@@ -177,6 +177,7 @@ void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st)
 void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);
 void launch_single_point(double2 *P, int64_t V, int64_t sq, int64_t sa, cudaStream_t st);
 void launch_norms(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st);
-void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st);
+void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st,
+                        bool gconjg = false);
 
 }  // namespace nrq

@@ -29,6 +29,12 @@ Modes (the reference's `program simulation`, src/main.f90:3301-3340):
   t), NaN where the grid has no sample, '(SP,E16.9,1X)' with the
   reference's F-formatted header.
 
+- **31**, MeasureHeavyQuarkoniumCorrelators_oneT (src/main.f90:523-780).
+  Arguments: Nx Ny Nz a0 ax ay az t smax Seed Qs Amplitude Coupling kspTol M
+  Re(c1) Im(c1) ... Re(c4) Im(c4) FileMesonCorrelator FileNorm
+  FileMesonCorrelator_gconjg.  Correlators at fixed CoM time t for
+  s = 0, 2a0, ..., from backward steps of the configuration and copies
+  evolved forward; the third file holds the _gconjg correlators.
 - **33**, MeasureHeavyQuarkoniumCorrelators_Equilibrium (src/main.f90:18-280).
   Arguments: Nx Ny Nz a0 ax ay az smax Seed Beta nefieldinit
   nequilibriumtimesteps kspTol M Re(c1) Im(c1) ... Re(c4) Im(c4)
@@ -41,8 +47,8 @@ Modes (the reference's `program simulation`, src/main.f90:3301-3340):
 precision; 1 precision form).  Progress goes to stdout as in the reference.
 Records follow Fortran's rule that a trailing X edit descriptor transmits
 no characters: values are separated by one blank and no record ends in one.
-The Wilson-line modes (5, 51, 52), the one-t correlator (31) and the
-analysis modes (1, 11, 4) are outside the hot path.
+The Wilson-line modes (5, 51, 52) and the analysis modes (1, 11, 4) are
+outside the hot path.
 """
 from __future__ import annotations
 
@@ -204,6 +210,71 @@ def mode_correlators_equilibrium(args, form=0, device=0):
     _correlators_run(ext, sp, smax, ksp_tol, mass, c, f_corr, f_norm, init, form, device)
 
 
+def mode_correlators_one_t(args, form=0, device=0):
+    """Mode 31, MeasureHeavyQuarkoniumCorrelators_oneT (src/main.f90:523-780):
+    transverse-polarised box initial condition evolved to the CoM time t;
+    for it1 = 1 .. nint(|smax/2|/a0) the configuration steps back to
+    t1 = t - it1 a0 and a copy of it, with a copy of the point source, runs
+    2 it1 coupled steps to t2 = t + it1 a0; the observables at s = 2 it1 a0
+    (and at s = 0 before the loop) go to three files: the correlators, the
+    norms and the _gconjg correlators."""
+    ext = [int(a) for a in args[0:3]]
+    sp = [float(a) for a in args[3:7]]
+    tcom, smax = float(args[7]), float(args[8])
+    seed = int(args[9])
+    qs, amp, coupling = float(args[10]), float(args[11]), float(args[12])
+    ksp_tol = float(args[13])
+    mass = float(args[14])
+    c = [complex(float(args[15 + 2 * k]), float(args[16 + 2 * k])) for k in range(4)]
+    f_corr, f_norm, f_gconjg = args[23], args[24], args[25]
+    t1steps = _nint(abs(smax / 2) / sp[0])
+    nwork = sum(2 * it1 for it1 in range(1, t1steps + 1))
+    lattice.InitModule(ext, sp, device=device)
+    try:
+        nrqcd.InitModule(mass, c, 1.0, ksp_tol, form=form)
+        g1, g2 = GaugeConfiguration(), GaugeConfiguration()
+        g1.TransversePolarisedOccupiedInit_Box(qs, amp, coupling, RandomSeed=seed, identity_links=False)
+        h1, h2 = NRQCDField(), NRQCDField()
+        h1.InitSinglePoint(1, 1)
+        for _ in range(_nint(abs(tcom) / sp[0])):
+            g1.Update(math.copysign(1.0, tcom))
+        with open(f_corr, "w") as fc, open(f_norm, "w") as fn, open(f_gconjg, "w") as fg:
+            fc.write(CORRELATOR_HEADER + "\n")
+            fg.write(CORRELATOR_HEADER + "\n")
+            fn.write(NORM_HEADER + "\n")
+
+            def observables(s, h):
+                fn.write(_line((s, h.GetNorm_Quark(), h.GetNorm_AntiQ()), 16, 9) + "\n")
+                for f, cor in ((fc, h.GetMesoncorrelators()), (fg, h.GetMesoncorrelators_gconjg())):
+                    vals = [s]
+                    for key in ("o1_1s0", "o1_3s1", "o8_1s0", "o8_3s1"):
+                        vals += [cor[key].real, cor[key].imag]
+                    f.write(_line(vals, 16, 9) + "\n")
+            observables(0.0, h1)
+            iwork = 0
+            for it1 in range(1, t1steps + 1):
+                t2steps = 2 * it1
+                h2.Assign(h1)
+                g2.assign(g1)
+                for _ in range(t2steps):
+                    iwork += 1
+                    h2.Update(g2, mass, c, 1.0)
+                    g2.Update(1.0)
+                    # '(F7.3,A1)' of real(iwork)/nwork*100 in default (single) precision
+                    pct = np.float32(iwork) / np.float32(nwork) * np.float32(100)
+                    print(f"{float(pct):7.3f}%", flush=True)
+                observables(sp[0] * t2steps, h2)
+                g1.Update(-1.0)
+        for o in (h1, h2):
+            o.Destructor()
+        for o in (g1, g2):
+            o.Deallocate()
+        nrqcd.FinalizeModule()
+    finally:
+        lattice.FinalizeModule()
+    print(" Simulation completed", flush=True)
+
+
 ZERO_TOL = 1e-12  # GetZeroTol() of the FP64 build, src/tolerances.f90:21-26
 
 
@@ -359,12 +430,14 @@ def main(argv=None):
         mode_energy_gauss(argv[1:], device=device)
     elif mode == 3:
         mode_ts_grid(argv[1:], form=form, device=device)
+    elif mode == 31:
+        mode_correlators_one_t(argv[1:], form=form, device=device)
     elif mode == 32:
         mode_correlators_free(argv[1:], form=form, device=device)
     elif mode == 33:
         mode_correlators_equilibrium(argv[1:], form=form, device=device)
     else:
-        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2, 3, 32 and 33): {mode}")
+        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2, 3, 31, 32 and 33): {mode}")
 
 
 if __name__ == "__main__":

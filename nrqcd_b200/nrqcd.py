@@ -192,6 +192,32 @@ class NRQCDField:
     def GetMesoncorrelator_O8_3S1_ZeroMomentum(self) -> complex:
         return complex(self._correlators()[3])
 
+    def _correlators_gconjg(self):
+        out = np.empty(8)
+        self._call("nrq_heavy_correlators_gconjg", _capi.dptr(out))
+        return out[0::2] + 1j * out[1::2]
+
+    def GetMesoncorrelator_O1_1S0_ZeroMomentum_gconjg(self) -> complex:
+        """src/nrqcd.f90:1728-1761"""
+        return complex(self._correlators_gconjg()[0])
+
+    def GetMesoncorrelator_O1_3S1_ZeroMomentum_gconjg(self) -> complex:
+        """src/nrqcd.f90:1769-1809"""
+        return complex(self._correlators_gconjg()[1])
+
+    def GetMesoncorrelator_O8_1S0_ZeroMomentum_gconjg(self) -> complex:
+        """src/nrqcd.f90:1817-1857"""
+        return complex(self._correlators_gconjg()[2])
+
+    def GetMesoncorrelator_O8_3S1_ZeroMomentum_gconjg(self) -> complex:
+        """src/nrqcd.f90:1865-1905"""
+        return complex(self._correlators_gconjg()[3])
+
+    def GetMesoncorrelators_gconjg(self) -> dict:
+        c = self._correlators_gconjg()
+        return {"o1_1s0": complex(c[0]), "o1_3s1": complex(c[1]), "o8_1s0": complex(c[2]),
+                "o8_3s1": complex(c[3])}
+
     def GetMesoncorrelators(self) -> dict:
         c = self._correlators()
         return {"o1_1s0": complex(c[0]), "o1_3s1": complex(c[1]), "o8_1s0": complex(c[2]),

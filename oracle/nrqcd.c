@@ -437,10 +437,12 @@ static void load_prop(const double *p, int64_t s, cplx M[36]) {
     for (int c = 0; c < 6; ++c) M[r * 6 + c] = q[c * 6 + r];
 }
 
-/* sum_x Tr( i * adag(x) Gam q(x) Gam ) * w over a list of Gamma matrices */
-static void correlator(const oc_lattice *L, const double *q, const double *a, int ngam,
-                       const cplx *gams, double weight_num, double weight_den, int noGam,
-                       double out[2]) {
+/* sum_x Tr( i * adag(x) Gam q(x) Gam ) * w over a list of Gamma matrices;
+   gconjg replaces adag = conjg(transpose(a)) by conjg(a) (the _gconjg
+   variants, src/nrqcd.f90:1728-1905) */
+static void correlator_any(const oc_lattice *L, const double *q, const double *a, int ngam,
+                           const cplx *gams, double weight_num, double weight_den, int noGam, int gconjg,
+                           double out[2]) {
   const int64_t V = oc_volume(L);
   double re = 0, im = 0;
 #pragma omp parallel for reduction(+ : re, im) schedule(static)
@@ -449,7 +451,7 @@ static void correlator(const oc_lattice *L, const double *q, const double *a, in
     load_prop(q, s, Q);
     load_prop(a, s, A);
     for (int i = 0; i < 6; ++i)
-      for (int j = 0; j < 6; ++j) Ad[i * 6 + j] = conj(A[j * 6 + i]);
+      for (int j = 0; j < 6; ++j) Ad[i * 6 + j] = gconjg ? conj(A[i * 6 + j]) : conj(A[j * 6 + i]);
     if (noGam) {
       m6_mul(Ad, Q, T);
       for (int k = 0; k < 36; ++k) C[k] = I * T[k];
@@ -471,11 +473,11 @@ static void correlator(const oc_lattice *L, const double *q, const double *a, in
   out[1] = im;
 }
 
-void oc_meson_o1_1s0(const oc_lattice *L, const double *q, const double *a, double out[2]) {
-  correlator(L, q, a, 0, NULL, 1, 1, 1, out);
+static void meson_o1_1s0(const oc_lattice *L, const double *q, const double *a, int gconjg, double out[2]) {
+  correlator_any(L, q, a, 0, NULL, 1, 1, 1, gconjg, out);
 }
 
-void oc_meson_o1_3s1(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+static void meson_o1_3s1(const oc_lattice *L, const double *q, const double *a, int gconjg, double out[2]) {
   cplx G[3 * 36];
   cplx Id3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
   for (int i = 1; i <= 3; ++i) {
@@ -483,20 +485,20 @@ void oc_meson_o1_3s1(const oc_lattice *L, const double *q, const double *a, doub
     oc_pauli(i, s);
     kron32(Id3, s, G + (i - 1) * 36);
   }
-  correlator(L, q, a, 3, G, 1, 3, 0, out);
+  correlator_any(L, q, a, 3, G, 1, 3, 0, gconjg, out);
 }
 
-void oc_meson_o8_1s0(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+static void meson_o8_1s0(const oc_lattice *L, const double *q, const double *a, int gconjg, double out[2]) {
   cplx G[8 * 36];
   for (int g = 1; g <= 8; ++g) {
     cplx T[9];
     oc_generator(g, (double *)T);
     c2cs(T, G + (g - 1) * 36);
   }
-  correlator(L, q, a, 8, G, 6, 8, 0, out);
+  correlator_any(L, q, a, 8, G, 6, 8, 0, gconjg, out);
 }
 
-void oc_meson_o8_3s1(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+static void meson_o8_3s1(const oc_lattice *L, const double *q, const double *a, int gconjg, double out[2]) {
   cplx G[24 * 36];
   int n = 0;
   for (int i = 1; i <= 3; ++i)
@@ -506,5 +508,28 @@ void oc_meson_o8_3s1(const oc_lattice *L, const double *q, const double *a, doub
       oc_pauli(i, s);
       kron32(T, s, G + (n++) * 36);
     }
-  correlator(L, q, a, 24, G, 6, 24, 0, out);
+  correlator_any(L, q, a, 24, G, 6, 24, 0, gconjg, out);
+}
+
+void oc_meson_o1_1s0(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+  meson_o1_1s0(L, q, a, 0, out);
+}
+void oc_meson_o1_3s1(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+  meson_o1_3s1(L, q, a, 0, out);
+}
+void oc_meson_o8_1s0(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+  meson_o8_1s0(L, q, a, 0, out);
+}
+void oc_meson_o8_3s1(const oc_lattice *L, const double *q, const double *a, double out[2]) {
+  meson_o8_3s1(L, q, a, 0, out);
+}
+
+/* the four _gconjg correlators (src/nrqcd.f90:1728-1905): out[8] = re/im of
+   O1(1S0), O1(3S1), O8(1S0), O8(3S1) with conjg(AntiQProp) in place of its
+   hermitian conjugate */
+void oc_meson_gconjg(const oc_lattice *L, const double *q, const double *a, double out[8]) {
+  meson_o1_1s0(L, q, a, 1, out);
+  meson_o1_3s1(L, q, a, 1, out + 2);
+  meson_o8_1s0(L, q, a, 1, out + 4);
+  meson_o8_3s1(L, q, a, 1, out + 6);
 }

@@ -111,6 +111,8 @@ void oc_meson_o1_1s0(const oc_lattice *L, const double *q, const double *a, doub
 void oc_meson_o1_3s1(const oc_lattice *L, const double *q, const double *a, double out[2]);
 void oc_meson_o8_1s0(const oc_lattice *L, const double *q, const double *a, double out[2]);
 void oc_meson_o8_3s1(const oc_lattice *L, const double *q, const double *a, double out[2]);
+/* the _gconjg correlators (nrqcd.f90:1728-1905); out[8] */
+void oc_meson_gconjg(const oc_lattice *L, const double *q, const double *a, double out[8]);
 
 int oc_num_threads(void);
 

@@ -94,6 +94,7 @@ def lib():
             "oc_meson_o1_3s1": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
             "oc_meson_o8_1s0": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
             "oc_meson_o8_3s1": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
+            "oc_meson_gconjg": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
             "oc_num_threads": (ctypes.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -320,6 +321,14 @@ def meson_correlators(n, q, anti):
         getattr(lib(), "oc_meson_" + name)(ctypes.byref(L), _p(q), _p(anti), _p(r))
         out[name] = complex(r[0], r[1])
     return out
+
+
+def meson_correlators_gconjg(n, q, anti):
+    """The _gconjg correlators (src/nrqcd.f90:1728-1905)."""
+    L = lattice(n, [1, 1, 1, 1])
+    r = np.empty(8)
+    lib().oc_meson_gconjg(ctypes.byref(L), _p(q), _p(anti), _p(r))
+    return {k: complex(r[2 * i], r[2 * i + 1]) for i, k in enumerate(("o1_1s0", "o1_3s1", "o8_1s0", "o8_3s1"))}
 
 
 def num_threads():

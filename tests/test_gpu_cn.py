@@ -106,6 +106,28 @@ def test_correlators_random_fields(oracle):
     assert abs(nq - oracle.heavy_norm(n, q)) < 1e-12 * nq
 
 
+def test_gconjg_correlators_random_fields(oracle):
+    """The _gconjg correlators (src/nrqcd.f90:1728-1905) on random
+    propagators: conj(A) instead of A^+ in every product, so they differ
+    from the plain ones on non-symmetric A."""
+    n = (5, 4, 3)
+    V = 60
+    rng = np.random.default_rng(9)
+    q = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    an = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    with lattice_ctx(n, A):
+        h = NRQCDField()
+        h.upload(q, an)
+        corr = h.GetMesoncorrelators_gconjg()
+        one = h.GetMesoncorrelator_O8_3S1_ZeroMomentum_gconjg()
+        plain = h.GetMesoncorrelators()
+    oc = oracle.meson_correlators_gconjg(n, q, an)
+    for k in oc:
+        assert abs(corr[k] - oc[k]) < 1e-11 * max(1, abs(oc[k])), k
+        assert abs(corr[k] - plain[k]) > 1e-3 * max(1, abs(oc[k])), k
+    assert one == corr["o8_3s1"]
+
+
 def test_forward_backward_returns_initial_propagator(oracle):
     n = (8, 8, 8)
     links, ef = hot(oracle, n, seed=4, Q=2.0)

@@ -1,4 +1,4 @@
-"""GPU runs of the drop-in driver (modes 2, 3 and 32 of the reference's
+"""GPU runs of the drop-in driver (modes 2, 3, 31 and 32 of the reference's
 `program simulation`), checked line by line against the FP64 oracle and the
 reference's output formats."""
 import re
@@ -111,3 +111,44 @@ def test_mode3_ts_grid_matches_oracle(oracle, tmp_path):
             seen += 1
         oracle.gauge_update(n, a, links, ef, 1.0)
     assert seen == 4
+
+
+def test_mode31_one_t_correlators_match_oracle(oracle, tmp_path):
+    """Mode 31 on 6^3: the configuration evolved to t = 0.1, then for
+    s = 2 a0, 4 a0 a backward step of it and a copy evolved forward 2 it1
+    steps; all three files against the oracle."""
+    n, a, M, c = (6, 6, 6), (0.05, 1.0, 1.0, 1.0), 1.0, [1, 1, 1, 1]
+    tcom, smax, seed, qs, amp, coupling = 0.1, 0.2, 5, 0.8, 1.0, 0.5
+    fc, fn, fg = tmp_path / "c.txt", tmp_path / "n.txt", tmp_path / "g.txt"
+    args = ["31", "6", "6", "6", "0.05", "1.0", "1.0", "1.0", str(tcom), str(smax), str(seed), str(qs), str(amp),
+            str(coupling), "1e-12", str(M), "1.0", "0.0", "1.0", "0.0", "1.0", "0.0", "1.0", "0.0",
+            str(fc), str(fn), str(fg)]
+    driver.main(args)
+    corr, norm, gcj = (f.read_text().splitlines() for f in (fc, fn, fg))
+    assert corr[0] == driver.CORRELATOR_HEADER == gcj[0] and norm[0] == driver.NORM_HEADER
+    assert len(corr) == len(norm) == len(gcj) == 4  # s = 0, 0.1, 0.2
+    links, ef = oracle.transverse_box(n, a, qs, amp, coupling, seed, identity_links=False)
+    oracle.gauge_update(n, a, links, ef, 1.0)
+    oracle.gauge_update(n, a, links, ef, 1.0)
+    q0, a0 = oracle.single_point(n, 1), oracle.single_point(n, 1)
+    keys = ("o1_1s0", "o1_3s1", "o8_1s0", "o8_3s1")
+
+    def check(row, s, q, an):
+        assert abs(float(corr[row].split()[0]) - s) < 1e-9
+        for lines, ref in ((corr, oracle.meson_correlators(n, q, an)),
+                           (gcj, oracle.meson_correlators_gconjg(n, q, an))):
+            vals = [float(v) for v in lines[row].split()]
+            for k, key in enumerate(keys):
+                g_ = complex(vals[1 + 2 * k], vals[2 + 2 * k])
+                assert abs(g_ - ref[key]) <= 1e-8 * max(1.0, abs(ref[key])), (row, key)
+        nv = [float(v) for v in norm[row].split()]
+        assert abs(nv[1] - oracle.heavy_norm(n, q)) < 1e-8 and abs(nv[2] - oracle.heavy_norm(n, an)) < 1e-8
+    check(1, 0.0, q0, a0)
+    for it1 in (1, 2):
+        oracle.gauge_update(n, a, links, ef, -1.0)
+        l2, e2 = links.copy(), ef.copy()
+        q, an = q0.copy(), a0.copy()
+        for _ in range(2 * it1):
+            oracle.cn_update(n, a, l2, e2, M, c, 1.0, q, an, tol=1e-14)
+            oracle.gauge_update(n, a, l2, e2, 1.0)
+        check(1 + it1, 0.05 * 2 * it1, q, an)

@@ -94,3 +94,21 @@ def test_equilibrium_init_draw_order_and_projection(oracle):
     links, ef, sw, en, dev = oracle.equilibrium_init(n, a, 10.0, 2, 0, tol=1e-3, seed=5)
     assert np.all(sw > 0) and np.all(dev <= 1e-3) and np.all(en > 0)
     assert abs(oracle.gauss_maxnorm(n, a, links, ef) - dev[-1]) == 0.0
+
+
+def test_gconjg_correlators_oracle(oracle):
+    """The _gconjg correlators (nrqcd.f90:1728-1905) use conj(A) where the
+    plain ones use A^+: equal to the plain ones when every A(x) is
+    symmetric, and O1(1S0) against a numpy restatement otherwise."""
+    n, V = (3, 2, 2), 12
+    rng = np.random.default_rng(3)
+    q = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    a = rng.normal(size=(V, 6, 6)) + 1j * rng.normal(size=(V, 6, 6))
+    sym = a + np.swapaxes(a, 1, 2)
+    p, g = oracle.meson_correlators(n, q, sym), oracle.meson_correlators_gconjg(n, q, sym)
+    for k in p:
+        assert abs(p[k] - g[k]) < 1e-12 * max(1.0, abs(p[k])), k
+    Q, A_ = np.swapaxes(q, 1, 2), np.swapaxes(a, 1, 2)  # [site][row][col]
+    want = np.sum(np.trace(1j * np.conj(A_) @ Q, axis1=1, axis2=2))
+    got = oracle.meson_correlators_gconjg(n, q, a)["o1_1s0"]
+    assert abs(got - want) < 1e-12 * abs(want)
