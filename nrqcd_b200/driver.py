@@ -32,9 +32,10 @@ Modes (the reference's `program simulation`, src/main.f90:3301-3340):
 - **31**, MeasureHeavyQuarkoniumCorrelators_oneT (src/main.f90:523-780).
   Arguments: Nx Ny Nz a0 ax ay az t smax Seed Qs Amplitude Coupling kspTol M
   Re(c1) Im(c1) ... Re(c4) Im(c4) FileMesonCorrelator FileNorm
-  FileMesonCorrelator_gconjg.  Correlators at fixed CoM time t for
-  s = 0, 2a0, ..., from backward steps of the configuration and copies
-  evolved forward; the third file holds the _gconjg correlators.
+  FileMesonCorrelator_gconjg.  Correlators for s = 0, 2a0, 4a0, ... from
+  copies of the configuration evolved forward 2 it1 steps, the
+  configuration stepping back by a0 after each; the third file holds the
+  _gconjg correlators.
 - **33**, MeasureHeavyQuarkoniumCorrelators_Equilibrium (src/main.f90:18-280).
   Arguments: Nx Ny Nz a0 ax ay az smax Seed Beta nefieldinit
   nequilibriumtimesteps kspTol M Re(c1) Im(c1) ... Re(c4) Im(c4)
@@ -212,11 +213,12 @@ def mode_correlators_equilibrium(args, form=0, device=0):
 
 def mode_correlators_one_t(args, form=0, device=0):
     """Mode 31, MeasureHeavyQuarkoniumCorrelators_oneT (src/main.f90:523-780):
-    transverse-polarised box initial condition evolved to the CoM time t;
-    for it1 = 1 .. nint(|smax/2|/a0) the configuration steps back to
-    t1 = t - it1 a0 and a copy of it, with a copy of the point source, runs
-    2 it1 coupled steps to t2 = t + it1 a0; the observables at s = 2 it1 a0
-    (and at s = 0 before the loop) go to three files: the correlators, the
+    transverse-polarised box initial condition evolved to the time t; for
+    it1 = 1 .. nint(|smax/2|/a0) a copy of the configuration (at
+    t1 = t - (it1-1) a0) and of the point source runs 2 it1 coupled steps,
+    its observables are written at s = 2 it1 a0, and the configuration then
+    steps back by a0 (the reference's order, main.f90:601-617).  The
+    observables at s = 0 come first.  Three files: the correlators, the
     norms and the _gconjg correlators."""
     ext = [int(a) for a in args[0:3]]
     sp = [float(a) for a in args[3:7]]

@@ -115,8 +115,9 @@ def test_mode3_ts_grid_matches_oracle(oracle, tmp_path):
 
 def test_mode31_one_t_correlators_match_oracle(oracle, tmp_path):
     """Mode 31 on 6^3: the configuration evolved to t = 0.1, then for
-    s = 2 a0, 4 a0 a backward step of it and a copy evolved forward 2 it1
-    steps; all three files against the oracle."""
+    it1 = 1, 2 a copy of it evolved forward 2 it1 steps (s = 2 it1 a0) and
+    the configuration stepped back once; all three files against the
+    oracle."""
     n, a, M, c = (6, 6, 6), (0.05, 1.0, 1.0, 1.0), 1.0, [1, 1, 1, 1]
     tcom, smax, seed, qs, amp, coupling = 0.1, 0.2, 5, 0.8, 1.0, 0.5
     fc, fn, fg = tmp_path / "c.txt", tmp_path / "n.txt", tmp_path / "g.txt"
@@ -144,11 +145,11 @@ def test_mode31_one_t_correlators_match_oracle(oracle, tmp_path):
         nv = [float(v) for v in norm[row].split()]
         assert abs(nv[1] - oracle.heavy_norm(n, q)) < 1e-8 and abs(nv[2] - oracle.heavy_norm(n, an)) < 1e-8
     check(1, 0.0, q0, a0)
-    for it1 in (1, 2):
-        oracle.gauge_update(n, a, links, ef, -1.0)
+    for it1 in (1, 2):  # the copy first, the backward step at the end of the row (main.f90:601-617)
         l2, e2 = links.copy(), ef.copy()
         q, an = q0.copy(), a0.copy()
         for _ in range(2 * it1):
             oracle.cn_update(n, a, l2, e2, M, c, 1.0, q, an, tol=1e-14)
             oracle.gauge_update(n, a, l2, e2, 1.0)
         check(1 + it1, 0.05 * 2 * it1, q, an)
+        oracle.gauge_update(n, a, links, ef, -1.0)
