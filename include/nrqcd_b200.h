@@ -141,6 +141,20 @@ int nrq_gauge_gauss_project(nrq_gauge *g, double tol, int64_t max_sweeps, int64_
 int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nefieldinit, int64_t nequilibrium,
                                double tol, int64_t seed, int64_t max_sweeps, int64_t *sweeps,
                                double *energies, double *deviations);
+/* CoulombGaugefixing(Tolerance, alpha, MaxIterations) ->
+ * CoulombGaugefixing_Links, src/gaugeconfiguration_su3.f90:2269-2456: Fourier
+ * accelerated steepest descent on the links (the electric field is not
+ * transformed, as in the reference).  *iterations gets the reference's loop
+ * counter after the loop (the iteration whose divergence met tol, or
+ * max_iterations + 1); deviations[k] (max_iterations entries, or NULL) the
+ * maximum |div|_F / 9 checked at iteration k + 1 (the value the reference
+ * prints).                                                                  */
+int nrq_gauge_coulomb_gaugefix(nrq_gauge *g, double tol, double alpha, int64_t max_iterations,
+                               int64_t *iterations, double *deviations);
+/* GetTransverseAACorrelator / GetTransverseEECorrelator, same file
+ * :1825-1972, and GetNorm2Momentum_G (src/lattice.f90:1081-1089): per
+ * momentum site in lattice order, V entries each (any may be NULL).         */
+int nrq_gauge_transverse_correlators(nrq_gauge *g, double *aa, double *ee, double *momenta);
 
 /* ---- heavy-quark field: src/nrqcd.f90:58-117 -------------------------- */
 int nrq_heavy_create(nrq_ctx *ctx, nrq_heavy **h);      /* NRQCDField() (:235-248) */

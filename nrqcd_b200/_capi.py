@@ -76,6 +76,9 @@ SIGNATURES = {
     "nrq_gauge_energy": (ctypes.c_int, [_vp, _dp]),
     "nrq_gauge_gauss": (ctypes.c_int, [_vp, _dp, _dp]),
     "nrq_gauge_gauss_project": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int64, _i64p, _dp]),
+    "nrq_gauge_coulomb_gaugefix": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int64, _i64p,
+                                                  _dp]),
+    "nrq_gauge_transverse_correlators": (ctypes.c_int, [_vp, _dp, _dp, _dp]),
     "nrq_gauge_equilibrium_init": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int64, ctypes.c_int64,
                                                   ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _i64p, _dp,
                                                   _dp]),

@@ -743,6 +743,142 @@ extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nef
   return NRQ_OK;
 }
 
+// ---------------------------------------------------------------- gluon distribution
+namespace {
+// cuFFT Z2Z plan over `batch` complex planes of the lattice (x fastest)
+bool lattice_fft_plan(nrq_ctx *ctx, int batch, cufftHandle *plan) {
+  const nrq::Lat L = ctx->lat;
+  int dims[3] = {(int)L.nz, (int)L.ny, (int)L.nx};
+  if (cufftPlanMany(plan, 3, dims, nullptr, 1, (int)L.V, nullptr, 1, (int)L.V, CUFFT_Z2Z, batch) != CUFFT_SUCCESS)
+    return false;
+  cufftSetStream(*plan, ctx->stream);
+  return true;
+}
+
+// FindMaxNorm2Momentum (lattice:422-465): |p|^2 is a sum over directions of
+// (2 sin(pi n_i / N_i) / a_i)^2, so its maximum is the sum of the maxima
+double max_norm2_momentum(const nrq_ctx *ctx) {
+  const double pi = std::acos(-1.0);
+  double s = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    double m = 0.0;
+    for (int64_t n = 0; n < ctx->n[i]; ++n) {
+      const double v = 2.0 * std::sin(pi * (double)n / (double)ctx->n[i]) / ctx->a[i + 1];
+      m = std::max(m, v * v);
+    }
+    s += m;
+  }
+  return std::sqrt(s);
+}
+}  // namespace
+
+extern "C" int nrq_gauge_coulomb_gaugefix(nrq_gauge *g, double tol, double alpha, int64_t max_iterations,
+                                          int64_t *iterations, double *deviations) {
+  if (!g || max_iterations < 0) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  const nrq::Lat L = ctx->lat;
+  const int64_t V = L.V;
+  int rc = set_device(ctx);
+  if (!rc) rc = gauge_sync64(g);
+  if (rc) return rc;
+  const unsigned nb_ = (unsigned)nblk(V, 128);
+  if ((rc = ensure_red(ctx, nb_))) return rc;
+  double2 *D = nullptr;
+  cufftHandle plan = 0;
+  bool planned = false;
+  auto cleanup = [&]() {
+    if (planned) cufftDestroy(plan);
+    if (D) cudaFree(D);
+  };
+  if (cudaMalloc(&D, sizeof(double2) * 9 * V) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->last_error = "CoulombGaugefixing: device allocation failed";
+    return NRQ_ERR_OOM;
+  }
+  if (!(planned = lattice_fft_plan(ctx, 9, &plan))) {
+    cleanup();
+    ctx->last_error = "CoulombGaugefixing: cufftPlanMany failed";
+    return NRQ_ERR_CUDA;
+  }
+  const double pmax = max_norm2_momentum(ctx);
+  // x2p scale a1 a2 a3 times p2x scale 1/Volume is 1/V; alpha folded in
+  const double scale = alpha / (double)V;
+  int64_t it;
+  for (it = 1; it <= max_iterations; ++it) {
+    nrq::k_cg_divergence<<<nb_, 128, 0, ctx->stream>>>(L, g->U, D, ctx->d_red);
+    if ((rc = check_launch(ctx, "k_cg_divergence")) || (rc = reduce_to_host(ctx, nb_, 1, 1u))) break;
+    const double dev = ctx->h_res[0];
+    if (deviations) deviations[it - 1] = dev;
+    if (!(dev > tol)) break;
+    bool ok = cufftExecZ2Z(plan, (cufftDoubleComplex *)D, (cufftDoubleComplex *)D, CUFFT_FORWARD) == CUFFT_SUCCESS;
+    if (ok) nrq::k_cg_accelerate<<<nb_, 128, 0, ctx->stream>>>(L, D, pmax, scale);
+    ok = ok && cufftExecZ2Z(plan, (cufftDoubleComplex *)D, (cufftDoubleComplex *)D, CUFFT_INVERSE) == CUFFT_SUCCESS;
+    if (!ok) {
+      ctx->last_error = "CoulombGaugefixing: cuFFT failure";
+      rc = NRQ_ERR_CUDA;
+      break;
+    }
+    nrq::k_cg_expah<<<nb_, 128, 0, ctx->stream>>>(V, D);
+    nrq::k_cg_transform<<<nb_, 128, 0, ctx->stream>>>(L, g->U, D);
+    if ((rc = check_launch(ctx, "Coulomb gauge transformation"))) break;
+  }
+  cleanup();
+  if (iterations) *iterations = it;
+  if (rc) return rc;
+  return gauge_written64(g);
+}
+
+extern "C" int nrq_gauge_transverse_correlators(nrq_gauge *g, double *aa, double *ee, double *momenta) {
+  if (!g) return NRQ_ERR_BAD_ARG;
+  nrq_ctx *ctx = g->ctx;
+  const nrq::Lat L = ctx->lat;
+  const int64_t V = L.V;
+  int rc = set_device(ctx);
+  if (!rc) rc = gauge_sync64(g);
+  if (rc) return rc;
+  double2 *F = nullptr;
+  double *out = nullptr;
+  cufftHandle plan = 0;
+  bool planned = false;
+  auto cleanup = [&]() {
+    if (planned) cufftDestroy(plan);
+    if (F) cudaFree(F);
+    if (out) cudaFree(out);
+  };
+  if (cudaMalloc(&F, sizeof(double2) * 48 * V) != cudaSuccess || cudaMalloc(&out, sizeof(double) * 3 * V) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    ctx->last_error = "transverse correlators: device allocation failed";
+    return NRQ_ERR_OOM;
+  }
+  if (!(planned = lattice_fft_plan(ctx, 48, &plan))) {
+    cleanup();
+    ctx->last_error = "transverse correlators: cufftPlanMany failed";
+    return NRQ_ERR_CUDA;
+  }
+  const unsigned nb_ = (unsigned)nblk(V, 128);
+  const double fwd = ctx->a[1] * ctx->a[2] * ctx->a[3];
+  nrq::k_gluon_fields<<<nb_, 128, 0, ctx->stream>>>(L, g->U, g->E, F);
+  bool ok = cudaGetLastError() == cudaSuccess &&
+            cufftExecZ2Z(plan, (cufftDoubleComplex *)F, (cufftDoubleComplex *)F, CUFFT_FORWARD) == CUFFT_SUCCESS;
+  if (ok) {
+    nrq::k_transverse_corr<<<nb_, 128, 0, ctx->stream>>>(L, F, fwd, (double)V * fwd, out);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  double *dst[3] = {aa, ee, momenta};
+  for (int k = 0; k < 3 && ok; ++k)
+    if (dst[k])
+      ok = cudaMemcpyAsync(dst[k], out + (int64_t)k * V, sizeof(double) * V, cudaMemcpyDeviceToHost, ctx->stream) ==
+           cudaSuccess;
+  ok = ok && cudaStreamSynchronize(ctx->stream) == cudaSuccess;
+  cleanup();
+  if (!ok) {
+    ctx->last_error = "transverse correlators: kernel, cuFFT or copy failure";
+    return NRQ_ERR_CUDA;
+  }
+  return NRQ_OK;
+}
+
 // ====================================================================== heavy field
 extern "C" int nrq_heavy_create(nrq_ctx *ctx, nrq_heavy **out) {
   if (!ctx || !out) return NRQ_ERR_BAD_ARG;

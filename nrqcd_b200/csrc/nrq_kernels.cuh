@@ -46,6 +46,17 @@ __global__ void k_gauss_g(Lat L, const double2 *__restrict__ U, const double *__
 __global__ void k_gauss_sweep(Lat L, const double2 *__restrict__ U, const double2 *__restrict__ G,
                               double *__restrict__ E, const GaussProjState *st, double kdt);
 
+// ---------------- gluon.cu
+__global__ void k_cg_divergence(Lat L, const double2 *__restrict__ U, double2 *__restrict__ D,
+                                double *__restrict__ partials);
+__global__ void k_cg_accelerate(Lat L, double2 *__restrict__ D, double pmax, double scale);
+__global__ void k_cg_expah(int64_t V, double2 *__restrict__ D);
+__global__ void k_cg_transform(Lat L, double2 *__restrict__ U, const double2 *__restrict__ G);
+__global__ void k_gluon_fields(Lat L, const double2 *__restrict__ U, const double *__restrict__ E,
+                               double2 *__restrict__ F);
+__global__ void k_transverse_corr(Lat L, const double2 *__restrict__ F, double fwd, double volume,
+                                  double *__restrict__ out);
+
 // ---------------- cn.cu
 // Per-species, per-term complex coefficients of the assembled CN operator:
 //   out = in + sum_t alpha_t G_t in      (t = kinetic, magnetic, Darwin, spin-orbit)

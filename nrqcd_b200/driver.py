@@ -4,6 +4,17 @@
 
 Modes (the reference's `program simulation`, src/main.f90:3301-3340):
 
+- **1**, MeasureGluondistribution (src/main.f90:3020-3296).  Arguments: Nx Ny
+  Nz a0 ax ay az CoMTime Seed Qs Amplitude Coupling GaugefixingMaxIterations
+  GaugefixingTolerance GaugefixingCoefficient FileGluondist.  Box initial
+  condition evolved to CoMTime, Coulomb gauge fixing of a copy, and per
+  momentum site |p| and sqrt(AA EE) of the transverse correlators,
+  '(2(SP,E13.6,1X))'.
+- **11**, MeasureGluondistribution_Equilibrium (src/main.f90:2725-3012): the
+  same output from the thermal EquilibriumInit.  Arguments: Nx Ny Nz a0 ax
+  ay az TimeRange Seed Beta nefieldinit nequilibriumtimesteps
+  TimeBetweenGluonMeasurements GaugefixingMaxIterations GaugefixingTolerance
+  GaugefixingCoefficient FileGluondist MeasureEnergy [EnergyFilename].
 - **2**, MeasureEnergyAndGaussLawDeviation (src/main.f90:2572-2718).
   Arguments: Nx Ny Nz a0 ax ay az CoMTime TimeRange Seed Qs Amplitude Coupling.
   Transverse-polarised box initial condition, then TimeSteps = ceil(TimeRange/a0)
@@ -48,7 +59,7 @@ Modes (the reference's `program simulation`, src/main.f90:3301-3340):
 precision; 1 precision form).  Progress goes to stdout as in the reference.
 Records follow Fortran's rule that a trailing X edit descriptor transmits
 no characters: values are separated by one blank and no record ends in one.
-The Wilson-line modes (5, 51, 52) and the analysis modes (1, 11, 4) are
+The Wilson-line modes (5, 51, 52) and the spectrum analysis (mode 4) are
 outside the hot path.
 """
 from __future__ import annotations
@@ -277,6 +288,79 @@ def mode_correlators_one_t(args, form=0, device=0):
     print(" Simulation completed", flush=True)
 
 
+def write_gluondist(g, filename, max_iterations, tolerance, alpha):
+    """PrintObservables of modes 1 and 11 (src/main.f90:3052-3170,
+    2775-2895): a Coulomb-gauge-fixed copy of the configuration, its
+    transverse AA and EE correlators, and per momentum site (lattice order)
+    |p| and sqrt(AA EE), '(2(SP,E13.6,1X))'."""
+    fixed = GaugeConfiguration()
+    fixed.assign(g)
+    fixed.CoulombGaugefixing(Tolerance_=tolerance, alpha_=alpha, MaxIterations_=max_iterations)
+    aa, ee, mom = fixed.GetTransverseCorrelators()
+    fixed.Deallocate()
+    dist = np.sqrt(aa * ee)
+    with open(filename, "w") as f:
+        for p_, n_ in zip(mom, dist):
+            f.write(_line((float(p_), float(n_)), 13, 6) + "\n")
+
+
+def mode_gluondist(args, device=0):
+    """Mode 1, MeasureGluondistribution (src/main.f90:3020-3296).  Arguments:
+    Nx Ny Nz a0 ax ay az CoMTime Seed Qs Amplitude Coupling
+    GaugefixingMaxIterations GaugefixingTolerance GaugefixingCoefficient
+    FileGluondist.  Transverse-polarised box initial condition,
+    ceiling(|CoMTime|/a0) leapfrog steps of sign(CoMTime), then the gluon
+    distribution."""
+    ext = [int(a) for a in args[0:3]]
+    sp = [float(a) for a in args[3:7]]
+    comtime = float(args[7])
+    seed = int(args[8])
+    qs, amp, coupling = float(args[9]), float(args[10]), float(args[11])
+    gf_maxit, gf_tol, gf_alpha = int(args[12]), float(args[13]), float(args[14])
+    f_out = args[15]
+    steps = math.ceil(abs(comtime) / sp[0])
+    lattice.InitModule(ext, sp, device=device)
+    try:
+        g = GaugeConfiguration()
+        g.TransversePolarisedOccupiedInit_Box(qs, amp, coupling, RandomSeed=seed, identity_links=False)
+        for _ in range(steps):
+            g.Update(math.copysign(1.0, comtime))
+        write_gluondist(g, f_out, gf_maxit, gf_tol, gf_alpha)
+        g.Deallocate()
+    finally:
+        lattice.FinalizeModule()
+    print(" Simulation completed", flush=True)
+
+
+def mode_gluondist_equilibrium(args, device=0):
+    """Mode 11, MeasureGluondistribution_Equilibrium (src/main.f90:2725-3012).
+    Arguments: Nx Ny Nz a0 ax ay az TimeRange Seed Beta nefieldinit
+    nequilibriumtimesteps TimeBetweenGluonMeasurements
+    GaugefixingMaxIterations GaugefixingTolerance GaugefixingCoefficient
+    FileGluondist MeasureEnergy [EnergyFilename].  EquilibriumInit, then the
+    gluon distribution (TimeRange and TimeBetweenGluonMeasurements are read
+    but unused, as in the reference)."""
+    ext = [int(a) for a in args[0:3]]
+    sp = [float(a) for a in args[3:7]]
+    seed = int(args[8])
+    beta = float(args[9])
+    nefieldinit, nequilibrium = int(args[10]), int(args[11])
+    gf_maxit, gf_tol, gf_alpha = int(args[13]), float(args[14]), float(args[15])
+    f_out = args[16]
+    measure = int(args[17]) != 0
+    energy_file = args[18] if measure else None
+    lattice.InitModule(ext, sp, device=device)
+    try:
+        g = GaugeConfiguration()
+        g.EquilibriumInit(beta, nefieldinit, nequilibrium, MeasureEnergy=measure, filename=energy_file,
+                          RandomSeed=seed)
+        write_gluondist(g, f_out, gf_maxit, gf_tol, gf_alpha)
+        g.Deallocate()
+    finally:
+        lattice.FinalizeModule()
+    print(" Simulation completed", flush=True)
+
+
 ZERO_TOL = 1e-12  # GetZeroTol() of the FP64 build, src/tolerances.f90:21-26
 
 
@@ -428,7 +512,11 @@ def main(argv=None):
     if not argv:
         raise SystemExit(__doc__)
     mode = int(argv[0])
-    if mode == 2:
+    if mode == 1:
+        mode_gluondist(argv[1:], device=device)
+    elif mode == 11:
+        mode_gluondist_equilibrium(argv[1:], device=device)
+    elif mode == 2:
         mode_energy_gauss(argv[1:], device=device)
     elif mode == 3:
         mode_ts_grid(argv[1:], form=form, device=device)
@@ -439,7 +527,7 @@ def main(argv=None):
     elif mode == 33:
         mode_correlators_equilibrium(argv[1:], form=form, device=device)
     else:
-        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 2, 3, 31, 32 and 33): {mode}")
+        raise SystemExit(f"Invalid simulation mode selected (this driver runs modes 1, 11, 2, 3, 31, 32 and 33): {mode}")
 
 
 if __name__ == "__main__":

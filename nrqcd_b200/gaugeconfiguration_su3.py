@@ -36,13 +36,16 @@ def _list_real8(x: float) -> str:
 
 
 def list_directed(items) -> str:
-    """One record of gfortran list-directed output: integers as I12, reals as
-    _list_real8, character items as themselves after one blank."""
+    """One record of gfortran list-directed output: default integers as I12,
+    numpy int64 (integer(int64)) as I21, reals as _list_real8, character
+    items as themselves after one blank."""
     out = []
     for v in items:
         if isinstance(v, str):
             out.append(" " + v)
-        elif isinstance(v, (int, np.integer)):
+        elif isinstance(v, np.int64):  # integer(int64): I21
+            out.append(f"{int(v):21d}")
+        elif isinstance(v, (int, np.integer)):  # default integer: I12
             out.append(f"{int(v):12d}")
         else:
             out.append(_list_real8(float(v)))
@@ -141,6 +144,39 @@ class GaugeConfiguration:
                     print(list_directed((r + 1, float(en[r]))), flush=True)
                 print(list_directed(("G[U,E]=", float(dev[r]))), flush=True)
         return sweeps[:n], en[:n], dev[:n]
+
+    def CoulombGaugefixing(self, Tolerance_=1e-8, alpha_=0.08, MaxIterations_=100, verbose=True):
+        """CoulombGaugefixing (src/gaugeconfiguration_su3.f90:2269-2456):
+        Fourier-accelerated gauge fixing of the links to Coulomb gauge.
+        Prints, as the reference does, the divergence checked at every
+        iteration and the final loop counter.  Returns (loop counter,
+        deviations)."""
+        n = int(MaxIterations_)
+        dev = np.full(max(n, 1), np.nan)
+        it = ctypes.c_int64()
+        self._call("nrq_gauge_coulomb_gaugefix", float(Tolerance_), float(alpha_), n, ctypes.byref(it),
+                   _capi.dptr(dev))
+        checked = dev[:min(it.value, n)]
+        if verbose:
+            for d in checked:
+                print(list_directed((float(d),)), flush=True)
+            print(list_directed((np.int64(it.value), "iterations in Coulomb gauge fixing performed")), flush=True)
+        return it.value, checked
+
+    def GetTransverseCorrelators(self):
+        """(AA, EE, |p|) per momentum site in lattice order
+        (src/gaugeconfiguration_su3.f90:1825-1972, src/lattice.f90:1081-1089)."""
+        aa, ee, mom = np.empty(self.V), np.empty(self.V), np.empty(self.V)
+        self._call("nrq_gauge_transverse_correlators", _capi.dptr(aa), _capi.dptr(ee), _capi.dptr(mom))
+        return aa, ee, mom
+
+    def GetTransverseAACorrelator(self):
+        """src/gaugeconfiguration_su3.f90:1825-1859"""
+        return self.GetTransverseCorrelators()[0]
+
+    def GetTransverseEECorrelator(self):
+        """src/gaugeconfiguration_su3.f90:1867-1905"""
+        return self.GetTransverseCorrelators()[1]
 
     def GaussProjection(self, tolerance=1e-3, max_sweeps=0):
         """The Gauss projection loop of EquilibriumInit

@@ -114,6 +114,13 @@ void oc_meson_o8_3s1(const oc_lattice *L, const double *q, const double *a, doub
 /* the _gconjg correlators (nrqcd.f90:1728-1905); out[8] */
 void oc_meson_gconjg(const oc_lattice *L, const double *q, const double *a, double out[8]);
 
+/* ---- gluon distribution (src/gaugeconfiguration_su3.f90:1825-1972, 2269-2478) */
+double  oc_norm2_momentum(const oc_lattice *L, int64_t site);
+int64_t oc_gauge_coulomb_gaugefix(const oc_lattice *L, double *links, double tol, double alpha,
+                                  int64_t max_iterations, double *deviations);
+void    oc_gauge_transverse_correlators(const oc_lattice *L, const double *links, const double *efield,
+                                        double *aa, double *ee, double *momenta);
+
 int oc_num_threads(void);
 
 #ifdef __cplusplus

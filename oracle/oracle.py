@@ -95,6 +95,10 @@ def lib():
             "oc_meson_o8_1s0": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
             "oc_meson_o8_3s1": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
             "oc_meson_gconjg": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp]),
+            "oc_norm2_momentum": (ctypes.c_double, [ctypes.POINTER(Lattice), ctypes.c_int64]),
+            "oc_gauge_coulomb_gaugefix": (ctypes.c_int64, [ctypes.POINTER(Lattice), _dp, ctypes.c_double,
+                                                           ctypes.c_double, ctypes.c_int64, _dp]),
+            "oc_gauge_transverse_correlators": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp, _dp, _dp]),
             "oc_num_threads": (ctypes.c_int, []),
         }
         for name, (res, args) in sig.items():
@@ -329,6 +333,24 @@ def meson_correlators_gconjg(n, q, anti):
     r = np.empty(8)
     lib().oc_meson_gconjg(ctypes.byref(L), _p(q), _p(anti), _p(r))
     return {k: complex(r[2 * i], r[2 * i + 1]) for i, k in enumerate(("o1_1s0", "o1_3s1", "o8_1s0", "o8_3s1"))}
+
+
+def coulomb_gaugefix(n, a, links, tol=1e-8, alpha=0.08, max_iterations=100):
+    """CoulombGaugefixing on the links in place (gauge:2269-2456); returns the
+    reference's loop counter and the deviation checked at each iteration."""
+    L = lattice(n, a)
+    dev = np.full(max(max_iterations, 1), np.nan)
+    it = lib().oc_gauge_coulomb_gaugefix(ctypes.byref(L), _p(links), tol, alpha, max_iterations, _p(dev))
+    return it, dev[:min(it, max_iterations)]
+
+
+def transverse_correlators(n, a, links, efield):
+    """(AA, EE, |p|) per momentum site (gauge:1825-1972, lattice:1081-1198)."""
+    L = lattice(n, a)
+    V = volume(n)
+    aa, ee, mom = np.empty(V), np.empty(V), np.empty(V)
+    lib().oc_gauge_transverse_correlators(ctypes.byref(L), _p(links), _p(efield), _p(aa), _p(ee), _p(mom))
+    return aa, ee, mom
 
 
 def num_threads():

@@ -112,3 +112,26 @@ def test_gconjg_correlators_oracle(oracle):
     want = np.sum(np.trace(1j * np.conj(A_) @ Q, axis1=1, axis2=2))
     got = oracle.meson_correlators_gconjg(n, q, a)["o1_1s0"]
     assert abs(got - want) < 1e-12 * abs(want)
+
+
+def test_coulomb_gaugefix_oracle_properties(oracle):
+    """Coulomb gauge fixing (gauge:2269-2478) leaves the plaquette energy
+    unchanged (a gauge transformation, U(3) as in the reference), meets the
+    tolerance, and the transverse correlators vanish on cold links and zero
+    field and at p = 0."""
+    n, a = (6, 6, 6), (0.05, 1.0, 1.0, 1.0)
+    links, ef = oracle.transverse_box(n, a, 1.0, 1.0, 0.5, 3, identity_links=False)
+    for _ in range(5):
+        oracle.gauge_update(n, a, links, ef, 1.0)
+    zero = np.zeros_like(ef)
+    e0 = oracle.energy(n, a, links, zero)
+    it, dev = oracle.coulomb_gaugefix(n, a, links, tol=1e-8)
+    assert 1 < it <= 100 and dev[-1] <= 1e-8 and np.all(np.diff(dev[:3]) < 0)
+    assert abs(oracle.energy(n, a, links, zero) - e0) < 1e-10 * abs(e0)
+    it2, dev2 = oracle.coulomb_gaugefix(n, a, links, tol=1e-8)
+    assert it2 == 1 and dev2[0] <= 1e-8
+    aa, ee, mom = oracle.transverse_correlators(n, a, links, ef)
+    assert aa[0] == 0 and ee[0] == 0 and mom[0] == 0 and np.all(aa >= -1e-15) and np.all(ee >= -1e-15)
+    cl, ce = oracle.cold(n, a)
+    aa, ee, _ = oracle.transverse_correlators(n, a, cl, ce)
+    assert np.abs(aa).max() < 1e-28 and np.abs(ee).max() == 0
