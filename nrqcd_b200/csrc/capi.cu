@@ -467,7 +467,23 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
         double u1 = rng.next(), u2 = rng.next();
         R[(size_t)(pol * 8 + a) * V + s] = make_double2(std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2), 0.0);
       }
+  // backward-derivative momentum per direction and coordinate (lattice:963-979):
+  // component (re, im) and modulus, in the host's arithmetic
+  std::vector<double> mtab;
+  {
+    const double pi = std::acos(-1.0);
+    for (int i = 0; i < 3; ++i)
+      for (int64_t n = 0; n < ctx->n[i]; ++n) {
+        const double ang = pi * (double)n / (double)ctx->n[i];
+        const double mag = 2.0 * std::sin(ang) / ctx->a[i + 1];
+        const double re = mag * std::cos(-ang), im = mag * std::sin(-ang);
+        mtab.push_back(re);
+        mtab.push_back(im);
+        mtab.push_back(std::hypot(re, im));
+      }
+  }
   double2 *dR = nullptr, *dA = nullptr, *dEf = nullptr;
+  double *dM = nullptr;
   cufftHandle plan16 = 0, plan24 = 0;
   bool p16 = false, p24 = false;
   auto cleanup = [&]() {
@@ -476,10 +492,12 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
     if (dR) cudaFree(dR);
     if (dA) cudaFree(dA);
     if (dEf) cudaFree(dEf);
+    if (dM) cudaFree(dM);
   };
   if (cudaMalloc(&dR, sizeof(double2) * 16 * V) != cudaSuccess ||
       cudaMalloc(&dA, sizeof(double2) * 24 * V) != cudaSuccess ||
-      cudaMalloc(&dEf, sizeof(double2) * 24 * V) != cudaSuccess) {
+      cudaMalloc(&dEf, sizeof(double2) * 24 * V) != cudaSuccess ||
+      cudaMalloc(&dM, sizeof(double) * mtab.size()) != cudaSuccess) {
     cudaGetLastError();
     cleanup();
     ctx->last_error = "transverse_box_init: device allocation failed";
@@ -500,7 +518,9 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
   p24 = true;
   cufftSetStream(plan16, ctx->stream);
   cufftSetStream(plan24, ctx->stream);
-  if (cudaMemcpyAsync(dR, R.data(), sizeof(double2) * 16 * V, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+  if (cudaMemcpyAsync(dR, R.data(), sizeof(double2) * 16 * V, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+      cudaMemcpyAsync(dM, mtab.data(), sizeof(double) * mtab.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+          cudaSuccess) {
     cleanup();
     return NRQ_ERR_CUDA;
   }
@@ -508,7 +528,7 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
   const double fwd_scale = ctx->a[1] * ctx->a[2] * ctx->a[3];
   const double volume = (double)V * fwd_scale;
   if (ok) {
-    nrq::k_ic_pspace<<<nblk(V, 128), 128, 0, ctx->stream>>>(L, dR, fwd_scale, Q, n0, coupling, dA, dEf);
+    nrq::k_ic_pspace<<<nblk(V, 128), 128, 0, ctx->stream>>>(L, dR, dM, fwd_scale, Q, n0, coupling, dA, dEf);
     ok = cudaGetLastError() == cudaSuccess;
   }
   ok = ok && cufftExecZ2Z(plan24, (cufftDoubleComplex *)dA, (cufftDoubleComplex *)dA, CUFFT_INVERSE) == CUFFT_SUCCESS;

@@ -454,23 +454,26 @@ __global__ void k_reduce_final(const double *__restrict__ partials, int64_t nblk
 // p-space construction of TransversePolarisedOccupiedInit (gauge:1349-1381)
 // R: 16 complex planes (pol*8 + a) holding x2p of the real normals (unscaled
 // FFT); writes A, Ef: 24 complex planes (i*8 + a) in p-space.
-__global__ void k_ic_pspace(Lat L, const double2 *__restrict__ R, double fwd_scale, double Q,
-                            double n0, double g, double2 *__restrict__ A, double2 *__restrict__ Ef) {
+// mtab: per direction i and coordinate n (offsets 0, nx, nx + ny) the
+// backward-derivative momentum component (re, im) and its modulus, computed
+// on the host with the reference's expression (lattice:963-979), so that the
+// box edge |p| < Q is decided as on the host also where |p| equals Q up to
+// rounding; |p| sums the squared moduli without fused multiply-adds.
+__global__ void k_ic_pspace(Lat L, const double2 *__restrict__ R, const double *__restrict__ mtab,
+                            double fwd_scale, double Q, double n0, double g, double2 *__restrict__ A,
+                            double2 *__restrict__ Ef) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= L.V) return;
   const int64_t V = L.V;
   int64_t pos[3];
   coords(L, s, pos[0], pos[1], pos[2]);
-  const int64_t ext[3] = {L.nx, L.ny, L.nz};
-  const double pi = 3.141592653589793;
+  const int64_t off[3] = {0, L.nx, L.nx + L.ny};
   cplx p[3];
   double pn2 = 0.0;
   for (int i = 0; i < 3; ++i) {
-    double ang = pi * (double)pos[i] / (double)ext[i];
-    double mag = 2.0 * sin(ang) / L.a[i];
-    p[i] = {mag * cos(-ang), mag * sin(-ang)};
-    double ab = hypot(p[i].re, p[i].im);
-    pn2 += ab * ab;
+    const double *m = mtab + 3 * (off[i] + pos[i]);
+    p[i] = {m[0], m[1]};
+    pn2 = __dadd_rn(pn2, __dmul_rn(m[2], m[2]));
   }
   double pn = sqrt(pn2);
   cplx eps1[3], eps2[3];

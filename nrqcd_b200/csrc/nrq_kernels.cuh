@@ -24,8 +24,9 @@ __global__ void k_energy(Lat L, const double2 *__restrict__ U, const double *__r
 __global__ void k_gauss(Lat L, const double2 *__restrict__ U, const double *__restrict__ E, double *partials);
 __global__ void k_reduce_final(const double *__restrict__ partials, int64_t nblk, int nq, unsigned maxmask,
                                double *out);
-__global__ void k_ic_pspace(Lat L, const double2 *__restrict__ R, double fwd_scale, double Q, double n0,
-                            double g, double2 *__restrict__ A, double2 *__restrict__ Ef);
+__global__ void k_ic_pspace(Lat L, const double2 *__restrict__ R, const double *__restrict__ mtab,
+                            double fwd_scale, double Q, double n0, double g, double2 *__restrict__ A,
+                            double2 *__restrict__ Ef);
 __global__ void k_ic_write(Lat L, const double2 *__restrict__ A, const double2 *__restrict__ Ef,
                            double inv_volume, int identity_links, double2 *__restrict__ U,
                            double *__restrict__ E);

@@ -96,6 +96,21 @@ def test_initial_condition_matches_oracle(oracle, identity_links):
     assert np.abs(lg - lo).max() < 1e-13
 
 
+@pytest.mark.parametrize("n,Q", [((6, 6, 6), 1.0), ((16, 16, 16), 2.0), ((12, 6, 8), 1.0)])
+def test_initial_condition_box_edge_on_a_lattice_momentum(oracle, n, Q):
+    """A saturation scale equal to lattice momenta (2 sin(pi/6) = 1 on 6 and
+    12 sites, 2 sin(pi/2) = 2 on 16): the device takes the momentum
+    components and moduli from a host table in the reference's arithmetic,
+    so the box edge |p| < Q falls as on the host."""
+    lo, eo = oracle.transverse_box(n, A, Q, 1.0, 0.5, 3, identity_links=False)
+    with lattice_ctx(n, A):
+        g = GaugeConfiguration()
+        g.TransversePolarisedOccupiedInit_Box(Q, 1.0, 0.5, RandomSeed=3, identity_links=False)
+        lg, eg = g.download()
+    assert np.abs(eg - eo).max() < 1e-13 * max(1.0, np.abs(eo).max())
+    assert np.abs(lg - lo).max() < 1e-13
+
+
 def test_cold_init():
     n = (4, 4, 4)
     with lattice_ctx(n, A):
