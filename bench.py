@@ -57,6 +57,8 @@ def parse():
     p.add_argument("--forms-sizes", type=int, nargs="+", default=list(FORMS_SIZES))
     p.add_argument("--no-drift", action="store_true")
     p.add_argument("--no-thermal", action="store_true")
+    p.add_argument("--no-gluon", action="store_true")
+    p.add_argument("--only-gluon", action="store_true", help="print only the gluon-distribution JSON")
     p.add_argument("--only-thermal", action="store_true", help="print only the thermal initial-condition JSON")
     p.add_argument("--stencil", default="timed", choices=["timed", "register", "tma", "tensor"],
                    help="FP64 stencil of the headline step (default: the solver's timed choice)")
@@ -239,6 +241,77 @@ def measure_thermal_ic(L, seed=1, cpu=True, cpu_sweeps=4, max_sweeps=200000):
         out["cpu_baseline"] = {"value": cps, "unit": "site-sweeps/s", "cores": oc.num_threads(), "kind": "port",
                                "sample": f"{done} projection sweeps of the oracle at {L}^3 ({dt:.2f} s)"}
         out["speedup_vs_cpu"] = out["site_sweeps_per_s"] / cps
+    return out
+
+
+# ------------------------------------------------------------------ gluon distribution
+# algorithmic bytes per site of one Coulomb gauge-fixing iteration outside the
+# FFTs: divergence (links 432 read, D 144 written), acceleration (D read and
+# written), exponential (D read and written), transformation (D 144, links
+# 432 read and written)
+GF_BYTES_SITE_ITER = (432 + 144) + 288 + 288 + (144 + 864)
+
+
+def measure_gluon_distribution(L, cpu=True, steps=10):
+    """Coulomb gauge fixing (tolerance 1e-8, alpha 0.08, at most 100
+    iterations) and the transverse AA/EE correlators of an L^3 box initial
+    condition (aQ = 0.5, n0 = 1, seed 1, random links) after `steps` leapfrog
+    steps, timed with CUDA events on the context's stream; the CPU leg times
+    two iterations and the correlators of the oracle on the same links."""
+    import torch
+    from nrqcd_b200 import GaugeConfiguration, _capi, lattice
+    ctx = lattice.context()
+    stream = torch.cuda.ExternalStream(_capi.load().nrq_cuda_stream(ctx))
+    g = GaugeConfiguration()
+    g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=1, identity_links=False)
+    for _ in range(steps):
+        g.Update(1.0)
+    links, ef = g.download()
+    w = GaugeConfiguration()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    w.assign(g)
+    w.CoulombGaugefixing(1e-8, 0.08, 100, verbose=False)  # warm-up (cuFFT plans, allocations)
+    w.GetTransverseCorrelators()
+    w.assign(g)
+    (it, dev), gf_ms = timed(lambda: w.CoulombGaugefixing(1e-8, 0.08, 100, verbose=False))
+    _, corr_ms = timed(w.GetTransverseCorrelators)
+    del w, g
+    V = L ** 3
+    transforms = int(min(it, 100)) - (1 if it <= 100 else 0)
+    out = {"config": {"lattice": [L, L, L], "initial_condition": "box aQ=0.5 n0=1 seed 1, random links",
+                      "leapfrog_steps": steps, "tolerance": 1e-8, "alpha": 0.08, "max_iterations": 100},
+           "gaugefix_loop_counter": int(it), "gauge_transformations": transforms,
+           "final_divergence": float(dev[-1]), "gaugefix_ms": gf_ms,
+           "gaugefix_ms_per_transformation": gf_ms / max(1, transforms),
+           "gaugefix_nonfft_bytes_per_site_iteration": GF_BYTES_SITE_ITER,
+           "correlators_ms": corr_ms,
+           "note": "per gauge-fixing iteration: divergence + its max, 9 forward and 9 inverse cuFFT Z2Z, "
+                   "acceleration, exponential, transformation; correlators: algebra coordinates (Jacobi "
+                   "ArgLogU), 48 forward cuFFT Z2Z, projection"}
+    if cpu:
+        from oracle import oracle as oc
+        n = (L, L, L)
+        l2 = links.copy()
+        t0 = time.perf_counter()
+        oc.coulomb_gaugefix(n, A, l2, tol=0.0, alpha=0.08, max_iterations=2)
+        t_gf = (time.perf_counter() - t0) / 2
+        t0 = time.perf_counter()
+        oc.transverse_correlators(n, A, links, ef)
+        t_corr = time.perf_counter() - t0
+        out["cpu_baseline"] = {"gaugefix_ms_per_transformation": t_gf * 1e3, "correlators_ms": t_corr * 1e3,
+                               "cores": oc.num_threads(), "kind": "port",
+                               "sample": f"2 gauge-fixing iterations and one correlator pass of the oracle at {L}^3"}
+        out["speedup_vs_cpu"] = {"gaugefix": t_gf * 1e3 / out["gaugefix_ms_per_transformation"],
+                                 "correlators": t_corr * 1e3 / corr_ms}
     return out
 
 
@@ -631,6 +704,14 @@ def main():
     h.InitSinglePoint(1, 1)
     lib = _capi.load()
     stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(ctx))
+    if args.only_gluon:
+        out = measure_gluon_distribution(L, cpu=not args.no_cpu_baseline)
+        if rank == 0:
+            print(json.dumps({"gluon_distribution": out}), flush=True)
+        del h, g
+        nrqcd.FinalizeModule()
+        lattice.FinalizeModule()
+        return
     if args.only_thermal:
         out = measure_thermal_ic(L, cpu=not args.no_cpu_baseline)
         if rank == 0:
@@ -733,6 +814,10 @@ def main():
     if not args.no_thermal and world == 1:
         thermal = measure_thermal_ic(L, cpu=not args.no_cpu_baseline)
 
+    gluon = None
+    if not args.no_gluon and world == 1:
+        gluon = measure_gluon_distribution(L, cpu=not args.no_cpu_baseline)
+
     forms = None
     if not args.no_forms and world == 1:
         forms = measure_all_forms(max(2, min(args.steps, 5)), sizes=tuple(args.forms_sizes))
@@ -780,6 +865,7 @@ def main():
             "batching_ensemble": ensemble,
             "precision_drift": drift,
             "thermal_initial_condition": thermal,
+            "gluon_distribution": gluon,
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_sample(min(L, 64))
