@@ -52,6 +52,11 @@
 #ifndef NRQ_MV4_SPW
 #define NRQ_MV4_SPW 1
 #endif
+// K = 12 of a block product as one m16n8k8 and one m16n8k4 MMA (1), or as
+// three m16n8k4 MMAs (0)
+#ifndef NRQ_MV4_K8
+#define NRQ_MV4_K8 1
+#endif
 
 namespace nrq {
 
@@ -161,6 +166,15 @@ __device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, doubl
       : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
       : "d"(a0), "d"(a1), "d"(b0));
 }
+// D(16x8) += A(16x8) B(8x8): the two k4 steps j, j+1 in one instruction
+// (a0, a1 the A fragment of step j, a2, a3 that of step j+1; b0, b1 the B
+// fragments of the two steps)
+__device__ __forceinline__ void dmma8(double (&d)[4], double a0, double a1, double a2, double a3, double b0,
+                                      double b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
 // sign flip by an XOR on the high word (m = 0 or the sign bit)
 __device__ __forceinline__ double flip(double v, unsigned m) {
   return __hiloint2double(__double2hiint(v) ^ (int)m, __double2loint(v));
@@ -246,6 +260,18 @@ __device__ __forceinline__ void nb_fast(double (&acc)[N][2][4], const uint32_t (
     nb_fast_load<BWD, SA, 1>(a0[1][i], a1[1][i], b0[1][i], wa0[i], wa1[i], sb[i]);
     nb_fast_load<BWD, SA, 2>(a0[2][i], a1[2][i], b0[2][i], wa0[i], wa1[i], sb[i]);
   }
+#if NRQ_MV4_K8
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp)
+      dmma8(acc[i][sp], flip(a0[0][i][sp], m0), flip(a1[0][i][sp], m1), flip(a0[1][i][sp], m0),
+            flip(a1[1][i][sp], m1), b0[0][i][sp], b0[1][i][sp]);
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) dmma(acc[i][sp], flip(a0[2][i][sp], m0), flip(a1[2][i][sp], m1), b0[2][i][sp]);
+#else
 #pragma unroll
   for (int j = 0; j < 3; ++j)
 #pragma unroll
@@ -253,6 +279,7 @@ __device__ __forceinline__ void nb_fast(double (&acc)[N][2][4], const uint32_t (
 #pragma unroll
       for (int sp = 0; sp < 2; ++sp)
         dmma(acc[i][sp], flip(a0[j][i][sp], m0), flip(a1[j][i][sp], m1), b0[j][i][sp]);
+#endif
 }
 
 // results of a mode stored from the epilogue tiles (RES: r, rh and p are the
@@ -443,9 +470,14 @@ __global__ void __maxnreg__(mv4::kMaxReg)
         else
           b0[j] = __ldg((const double *)(sg + (int64_t)(sp * 36 + pl) * V) + part);
       }
+      const unsigned g0 = bwd ? mb0 : mf0, g1 = bwd ? mb1 : mf1;
+#if NRQ_MV4_K8
+      dmma8(ac[sp], flip(a0[0], g0), flip(a1[0], g1), flip(a0[1], g0), flip(a1[1], g1), b0[0], b0[1]);
+      dmma(ac[sp], flip(a0[2], g0), flip(a1[2], g1), b0[2]);
+#else
 #pragma unroll
-      for (int j = 0; j < 3; ++j)
-        dmma(ac[sp], flip(a0[j], bwd ? mb0 : mf0), flip(a1[j], bwd ? mb1 : mf1), b0[j]);
+      for (int j = 0; j < 3; ++j) dmma(ac[sp], flip(a0[j], g0), flip(a1[j], g1), b0[j]);
+#endif
     }
   };
   // one neighbour (direction I, forward or backward) of the warp's sites:
@@ -562,13 +594,22 @@ __global__ void __maxnreg__(mv4::kMaxReg)
             b0[0] = lds_at<0>(sbs);
             b0[1] = lds_at<2 * kTileS * 16>(sbs);
             b0[2] = lds_at<4 * kTileS * 16>(sbs);
+            double da0[3], da1[3];
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
               cplx cd = ad * dv[j] + bv[j] * am;
               if (j == c) cd = cd + dg;
               if (s != h) cd = cplx{0.0, 0.0};
-              dmma(acc[i][sp], part ? -cd.im : cd.re, part ? cd.re : cd.im, b0[j]);
+              da0[j] = part ? -cd.im : cd.re;
+              da1[j] = part ? cd.re : cd.im;
             }
+#if NRQ_MV4_K8
+            dmma8(acc[i][sp], da0[0], da1[0], da0[1], da1[1], b0[0], b0[1]);
+            dmma(acc[i][sp], da0[2], da1[2], b0[2]);
+#else
+#pragma unroll
+            for (int j = 0; j < 3; ++j) dmma(acc[i][sp], da0[j], da1[j], b0[j]);
+#endif
           }
         }
         // +x: block at x (forward), spinor at x+1; -x: block and spinor at x-1
