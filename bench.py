@@ -801,6 +801,17 @@ def main():
                "path": "nrq_gauge_upload + nrq_heavy_upload + nrq_heavy_update_cn + nrq_gauge_update + "
                        "nrq_heavy_download + nrq_gauge_download, pinned host buffers"}
 
+    # the host-synchronised loops of the gluon observables and the thermal
+    # initial condition run first, before the ensemble's and the forms' state
+    # fills the device
+    gluon = None
+    if not args.no_gluon and world == 1:
+        gluon = measure_gluon_distribution(L, cpu=not args.no_cpu_baseline)
+
+    thermal = None
+    if not args.no_thermal and world == 1:
+        thermal = measure_thermal_ic(L, cpu=not args.no_cpu_baseline)
+
     ensemble = None
     if not args.no_ensemble and world == 1:
         ensemble = measure_ensemble(max(2, min(args.steps, 3)), 2,
@@ -809,14 +820,6 @@ def main():
     drift = None
     if not args.no_drift and world == 1:
         drift = [measure_precision_drift(L, n0, 20) for n0 in (0.5, 1.0, 2.0)]
-
-    thermal = None
-    if not args.no_thermal and world == 1:
-        thermal = measure_thermal_ic(L, cpu=not args.no_cpu_baseline)
-
-    gluon = None
-    if not args.no_gluon and world == 1:
-        gluon = measure_gluon_distribution(L, cpu=not args.no_cpu_baseline)
 
     forms = None
     if not args.no_forms and world == 1:

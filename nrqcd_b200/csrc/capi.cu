@@ -294,6 +294,9 @@ extern "C" int nrq_finalize(nrq_ctx *ctx) {
   if (ctx->h_res) cudaFreeHost(ctx->h_res);
   if (ctx->d_stage) cudaFree(ctx->d_stage);
   if (ctx->d_proj) cudaFree(ctx->d_proj);
+  if (ctx->fft9_ok) cufftDestroy((cufftHandle)ctx->fft9);
+  if (ctx->fft48_ok) cufftDestroy((cufftHandle)ctx->fft48);
+  if (ctx->d_gluon) cudaFree(ctx->d_gluon);
   for (auto &r : ctx->prof_recs) {
     cudaEventDestroy(r.a);
     cudaEventDestroy(r.b);
@@ -765,14 +768,34 @@ extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nef
 
 // ---------------------------------------------------------------- gluon distribution
 namespace {
-// cuFFT Z2Z plan over `batch` complex planes of the lattice (x fastest)
+// cuFFT Z2Z plan over `batch` (9 or 48) complex planes of the lattice (x
+// fastest), created once per context
 bool lattice_fft_plan(nrq_ctx *ctx, int batch, cufftHandle *plan) {
-  const nrq::Lat L = ctx->lat;
-  int dims[3] = {(int)L.nz, (int)L.ny, (int)L.nx};
-  if (cufftPlanMany(plan, 3, dims, nullptr, 1, (int)L.V, nullptr, 1, (int)L.V, CUFFT_Z2Z, batch) != CUFFT_SUCCESS)
-    return false;
+  int *h = batch == 9 ? &ctx->fft9 : &ctx->fft48;
+  bool *ok = batch == 9 ? &ctx->fft9_ok : &ctx->fft48_ok;
+  if (!*ok) {
+    const nrq::Lat L = ctx->lat;
+    int dims[3] = {(int)L.nz, (int)L.ny, (int)L.nx};
+    cufftHandle p = 0;
+    if (cufftPlanMany(&p, 3, dims, nullptr, 1, (int)L.V, nullptr, 1, (int)L.V, CUFFT_Z2Z, batch) != CUFFT_SUCCESS)
+      return false;
+    *h = (int)p;
+    *ok = true;
+  }
+  *plan = (cufftHandle)*h;
   cufftSetStream(*plan, ctx->stream);
   return true;
+}
+
+// the gluon observables' device buffer (grown on demand, kept)
+int ensure_gluon(nrq_ctx *ctx, size_t bytes) {
+  if (ctx->gluon_bytes >= bytes) return NRQ_OK;
+  if (ctx->d_gluon) cudaFree(ctx->d_gluon);
+  ctx->d_gluon = nullptr;
+  ctx->gluon_bytes = 0;
+  NRQ_CUDA_TRY(ctx, cudaMalloc(&ctx->d_gluon, bytes));
+  ctx->gluon_bytes = bytes;
+  return NRQ_OK;
 }
 
 // FindMaxNorm2Momentum (lattice:422-465): |p|^2 is a sum over directions of
@@ -803,20 +826,10 @@ extern "C" int nrq_gauge_coulomb_gaugefix(nrq_gauge *g, double tol, double alpha
   if (rc) return rc;
   const unsigned nb_ = (unsigned)nblk(V, 128);
   if ((rc = ensure_red(ctx, nb_))) return rc;
-  double2 *D = nullptr;
+  if ((rc = ensure_gluon(ctx, sizeof(double2) * 9 * V))) return rc;
+  double2 *D = (double2 *)ctx->d_gluon;
   cufftHandle plan = 0;
-  bool planned = false;
-  auto cleanup = [&]() {
-    if (planned) cufftDestroy(plan);
-    if (D) cudaFree(D);
-  };
-  if (cudaMalloc(&D, sizeof(double2) * 9 * V) != cudaSuccess) {
-    cudaGetLastError();
-    ctx->last_error = "CoulombGaugefixing: device allocation failed";
-    return NRQ_ERR_OOM;
-  }
-  if (!(planned = lattice_fft_plan(ctx, 9, &plan))) {
-    cleanup();
+  if (!lattice_fft_plan(ctx, 9, &plan)) {
     ctx->last_error = "CoulombGaugefixing: cufftPlanMany failed";
     return NRQ_ERR_CUDA;
   }
@@ -842,7 +855,6 @@ extern "C" int nrq_gauge_coulomb_gaugefix(nrq_gauge *g, double tol, double alpha
     nrq::k_cg_transform<<<nb_, 128, 0, ctx->stream>>>(L, g->U, D);
     if ((rc = check_launch(ctx, "Coulomb gauge transformation"))) break;
   }
-  cleanup();
   if (iterations) *iterations = it;
   if (rc) return rc;
   return gauge_written64(g);
@@ -856,23 +868,11 @@ extern "C" int nrq_gauge_transverse_correlators(nrq_gauge *g, double *aa, double
   int rc = set_device(ctx);
   if (!rc) rc = gauge_sync64(g);
   if (rc) return rc;
-  double2 *F = nullptr;
-  double *out = nullptr;
+  if ((rc = ensure_gluon(ctx, sizeof(double2) * 48 * V + sizeof(double) * 3 * V))) return rc;
+  double2 *F = (double2 *)ctx->d_gluon;
+  double *out = (double *)(F + 48 * V);
   cufftHandle plan = 0;
-  bool planned = false;
-  auto cleanup = [&]() {
-    if (planned) cufftDestroy(plan);
-    if (F) cudaFree(F);
-    if (out) cudaFree(out);
-  };
-  if (cudaMalloc(&F, sizeof(double2) * 48 * V) != cudaSuccess || cudaMalloc(&out, sizeof(double) * 3 * V) != cudaSuccess) {
-    cudaGetLastError();
-    cleanup();
-    ctx->last_error = "transverse correlators: device allocation failed";
-    return NRQ_ERR_OOM;
-  }
-  if (!(planned = lattice_fft_plan(ctx, 48, &plan))) {
-    cleanup();
+  if (!lattice_fft_plan(ctx, 48, &plan)) {
     ctx->last_error = "transverse correlators: cufftPlanMany failed";
     return NRQ_ERR_CUDA;
   }
@@ -891,7 +891,6 @@ extern "C" int nrq_gauge_transverse_correlators(nrq_gauge *g, double *aa, double
       ok = cudaMemcpyAsync(dst[k], out + (int64_t)k * V, sizeof(double) * V, cudaMemcpyDeviceToHost, ctx->stream) ==
            cudaSuccess;
   ok = ok && cudaStreamSynchronize(ctx->stream) == cudaSuccess;
-  cleanup();
   if (!ok) {
     ctx->last_error = "transverse correlators: kernel, cuFFT or copy failure";
     return NRQ_ERR_CUDA;

@@ -25,6 +25,13 @@ struct nrq_ctx {
   size_t stage_bytes = 0;
   // state of a Gauss projection (nrq::GaussProjState), allocated on first use
   void *d_proj = nullptr;
+  // gluon observables: cuFFT plans over 9 and 48 complex planes and their
+  // device buffer, created on first use and kept (as the reference keeps its
+  // FFT descriptor, src/xpfft.f90:129-139); cufftHandle is an int
+  int fft9 = 0, fft48 = 0;
+  bool fft9_ok = false, fft48_ok = false;
+  void *d_gluon = nullptr;
+  size_t gluon_bytes = 0;
   std::string last_error;
   int sm_count = 148;
   // opt-in per-class kernel timing (events recorded on `stream`)
