@@ -201,11 +201,6 @@ int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[3]);
 /* Force a stencil (NRQ_STENCIL_*) or restore the timed choice (-1).
  * NRQ_ERR_BAD_ARG if the stencil cannot describe this lattice.            */
 int nrq_cn_set_stencil(nrq_cn *cn, int stencil);
-/* FP32 Chebyshev step of the precision forms (forms 1 and 2; no reference
- * counterpart): staged = 1 (default) stages the spinor operand in shared
- * memory by TMA where the lattice allows it (even V), 0 keeps the
- * register-tiled step.  Both give the same results.                       */
-int nrq_cn_set_fp32_stencil(nrq_cn *cn, int staged);
 /* NRQCDField%Update(GaugeConf, Mass, WilsonCoeffs, StepWidth) =
  * Update_CrankNicholson, src/nrqcd.f90:1053-1168: quark (+M, c) and
  * antiquark (-M, conj c); per column RHS = A psi, solve A^H psi' = RHS with

@@ -1105,12 +1105,6 @@ extern "C" int nrq_cn_set_stencil(nrq_cn *cn, int stencil) {
   return NRQ_OK;
 }
 
-extern "C" int nrq_cn_set_fp32_stencil(nrq_cn *cn, int staged) {
-  if (!cn || staged < 0 || staged > 1) return NRQ_ERR_BAD_ARG;
-  cn->fp32_staged = staged;
-  return NRQ_OK;
-}
-
 extern "C" int nrq_cn_finalize(nrq_cn *cn) {
   if (!cn) return NRQ_ERR_NOT_INITIALISED;
   cudaSetDevice(cn->ctx->device);
@@ -1488,7 +1482,7 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     for (int k = 0; k < m; ++k) {
       ProfScope ps(ctx, 0, (double)V * (576.0 * 6 + 756.0));
       nrq::launch_cheb32(k == 0, L, CH, cn->U32, cn->D32, cn->B32, cn->DE32, dcur, dnext, cn->r32, cn->e32, coef[k],
-                         scal_err(cn->scal), cn->fp32_staged != 0, st);
+                         st);
       std::swap(dcur, dnext);
     }
     inner += m;

@@ -22,9 +22,7 @@
 #include <algorithm>
 #include <type_traits>
 
-#include "../../include/nrqcd_b200.h"
 #include "nrq_kernels.cuh"
-#include "stage.cuh"
 
 namespace nrq {
 
@@ -347,213 +345,6 @@ __global__ void __launch_bounds__(192, 2) k_cheb32(Lat L, CnCoef C, const float2
   cheb32_tile<FIRST, 1>(L, C, U, Dsum, Bsum, DE, d, dn, r, e, K, blockIdx.x);
 }
 
-// ------------------------------------------------------------------ TMA-staged FP32 Chebyshev step
-// The same step with the spinor operand staged in shared memory: per block
-// (32 sites, 6 warps = species x colour row) and per phase (the site itself,
-// then the 6 neighbours) one 2D TMA copy brings the 72 planes x 34 sites
-// around the block's neighbours (start rounded down to an even site, so the
-// copy starts on a 16-byte boundary) into one of two buffers, the next
-// phase's copy in flight while this phase is computed.  The three warps of a
-// species read each spinor value from shared memory instead of loading it
-// three times; a lane whose neighbour lies outside the tile (periodic wraps)
-// loads it from global memory.  Requires V even (the plane stride of the
-// tensor map is a multiple of 16 bytes).  Mbarrier waits are bounded: on
-// expiry *err = NRQ_ERR_TIMEOUT and the block skips the remaining work, the
-// issuing thread waiting (bounded) for its copies in flight before exit.
-namespace ch32 {
-constexpr int kBox = 34;                                 // sites per tile
-constexpr uint32_t kTileBytes = 72u * kBox * 8u;          // 19,584
-constexpr int kPhases = 7;                               // site, +x, -x, +y, -y, +z, -z
-}  // namespace ch32
-
-template <bool FIRST>
-__global__ void __launch_bounds__(192, 2) k_cheb32t(Lat L, CnCoef C, const float2 *__restrict__ U,
-                                                    const float2 *__restrict__ Dsum, const float *__restrict__ Bsum,
-                                                    const float2 *__restrict__ DE, const __grid_constant__ CUtensorMap mapD,
-                                                    const float2 *__restrict__ D, float2 *__restrict__ Dn,
-                                                    float2 *__restrict__ R, float2 *__restrict__ Ev, ChebCoef K,
-                                                    int *err) {
-  using namespace ch32;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  // tile buffers on a 128-byte boundary (the launch adds 128 bytes of slack)
-  unsigned char *const base =
-      smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  unsigned char *tile[2] = {base, base + kTileBytes};
-  __shared__ __align__(8) uint64_t bar[2];
-  __shared__ int tstart[kPhases];
-  __shared__ int dead_s;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sp = warp / 3, c = warp % 3;
-  const int64_t V = L.V;
-  const int64_t x0b = (int64_t)blockIdx.x * 32;
-  const int64_t x0 = x0b + lane;
-  const bool active = x0 < V;
-  const int64_t x = active ? x0 : 0;
-  const int64_t pb = (int64_t)(sp * 36) * V;
-  // neighbour of this lane's site and its phase index (0 = the site)
-  auto nbr = [&](int ph) -> int64_t {
-    if (ph == 0) return x;
-    const int I = (ph - 1) >> 1;
-    return nb(L, x, I, ((ph - 1) & 1) ? -1 : +1);
-  };
-  if (threadIdx.x == 0) {
-    dead_s = 0;
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-  }
-  if (threadIdx.x < kPhases) {
-    // tile start: the neighbour of the block's middle site (clamped to the
-    // lattice) minus 17, rounded down to an even site; the tile then holds
-    // the neighbours of every lane whose neighbour lies in the same row run
-    const int ph = threadIdx.x;
-    const int64_t mid = min(x0b + 16, V - 1);
-    const int64_t y = ph == 0 ? mid : nb(L, mid, (ph - 1) >> 1, ((ph - 1) & 1) ? -1 : +1);
-    tstart[ph] = (int)((y - 17) & ~(int64_t)1);
-  }
-  __syncthreads();
-  int issued = 0;  // thread 0: copies issued
-  auto issue = [&](int ph) {
-    mbar_expect_tx(&bar[ph & 1], kTileBytes);
-    tma_2d(tile[ph & 1], &mapD, tstart[ph], 0, &bar[ph & 1]);
-    issued = ph + 1;
-  };
-  if (threadIdx.x == 0) {
-    issue(0);
-    issue(1);
-  }
-  bool dead = false;
-  auto wait_phase = [&](int ph) {
-    if (!dead && !mbar_wait(&bar[ph & 1], (uint32_t)((ph >> 1) & 1))) {
-      dead = true;
-      atomicExch(err, NRQ_ERR_TIMEOUT);
-      dead_s = 1;
-    }
-  };
-  // the lane's spinor value of column col, row r of its species at neighbour y
-  auto spin = [&](int ph, int64_t y, int col, int r) -> cf {
-    const int64_t off = y - tstart[ph];
-    const int pl = sp * 36 + col * 6 + r;
-    if (off >= 0 && off < kBox) {
-      const float2 v = *reinterpret_cast<const float2 *>(tile[ph & 1] + ((uint32_t)pl * kBox + (uint32_t)off) * 8u);
-      return {v.x, v.y};
-    }
-    return ldf(D + (int64_t)pl * V + y);
-  };
-  const cf ak = tof(C.kin[sp]), am = tof(C.mag[sp]), ad = tof(C.dar[sp]), aso = tof(C.so[sp]);
-  cf acc[6][2];
-  // ---- phase 0: the site-diagonal term
-  wait_phase(0);
-  {
-    cf Cd[3];
-#pragma unroll
-    for (int cp = 0; cp < 3; ++cp) {
-      cf dv = ldf(Dsum + (int64_t)(cp * 3 + c) * V + x);
-      float bv = __ldg(Bsum + (int64_t)(cp * 3 + c) * V + x);
-      Cd[cp] = ad * dv + bv * am;
-    }
-    Cd[c] = Cd[c] + (float)C.dkin * ak + cf{1.f, 0.f};
-#pragma unroll
-    for (int col = 0; col < 6; ++col)
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        cf a_ = Cd[0] * spin(0, x, col, s);
-        cmacf(a_, Cd[1], spin(0, x, col, 2 + s));
-        cmacf(a_, Cd[2], spin(0, x, col, 4 + s));
-        acc[col][s] = a_;
-      }
-  }
-  const cf cs0 = timesi(aso), cs1 = -timesi(aso);
-  auto neighbour = [&](auto Ic, auto DIRc) {
-    constexpr int I = decltype(Ic)::value, DIR = decltype(DIRc)::value;
-    constexpr int K0 = (I + 2) % 3, K1 = (I + 1) % 3;
-    constexpr int ph = 1 + 2 * I + DIR;
-    const int64_t y = nbr(ph);
-    const int64_t ms = DIR == 0 ? x : y;
-    const float2 *Up = U + (int64_t)(I * 9) * V + ms;
-    const float2 *D0 = DE + (int64_t)((I * 2 + 0) * 9) * V + ms;
-    const float2 *D1 = DE + (int64_t)((I * 2 + 1) * 9) * V + ms;
-    const cf ck = (-0.5f * (float)C.inva2[I]) * ak;
-    const cf s0 = DIR == 0 ? cs0 : -cs0, s1 = DIR == 0 ? cs1 : -cs1;
-    cf Wm[2][3][2];
-#pragma unroll
-    for (int cp = 0; cp < 3; ++cp) {
-      const int e = DIR == 0 ? (cp * 3 + c) : (c * 3 + cp);
-      cf u = ldf(Up + (int64_t)e * V), d0 = ldf(D0 + (int64_t)e * V), d1 = ldf(D1 + (int64_t)e * V);
-      if (DIR == 1) {
-        u = conjf_(u);
-        d0 = conjf_(d0);
-        d1 = conjf_(d1);
-      }
-      const cf ku = ck * u, e0 = s0 * d0, e1 = s1 * d1;
-#pragma unroll
-      for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          cf v = (s == t) ? ku : cf{0.f, 0.f};
-          v = v + sigf<K0>(s, t, e0);
-          v = v + sigf<K1>(s, t, e1);
-          Wm[s][cp][t] = v;
-        }
-    }
-    wait_phase(ph);
-#pragma unroll
-    for (int col = 0; col < 6; ++col) {
-      cf w[6];
-#pragma unroll
-      for (int r = 0; r < 6; ++r) w[r] = spin(ph, y, col, r);
-#pragma unroll
-      for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int cp = 0; cp < 3; ++cp) {
-          cmacf(acc[col][s], Wm[s][cp][0], w[2 * cp]);
-          cmacf(acc[col][s], Wm[s][cp][1], w[2 * cp + 1]);
-        }
-    }
-  };
-  // after phase ph is consumed by every warp, its buffer takes phase ph + 2
-  auto release = [&](int ph) {
-    __syncthreads();
-    if (threadIdx.x == 0 && ph + 2 < kPhases && !dead_s) {
-      fence_proxy_async_smem();
-      issue(ph + 2);
-    }
-  };
-  using I0 = std::integral_constant<int, 0>;
-  using I1 = std::integral_constant<int, 1>;
-  using I2 = std::integral_constant<int, 2>;
-  release(0);
-  neighbour(I0{}, I0{});
-  release(1);
-  neighbour(I0{}, I1{});
-  release(2);
-  neighbour(I1{}, I0{});
-  release(3);
-  neighbour(I1{}, I1{});
-  release(4);
-  neighbour(I2{}, I0{});
-  release(5);
-  neighbour(I2{}, I1{});
-  // copies in flight (only after an expired wait): wait, bounded, for the
-  // last copy issued into each buffer before the block exits
-  if (threadIdx.x == 0 && dead_s) {
-    for (int ph = max(0, issued - 2); ph < issued; ++ph)
-      if (!mbar_wait(&bar[ph & 1], (uint32_t)((ph >> 1) & 1))) break;
-  }
-  if (!active || dead) return;
-  const cf c1 = tof(K.c1[sp]), c2 = tof(K.c2[sp]);
-#pragma unroll
-  for (int col = 0; col < 6; ++col)
-#pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      const int64_t o = pb + (int64_t)(col * 6 + 2 * c + s) * V + x;
-      const cf d = ldf(D + o);
-      const cf r = ldf(R + o) - acc[col][s];
-      stf(R + o, r);
-      stf(Ev + o, FIRST ? d : ldf(Ev + o) + d);
-      stf(Dn + o, c1 * d + c2 * r);
-    }
-}
-
 // ------------------------------------------------------------------ batched
 // Step `step` of the inner Chebyshev solve for every field of a batch in one
 // launch.  The table holds the fields grouped by mass in tiles of NF fields;
@@ -666,20 +457,8 @@ void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, cons
 }
 void launch_cheb32(bool first, Lat L, const CnCoef &C, const float2 *U, const float2 *Dsum, const float *Bsum,
                    const float2 *DE, const float2 *D, float2 *Dn, float2 *R, float2 *E, const ChebCoef &K,
-                   int *err, bool staged, cudaStream_t st) {
+                   cudaStream_t st) {
   const unsigned nb_ = (unsigned)((L.V + 31) / 32);
-  // the TMA-staged step for even V (16-byte plane stride) within 32-bit
-  // site indices; the register-tiled step otherwise
-  CUtensorMap mapD;
-  if (staged && err && L.V % 2 == 0 && L.V >= 64 && L.V < 0x7fffffffLL &&
-      stage::encode(&mapD, D, (uint64_t)L.V, 72, ch32::kBox, 72)) {
-    const size_t sm = 2 * ch32::kTileBytes + 128;
-    if (first)
-      k_cheb32t<true><<<nb_, 192, sm, st>>>(L, C, U, Dsum, Bsum, DE, mapD, D, Dn, R, E, K, err);
-    else
-      k_cheb32t<false><<<nb_, 192, sm, st>>>(L, C, U, Dsum, Bsum, DE, mapD, D, Dn, R, E, K, err);
-    return;
-  }
   if (first)
     k_cheb32<true><<<nb_, 192, 0, st>>>(L, C, U, Dsum, Bsum, DE, D, Dn, R, E, K);
   else

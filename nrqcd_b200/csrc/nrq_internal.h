@@ -143,9 +143,6 @@ struct nrq_cn {
   bool tma_ok = false;
   bool stencil_tuned = false;
   double tune_ms[3] = {-1.0, -1.0, -1.0};
-  // FP32 Chebyshev step of the precision forms: TMA-staged where the lattice
-  // allows (1, default) or register-tiled (0)
-  int fp32_staged = 1;
   // tensor-core stencil: forward 6x6 blocks (6 per site: direction x
   // species, 36 complex each) built for the coefficients w_coef from the
   // current gauge field (w_valid cleared by every preparation)

@@ -183,7 +183,7 @@ void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, cons
                       const double2 *DE, double *partials, double *out, cudaStream_t st);
 void launch_cheb32(bool first, Lat L, const CnCoef &C, const float2 *U, const float2 *Dsum, const float *Bsum,
                    const float2 *DE, const float2 *D, float2 *Dn, float2 *R, float2 *E, const ChebCoef &K,
-                   int *err, bool staged, cudaStream_t st);
+                   cudaStream_t st);
 void launch_add_e(int64_t n, double2 *X, const float2 *E, cudaStream_t st);
 void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st);
 void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);

@@ -80,13 +80,6 @@ def SetStencil(stencil=None):
                 f"Error in {modulename}: stencil")
 
 
-def SetFP32Stencil(staged=True):
-    """FP32 Chebyshev step of the precision forms: staged in shared memory by
-    TMA (default, even lattices) or register-tiled; the results are equal."""
-    _capi.check(_capi.load().nrq_cn_set_fp32_stencil(solver_handle(), int(bool(staged))), lattice.context(),
-                f"Error in {modulename}: FP32 stencil")
-
-
 def StencilInfo():
     """(stencil in use, per-launch ms of each stencil timed on the first
     update; -1 where not timed)."""

@@ -137,32 +137,3 @@ def test_precision_form_drift_against_fp64_oracle(oracle, n0):
     assert abs(en - e_ref) <= 1e-5 * max(abs(e_ref), 1e-12)
     assert np.abs(gq - q).max() < 1e-6 and np.abs(ga - an).max() < 1e-6
     assert abs(nq - 1) < 1e-9 and abs(na - 1) < 1e-9
-
-
-@pytest.mark.parametrize("n", [(8, 8, 8), (32, 32, 32), (34, 6, 4)])
-def test_staged_chebyshev_step_equals_register_tiled(oracle, n):
-    """The TMA-staged FP32 Chebyshev step (even lattices) reads the same
-    spinor values from shared memory that the register-tiled step loads and
-    applies the same arithmetic: every propagator bit and every step count
-    agree (8^3: blocks span rows, most neighbours from global memory; 32^3:
-    row-aligned tiles; 34 x 6 x 4: tiles crossing rows)."""
-    from nrqcd_b200 import nrqcd
-    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 7, identity_links=False)
-    M, c = 1.0, [1, 1, 1, 1]
-    out = []
-    for staged in (True, False):
-        with lattice_ctx(n, A, cn=(M, c, 1.0, 1e-10, 10000, FORM_PRECISION)):
-            nrqcd.SetFP32Stencil(staged)
-            g = GaugeConfiguration()
-            g.upload(links, ef)
-            h = NRQCDField()
-            h.InitSinglePoint(1, 1)
-            stats = []
-            for _ in range(3):
-                st = h.Update(g, M, c, 1.0)
-                assert st["converged"] == 1
-                stats.append((st["iterations"], st["matvecs"]))
-            q, a = h.download()
-            out.append((q, a, stats))
-    assert out[0][2] == out[1][2]
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
