@@ -109,5 +109,8 @@ class Lattice:
 def _resolve(lat):
     """(ctx, V, is_open) of a standalone Lattice, or of the module context."""
     if lat is None:
-        return context(), GetLatticeSize(), IsModuleInitialised
+        # the object belongs to this module context: once it is finalised (or
+        # replaced by a new InitModule), the object's handle is stale
+        c = context()
+        return c, GetLatticeSize(), (lambda: _ctx is c)
     return lat.ctx, lat.V, lambda: lat.is_open

@@ -59,3 +59,23 @@ def test_module_guards_without_device():
     if not gpu_available():
         with pytest.raises(NrqcdError):
             nrqcd.InitModule(1.0, [1, 1, 1, 1], 1.0, 1e-12)
+
+
+def test_objects_outliving_their_module_context_are_not_destroyed_through_a_new_one():
+    """A gauge or heavy object still referenced after lattice.FinalizeModule
+    belongs to the finalised context: its handle must not be passed to the
+    library once another module context is open (the open check compares the
+    context itself, not 'some module context is open')."""
+    import numpy as np
+    from nrqcd_b200 import lattice
+    saved = (lattice._ctx, lattice._extents, lattice._spacings)
+    try:
+        lattice._ctx, lattice._extents, lattice._spacings = object(), np.array([2, 2, 2]), np.ones(4)
+        ctx, V, is_open = lattice._resolve(None)
+        assert ctx is lattice._ctx and V == 8 and is_open()
+        lattice._ctx = object()  # finalised and replaced by a new InitModule
+        assert not is_open()
+        lattice._ctx = None  # finalised
+        assert not is_open()
+    finally:
+        lattice._ctx, lattice._extents, lattice._spacings = saved

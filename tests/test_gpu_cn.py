@@ -177,3 +177,38 @@ def test_errors_fail_loudly():
             h.InitSinglePoint(0, 1)
         with pytest.raises(NrqcdError):
             nrqcd.InitModule(1.0, [1, 1, 1, 1], 1.0, 1e-12)
+
+
+@pytest.mark.parametrize("tol", [1e-10, 1e-12])
+def test_history_start_and_half_step_exit(oracle, tol):
+    """The plain solve's start extrapolated from the field's last two
+    corrections (the default) and the half-step exit: over coupled steps on
+    an evolving 16^3 field it starts at a smaller residual and needs fewer
+    stencil launches than the start 2b - psi alone, ends at the same
+    tolerance, and both evolutions agree to the tolerance's level."""
+    from nrqcd_b200 import nrqcd
+    n = (16, 16, 16)
+    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 4, identity_links=False)
+    M, c = 1.0, [1, 1, 1, 1]
+    runs = {}
+    for hist in (True, False):
+        with lattice_ctx(n, A, cn=(M, c, 1.0, tol)):
+            nrqcd.SetHistoryGuess(hist)
+            g = GaugeConfiguration()
+            g.upload(links, ef)
+            h = NRQCDField()
+            h.InitSinglePoint(1, 1)
+            stats = []
+            for _ in range(6):
+                stats.append(h.Update(g, M, c, 1.0))
+                g.Update(1.0)
+            q, a = h.download()
+            del g, h
+        for st in stats:
+            assert st["converged"] == 1 and st["max_rel_residual"] <= tol
+        runs[hist] = (q, a, stats)
+    late_h, late_p = runs[True][2][3:], runs[False][2][3:]
+    assert all(x["initial_rel_residual"] < 0.2 * y["initial_rel_residual"] for x, y in zip(late_h, late_p))
+    assert sum(x["matvecs"] for x in late_h) < sum(y["matvecs"] for y in late_p)
+    assert np.abs(runs[True][0] - runs[False][0]).max() < 50 * tol
+    assert np.abs(runs[True][1] - runs[False][1]).max() < 50 * tol
