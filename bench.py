@@ -320,8 +320,12 @@ def measure_gluon_distribution(L, cpu=True, steps=10):
 
 
 # ------------------------------------------------------------------ CN forms
-FORMS = {"plain_fp64_bicgstab": 0, "precision_fp32_chebyshev_fp64_refinement": 1,
-         "learned_guess_precision": 2}
+# name -> (form, plain-form history start); the speed-ups are against
+# plain_fp64_bicgstab, the library's default plain solve (with the start
+# extrapolated from the field's history); the plain solve from 2b - psi
+# alone is reported beside it
+FORMS = {"plain_fp64_bicgstab": (0, 1), "plain_fp64_bicgstab_no_history": (0, 0),
+         "precision_fp32_chebyshev_fp64_refinement": (1, 1), "learned_guess_precision": (2, 1)}
 FORMS_SIZES = (64, 96, 128)
 
 
@@ -356,10 +360,11 @@ def measure_cn_forms(L, steps, params, tol=1e-10, seed=1):
         g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=seed, identity_links=True)
         stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(lat.ctx))
         cw = _capi.coeffs(WILSON)
-        for name, form in FORMS.items():
+        for name, (form, hist) in FORMS.items():
             cn = ctypes.c_void_p()
             _capi.check(lib.nrq_cn_init(lat.ctx, MASS, _capi.dptr(cw), 1.0, tol, 10000, form, ctypes.byref(cn)),
                         lat.ctx, "nrq_cn_init")
+            _capi.check(lib.nrq_cn_set_history_guess(cn, hist), lat.ctx, "history guess")
             net = None
             if form == 2:
                 net = LearnedGuess(lat=lat)

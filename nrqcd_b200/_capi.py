@@ -96,6 +96,7 @@ SIGNATURES = {
     "nrq_cn_finalize": (ctypes.c_int, [_vp]),
     "nrq_cn_stencil_info": (ctypes.c_int, [_vp, _ip, _dp]),
     "nrq_cn_set_stencil": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "nrq_cn_set_history_guess": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_heavy_update_cn": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,
                                            ctypes.POINTER(CnStats)]),
     "nrq_cn_apply": (ctypes.c_int, [_vp, _vp, ctypes.c_double, _dp, ctypes.c_double, ctypes.c_int, _vp, _vp]),

@@ -1105,6 +1105,12 @@ extern "C" int nrq_cn_set_stencil(nrq_cn *cn, int stencil) {
   return NRQ_OK;
 }
 
+extern "C" int nrq_cn_set_history_guess(nrq_cn *cn, int on) {
+  if (!cn || on < 0 || on > 1) return NRQ_ERR_BAD_ARG;
+  cn->history_guess = on != 0;
+  return NRQ_OK;
+}
+
 extern "C" int nrq_cn_finalize(nrq_cn *cn) {
   if (!cn) return NRQ_ERR_NOT_INITIALISED;
   cudaSetDevice(cn->ctx->device);
@@ -1548,11 +1554,21 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     matvecs += 1;
     vstreams += 1;  // extra write of x0
   }
+  if (cn->history_guess && h->hist_count >= 1) {  // x0 += 2 t1 - t2 (or t1)
+    ProfScope ps(ctx, 1, (double)L.V * (1152.0 * 2 + 576.0 * h->hist_count));
+    nrq::launch_hist_extrapolate(72 * L.V, cn->x, hist_v1(h), hist_v2(h), st);
+    vstreams += 2;
+  }
   bool restart = true, just_restarted = false;
   int64_t its = 0;
   int status = NRQ_OK;
   double *hs = cn->h_scal;
   double initial = -1.0;  // relative residual of the start, read after the first restart
+  // largest relative residual of the unconverged columns at the last read
+  // and the reduction of the last iteration; the half-step check runs when
+  // the predicted |s| is within kHalfWindow of the tolerance
+  double last_rel = 1.0, last_factor = 1e-2;
+  constexpr double kHalfWindow = 3.0;
   for (;;) {
     if (restart) {
       nrq::MvArgs a{};
@@ -1583,14 +1599,40 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       if ((rc = mv(cn, nrq::MV_V, CH, g, a))) return rc;
       fin(cn, 1);
       const bool tma = mv_t_needs_s(cn, CH);
+      // half-step exit: close to the tolerance, |s| = |r - alpha v| is
+      // checked before t = A^H s; when every column meets the tolerance
+      // there, x += alpha p ends the iteration and the restart pass confirms
+      // (predicted |s|: the last residual times the square root of the last
+      // pass's reduction, a half step being about half an iteration)
+      const bool check_half = tma && last_rel * std::sqrt(last_factor) < kHalfWindow * cn->tol;
       nrq::MvArgs b{};
       if (tma) {  // s = r - alpha v materialised, then t = A^H s
         {
           ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 3);
-          nrq::launch_vec_s(L, cn->s, cn->r, cn->v, cn->scal, st);
+          nrq::launch_vec_s(L, cn->s, cn->r, cn->v, cn->scal, st, check_half ? cn->partials : nullptr);
         }
         b.in = cn->s;
         vstreams += 3;
+        if (check_half) {
+          fin(cn, 4);
+          if ((rc = check_launch(ctx, "cn half step"))) return rc;
+          NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(hs, cn->scal, kScalBytes, cudaMemcpyDeviceToHost, st));
+          NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
+          bool half = true;
+          for (int k = 0; k < nrq::CN_COLS; ++k) {
+            const double *sc = hs + k * nrq::SC_STRIDE;
+            half = half && (sc[nrq::SC_CONV] != 0.0 || sc[nrq::SC_HALF] != 0.0);
+          }
+          if (half && *scal_err(hs) == 0) {
+            ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 3);
+            nrq::launch_vec_xp(L, cn->x, cn->p, cn->scal, st);
+            matvecs += 1;
+            vstreams += 3;
+            ++its;
+            restart = true;
+            continue;
+          }
+        }
       } else {    // s formed on the fly inside the stencil
         b.in = cn->r;
         b.in2 = cn->v;
@@ -1626,6 +1668,17 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, sizeof(int), st));
       break;
     }
+    {
+      double rel = 0.0;
+      for (int k = 0; k < nrq::CN_COLS; ++k) {
+        const double *s = hs + k * nrq::SC_STRIDE;
+        if (s[nrq::SC_BB] > 0 && s[nrq::SC_CONV] == 0.0)
+          rel = std::max(rel, std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]));
+      }
+      // reduction of the last full iteration (a restart keeps the previous one)
+      if (!just_restarted && last_rel > 0.0 && rel > 0.0) last_factor = std::min(1.0, rel / last_rel);
+      last_rel = rel;
+    }
     if (initial < 0.0) {
       initial = 0.0;
       for (int k = 0; k < nrq::CN_COLS; ++k) {
@@ -1654,9 +1707,20 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     }
     if (brk) restart = true;
   }
-  // result -> propagator (swap buffers); a plain step leaves no history
+  // the step's correction to the extrapolated start goes into the history
+  // (history_guess), otherwise a plain step leaves none
+  bool keep = false;
+  if (cn->history_guess && status == NRQ_OK) {
+    if ((rc = nrqh::ensure_hist(h))) return rc;
+    ProfScope ps(ctx, 1, (double)L.V * (1152.0 * 3 + 576.0));
+    nrq::launch_hist_store(72 * L.V, cn->x, cn->b, h->P, hist_next(h), st);
+    if ((rc = check_launch(ctx, "k_hist_store"))) return rc;
+    keep = true;
+  }
+  // result -> propagator (swap buffers)
   std::swap(h->P, cn->x);
-  h->hist_count = 0;
+  if (keep) hist_push(h);
+  else h->hist_count = 0;
   double maxrel = 0.0;
   bool conv = true;
   for (int k = 0; k < nrq::CN_COLS; ++k) {

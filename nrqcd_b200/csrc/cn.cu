@@ -236,9 +236,35 @@ __global__ void __launch_bounds__(384) k_vec_p(int64_t V, double2 *__restrict__ 
   }
 }
 
-// s = r - alpha v (materialised for the TMA-staged stencil)
+// s = r - alpha v (materialised for the TMA-staged and tensor-core
+// stencils); with partials, also the per-column partial sums of |s|^2 for
+// the half-step convergence check
 __global__ void __launch_bounds__(384) k_vec_s(int64_t V, double2 *__restrict__ S, const double2 *__restrict__ R,
-                                               const double2 *__restrict__ Vv, const double *__restrict__ scal) {
+                                               const double2 *__restrict__ Vv, const double *__restrict__ scal,
+                                               double *__restrict__ partials) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  const int64_t pb = (int64_t)(w * 6) * V;
+  const cplx al = scal_c(scal, w, SC_ALPHA);
+  double q = 0.0;
+  if (x0 < V) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int64_t o = pb + (int64_t)r * V + x0;
+      const cplx s = ldg(R + o) - al * ldg(Vv + o);
+      st(S + o, s);
+      q += norm2(s);
+    }
+  }
+  if (!partials) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
+  if (lane == 0) partials[(int64_t)blockIdx.x * CN_COLS + w] = q;
+}
+
+// x += alpha p: the solution after a half step that met the tolerance
+__global__ void __launch_bounds__(384) k_vec_xp(int64_t V, double2 *__restrict__ X, const double2 *__restrict__ P,
+                                                const double *__restrict__ scal) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
   if (x0 >= V) return;
@@ -247,7 +273,7 @@ __global__ void __launch_bounds__(384) k_vec_s(int64_t V, double2 *__restrict__ 
 #pragma unroll
   for (int r = 0; r < 6; ++r) {
     const int64_t o = pb + (int64_t)r * V + x0;
-    st(S + o, ldg(R + o) - al * ldg(Vv + o));
+    st(X + o, ld(X + o) + al * ldg(P + o));
   }
 }
 
@@ -287,9 +313,14 @@ __global__ void __launch_bounds__(384) k_vec_xr_s(int64_t V, double2 *__restrict
     for (int k = 0; k < 3; ++k) partials[((int64_t)blockIdx.x * CN_COLS + w) * 3 + k] = q[k];
 }
 
-void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st) {
+void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st,
+                  double *partials) {
   unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
-  k_vec_s<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, s, r, v, scal);
+  k_vec_s<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, s, r, v, scal, partials);
+}
+void launch_vec_xp(Lat L, double2 *x, const double2 *p, const double *scal, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  k_vec_xp<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, x, p, scal);
 }
 void launch_vec_xr_s(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *s, const double2 *t,
                      const double2 *rh, const double *scal, double *partials, cudaStream_t st) {
@@ -313,7 +344,7 @@ __device__ __forceinline__ cplx cdiv_safe(cplx a, cplx b) { return cdiv(a, b); }
 __global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restrict__ partials,
                               double *__restrict__ scal, double tol) {
   const int col = blockIdx.x;
-  const int nq = (stage == 0 || stage == 1) ? 2 : 3;
+  const int nq = stage == 4 ? 1 : (stage == 0 || stage == 1) ? 2 : 3;
   __shared__ double sh[3][256];
   double acc[3] = {0.0, 0.0, 0.0};
   for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x)
@@ -353,6 +384,10 @@ __global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restri
     if (!conv && q2 > 0.0) om = (1.0 / q2) * cplx{q0, q1};
     sc[SC_OMEGA] = om.re;
     sc[SC_OMEGA + 1] = om.im;
+  } else if (stage == 4) {  // half step: |s|^2 against the tolerance
+    sc[SC_SS] = q0;
+    sc[SC_HALF] = (!conv && q0 <= tol * tol * sc[SC_BB]) ? 1.0 : 0.0;
+    if (!isfinite(q0)) sc[SC_NONFIN] = 1.0;
   } else {  // stage 3: rho_new = rh.r, rr = r.r
     if (!conv) {
       sc[SC_RR] = q2;
@@ -645,6 +680,39 @@ void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &
   nblk = (V + 127) / 128;
   if (gconjg) k_correlators<true><<<(unsigned)nblk, 128, 0, st>>>(P, V, partials);
   else k_correlators<false><<<(unsigned)nblk, 128, 0, st>>>(P, V, partials);
+}
+
+// ------------------------------------------------------------ history-extrapolated start
+// The plain solve's start 2b - psi misses t = x - (2b - psi); consecutive
+// steps' t are strongly correlated, so x0 = 2b - psi + 2 t1 - t2 (or + t1
+// with one step of history) starts closer.  The history is kept in FP32.
+__global__ void k_hist_extrapolate(int64_t n, double2 *__restrict__ X, const float2 *__restrict__ T1,
+                                   const float2 *__restrict__ T2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float2 a = T1[i];
+  double dx = a.x, dy = a.y;
+  if (T2) {
+    const float2 b = T2[i];
+    dx = 2.0 * dx - (double)b.x;
+    dy = 2.0 * dy - (double)b.y;
+  }
+  const double2 x = X[i];
+  X[i] = make_double2(x.x + dx, x.y + dy);
+}
+// t = x - (2b - psi) of the step just solved
+__global__ void k_hist_store(int64_t n, const double2 *__restrict__ X, const double2 *__restrict__ B,
+                             const double2 *__restrict__ Psi, float2 *__restrict__ T) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double2 x = X[i], b = B[i], p = Psi[i];
+  T[i] = make_float2((float)(x.x - (2.0 * b.x - p.x)), (float)(x.y - (2.0 * b.y - p.y)));
+}
+void launch_hist_extrapolate(int64_t n, double2 *X, const float2 *T1, const float2 *T2, cudaStream_t st) {
+  k_hist_extrapolate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, X, T1, T2);
+}
+void launch_hist_store(int64_t n, const double2 *X, const double2 *B, const double2 *Psi, float2 *T, cudaStream_t st) {
+  k_hist_store<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, X, B, Psi, T);
 }
 
 }  // namespace nrq

@@ -143,6 +143,9 @@ struct nrq_cn {
   bool tma_ok = false;
   bool stencil_tuned = false;
   double tune_ms[3] = {-1.0, -1.0, -1.0};
+  // plain form: start from 2b - psi + 2 t1 - t2 with the field's history of
+  // corrections (FP32); on by default
+  bool history_guess = true;
   // tensor-core stencil: forward 6x6 blocks (6 per site: direction x
   // species, 36 complex each) built for the coefficients w_coef from the
   // current gauge field (w_valid cleared by every preparation)

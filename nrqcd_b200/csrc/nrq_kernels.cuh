@@ -103,7 +103,9 @@ enum {
   SC_BB = 9,
   SC_CONV = 10,  // 1.0 when converged
   SC_BREAK = 11, // 1.0 on breakdown (restart requested)
-  SC_NONFIN = 12
+  SC_NONFIN = 12,
+  SC_SS = 13,    // |s|^2 of the half step (when checked)
+  SC_HALF = 14   // 1.0 when the half step s = r - alpha v met the tolerance
 };
 
 void launch_cn_prepare(Lat L, const double2 *U, const double *E, double2 *Dsum, double *Bsum, double2 *DE,
@@ -113,7 +115,9 @@ void launch_cn_mv(int mode, Lat L, const CnCoef &C, const double2 *U, const doub
 void launch_vec_xr(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *v, const double2 *t,
                    const double2 *rh, const double *scal, double *partials, cudaStream_t st);
 void launch_vec_p(Lat L, double2 *p, const double2 *r, const double2 *v, const double *scal, cudaStream_t st);
-void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st);
+void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st,
+                  double *partials = nullptr);
+void launch_vec_xp(Lat L, double2 *x, const double2 *p, const double *scal, cudaStream_t st);
 void launch_vec_xr_s(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *s, const double2 *t,
                      const double2 *rh, const double *scal, double *partials, cudaStream_t st);
 // TMA-staged stencil (cn_mv3.cu); returns nonzero if the tensor maps cannot
@@ -189,6 +193,8 @@ void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st)
 void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);
 void launch_single_point(double2 *P, int64_t V, int64_t sq, int64_t sa, cudaStream_t st);
 void launch_norms(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st);
+void launch_hist_extrapolate(int64_t n, double2 *X, const float2 *T1, const float2 *T2, cudaStream_t st);
+void launch_hist_store(int64_t n, const double2 *X, const double2 *B, const double2 *Psi, float2 *T, cudaStream_t st);
 void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st,
                         bool gconjg = false);
 

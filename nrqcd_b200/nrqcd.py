@@ -80,6 +80,14 @@ def SetStencil(stencil=None):
                 f"Error in {modulename}: stencil")
 
 
+def SetHistoryGuess(on=True):
+    """Plain form: start each solve from the extrapolation 2b - psi plus
+    2 t1 - t2 of the field's last two corrections (FP32 history; the
+    default), or from 2b - psi alone (on=False)."""
+    _capi.check(_capi.load().nrq_cn_set_history_guess(solver_handle(), int(bool(on))), lattice.context(),
+                f"Error in {modulename}: history guess")
+
+
 def StencilInfo():
     """(stencil in use, per-launch ms of each stencil timed on the first
     update; -1 where not timed)."""
