@@ -1377,13 +1377,17 @@ extern "C" int nrq_learn_record(nrq_learn *net, nrq_cn *cn, nrq_heavy *h, const 
   int rc = set_device(ctx);
   if (!rc) rc = nrqh::ensure_hist(h);
   if (rc) return rc;
-  // the step itself runs without the learned guess; the history it leaves
-  // is the exact t = x - (2 RHS - psi)
+  // the step itself runs without the learned guess and without the
+  // history start (which would also write the history); the history it
+  // leaves is the exact t = x - (2 RHS - psi)
   const int cnt = h->hist_count, head = h->hist_head;
   nrq_learn *saved = cn->learn;
+  const bool saved_hist = cn->history_guess;
   cn->learn = nullptr;
+  cn->history_guess = false;
   rc = nrq_heavy_update_cn(cn, h, g, mass, c, dt, stats);
   cn->learn = saved;
+  cn->history_guess = saved_hist;
   h->hist_count = cnt;
   h->hist_head = head;
   if (rc) {
