@@ -320,13 +320,12 @@ def measure_gluon_distribution(L, cpu=True, steps=10):
 
 
 # ------------------------------------------------------------------ CN forms
-# name -> (form, history start); the speed-ups are against
-# plain_fp64_bicgstab, the library's default plain solve (with the start
-# extrapolated from the field's history); the plain and precision solves
-# from 2b - psi alone are reported beside them
+# name -> (form, history start of the plain form); the speed-ups are
+# against plain_fp64_bicgstab, the library's default plain solve (with the
+# start extrapolated from the field's history); the plain solve from 2b - psi
+# alone is reported beside it
 FORMS = {"plain_fp64_bicgstab": (0, 1), "plain_fp64_bicgstab_no_history": (0, 0),
-         "precision_fp32_chebyshev_fp64_refinement": (1, 1),
-         "precision_fp32_chebyshev_fp64_refinement_no_history": (1, 0), "learned_guess_precision": (2, 1)}
+         "precision_fp32_chebyshev_fp64_refinement": (1, 1), "learned_guess_precision": (2, 1)}
 FORMS_SIZES = (64, 96, 128)
 
 

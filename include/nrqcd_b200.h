@@ -201,12 +201,14 @@ int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[3]);
 /* Force a stencil (NRQ_STENCIL_*) or restore the timed choice (-1).
  * NRQ_ERR_BAD_ARG if the stencil cannot describe this lattice.            */
 int nrq_cn_set_stencil(nrq_cn *cn, int stencil);
-/* Plain and precision forms (0, 1; no reference counterpart): on = 1 (the
- * default) starts every solve from 2b - psi + 2 t1 - t2, t1 and t2 the corrections
+/* Plain form (form 0; no reference counterpart): on = 1 (the default)
+ * starts every solve from 2b - psi + 2 t1 - t2, t1 and t2 the corrections
  * to that start of the field's last two steps (one step: + t1), kept per
  * field in FP32 (2 x 576 B per site); 0 starts from 2b - psi.  Any upload,
  * copy or point source restarts the history.  The tolerance and the final
- * true-residual check are the same either way.                            */
+ * true-residual check are the same either way.  (The precision form keeps
+ * its start: its refinement passes are set by the FP32 gain per pass, and
+ * the smaller start did not remove one at 64^3 or 96^3.)                  */
 int nrq_cn_set_history_guess(nrq_cn *cn, int on);
 /* NRQCDField%Update(GaugeConf, Mass, WilsonCoeffs, StepWidth) =
  * Update_CrankNicholson, src/nrqcd.f90:1053-1168: quark (+M, c) and

@@ -1383,14 +1383,6 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
   // learned form: x = 2 RHS - psi + w1 u + w2 v (network), history restarted
   // with the network's part; every refinement correction is added to it
   const bool learned = cn->form == 2 && nrqh::learned_ready(cn->learn);
-  // otherwise, as the plain form, the start extrapolated from the field's
-  // last two corrections (history_guess)
-  const bool history = !learned && cn->history_guess;
-  if (history && h->hist_count >= 1) {
-    ProfScope ps(ctx, 1, (double)V * (1152.0 * 2 + 576.0 * h->hist_count));
-    nrq::launch_hist_extrapolate(72 * V, cn->x, hist_v1(h), hist_v2(h), st);
-    vstreams += 2;
-  }
   if (learned) {
     if ((rc = nrqh::ensure_hist(h))) return rc;
     ProfScope ps(ctx, 3, (double)V * (1152.0 * 4 + 576.0 * 6 + 432.0 * 3 + 128.0));
@@ -1511,16 +1503,8 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     vstreams += 3;
   }
   if (status == NRQ_OK && !conv) status = NRQ_ERR_NOT_CONVERGED;
-  bool keep = learned && status == NRQ_OK;
-  if (history && status == NRQ_OK) {  // t = x - (2b - psi) of this step
-    if ((rc = nrqh::ensure_hist(h))) return rc;
-    ProfScope ps(ctx, 1, (double)V * (1152.0 * 3 + 576.0));
-    nrq::launch_hist_store(72 * V, cn->x, cn->b, h->P, hist_next(h), st);
-    if ((rc = check_launch(ctx, "k_hist_store"))) return rc;
-    keep = true;
-  }
   std::swap(h->P, cn->x);
-  if (keep) hist_push(h);
+  if (learned && status == NRQ_OK) hist_push(h);
   else h->hist_count = 0;
   double maxrel = 0.0;
   for (int k = 0; k < nrq::CN_COLS; ++k) {
