@@ -79,3 +79,39 @@ def test_objects_outliving_their_module_context_are_not_destroyed_through_a_new_
         assert not is_open()
     finally:
         lattice._ctx, lattice._extents, lattice._spacings = saved
+
+
+def test_header_is_plain_c_and_links(lib, tmp_path):
+    """A C99 program includes the header and links the library the way the
+    reference's Fortran binding would: the header is valid C (no C++ or torch
+    types) and the entry points resolve at link time.  Without a GPU,
+    nrq_init reports an error and no context; with one, it opens and
+    finalises a context."""
+    import shutil
+    import subprocess
+    from nrqcd_b200 import build
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "nrqcd_b200.h"
+int main(void) {
+  int64_t ext[3] = {4, 4, 4};
+  double sp[4] = {0.05, 1.0, 1.0, 1.0};
+  nrq_ctx *ctx = NULL;
+  int rc = nrq_init(ext, sp, 0, &ctx);
+  printf("%d %s\n", rc, nrq_status_string(rc));
+  if (rc == NRQ_OK) return nrq_finalize(ctx) == NRQ_OK ? 0 : 5;
+  return ctx == NULL ? 3 : 4;
+}
+''')
+    exe = tmp_path / "abi"
+    libdir = os.path.dirname(build.LIB)
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src),
+                        "-L", libdir, "-lnrqcd_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == (0 if gpu_available() else 3), run.stdout + run.stderr
