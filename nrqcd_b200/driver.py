@@ -213,7 +213,8 @@ def mode_correlators_equilibrium(args, form=0, device=0):
     mass = float(args[13])
     c = [complex(float(args[14 + 2 * k]), float(args[15 + 2 * k])) for k in range(4)]
     f_corr, f_norm = args[22], args[23]
-    measure = int(args[24]) != 0
+    # MeasureEnergy, read with (I1): a missing argument reads as blank, i.e. 0
+    measure = len(args) > 24 and int(args[24] or 0) != 0
     energy_file = args[25] if measure else None
 
     def init(g):
@@ -347,7 +348,7 @@ def mode_gluondist_equilibrium(args, device=0):
     nefieldinit, nequilibrium = int(args[10]), int(args[11])
     gf_maxit, gf_tol, gf_alpha = int(args[13]), float(args[14]), float(args[15])
     f_out = args[16]
-    measure = int(args[17]) != 0
+    measure = len(args) > 17 and int(args[17] or 0) != 0
     energy_file = args[18] if measure else None
     lattice.InitModule(ext, sp, device=device)
     try:
