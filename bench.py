@@ -41,6 +41,11 @@ MASS = 1.0
 WILSON = [1.0, 1.0, 1.0, 1.0]
 A = (0.05, 1.0, 1.0, 1.0)
 TOL = 1e-12
+# DRAM bytes per site of an average tensor-core stencil launch of the plain
+# solve, from one ncu capture of a 64^3 update (dram__bytes_read.sum +
+# dram__bytes_write.sum over its 2 residual, 4 v and 3 t launches: 10,773,
+# 7,760 and 6,377 B/site)
+STENCIL_DRAM_BYTES_PER_SITE = 7968.0
 # FP64 stencils of the solver, by NRQ_STENCIL_* index
 STENCIL_NAMES = {0: "k_cn_mv2 (register-tiled)", 1: "k_cn_mv3 (TMA-staged)", 2: "k_cn_mv4 (FP64 tensor cores)"}
 
@@ -859,7 +864,9 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "CN 12-column stencil: " + stencil["in_use"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                         "traffic": None,
+                         "traffic": (STENCIL_DRAM_BYTES_PER_SITE * V / 1e9 if tensor else None),
+                         "traffic_unit": "GB per launch (ncu capture of one 64^3 update, per site x V)",
+                         "algorithmic_GB_per_launch": sten["bytes"] / max(1, sten["launches"]) / 1e9,
                          "launches": sten["launches"], "avg_launch_ms": sten["ms"] / max(1, sten["launches"]),
                          "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9,
                          "fp64": {"flops_per_site_per_launch": flops_site, "achieved_tflops": fp64_achieved,
