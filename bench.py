@@ -855,6 +855,16 @@ def main():
         flops_site = 2 * (6 * 6 * 36 + 6 * 18 + (0 if tensor else 270)) * 4 * 2
         fp64_achieved = flops_site * V * sten["launches"] / (sten["ms"] / 1000.0) / 1e12 if sten["ms"] > 0 else None
         step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
+        # the build plan's per-site byte model of a coupled step: leapfrog
+        # 1872 B; per species and 6-column matvec 1776 B (spinor in and out,
+        # U and E, derived blocks not credited) and per 6-column vector
+        # stream 576 B, with the matvecs and streams the solves executed
+        mv = float(np.mean([st["matvecs"] for st in iters])) if iters else 0.0
+        vs = float(np.mean([st["vector_streams"] for st in iters])) if iters else 0.0
+        model_site = 1872.0 + 2 * (mv * 1776.0 + vs * 576.0)
+        model_gbps = model_site * V / (ms_per_step / 1000.0) / 1e9
+        model = {"bytes_per_site_step": model_site, "matvecs_per_step": mv, "vector_streams_per_step": vs,
+                 "GBps": model_gbps, "frac": model_gbps / peak, "peak_source": peak_src}
         its = [s["iterations"] for s in iters]
         line = {
             "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
@@ -869,6 +879,7 @@ def main():
                          "algorithmic_GB_per_launch": sten["bytes"] / max(1, sten["launches"]) / 1e9,
                          "launches": sten["launches"], "avg_launch_ms": sten["ms"] / max(1, sten["launches"]),
                          "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9,
+                         "byte_model_of_the_plan": model,
                          "fp64": {"flops_per_site_per_launch": flops_site, "achieved_tflops": fp64_achieved,
                                   "peak_tflops": p64.value, "peak_source": "measured (FP64 FMA probe)",
                                   "frac": fp64_achieved / p64.value if fp64_achieved else None,
