@@ -237,8 +237,9 @@ def measure_thermal_ic(L, seed=1, cpu=True, cpu_sweeps=4, max_sweeps=200000):
            "algorithmic_bytes_per_site_sweep": THERMAL_BYTES_SITE_SWEEP,
            "algorithmic_GBps": THERMAL_BYTES_SITE_SWEEP * V * sweeps / (ms / 1000.0) / 1e9,
            "draw_ms": draw_ms,
-           "draw_note": "cold links, host ranlxd draw of the thermal field (a sequential stream, as in the "
-                        "reference) and its upload"}
+           "draw_note": "cold links, host ranlxd draw of the thermal field (the reference's one stream, split "
+                        "over host threads that jump to their share) and its upload",
+           "draw_threads": min(os.cpu_count() or 1, 32)}
     if cpu:
         from oracle import oracle as oc
         n = (L, L, L)

@@ -396,14 +396,13 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
   }
   // real parts of complex Box-Muller normals, per site, per polarisation
   // (gauge:1334-1340, random.f90:238-255): plane (pol*8 + a)
+  // (pair e = 16 s + 8 pol + a of the stream; drawn on host threads that
+  // jump to their share)
   std::vector<double2> R((size_t)16 * V);
   const double twopi = 2.0 * std::acos(-1.0);
-  for (int64_t s = 0; s < V; ++s)
-    for (int pol = 0; pol < 2; ++pol)
-      for (int a = 0; a < 8; ++a) {
-        double u1 = rng.next(), u2 = rng.next();
-        R[(size_t)(pol * 8 + a) * V + s] = make_double2(std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2), 0.0);
-      }
+  nrqh::draw_pairs(2, seed, 0, (size_t)16 * V, [&](size_t e, double u1, double u2) {
+    R[(e % 16) * (size_t)V + e / 16] = make_double2(std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2), 0.0);
+  });
   // backward-derivative momentum per direction and coordinate (lattice:963-979):
   // component (re, im) and modulus, in the host's arithmetic
   std::vector<double> mtab;
@@ -678,11 +677,11 @@ extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nef
   std::vector<double> ef((size_t)24 * V);  // the reference's efield(8,3,V)
   for (int64_t r = 0; r < nefieldinit; ++r) {
     // Box-Muller pairs in the reference's order: site, direction, generator
-    // (random.f90:238-255); the real part, times sigma, times a0
-    for (size_t i = 0; i < ef.size(); ++i) {
-      const double u1 = rng.next(), u2 = rng.next();
+    // (random.f90:238-255); the real part, times sigma, times a0.  Round r
+    // starts at number 48 V r of the stream; host threads jump to their share.
+    nrqh::draw_pairs(2, seed, (uint64_t)r * ef.size() * 2, ef.size(), [&](size_t i, double u1, double u2) {
       ef[i] = (sigma * (std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2))) * a0;
-    }
+    });
     if ((rc = ensure_stage(ctx, sizeof(double) * 24 * V))) return rc;
     NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_stage, ef.data(), sizeof(double) * 24 * V, cudaMemcpyHostToDevice,
                                       ctx->stream));

@@ -1,7 +1,9 @@
 """The host generator of the device initial conditions (ranlxd, luxury
 level 2, nrqcd_b200/csrc/ranlxd_host.h) against the CPU oracle's generator:
 bit-identical streams over many refills, for several seeds (plain C++; no
-GPU)."""
+GPU).  The jump (the recurrence as a congruential generator modulo
+b^12 - b^5 + 1, b = 2^48) lands on the same numbers as sequential calls, and
+the threaded pair draw of the initial conditions equals one sequential pass."""
 import os
 import shutil
 import subprocess
@@ -53,3 +55,106 @@ def test_host_stream_equals_oracle(oracle, host_stream, seed, level):
     got = host_stream(seed, N, level)
     want = oracle.Ranlxd(level, seed).draw(N)
     assert got.shape == want.shape and np.array_equal(got, want)
+
+
+JUMP_SRC = r'''
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include "ranlxd_host.h"
+// mode 0: numbers [n, n + k) after jump(n), for each n on the command line
+// mode 1: jump(n) against jump(n - d) and d calls of next(), far into the stream
+// mode 2: draw_pairs on several threads against one sequential pass
+int main(int argc, char **argv) {
+  const int mode = std::atoi(argv[1]), level = std::atoi(argv[2]);
+  const long seed = std::atol(argv[3]);
+  if (mode == 0) {
+    const long k = std::atol(argv[4]);
+    for (int a = 5; a < argc; ++a) {
+      nrqh::Ranlxd r;
+      r.init(level, seed);
+      if (!r.jump(std::strtoull(argv[a], nullptr, 10))) return 3;
+      for (long i = 0; i < k; ++i) {
+        double v = r.next();
+        std::fwrite(&v, sizeof v, 1, stdout);
+      }
+    }
+    return 0;
+  }
+  if (mode == 1) {
+    long bad = 0;
+    for (int a = 4; a < argc; ++a) {
+      const unsigned long long n = std::strtoull(argv[a], nullptr, 10);
+      nrqh::Ranlxd x, y;
+      x.init(level, seed);
+      y.init(level, seed);
+      if (!x.jump(n) || !y.jump(n - 1000)) return 3;
+      for (int i = 0; i < 1000; ++i) y.next();
+      for (int i = 0; i < 600; ++i) bad += x.next() != y.next();
+    }
+    std::printf("%ld\n", bad);
+    return 0;
+  }
+  const size_t count = std::atol(argv[4]);
+  const unsigned long long first = std::strtoull(argv[5], nullptr, 10);
+  std::vector<double> got(2 * count), want(2 * count);
+  if (!nrqh::draw_pairs(level, seed, first, count, [&](size_t i, double u1, double u2) {
+        got[2 * i] = u1;
+        got[2 * i + 1] = u2;
+      }, 8))
+    return 3;
+  nrqh::Ranlxd r;
+  r.init(level, seed);
+  for (unsigned long long i = 0; i < first; ++i) r.next();
+  for (size_t i = 0; i < 2 * count; ++i) want[i] = r.next();
+  long bad = 0;
+  for (size_t i = 0; i < 2 * count; ++i) bad += got[i] != want[i];
+  std::printf("%ld\n", bad);
+  return 0;
+}
+'''
+
+
+@pytest.fixture(scope="module")
+def jump_exe(tmp_path_factory):
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    d = tmp_path_factory.mktemp("ranlxd_jump")
+    (d / "jump.cpp").write_text(JUMP_SRC)
+    exe = d / "jump"
+    r = subprocess.run([cxx, "-O2", "-std=c++17", "-pthread", "-I", os.path.join(ROOT, "nrqcd_b200", "csrc"),
+                        str(d / "jump.cpp"), "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+@pytest.mark.parametrize("seed,level", [(1, 2), (2147483647, 2), (12345, 1)])
+def test_jump_lands_on_the_oracle_stream(oracle, jump_exe, seed, level):
+    """Offsets at, before and after block boundaries (12 numbers per refill)
+    and inside blocks, against the oracle's sequential stream."""
+    k = 40
+    offsets = [0, 1, 11, 12, 13, 23, 24, 143, 144, 145, 1001, 12347, 30000 - k]
+    out = subprocess.run([str(jump_exe), "0", str(level), str(seed), str(k)] + [str(n) for n in offsets],
+                         capture_output=True, check=True).stdout
+    got = np.frombuffer(out, dtype=np.float64).reshape(len(offsets), k)
+    want = oracle.Ranlxd(level, seed).draw(30000)
+    for row, n in zip(got, offsets):
+        assert np.array_equal(row, want[n:n + k]), n
+
+
+def test_jump_far_into_the_stream(jump_exe):
+    """jump(n) equals jump(n - 1000) followed by 1000 calls, up to 10^15."""
+    offsets = [10 ** 6 + 7, 48 * 64 ** 3 * 3 + 5, 10 ** 12 + 11, 10 ** 15 + 3]
+    r = subprocess.run([str(jump_exe), "1", "2", "7"] + [str(n) for n in offsets], capture_output=True, text=True,
+                       check=True)
+    assert r.stdout.split() == ["0"]
+
+
+@pytest.mark.parametrize("first", [0, 48 * 1000 * 2 + 1])
+def test_threaded_pair_draw_equals_one_pass(jump_exe, first):
+    """The initial conditions' threaded draw (8 threads over 600,000 pairs)
+    hands every pair the numbers one sequential pass would."""
+    r = subprocess.run([str(jump_exe), "2", "2", "3", "600000", str(first)], capture_output=True, text=True,
+                       check=True)
+    assert r.stdout.split() == ["0"]
