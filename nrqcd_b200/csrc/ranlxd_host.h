@@ -246,7 +246,7 @@ template <class F>
 bool draw_pairs(int level, int64_t seed, uint64_t first, size_t count, F f, unsigned max_threads = 32) {
   Ranlxd probe;
   if (!probe.init(level, seed)) return false;
-  const size_t min_share = 1 << 16;
+  const size_t min_share = 1 << 12;  // ~0.5 ms of drawing per thread at least
   unsigned nt = std::thread::hardware_concurrency();
   nt = std::max(1u, std::min(nt, max_threads));
   nt = (unsigned)std::min<size_t>(nt, (count + min_share - 1) / min_share);
