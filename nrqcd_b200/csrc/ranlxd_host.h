@@ -151,7 +151,11 @@ inline bool from_lcg(const Num &z, int64_t *h) {
 // fractions, subtract-with-borrow x_n = x_{n-5} - x_{n-12} - c, pr recurrence
 // steps per 12 delivered numbers (pr = 397 at luxury level 2), seeded from a
 // 31-bit shift register — the generator of src/ranlxd_generator.f90:72-350
-// as random%InitModule uses it (src/random.f90:126-140).
+// as random%InitModule uses it (src/random.f90:126-140).  The words are
+// carried as 48-bit integers: the reference's double arithmetic on them is
+// exact, so the integer recurrence delivers the same numbers, with a borrow
+// chain of two integer operations per step instead of a floating-point
+// subtract, compare and select.
 class Ranlxd {
  public:
   bool init(int level, int64_t seed) {
@@ -166,22 +170,18 @@ class Ranlxd {
       v >>= 1;
     }
     int ib = 0, jb = 18;
-    const double unit = std::ldexp(1.0, -48);
     for (int k = 0; k < 12; ++k) {
-      double acc = 0.0;
+      int64_t acc = 0;
       for (int l = 0; l < 48; ++l) {
-        acc = 2.0 * acc + (double)((bits[ib] + 1) & 1);
+        acc = 2 * acc + ((bits[ib] + 1) & 1);
         bits[ib] = (bits[ib] + bits[jb]) & 1;
         ib = (ib + 1) % 31;
         jb = (jb + 1) % 31;
       }
-      w_[k] = unit * acc;
-      seeded_[k] = (int64_t)acc;
+      x_[k] = seeded_[k] = acc;
     }
-    borrow_ = 0.0;
-    pos_ = 11;
-    lag_ = 7;
-    last_ = 0;
+    carry_ = 0;
+    next_ = 12;
     return true;
   }
   // Position the stream so that the next call of next() returns number n
@@ -193,49 +193,53 @@ class Ranlxd {
     const uint64_t blocks = n / 12;
     if (blocks > UINT64_MAX / (uint64_t)pr_) return false;
     const swb::Num z = swb::mul(swb::pow(swb::inverse_base(), blocks * (uint64_t)pr_), swb::to_lcg(seeded_, 0));
-    int64_t h[12];
-    if (!swb::from_lcg(z, h)) return false;
-    const double unit = std::ldexp(1.0, -48);
-    const int oldest = (int)((blocks % 12) * (uint64_t)(pr_ % 12) % 12);
-    for (int k = 0; k < 12; ++k) w_[(oldest + k) % 12] = unit * (double)h[k];
-    borrow_ = 0.0;
-    pos_ = (oldest + 11) % 12;
-    last_ = oldest;
-    lag_ = (oldest + 7) % 12;
-    for (uint64_t k = 0; k < n % 12; ++k) next();
+    if (!swb::from_lcg(z, x_)) return false;
+    carry_ = 0;
+    refill();
+    next_ = (int)(n % 12);
     return true;
   }
   double next() {
-    pos_ = pos_ == 11 ? 0 : pos_ + 1;
-    if (pos_ == last_) refill();
-    return w_[pos_];
+    if (next_ == 12) {
+      refill();
+      next_ = 0;
+    }
+    return out_[next_++];
   }
 
  private:
-  // pr_ subtract-with-borrow steps; the ring indices wrap by comparison (the
-  // arithmetic of every step is unchanged)
-  void refill() {
-    const double unit = std::ldexp(1.0, -48);
-    int i = pos_, j = lag_;
-    double borrow = borrow_;
-    for (int k = 0; k < pr_; ++k) {
-      double y = (w_[j] - w_[i]) - borrow;
-      const bool neg = y < 0.0;
-      borrow = neg ? unit : 0.0;
-      if (neg) y += 1.0;
-      w_[i] = y;
-      i = i == 11 ? 0 : i + 1;
-      j = j == 11 ? 0 : j + 1;
-    }
-    borrow_ = borrow;
-    pos_ = i;
-    lag_ = j;
-    last_ = i;
+  // one recurrence step on ring slot i (the oldest word) with lag slot j
+  static inline void step(int64_t *x, int i, int j, int64_t &c) {
+    int64_t y = x[j] - x[i] - c;
+    c = (int64_t)((uint64_t)y >> 63);
+    x[i] = y + (c << 48);
   }
-  double w_[12];
+  // pr_ steps over the ring held oldest-first from slot 0, then the ring
+  // rotated back to oldest-first and the 12 newest words handed out oldest
+  // first (the order ranlxd delivers them)
+  void refill() {
+    int64_t c = carry_;
+    int64_t *x = x_;
+    for (int rep = 0; rep < pr_ / 12; ++rep) {
+#pragma GCC unroll 12
+      for (int i = 0; i < 12; ++i) step(x, i, i < 5 ? i + 7 : i - 5, c);
+    }
+    const int rest = pr_ % 12;
+    for (int i = 0; i < rest; ++i) step(x, i, i < 5 ? i + 7 : i - 5, c);
+    int64_t r[12];
+    for (int k = 0; k < 12; ++k) r[k] = x[(rest + k) % 12];
+    const double unit = std::ldexp(1.0, -48);
+    for (int k = 0; k < 12; ++k) {
+      x[k] = r[k];
+      out_[k] = unit * (double)r[k];
+    }
+    carry_ = c;
+  }
+  int64_t x_[12] = {};
   int64_t seeded_[12] = {};
-  double borrow_ = 0.0;
-  int pr_ = 397, pos_ = 11, lag_ = 7, last_ = 0;
+  int64_t carry_ = 0;
+  double out_[12] = {};
+  int pr_ = 397, next_ = 12;
 };
 
 // f(i, u[first + 2i], u[first + 2i + 1]) for i < count, u the stream of
