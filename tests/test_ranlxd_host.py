@@ -158,3 +158,35 @@ def test_threaded_pair_draw_equals_one_pass(jump_exe, first):
     r = subprocess.run([str(jump_exe), "2", "2", "3", "600000", str(first)], capture_output=True, text=True,
                        check=True)
     assert r.stdout.split() == ["0"]
+
+
+@pytest.mark.parametrize("seed,level,pr", [(1, 2, 397), (987654, 2, 397), (12345, 1, 202)])
+def test_oracle_stream_is_the_published_recurrence(oracle, seed, level, pr):
+    """The oracle's stream, read without its code: every block of 12
+    delivered numbers is the ring of 48-bit words after a refill, and the
+    subtract-with-borrow recurrence with lags (12, 5) in base b = 2^48 is the
+    congruential generator Z -> Z / b modulo m = b^12 - b^5 + 1 (the borrow
+    enters Z as -c b^12).  So consecutive blocks k, k+1 must satisfy
+    Z_{k+1} = b^-pr Z_k (mod m) for one borrow c_k and one c_{k+1} in {0, 1}:
+    this pins the lags, the borrow convention and the luxury level's pr
+    steps per block with Python integers alone."""
+    b = 1 << 48
+    m = b ** 12 - b ** 5 + 1
+    step = pow(pow(b, -1, m), pr, m)
+    words = (oracle.Ranlxd(level, seed).draw(12 * 40) * b).astype(np.int64)
+    assert np.array_equal(words.astype(np.float64) / b, oracle.Ranlxd(level, seed).draw(12 * 40))
+
+    def lcg(h, c):
+        h = [int(v) for v in h]
+        z = sum(h[k] * b ** k for k in range(5)) + sum((h[k] - h[k - 5]) * b ** k for k in range(5, 12))
+        return (z - c * b ** 12) % m
+
+    blocks = words.reshape(40, 12)
+    for k in range(39):
+        here = {lcg(blocks[k], c) * step % m for c in (0, 1)}
+        there = {lcg(blocks[k + 1], c) for c in (0, 1)}
+        assert here & there, k
+    # a wrong decimation or lag fails the same check
+    wrong = pow(pow(b, -1, m), pr + 1, m)
+    assert not any({lcg(blocks[k], c) * wrong % m for c in (0, 1)} & {lcg(blocks[k + 1], c) for c in (0, 1)}
+                   for k in range(39))
