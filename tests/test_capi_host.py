@@ -115,3 +115,11 @@ int main(void) {
     assert r.returncode == 0, r.stderr
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert run.returncode == (0 if gpu_available() else 3), run.stdout + run.stderr
+
+
+def test_integration_notes_cover_every_entry_point():
+    """Every entry point the header declares is named in the integration
+    notes, with the reference routine it replaces or its role."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [s for s in declared_symbols() if s not in doc]
+    assert not missing, missing
