@@ -151,11 +151,12 @@ def test_jump_far_into_the_stream(jump_exe):
     assert r.stdout.split() == ["0"]
 
 
-@pytest.mark.parametrize("first", [0, 48 * 1000 * 2 + 1])
-def test_threaded_pair_draw_equals_one_pass(jump_exe, first):
-    """The initial conditions' threaded draw (8 threads over 600,000 pairs)
-    hands every pair the numbers one sequential pass would."""
-    r = subprocess.run([str(jump_exe), "2", "2", "3", "600000", str(first)], capture_output=True, text=True,
+@pytest.mark.parametrize("count,first", [(600000, 0), (600000, 48 * 1000 * 2 + 1), (4097 * 3, 7), (5, 11), (0, 0)])
+def test_threaded_pair_draw_equals_one_pass(jump_exe, count, first):
+    """The initial conditions' threaded draw (up to 8 threads; shares of at
+    least 4,096 pairs, so a few pairs run on one thread and an empty draw
+    starts none) hands every pair the numbers one sequential pass would."""
+    r = subprocess.run([str(jump_exe), "2", "2", "3", str(count), str(first)], capture_output=True, text=True,
                        check=True)
     assert r.stdout.split() == ["0"]
 
