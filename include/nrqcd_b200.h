@@ -87,11 +87,6 @@ void *nrq_cuda_stream(nrq_ctx *ctx);
 enum { NRQ_PROF_CLASSES = 6 };
 int nrq_profile_enable(nrq_ctx *ctx, int enable);
 int nrq_profile_read(nrq_ctx *ctx, int64_t launches[6], double milliseconds[6], double bytes[6]);
-/* Measured arithmetic peaks of this device (TFLOP/s): FP64 FMA and packed
- * FP32 FMA throughput of issue-bound probe kernels (compute-side roofline
- * denominators of the benchmark).                                         */
-int nrq_measure_peaks(nrq_ctx *ctx, double *fp64_tflops, double *fp32_tflops);
-
 /* ---- gauge configuration: src/gaugeconfiguration_su3.f90:33-116 -------- */
 int nrq_gauge_create(nrq_ctx *ctx, nrq_gauge **g);      /* Allocate (:124-140)   */
 int nrq_gauge_destroy(nrq_gauge *g);                    /* Deallocate            */
@@ -352,10 +347,15 @@ int nrq_cn_attach_learned(nrq_cn *cn, nrq_learn *net);
  *
  * Partial sums go into a fixed 128 KiB device array in the library.  That
  * caps the lattice at NRQ_NOALLOC_MAX_SITES sites (for example 160^3);
- * larger lattices return NRQ_ERR_CAPACITY.  The first call on a device looks
- * up the array's address and caches it, so make that first call before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race and must be serialised.                                              */
+ * larger lattices return NRQ_ERR_CAPACITY.  The first call in a CUDA
+ * context looks up the array's address and caches it under the context's
+ * unique id, so make that first call before any stream capture.  The cached
+ * address is not reused in another context: after cudaDeviceReset (or under
+ * another driver-API context) the next call looks it up again, and should
+ * likewise come before any capture.  An error already pending from the
+ * caller's earlier work returns NRQ_ERR_CUDA and is left pending.  All calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised.                                                               */
 #define NRQ_NOALLOC_MAX_SITES 4194304
 int nrq_gauge_energy_noalloc(const int64_t extents[3], const double spacings[4],
                              const double *links_soa, const double *efield_soa,

@@ -69,7 +69,11 @@ def build(verbose: bool = False, extra_flags=None, ptxas_verbose: bool = False) 
                 sys.stdout.write(r.stdout + r.stderr)
             if r.returncode != 0:
                 raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
-    if _newer(LIB, objs):
+    # objects of translation units that no longer exist force a relink
+    stale = [f for f in os.listdir(BUILD_DIR) if f.endswith(".o") and os.path.join(BUILD_DIR, f) not in objs]
+    for f in stale:
+        os.remove(os.path.join(BUILD_DIR, f))
+    if stale or _newer(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcufft", "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -400,10 +400,10 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
   // jump to their share)
   std::vector<double2> R((size_t)16 * V);
   const double twopi = 2.0 * std::acos(-1.0);
-  if (!nrqh::draw_pairs(2, seed, 0, (size_t)16 * V, [&](size_t e, double u1, double u2) {
+  if (!nrqh::draw_pairs_noexcept(2, seed, 0, (size_t)16 * V, [&](size_t e, double u1, double u2) {
         R[(e % 16) * (size_t)V + e / 16] = make_double2(std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2), 0.0);
       })) {
-    ctx->last_error = "transverse_box_init: the random stream could not be positioned";
+    ctx->last_error = "transverse_box_init: the random stream could not be positioned or drawn";
     return NRQ_ERR_BAD_ARG;
   }
   // backward-derivative momentum per direction and coordinate (lattice:963-979):
@@ -682,10 +682,11 @@ extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nef
     // Box-Muller pairs in the reference's order: site, direction, generator
     // (random.f90:238-255); the real part, times sigma, times a0.  Round r
     // starts at number 48 V r of the stream; host threads jump to their share.
-    if (!nrqh::draw_pairs(2, seed, (uint64_t)r * ef.size() * 2, ef.size(), [&](size_t i, double u1, double u2) {
+    if (!nrqh::draw_pairs_noexcept(2, seed, (uint64_t)r * ef.size() * 2, ef.size(),
+                                   [&](size_t i, double u1, double u2) {
           ef[i] = (sigma * (std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2))) * a0;
         })) {
-      ctx->last_error = "equilibrium_init: the random stream could not be positioned";
+      ctx->last_error = "equilibrium_init: the random stream could not be positioned or drawn";
       return NRQ_ERR_BAD_ARG;
     }
     if ((rc = ensure_stage(ctx, sizeof(double) * 24 * V))) return rc;

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <algorithm>
 #include <cstddef>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -255,30 +256,53 @@ bool draw_pairs(int level, int64_t seed, uint64_t first, size_t count, F f, unsi
   nt = std::max(1u, std::min(nt, max_threads));
   nt = (unsigned)std::min<size_t>(nt, (count + min_share - 1) / min_share);
   if (nt == 0) return true;
-  auto share = [&](unsigned t) {
-    const size_t lo = count * t / nt, hi = count * (t + 1) / nt;
-    Ranlxd r;
-    r.init(level, seed);
-    if (!r.jump(first + 2 * (uint64_t)lo)) return false;
-    for (size_t i = lo; i < hi; ++i) {
-      const double u1 = r.next(), u2 = r.next();
-      f(i, u1, u2);
+  // a share never throws: an exception from f (or from the generator) is
+  // kept and rethrown on the calling thread once every worker has joined
+  std::vector<std::exception_ptr> errs(nt);
+  auto share = [&](unsigned t) -> char {
+    try {
+      const size_t lo = count * t / nt, hi = count * (t + 1) / nt;
+      Ranlxd r;
+      r.init(level, seed);
+      if (!r.jump(first + 2 * (uint64_t)lo)) return 0;
+      for (size_t i = lo; i < hi; ++i) {
+        const double u1 = r.next(), u2 = r.next();
+        f(i, u1, u2);
+      }
+      return 1;
+    } catch (...) {
+      errs[t] = std::current_exception();
+      return 0;
     }
-    return true;
   };
   std::vector<std::thread> pool;
   std::vector<char> ok(nt, 1);
   unsigned started = 1;
   try {
+    pool.reserve(nt);
     for (; started < nt; ++started) pool.emplace_back([&, started] { ok[started] = share(started); });
   } catch (...) {  // no more threads: the remaining shares run here
   }
   ok[0] = share(0);
   for (unsigned t = started; t < nt; ++t) ok[t] = share(t);
   for (auto &th : pool) th.join();
+  for (auto &e : errs)
+    if (e) std::rethrow_exception(e);
   for (char c : ok)
     if (!c) return false;
   return true;
+}
+
+// draw_pairs for callers behind the C ABI: an exception (from f, or a
+// thread or vector that could not be created) becomes a false return
+template <class F>
+bool draw_pairs_noexcept(int level, int64_t seed, uint64_t first, size_t count, F f,
+                         unsigned max_threads = 32) noexcept {
+  try {
+    return draw_pairs(level, seed, first, count, f, max_threads);
+  } catch (...) {
+    return false;
+  }
 }
 
 }  // namespace nrqh

@@ -60,11 +60,13 @@ def test_host_stream_equals_oracle(oracle, host_stream, seed, level):
 JUMP_SRC = r'''
 #include <cstdio>
 #include <cstdlib>
+#include <stdexcept>
 #include <vector>
 #include "ranlxd_host.h"
 // mode 0: numbers [n, n + k) after jump(n), for each n on the command line
 // mode 1: jump(n) against jump(n - d) and d calls of next(), far into the stream
 // mode 2: draw_pairs on several threads against one sequential pass
+// mode 3: an exception thrown by the callback reaches the caller
 int main(int argc, char **argv) {
   const int mode = std::atoi(argv[1]), level = std::atoi(argv[2]);
   const long seed = std::atol(argv[3]);
@@ -97,6 +99,18 @@ int main(int argc, char **argv) {
   }
   const size_t count = std::atol(argv[4]);
   const unsigned long long first = std::strtoull(argv[5], nullptr, 10);
+  if (mode == 3) {  // the callback throws at pair argv[6]: caught here, after every worker joined
+    const size_t bad_at = std::atol(argv[6]);
+    try {
+      nrqh::draw_pairs(level, seed, first, count, [&](size_t i, double, double) {
+        if (i == bad_at) throw std::runtime_error("planted");
+      }, 8);
+    } catch (const std::runtime_error &e) {
+      std::printf("caught %s\n", e.what());
+      return 0;
+    }
+    return 4;
+  }
   std::vector<double> got(2 * count), want(2 * count);
   if (!nrqh::draw_pairs(level, seed, first, count, [&](size_t i, double u1, double u2) {
         got[2 * i] = u1;
@@ -191,3 +205,12 @@ def test_oracle_stream_is_the_published_recurrence(oracle, seed, level, pr):
     wrong = pow(pow(b, -1, m), pr + 1, m)
     assert not any({lcg(blocks[k], c) * wrong % m for c in (0, 1)} & {lcg(blocks[k + 1], c) for c in (0, 1)}
                    for k in range(39))
+
+
+@pytest.mark.parametrize("bad_at", [0, 4096 * 3 + 5, 40000 - 1])
+def test_threaded_draw_passes_a_callback_exception_to_the_caller(jump_exe, bad_at):
+    """An exception thrown by the callback on any worker thread (or on the
+    calling thread's own share) is rethrown to the caller after every worker
+    has joined, instead of terminating the process."""
+    r = subprocess.run([str(jump_exe), "3", "2", "3", "40000", "0", str(bad_at)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.split() == ["caught", "planted"], (r.returncode, r.stdout, r.stderr)
