@@ -141,6 +141,9 @@ def run_reference(args, rank):
     if rank != 0:
         return
     from oracle import oracle as oc
+    # rank 0 runs alone on the host: every core it may use (a launcher sets
+    # OMP_NUM_THREADS=1 per rank)
+    oc.set_num_threads(len(os.sched_getaffinity(0)))
     L = args.size
     n = (L, L, L)
     V = L ** 3
@@ -163,7 +166,8 @@ def run_reference(args, rank):
     dt = time.perf_counter() - t0
     value = V * steps / dt
     cores = oc.num_threads()
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "site-updates/s",
+            "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(L, 1),
@@ -653,6 +657,74 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
 
 
 # ------------------------------------------------------------------ our arm
+def measure_fp64_peak(n=8192, reps=5):
+    """FP64 arithmetic peak of this GPU for the compute side of the stencil's
+    roofline: a cuBLAS DGEMM (torch.matmul, float64) of n^3, best of `reps`,
+    CUDA events; measured after the timed region."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1000.0) / 1e12
+
+
+def member_seed(rank):
+    """ranlxd seed of the ensemble member a rank evolves (replicas)."""
+    return 1 + rank
+
+
+def timed_steps(step, steps, dist, timer):
+    """The timed region of every rank: a barrier, `steps` calls of step()
+    between timer.start() and timer.stop() (milliseconds), a barrier, and the
+    max of the durations over the ranks."""
+    if dist is not None:
+        dist.barrier()
+    timer.start()
+    for _ in range(steps):
+        step()
+    ms = timer.stop()
+    if dist is not None:
+        dist.barrier()
+    return max_over_ranks(ms, dist)
+
+
+def whole_job_rate(world, sites, steps, ms):
+    """Site-updates per second of the whole job: every rank's lattice
+    advanced `steps` times within the slowest rank's `ms`."""
+    return world * sites * steps / (ms / 1000.0)
+
+
+class CudaEventTimer:
+    """Device time on `stream` between start() and stop() (milliseconds)."""
+
+    def __init__(self, stream):
+        import torch
+        self.torch = torch
+        self.stream = stream
+
+    def start(self):
+        self.torch.cuda.synchronize()
+        self.e0 = self.torch.cuda.Event(enable_timing=True)
+        self.e1 = self.torch.cuda.Event(enable_timing=True)
+        self.e0.record(self.stream)
+
+    def stop(self):
+        self.e1.record(self.stream)
+        self.e1.synchronize()
+        self.torch.cuda.synchronize()
+        return self.e0.elapsed_time(self.e1)
+
+
 def max_over_ranks(x, dist=None):
     """Max of a per-rank float over all ranks (the timed region's duration);
     identity without a process group.  NCCL reduces a CUDA tensor, gloo a
@@ -666,9 +738,29 @@ def max_over_ranks(x, dist=None):
     return float(t.item())
 
 
+def free_port():
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def relaunch_ranks(n):
+    """`--gpus N` without a launcher: start the N ranks with
+    torch.distributed.run on this node (rendezvous on 127.0.0.1) and return
+    its exit status; rank 0's JSON line passes through."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(relaunch_ranks(args.gpus))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but the launcher started {world} ranks")
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
@@ -714,7 +806,7 @@ def main():
         nrqcd.SetStencil({"register": nrqcd.STENCIL_REGISTER, "tma": nrqcd.STENCIL_TMA,
                           "tensor": nrqcd.STENCIL_TENSOR}[args.stencil])
     g = GaugeConfiguration()
-    g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=1 + rank, identity_links=True)
+    g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=member_seed(rank), identity_links=True)
     h = NRQCDField()
     h.InitSinglePoint(1, 1)
     lib = _capi.load()
@@ -758,29 +850,17 @@ def main():
     # ---------------- timed region
     clocks = ClockSampler(local)
     clocks.start()
-    if dist is not None:
-        dist.barrier()
     torch.cuda.synchronize()
     _capi.profile_enable(ctx, True)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
-    ev1.synchronize()
-    torch.cuda.synchronize()
+    ms = timed_steps(step, args.steps, dist, CudaEventTimer(stream))
     prof = _capi.profile_read(ctx)
     _capi.profile_enable(ctx, False)
-    if dist is not None:
-        dist.barrier()
     clk = clocks.stop()
-    ms = max_over_ranks(ev0.elapsed_time(ev1), dist)
     ms_per_step = ms / args.steps
-    value = world * V * args.steps / (ms / 1000.0)
+    value = whole_job_rate(world, V, args.steps, ms)
     norm_q, norm_a = h.GetNorm_Quark(), h.GetNorm_AntiQ()
     which, tune_ms = nrqcd.StencilInfo()
-    p64, p32 = ctypes.c_double(), ctypes.c_double()
-    _capi.check(lib.nrq_measure_peaks(ctx, ctypes.byref(p64), ctypes.byref(p32)), ctx, "measure_peaks")
+    p64 = measure_fp64_peak()
     stencil = {"in_use": nrqcd.STENCIL_NAMES[which],
                "tuning_ms_per_launch": {"k_cn_mv2": float(tune_ms[0]), "k_cn_mv3_with_vec_s": float(tune_ms[1]),
                                         "k_cn_mv4_with_vec_s": float(tune_ms[2])}}
@@ -846,13 +926,19 @@ def main():
         if os.path.exists(peaks_path):
             peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
         sten = prof["cn_stencil"]
+        # the library's stencil class counts the byte model's bytes of a
+        # 12-column launch: U and E once per species (2 x 624 B) plus 1152 B
+        # per vector stream; the tensor-core stencil's design reads its cached
+        # 6x6 blocks (3456 B) and diagonal matrices (216 B) in place of U and
+        # E, reported beside it and not credited
         achieved = sten["bytes"] / (sten["ms"] / 1000.0) / 1e9 if sten["ms"] > 0 else None
+        tensor = which == nrqcd.STENCIL_TENSOR
+        design_bytes = sten["bytes"] + (sten["launches"] * V * (3456.0 + 216.0 - 1248.0) if tensor else 0.0)
         # FP64 arithmetic of one 12-column stencil launch per site: 2 species x
         # (6 neighbours x 6 columns x 36 + 6 columns x 18) complex FMAs (4 DFMA
         # each, 2 flops per DFMA) plus the block assembly (~270 complex FMAs)
         # (the tensor-core stencil reads the blocks assembled once per update,
         # and its MMA tiles carry 16/12 x 8/6 of these products with padding)
-        tensor = which == nrqcd.STENCIL_TENSOR
         flops_site = 2 * (6 * 6 * 36 + 6 * 18 + (0 if tensor else 270)) * 4 * 2
         fp64_achieved = flops_site * V * sten["launches"] / (sten["ms"] / 1000.0) / 1e12 if sten["ms"] > 0 else None
         step_bytes = sum(v["bytes"] for v in prof.values()) / args.steps
@@ -878,13 +964,18 @@ def main():
                          "traffic": (STENCIL_DRAM_BYTES_PER_SITE * V / 1e9 if tensor else None),
                          "traffic_unit": "GB per launch (ncu capture of one 64^3 update, per site x V)",
                          "algorithmic_GB_per_launch": sten["bytes"] / max(1, sten["launches"]) / 1e9,
+                         "algorithmic_bytes": "per 12-column launch: U and E once per species (2 x 624 B/site) "
+                                              "+ 1152 B/site per vector stream",
+                         "design_bytes_incl_cached_blocks": {
+                             "GB_per_launch": design_bytes / max(1, sten["launches"]) / 1e9,
+                             "GBps": design_bytes / (sten["ms"] / 1000.0) / 1e9 if sten["ms"] > 0 else None,
+                             "frac": (design_bytes / (sten["ms"] / 1000.0) / 1e9 / peak) if sten["ms"] > 0 else None},
                          "launches": sten["launches"], "avg_launch_ms": sten["ms"] / max(1, sten["launches"]),
                          "step_algorithmic_GBps": step_bytes / (ms_per_step / 1000.0) / 1e9,
                          "byte_model_of_the_plan": model,
                          "fp64": {"flops_per_site_per_launch": flops_site, "achieved_tflops": fp64_achieved,
-                                  "peak_tflops": p64.value, "peak_source": "measured (FP64 FMA probe)",
-                                  "frac": fp64_achieved / p64.value if fp64_achieved else None,
-                                  "fp32_packed_peak_tflops": p32.value}},
+                                  "peak_tflops": p64, "peak_source": "measured (cuBLAS DGEMM, torch.matmul)",
+                                  "frac": fp64_achieved / p64 if fp64_achieved else None}},
             "kernel_classes": prof,
             "stencil": stencil,
             "cn": {"iterations_per_step": float(np.mean(its)) if its else None,

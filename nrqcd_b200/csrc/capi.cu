@@ -1068,13 +1068,14 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
 }
 
 namespace {
-// algorithmic bytes of one 12-column stencil launch: vector streams of
-// 12 x 6 complex per site plus the gauge inputs U and E read once, or for
-// the tensor-core stencil its 6x6 blocks (6 x 576 B) and the diagonal
-// colour matrices (216 B) read once
-double mv_bytes(const nrq_ctx *ctx, int mode, bool tensor = false) {
-  const int streams[6] = {2, 3, 5, 3, 3, 3};  // PLAIN, RHS, RES, V, T, RESC
-  return (double)ctx->lat.V * (1152.0 * streams[mode] + (tensor ? 3456.0 + 216.0 : 432.0 + 192.0));
+// algorithmic bytes of one 12-column stencil launch, whichever stencil runs:
+// vector streams of 12 x 6 complex per site plus the gauge inputs U (432 B)
+// and E (192 B) once per species, from which the operator's blocks are
+// formed.  Derived data a stencil reads instead (the tensor-core stencil's
+// cached blocks) is extra traffic and is not counted.
+double mv_bytes(const nrq_ctx *ctx, int mode) {
+  const int streams[6] = {2, 3, 5, 3, 2, 3};  // PLAIN, RHS, RES, V, T, RESC
+  return (double)ctx->lat.V * (1152.0 * streams[mode] + 2.0 * (432.0 + 192.0));
 }
 // the tensor-core stencil's backward blocks are -W^H of the forward ones,
 // which holds when every off-diagonal coefficient is imaginary (real
@@ -1121,7 +1122,7 @@ int mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq
     double sign = 0.0;
     int rc = ensure_blocks(cn, C, g, &sign);
     if (rc) return rc;
-    ProfScope ps(ctx, 0, mv_bytes(ctx, mode, true));
+    ProfScope ps(ctx, 0, mv_bytes(ctx, mode));
     if (nrq::launch_cn_mv4(mode, ctx->lat, C, sign, cn->Wblk, cn->Dsum, cn->Bsum, a, scal_err(cn->scal),
                            ctx->sm_count, ctx->stream) == 0) {
       cn->last_stencil = NRQ_STENCIL_TENSOR;

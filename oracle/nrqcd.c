@@ -38,6 +38,16 @@ int oc_num_threads(void) {
 #endif
 }
 
+/* threads of the following parallel regions (a launcher may have set
+   OMP_NUM_THREADS=1 before the OpenMP runtime loaded) */
+void oc_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
 void oc_heavy_init_single_point(const oc_lattice *L, int64_t lat_index_1based, double *prop_) {
   const int64_t V = oc_volume(L);
   cplx *prop = (cplx *)prop_;

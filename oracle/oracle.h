@@ -122,6 +122,7 @@ void    oc_gauge_transverse_correlators(const oc_lattice *L, const double *links
                                         double *aa, double *ee, double *momenta);
 
 int oc_num_threads(void);
+void oc_set_num_threads(int n);
 
 #ifdef __cplusplus
 }

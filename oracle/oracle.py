@@ -100,6 +100,7 @@ def lib():
                                                            ctypes.c_double, ctypes.c_int64, _dp]),
             "oc_gauge_transverse_correlators": (None, [ctypes.POINTER(Lattice), _dp, _dp, _dp, _dp, _dp]),
             "oc_num_threads": (ctypes.c_int, []),
+            "oc_set_num_threads": (None, [ctypes.c_int]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -355,3 +356,7 @@ def transverse_correlators(n, a, links, efield):
 
 def num_threads():
     return lib().oc_num_threads()
+
+
+def set_num_threads(n):
+    lib().oc_set_num_threads(int(n))
