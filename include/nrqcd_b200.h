@@ -176,7 +176,9 @@ int nrq_heavy_correlators_gconjg(nrq_heavy *h, double out[8]);
  * form: 0 = plain FP64 (BiCGStab, fused stencil/axpy/dot kernels);
  *       1 = precision (FP32 Chebyshev inner iterations inside FP64
  *           iterative refinement to the same tol; real Wilson coefficients).
- * maxits bounds the Krylov iterations (the reference's PETSc default 1e4).  */
+ * maxits bounds the Krylov iterations (the reference's PETSc default 1e4):
+ * BiCGStab iterations of the plain form, FP32 Chebyshev inner steps of the
+ * precision forms (over all refinement passes of one update).              */
 int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double stepwidth, double tol,
                 int64_t maxits, int form, nrq_cn **cn);
 /* FinalizeModule, src/nrqcd.f90:199-212 */

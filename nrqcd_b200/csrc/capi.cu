@@ -1423,7 +1423,10 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
       const double *s = hs + kk * nrq::SC_STRIDE;
       if (s[nrq::SC_BB] > 0) worst = std::max(worst, std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]));
     }
-    const int m = inner_steps(worst / (0.3 * cn->tol));
+    // maxits bounds the FP32 inner steps of the whole update
+    int m = inner_steps(worst / (0.3 * cn->tol));
+    if (inner + m > cn->maxits) m = (int)(cn->maxits - inner);
+    if (m <= 0) break;
     // FP32 inner Chebyshev solve of A^H e = r, then x += e
     float2 *dcur = cn->dA32, *dnext = cn->dB32;
     for (int k = 0; k < m; ++k) {
