@@ -47,7 +47,8 @@ TOL = 1e-12
 # 7,760 and 6,377 B/site)
 STENCIL_DRAM_BYTES_PER_SITE = 7968.0
 # FP64 stencils of the solver, by NRQ_STENCIL_* index
-STENCIL_NAMES = {0: "k_cn_mv2 (register-tiled)", 1: "k_cn_mv3 (TMA-staged)", 2: "k_cn_mv4 (FP64 tensor cores)"}
+STENCIL_NAMES = {0: "k_cn_mv2 (register-tiled)", 1: "k_cn_mv3 (TMA-staged)", 2: "k_cn_mv4 (FP64 tensor cores)",
+                 3: "k_cn_mv5 (FP64 FMA on cached blocks)"}
 
 
 def parse():
@@ -69,7 +70,7 @@ def parse():
     p.add_argument("--no-gluon", action="store_true")
     p.add_argument("--only-gluon", action="store_true", help="print only the gluon-distribution JSON")
     p.add_argument("--only-thermal", action="store_true", help="print only the thermal initial-condition JSON")
-    p.add_argument("--stencil", default="timed", choices=["timed", "register", "tma", "tensor"],
+    p.add_argument("--stencil", default="timed", choices=["timed", "register", "tma", "tensor", "fma"],
                    help="FP64 stencil of the headline step (default: the solver's timed choice)")
     p.add_argument("--only-drift", action="store_true", help="print only the precision-drift JSON")
     return p.parse_args()
@@ -401,7 +402,7 @@ def measure_cn_forms(L, steps, params, tol=1e-10, seed=1):
             e1.synchronize()
             ms = e0.elapsed_time(e1) / steps
             which = ctypes.c_int()
-            tune = np.zeros(3)
+            tune = np.zeros(4)
             _capi.check(lib.nrq_cn_stencil_info(cn, ctypes.byref(which), _capi.dptr(tune)), lat.ctx, "stencil_info")
             out[name] = {"s_per_step": ms / 1000.0, "tol": tol,
                          "max_rel_residual": max(st["max_rel_residual"] for st in stats),
@@ -804,7 +805,7 @@ def main():
     nrqcd.InitModule(MASS, WILSON, 1.0, TOL)
     if args.stencil != "timed":
         nrqcd.SetStencil({"register": nrqcd.STENCIL_REGISTER, "tma": nrqcd.STENCIL_TMA,
-                          "tensor": nrqcd.STENCIL_TENSOR}[args.stencil])
+                          "tensor": nrqcd.STENCIL_TENSOR, "fma": nrqcd.STENCIL_FMA}[args.stencil])
     g = GaugeConfiguration()
     g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=member_seed(rank), identity_links=True)
     h = NRQCDField()
@@ -863,7 +864,8 @@ def main():
     p64 = measure_fp64_peak()
     stencil = {"in_use": nrqcd.STENCIL_NAMES[which],
                "tuning_ms_per_launch": {"k_cn_mv2": float(tune_ms[0]), "k_cn_mv3_with_vec_s": float(tune_ms[1]),
-                                        "k_cn_mv4_with_vec_s": float(tune_ms[2])}}
+                                        "k_cn_mv4_with_vec_s": float(tune_ms[2]),
+                                        "k_cn_mv5_with_vec_s": float(tune_ms[3])}}
 
     # ---------------- end-to-end through the C ABI with host buffers
     e2e = None
@@ -932,8 +934,9 @@ def main():
         # 6x6 blocks (3456 B) and diagonal matrices (216 B) in place of U and
         # E, reported beside it and not credited
         achieved = sten["bytes"] / (sten["ms"] / 1000.0) / 1e9 if sten["ms"] > 0 else None
-        tensor = which == nrqcd.STENCIL_TENSOR
-        design_bytes = sten["bytes"] + (sten["launches"] * V * (3456.0 + 216.0 - 1248.0) if tensor else 0.0)
+        tensor = which in (nrqcd.STENCIL_TENSOR, nrqcd.STENCIL_FMA)
+        blk_bytes = 3552.0 if which == nrqcd.STENCIL_FMA else 3456.0
+        design_bytes = sten["bytes"] + (sten["launches"] * V * (blk_bytes + 216.0 - 1248.0) if tensor else 0.0)
         # FP64 arithmetic of one 12-column stencil launch per site: 2 species x
         # (6 neighbours x 6 columns x 36 + 6 columns x 18) complex FMAs (4 DFMA
         # each, 2 flops per DFMA) plus the block assembly (~270 complex FMAs)

@@ -186,15 +186,24 @@ int nrq_cn_finalize(nrq_cn *cn);
 /* FP64 stencils of the solver (no reference counterpart: PETSc applies its
  * assembled matrix; these apply the same operator matrix-free).
  * REGISTER: register-tiled; TMA: TMA-staged; TENSOR: FP64 tensor-core MMAs
- * on per-update 6x6 blocks (real Wilson coefficients; otherwise the TMA or
+ * on per-update 6x6 blocks; FMA: FP64 FMAs on the same per-update blocks
+ * (TENSOR and FMA need real Wilson coefficients; otherwise the TMA or
  * register-tiled stencil runs).                                           */
 #define NRQ_STENCIL_REGISTER 0
 #define NRQ_STENCIL_TMA 1
 #define NRQ_STENCIL_TENSOR 2
+#define NRQ_STENCIL_FMA 3
 /* The stencil the solver uses and the per-launch milliseconds of each one
  * measured on its first update (index = NRQ_STENCIL_*; -1 before it, or for
  * one that does not apply to the lattice or coefficients).               */
-int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[3]);
+int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[4]);
+/* Test hook of the FMA stencil's bounded pipeline waits (no reference
+ * counterpart).  wait_cycles bounds every wait (0 restores the default,
+ * about two seconds); stall_load >= 0 makes the stencil's loader stop
+ * before that load of every CTA, so the wait for it runs out: the update
+ * then returns NRQ_ERR_TIMEOUT, nothing faults, and the context stays
+ * usable.  -1 (the default) stops nowhere.                                */
+int nrq_cn_set_wait_test(nrq_cn *cn, int64_t wait_cycles, int stall_load);
 /* Force a stencil (NRQ_STENCIL_*) or restore the timed choice (-1).
  * NRQ_ERR_BAD_ARG if the stencil cannot describe this lattice.            */
 int nrq_cn_set_stencil(nrq_cn *cn, int stencil);

@@ -94,6 +94,7 @@ SIGNATURES = {
                                    ctypes.c_int64, ctypes.c_int, _pp]),
     "nrq_cn_finalize": (ctypes.c_int, [_vp]),
     "nrq_cn_stencil_info": (ctypes.c_int, [_vp, _ip, _dp]),
+    "nrq_cn_set_wait_test": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int]),
     "nrq_cn_set_stencil": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_cn_set_history_guess": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_heavy_update_cn": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,

@@ -1025,16 +1025,23 @@ extern "C" int nrq_cn_init(nrq_ctx *ctx, double mass, const double c[8], double 
   return NRQ_OK;
 }
 
-extern "C" int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[3]) {
+extern "C" int nrq_cn_stencil_info(const nrq_cn *cn, int *stencil, double ms[4]) {
   if (!cn) return NRQ_ERR_BAD_ARG;
   if (stencil) *stencil = cn->stencil;
   if (ms)
-    for (int k = 0; k < 3; ++k) ms[k] = cn->tune_ms[k];
+    for (int k = 0; k < 4; ++k) ms[k] = cn->tune_ms[k];
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_set_wait_test(nrq_cn *cn, int64_t wait_cycles, int stall_load) {
+  if (!cn || wait_cycles < 0 || stall_load < -1) return NRQ_ERR_BAD_ARG;
+  cn->wait_cycles = wait_cycles > 0 ? (long long)wait_cycles : nrq_wait_cycles_default;
+  cn->stall_load = stall_load;
   return NRQ_OK;
 }
 
 extern "C" int nrq_cn_set_stencil(nrq_cn *cn, int stencil) {
-  if (!cn || stencil < -1 || stencil > NRQ_STENCIL_TENSOR) return NRQ_ERR_BAD_ARG;
+  if (!cn || stencil < -1 || stencil > NRQ_STENCIL_FMA) return NRQ_ERR_BAD_ARG;
   if (stencil > NRQ_STENCIL_REGISTER && !cn->tma_ok) {
     cn->ctx->last_error = "nrq_cn_set_stencil: tensor maps cannot describe this lattice";
     return NRQ_ERR_BAD_ARG;
@@ -1059,7 +1066,7 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
                   (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->s, (void *)cn->scal,
                   (void *)cn->partials, (void *)cn->U32, (void *)cn->DE32, (void *)cn->D32, (void *)cn->B32,
                   (void *)cn->r32, (void *)cn->dA32, (void *)cn->dB32, (void *)cn->e32, (void *)cn->bounds,
-                  (void *)cn->Wblk})
+                  (void *)cn->Wblk, (void *)cn->Wblk5})
     if (p) cudaFree(p);
   if (cn->h_scal) cudaFreeHost(cn->h_scal);
   if (cn->h_bounds) cudaFreeHost(cn->h_bounds);
@@ -1087,9 +1094,8 @@ bool offdiag_imaginary(const nrq::CnCoef &C) {
 }
 // +1 / -1 when the current blocks were built for C / for the coefficients
 // whose off-diagonal terms are those of C negated (A vs A^H), 0 otherwise
-double blocks_sign(const nrq_cn *cn, const nrq::CnCoef &C) {
-  if (!cn->w_valid) return 0.0;
-  const nrq::CnCoef &w = cn->w_coef;
+double blocks_sign(bool valid, const nrq::CnCoef &w, const nrq::CnCoef &C) {
+  if (!valid) return 0.0;
   bool same = true, neg = true;
   for (int sp = 0; sp < 2; ++sp) {
     same = same && C.kin[sp].im == w.kin[sp].im && C.so[sp].im == w.so[sp].im;
@@ -1099,7 +1105,7 @@ double blocks_sign(const nrq_cn *cn, const nrq::CnCoef &C) {
 }
 int ensure_blocks(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *sign) {
   nrq_ctx *ctx = cn->ctx;
-  *sign = blocks_sign(cn, C);
+  *sign = blocks_sign(cn->w_valid, cn->w_coef, C);
   if (*sign != 0.0) return NRQ_OK;
   const int64_t V = ctx->lat.V;
   if (!cn->Wblk) NRQ_CUDA_TRY(ctx, cudaMalloc((void **)&cn->Wblk, sizeof(double2) * 216 * V));
@@ -1112,12 +1118,40 @@ int ensure_blocks(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *
   *sign = 1.0;
   return check_launch(ctx, "k_cn_blocks");
 }
+// the FMA stencil's blocks (row-major, 37 entries per block)
+int ensure_blocks5(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *sign) {
+  nrq_ctx *ctx = cn->ctx;
+  *sign = blocks_sign(cn->w5_valid, cn->w5_coef, C);
+  if (*sign != 0.0) return NRQ_OK;
+  const int64_t V = ctx->lat.V;
+  if (!cn->Wblk5)
+    NRQ_CUDA_TRY(ctx, cudaMalloc((void **)&cn->Wblk5, sizeof(double2) * nrq::cn_mv5_block_entries(V)));
+  {
+    ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 3552.0));
+    nrq::launch_cn_blocks5(ctx->lat, C, g->U, cn->DE, cn->Wblk5, ctx->stream);
+  }
+  cn->w5_coef = C;
+  cn->w5_valid = true;
+  *sign = 1.0;
+  return check_launch(ctx, "k_cn_blocks5");
+}
 // The stencil launch of one 12-column application.  The tensor-core stencil
 // needs imaginary off-diagonal coefficients and tensor maps; otherwise the
 // TMA-staged stencil runs, and without tensor maps the register-tiled one.
 // cn->last_stencil records which ran (the partial rows it left).
 int mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq::MvArgs &a) {
   nrq_ctx *ctx = cn->ctx;
+  if (cn->stencil == NRQ_STENCIL_FMA && offdiag_imaginary(C)) {
+    double sign = 0.0;
+    int rc = ensure_blocks5(cn, C, g, &sign);
+    if (rc) return rc;
+    ProfScope ps(ctx, 0, mv_bytes(ctx, mode));
+    if (nrq::launch_cn_mv5(mode, ctx->lat, C, sign, cn->Wblk5, cn->Dsum, cn->Bsum, a, scal_err(cn->scal),
+                           ctx->sm_count, ctx->stream, cn->wait_cycles, cn->stall_load) == 0) {
+      cn->last_stencil = NRQ_STENCIL_FMA;
+      return NRQ_OK;
+    }
+  }
   if (cn->stencil == NRQ_STENCIL_TENSOR && offdiag_imaginary(C)) {
     double sign = 0.0;
     int rc = ensure_blocks(cn, C, g, &sign);
@@ -1147,7 +1181,7 @@ int mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq
 // the MV_T input: the register-tiled stencil forms s = r - alpha v on the
 // fly, the staged ones read a materialised s
 bool mv_t_needs_s(const nrq_cn *cn, const nrq::CnCoef &CH) {
-  if (cn->stencil == NRQ_STENCIL_TENSOR && offdiag_imaginary(CH)) return true;
+  if ((cn->stencil == NRQ_STENCIL_TENSOR || cn->stencil == NRQ_STENCIL_FMA) && offdiag_imaginary(CH)) return true;
   return cn->tma_ok && cn->stencil != NRQ_STENCIL_REGISTER;
 }
 void fin(nrq_cn *cn, int stage) {
@@ -1157,6 +1191,7 @@ void fin(nrq_cn *cn, int stage) {
   int64_t rows = cn->nblocks;
   if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TMA) rows = 3 * cn->nblocks;
   if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TENSOR) rows = nrq::cn_mv4_rows(ctx->lat.V, ctx->sm_count);
+  if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_FMA) rows = nrq::cn_mv5_rows(ctx->lat.V, ctx->sm_count);
   ProfScope ps(ctx, 2, (double)rows * 12 * 3 * 8);
   nrq::launch_cn_finalize(stage, rows, cn->partials, cn->scal, cn->tol, ctx->stream);
 }
@@ -1186,9 +1221,9 @@ int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
   NRQ_CUDA_TRY(ctx, cudaEventCreate(&e0));
   NRQ_CUDA_TRY(ctx, cudaEventCreate(&e1));
   int rc = NRQ_OK;
-  for (int which = 0; which < 3 && !rc; ++which) {
+  for (int which = 0; which < 4 && !rc; ++which) {
     cn->tune_ms[which] = -1.0;
-    if (which == NRQ_STENCIL_TENSOR && !tensor) continue;
+    if ((which == NRQ_STENCIL_TENSOR || which == NRQ_STENCIL_FMA) && !tensor) continue;
     cn->stencil = which;
     for (int r = 0; r < reps + 1 && !rc; ++r) {
       if (r == 1) cudaEventRecord(e0, st);
@@ -1219,21 +1254,27 @@ int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
     cudaEventElapsedTime(&ms, e0, e1);
     if (cn->last_stencil == which) cn->tune_ms[which] = ms / reps;
   }
-  // the tensor-core stencil also builds its blocks once per update: charge
-  // that against the launches an update makes (about 10 for the plain
-  // BiCGStab solve, 3 for the precision forms: right-hand side and
-  // refinement residuals)
-  double build_ms = 0.0;
-  if (!rc && cn->tune_ms[NRQ_STENCIL_TENSOR] > 0.0) {
-    cn->w_valid = false;
+  // the block stencils also build their blocks once per update: charge that
+  // against the launches an update makes (about 10 for the plain BiCGStab
+  // solve, 3 for the precision forms: right-hand side and refinement
+  // residuals)
+  double build_ms[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int which : {NRQ_STENCIL_TENSOR, NRQ_STENCIL_FMA}) {
+    if (rc || cn->tune_ms[which] <= 0.0) continue;
     double sign = 0.0;
     cudaEventRecord(e0, st);
-    rc = ensure_blocks(cn, CH, g, &sign);
+    if (which == NRQ_STENCIL_TENSOR) {
+      cn->w_valid = false;
+      rc = ensure_blocks(cn, CH, g, &sign);
+    } else {
+      cn->w5_valid = false;
+      rc = ensure_blocks5(cn, CH, g, &sign);
+    }
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    build_ms = ms;
+    build_ms[which] = ms;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1241,11 +1282,9 @@ int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
   if (rc) return rc;
   if ((rc = check_launch(ctx, "stencil tuning"))) return rc;
   const double per_update = cn->form == 0 ? 10.0 : 3.0;
-  auto cost = [&](int which) {
-    return per_update * cn->tune_ms[which] + (which == NRQ_STENCIL_TENSOR ? build_ms : 0.0);
-  };
+  auto cost = [&](int which) { return per_update * cn->tune_ms[which] + build_ms[which]; };
   int best = NRQ_STENCIL_REGISTER;
-  for (int which = 1; which < 3; ++which)
+  for (int which = 1; which < 4; ++which)
     if (cn->tune_ms[which] > 0.0 && cost(which) < cost(best)) best = which;
   cn->stencil = best;
   return NRQ_OK;
@@ -1256,7 +1295,8 @@ int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
   if (rc) return rc;
   ProfScope ps(ctx, 3, (double)ctx->lat.V * (432.0 + 192.0));
   nrq::launch_cn_prepare(ctx->lat, g->U, g->E, cn->Dsum, cn->Bsum, cn->DE, ctx->stream);
-  cn->w_valid = false;  // the tensor-core blocks follow the new gauge field on demand
+  cn->w_valid = false;  // the cached blocks follow the new gauge field on demand
+  cn->w5_valid = false;
   return check_launch(ctx, "k_cn_prepare");
 }
 }  // namespace

@@ -116,6 +116,8 @@ inline void hist_push(nrq_heavy *h) {
 struct nrq_learn;
 
 struct nrq_cn_stats_internal;
+// about two seconds at 2 GHz: the default bound of a pipeline wait
+constexpr long long nrq_wait_cycles_default = 4000000000LL;
 
 struct nrq_cn {
   nrq_ctx *ctx = nullptr;
@@ -133,7 +135,8 @@ struct nrq_cn {
   // Krylov vectors, 72 planes each
   double2 *b = nullptr, *x = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr,
           *t = nullptr, *s = nullptr;
-  // FP64 stencil (NRQ_STENCIL_*): register-tiled, TMA-staged or tensor-core.
+  // FP64 stencil (NRQ_STENCIL_*): register-tiled, TMA-staged, tensor-core
+  // or FMA on cached blocks.
   // Chosen by timing the applicable ones on the first update (tune_ms, per
   // launch) unless forced; tma_ok: tensor maps can describe the lattice.
   // last_stencil: the stencil of the latest launch (its partial-row count).
@@ -142,7 +145,7 @@ struct nrq_cn {
   int last_stencil = 0;
   bool tma_ok = false;
   bool stencil_tuned = false;
-  double tune_ms[3] = {-1.0, -1.0, -1.0};
+  double tune_ms[4] = {-1.0, -1.0, -1.0, -1.0};
   // plain form: start from 2b - psi + 2 t1 - t2 with the field's history of
   // corrections (FP32); on by default
   bool history_guess = true;
@@ -152,6 +155,14 @@ struct nrq_cn {
   double2 *Wblk = nullptr;
   bool w_valid = false;
   nrq::CnCoef w_coef{};
+  // FP64 FMA stencil: the same blocks, row-major, 37 entries per block
+  double2 *Wblk5 = nullptr;
+  bool w5_valid = false;
+  nrq::CnCoef w5_coef{};
+  // bound of the FMA stencil's pipeline waits (clock cycles) and, for the
+  // test of the timeout path, the load its producer stops before (-1: none)
+  long long wait_cycles = nrq_wait_cycles_default;
+  int stall_load = -1;
   // precision form (form 1): FP32 copies of the per-step matrices and the
   // FP32 Chebyshev vectors; spectral bounds of the hermitian part
   float2 *U32 = nullptr, *DE32 = nullptr, *D32 = nullptr;

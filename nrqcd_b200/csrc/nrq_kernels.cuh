@@ -136,6 +136,18 @@ int64_t cn_mv4_units(int64_t V);
 int64_t cn_mv4_rows(int64_t V, int sm_count);
 int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double2 *W, const double2 *Dsum,
                   const double *Bsum, const MvArgs &a, int *err, int sm_count, cudaStream_t st);
+// FP64 FMA stencil (cn_mv5.cu) on the same forward blocks, stored row-major
+// with 37 entries per block (cn_mv5_block_entries complex in all); the same
+// conditions as the tensor-core stencil.  wait_cycles bounds every pipeline
+// wait; stall_load >= 0 stops the producer before that load (the test of the
+// timeout path).  One partial row per CTA (cn_mv5_rows).
+void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, cudaStream_t st);
+int64_t cn_mv5_units(int64_t V);
+int64_t cn_mv5_rows(int64_t V, int sm_count);
+int64_t cn_mv5_block_entries(int64_t V);
+int launch_cn_mv5(int mode, Lat L, const CnCoef &C, double nb_sign, const double2 *W, const double2 *Dsum,
+                  const double *Bsum, const MvArgs &a, int *err, int sm_count, cudaStream_t st,
+                  long long wait_cycles, int stall_load);
 // finalize stages: 0 = after RES (rr, bb), 1 = alpha (rh.v), 2 = omega (t.s, t.t), 3 = beta (rh.r, r.r)
 void launch_cn_finalize(int stage, int64_t nblocks, const double *partials, double *scal, double tol,
                         cudaStream_t st);

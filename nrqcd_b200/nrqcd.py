@@ -68,8 +68,9 @@ def solver_handle():
 STENCIL_REGISTER = 0  # register-tiled FP64 stencil (k_cn_mv2)
 STENCIL_TMA = 1       # TMA-staged FP64 stencil (k_cn_mv3)
 STENCIL_TENSOR = 2    # FP64 tensor-core stencil on per-update 6x6 blocks (k_cn_mv4)
+STENCIL_FMA = 3       # FP64 FMA stencil on the same per-update blocks (k_cn_mv5)
 STENCIL_NAMES = {STENCIL_REGISTER: "k_cn_mv2 (register-tiled)", STENCIL_TMA: "k_cn_mv3 (TMA-staged)",
-                 STENCIL_TENSOR: "k_cn_mv4 (FP64 tensor cores)"}
+                 STENCIL_TENSOR: "k_cn_mv4 (FP64 tensor cores)", STENCIL_FMA: "k_cn_mv5 (FP64 FMA on cached blocks)"}
 
 
 def SetStencil(stencil=None):
@@ -88,11 +89,19 @@ def SetHistoryGuess(on=True):
                 f"Error in {modulename}: history guess")
 
 
+def SetWaitTest(wait_cycles=0, stall_load=-1):
+    """Test hook of the FMA stencil's bounded pipeline waits: the bound in
+    clock cycles (0: the default, about two seconds) and the load its loader
+    stops before (-1: none), so that the wait for it runs out."""
+    _capi.check(_capi.load().nrq_cn_set_wait_test(solver_handle(), int(wait_cycles), int(stall_load)),
+                lattice.context(), f"Error in {modulename}: wait test")
+
+
 def StencilInfo():
     """(stencil in use, per-launch ms of each stencil timed on the first
     update; -1 where not timed)."""
     which = ctypes.c_int()
-    ms = np.zeros(3)
+    ms = np.zeros(4)
     _capi.check(_capi.load().nrq_cn_stencil_info(solver_handle(), ctypes.byref(which), _capi.dptr(ms)),
                 lattice.context(), f"Error in {modulename}: stencil info")
     return int(which.value), ms

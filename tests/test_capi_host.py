@@ -131,7 +131,7 @@ EXPECTED_SYMBOLS = {
     "nrq_heavy_init_single_point", "nrq_heavy_norms", "nrq_heavy_correlators", "nrq_heavy_correlators_gconjg",
     "nrq_heavy_update_cn",
     "nrq_cn_init", "nrq_cn_finalize", "nrq_cn_apply", "nrq_cn_stencil_info", "nrq_cn_set_stencil",
-    "nrq_cn_set_history_guess", "nrq_cn_attach_learned",
+    "nrq_cn_set_history_guess", "nrq_cn_attach_learned", "nrq_cn_set_wait_test",
     "nrq_cn_batch_create", "nrq_cn_batch_destroy", "nrq_cn_batch_update", "nrq_cn_batch_info",
     "nrq_cn_batch_residuals", "nrq_cn_batch_attach_learned",
     "nrq_ensemble_create", "nrq_ensemble_destroy", "nrq_ensemble_step",

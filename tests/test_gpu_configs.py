@@ -25,7 +25,12 @@ envelope at the same step, and never below 1e-13.  The solves run to a
 relative residual of 1e-12 on the GPU and 1e-14 in the oracle; each CN step
 then differs by at most about 1e-12 per propagator entry (amplitude <= 1/sqrt 6),
 and the differences of k steps add up to at most k times that: the
-propagator tolerance after k coupled steps is 2e-12 k."""
+propagator tolerance after k coupled steps is 2e-12 k, and the norms
+likewise agree to 2e-12 k.  Energies after long evolutions are compared
+within 50 times the oracle's own one-ulp envelope of the energy (never below
+1e-12 relative): a sum over every plaquette, it magnifies the fields'
+rounding-level differences (16^3 after 200 leapfrog steps: 4e-11 absolute,
+1.8e-12 relative)."""
 import numpy as np
 import pytest
 
@@ -46,7 +51,7 @@ def initial_condition(oracle, n):
 def leapfrog_with_envelope(oracle, n, links, ef, marks):
     """The oracle's leapfrog from (links, ef) and from the same field with
     every E component one ulp higher: {step: (links, ef, envelope_links,
-    envelope_efield)} at the given steps."""
+    envelope_efield, envelope_energy)} at the given steps."""
     l1, e1 = links.copy(), ef.copy()
     l2, e2 = links.copy(), np.nextafter(ef, np.inf)
     out = {}
@@ -54,13 +59,20 @@ def leapfrog_with_envelope(oracle, n, links, ef, marks):
         oracle.gauge_update(n, A, l1, e1, 1.0)
         oracle.gauge_update(n, A, l2, e2, 1.0)
         if s in marks:
-            out[s] = (l1.copy(), e1.copy(), float(np.abs(l1 - l2).max()), float(np.abs(e1 - e2).max()))
+            de = abs(oracle.energy(n, A, l1, e1) - oracle.energy(n, A, l2, e2))
+            out[s] = (l1.copy(), e1.copy(), float(np.abs(l1 - l2).max()), float(np.abs(e1 - e2).max()), de)
     return out
+
+
+def energy_tol(e, envelope):
+    """An energy after a long evolution: 50 times the oracle's own one-ulp
+    envelope of it, and never below 1e-12 relative."""
+    return max(1e-12 * abs(e), 50 * envelope)
 
 
 def assert_leapfrog_parity(g, ref, step):
     gl, ge = g.download()
-    lref, eref, env_l, env_e = ref[step]
+    lref, eref, env_l, env_e, _ = ref[step]
     dl, de = float(np.abs(gl - lref).max()), float(np.abs(ge - eref).max())
     assert dl <= max(1e-13, 50 * env_l), (step, dl, env_l)
     assert de <= max(1e-14, 50 * env_e), (step, de, env_e)
@@ -86,9 +98,9 @@ def test_c1_16cubed_leapfrog_then_coupled_steps(oracle):
             g.Update(1.0)
             if s in marks:
                 assert_leapfrog_parity(g, ref, s)
-        lf_links, lf_ef = ref[200][0], ref[200][1]
+        lf_links, lf_ef, env_energy = ref[200][0], ref[200][1], ref[200][4]
         e_lf = g.GetEnergy()
-        assert abs(e_lf - oracle.energy(n, A, lf_links, lf_ef)) <= 1e-12 * abs(e_lf)
+        assert abs(e_lf - oracle.energy(n, A, lf_links, lf_ef)) <= energy_tol(e_lf, env_energy)
 
         # 100 coupled steps, the driver's order: CN step, then leapfrog step
         h = NRQCDField()
@@ -109,14 +121,15 @@ def test_c1_16cubed_leapfrog_then_coupled_steps(oracle):
                 assert np.abs(gl - ol).max() <= 1e-13 and np.abs(ge - oe).max() <= 1e-14, s
         # observables after the coupled loop, against the oracle's
         e_end = g.GetEnergy()
-        assert abs(e_end - oracle.energy(n, A, ol, oe)) <= 1e-12 * abs(e_end)
+        assert abs(e_end - oracle.energy(n, A, ol, oe)) <= energy_tol(e_end, env_energy)
         drift_gpu = abs(e_end - e_start) / abs(e_start)
         drift_oracle = abs(oracle.energy(n, A, ol, oe) - e_start) / abs(e_start)
-        assert abs(drift_gpu - drift_oracle) <= 1e-11
+        assert abs(drift_gpu - drift_oracle) <= energy_tol(e_end, env_energy) / abs(e_start)
         assert g.GetGdeviation() <= 1e-12 and abs(g.GetDeviationFromGaussLaw()) <= 1e-12
         assert abs(oracle.gauss_maxnorm(n, A, ol, oe) - g.GetGdeviation()) <= 1e-13
         nq, na = h.GetNorm_Quark(), h.GetNorm_AntiQ()
-        assert abs(nq - oracle.heavy_norm(n, oq)) <= 1e-12 and abs(na - oracle.heavy_norm(n, oa)) <= 1e-12
+        assert abs(nq - oracle.heavy_norm(n, oq)) <= 2 * 100 * TOL
+        assert abs(na - oracle.heavy_norm(n, oa)) <= 2 * 100 * TOL
         assert abs(nq - 1.0) <= 100 * TOL and abs(na - 1.0) <= 100 * TOL
 
         # forward then backward: leapfrog(-1) then CN(-1) undoes a coupled step
@@ -164,8 +177,9 @@ def test_c2_32cubed_thousand_leapfrog_steps_then_cn(oracle, c2_fields, mass):
             if s in (1, 10):
                 gq, ga = h.download()
                 assert np.abs(gq - oq).max() <= 2e-12 * s and np.abs(ga - oa).max() <= 2e-12 * s, s
-        assert abs(h.GetNorm_Quark() - oracle.heavy_norm(n, oq)) <= 1e-12
-        assert abs(h.GetNorm_AntiQ() - oracle.heavy_norm(n, oa)) <= 1e-12
+        # each of the 10 solves may move the norm by about its residual
+        assert abs(h.GetNorm_Quark() - oracle.heavy_norm(n, oq)) <= 2 * 10 * TOL
+        assert abs(h.GetNorm_AntiQ() - oracle.heavy_norm(n, oa)) <= 2 * 10 * TOL
         corr = h.GetMesoncorrelators()
         want = oracle.meson_correlators(n, oq, oa)
         for k, v in want.items():
@@ -181,7 +195,7 @@ def c64(oracle):
     return n, links, ef
 
 
-@pytest.mark.parametrize("stencil", [nrqcd.STENCIL_REGISTER, nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR])
+@pytest.mark.parametrize("stencil", [nrqcd.STENCIL_REGISTER, nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR, nrqcd.STENCIL_FMA])
 def test_64cubed_operator_every_stencil(oracle, c64, stencil):
     """One A and one A^H application at the headline size: the tensor-core
     stencil runs here with many units per CTA, a regime smaller lattices do

@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 A = (0.05, 1.0, 1.0, 1.0)
 N = (8, 8, 8)
 M, C = 1.0, [1.0, 1.0, 1.0, 1.0]
-STENCILS = [nrqcd.STENCIL_REGISTER, nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR]
+STENCILS = [nrqcd.STENCIL_REGISTER, nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR, nrqcd.STENCIL_FMA]
 
 
 def raw_update(h, g):
@@ -96,3 +96,32 @@ def test_nan_in_a_field_reports_nonfinite(oracle, where, form, tol, stencil):
         # the same context, clean fields: the next step is right
         del g, h
         clean_step_matches_oracle(oracle, links, ef, tol)
+
+
+@pytest.mark.parametrize("form,tol", [(nrqcd.FORM_PLAIN_FP64, 1e-12), (nrqcd.FORM_PRECISION, 1e-10)])
+def test_pipeline_wait_that_runs_out_reports_timeout(oracle, form, tol):
+    """The FMA stencil's loader stops before its fourth load in every CTA
+    (a load that nothing will issue), with the waits bounded at about a
+    millisecond: the consumers' wait for it runs out, the stencil records
+    NRQ_ERR_TIMEOUT and drains the loads it did issue, the update returns
+    NRQ_ERR_TIMEOUT, and the same context then runs a clean step."""
+    links, ef = oracle.transverse_box(N, A, 3.0, 1.0, 0.0, 5, identity_links=False)
+    with lattice_ctx(N, A, cn=(M, C, 1.0, tol, 10000, form)):
+        nrqcd.SetStencil(nrqcd.STENCIL_FMA)
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        nrqcd.SetWaitTest(wait_cycles=2_000_000, stall_load=3)
+        rc, st = raw_update(h, g)
+        assert rc == _capi.NRQ_ERR_TIMEOUT, (rc, st)
+        assert b"wait" in _capi.load().nrq_last_error(_capi_ctx())
+        nrqcd.SetWaitTest()
+        del g, h
+        clean_step_matches_oracle(oracle, links, ef, tol)
+        assert nrqcd.StencilInfo()[0] == nrqcd.STENCIL_FMA
+
+
+def _capi_ctx():
+    from nrqcd_b200 import lattice
+    return lattice.context()

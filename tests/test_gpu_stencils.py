@@ -1,14 +1,14 @@
 """GPU parity of each FP64 stencil of the Crank-Nicolson solver (register-
-tiled, TMA-staged, FP64 tensor-core), forced one at a time, against the
-oracle through the C ABI.
+tiled, TMA-staged, FP64 tensor-core, FP64 FMA on cached blocks), forced one
+at a time, against the oracle through the C ABI.
 
-The tensor-core stencil applies per-update 6x6 blocks and derives the
+The tensor-core and FMA stencils apply per-update 6x6 blocks and derive the
 backward blocks from the forward ones (-W^H), which needs real Wilson
 coefficients; with complex ones the solver runs the TMA-staged stencil
 instead, and the results must not change.  Lattices cover a partial last
-16-site unit (V = 216), rows shorter than a unit (4^3, every x neighbour
-wraps inside the tiles), rows of exactly one unit (16 x 4 x 4) and units
-spanning rows (10 x 6 x 4).
+unit (V = 216; units of 16 and 20 sites), rows shorter than a unit (4^3,
+every x neighbour wraps inside the tiles), rows of exactly one 16-site unit
+(16 x 4 x 4) and units spanning rows (10 x 6 x 4).
 
 Tolerances as for the other FP64 parity tests: matvec 1e-13 relative, CN
 steps to kspTol 1e-13 agree with the oracle to 5e-13 absolute."""
@@ -21,7 +21,7 @@ from tests.gpu_util import lattice_ctx
 pytestmark = pytest.mark.gpu
 
 A = (0.05, 1.0, 1.0, 1.0)
-STENCILS = [nrqcd.STENCIL_REGISTER, nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR]
+STENCILS = [nrqcd.STENCIL_REGISTER, nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR, nrqcd.STENCIL_FMA]
 SHAPES = [(4, 4, 4), (6, 6, 6), (16, 4, 4), (10, 6, 4)]
 
 
@@ -85,7 +85,7 @@ def test_cn_steps_match_oracle(oracle, stencil, n):
     assert np.abs(gq - q).max() < 5e-13 and np.abs(ga - an).max() < 5e-13
 
 
-@pytest.mark.parametrize("stencil", [nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR])
+@pytest.mark.parametrize("stencil", [nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR, nrqcd.STENCIL_FMA])
 def test_precision_form_residual_stencil(oracle, stencil):
     """The FP64 refinement residual (FP32 outputs) of the precision form."""
     n = (8, 8, 8)
@@ -134,7 +134,7 @@ def test_stencils_agree_and_timed_choice(oracle):
 def test_staged_stencils_rejected_for_odd_volume():
     with lattice_ctx((5, 5, 5), A, cn=(1.0, [1, 1, 1, 1], 1.0, 1e-12)):
         nrqcd.SetStencil(nrqcd.STENCIL_REGISTER)
-        for stencil in (nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR):
+        for stencil in (nrqcd.STENCIL_TMA, nrqcd.STENCIL_TENSOR, nrqcd.STENCIL_FMA):
             with pytest.raises(NrqcdError):
                 nrqcd.SetStencil(stencil)
         with pytest.raises(NrqcdError):
