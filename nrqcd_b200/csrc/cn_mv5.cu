@@ -26,8 +26,9 @@
 // 32-site unit) and one producer warp.  Ten loads per unit, per stage and species
 // (stage 0: diagonal matrices, +x and -x; 1: +y; 2: -y; 3: +z; 4: -z): a
 // spinor tile (34 sites x 36 planes) and a block tile (34 sites x 36 entry
-// planes) by TMA, into a ring of four shared-memory buffers completed on
-// mbarriers.  The producer refills a buffer once the four consumer warps of
+// planes) by TMA, into a ring of five shared-memory buffers completed on
+// mbarriers; the unit's diagonal matrices go with its first load into one
+// of two further buffers.  The producer refills a buffer once the four consumer warps of
 // its species released it and its previous load has landed.  The periodic
 // x neighbours that wrap outside a unit's tile (one site at each row end)
 // arrive as two extra one-site spinor columns and one block column with
@@ -61,24 +62,28 @@ constexpr int kThreads = (kWarps + 1) * 32;
 constexpr int kMaxReg = 168;              // three warps on one SM quarter: 3 x 32 x 168 <= 16384
 constexpr int kStages = 5;                // stages per unit
 constexpr int kLoads = 2 * kStages;       // loads per unit: (stage, species)
-constexpr int kBufs = 4;                  // ring of load buffers
+constexpr int kBufs = 5;                  // ring of load buffers
 constexpr int kTileS = kUnit + 2;         // tile width in sites (x0 - 1 .. x0 + 32)
 constexpr uint32_t kTileBytes = 36u * kTileS * 16u;    // 19584: 36 planes x 34 sites
 constexpr uint32_t kOffW = kTileBytes;                 // block tile (36 entry planes)
-constexpr uint32_t kOffD = 2u * kTileBytes;            // 39168: D, 9 planes x 32 sites x 16 B
-constexpr uint32_t kOffB = kOffD + 9u * kUnit * 16u;   // 43776: B, 9 planes x 32 sites x 8 B
 // stage 0 only: the x-wrap columns, 36 planes x 16 B each (the spinor and the
 // block at the -x neighbour of the unit's x = 0 site, the spinor at the +x
 // neighbour of its x = nx - 1 site)
-constexpr uint32_t kOffX = kOffB + 9u * kUnit * 8u;    // 46080
+constexpr uint32_t kOffX = 2u * kTileBytes;            // 39168
 constexpr uint32_t kColBytes = 36u * 16u;              // 576
 constexpr uint32_t kColStride = 640u;                  // 128-byte aligned column starts
-constexpr uint32_t kBufBytes = ((kOffX + 3u * kColStride) + 1023u) & ~1023u;  // 48128
-constexpr uint32_t kSmemBytes = kBufs * kBufBytes + 1024u;                     // 193536
-static_assert(kOffW % 128 == 0 && kOffD % 128 == 0 && kOffB % 128 == 0 && kOffX % 128 == 0 &&
-                  kColStride % 128 == 0 && kColStride >= kColBytes && kBufBytes % 1024 == 0,
+constexpr uint32_t kBufBytes = ((kOffX + 3u * kColStride) + 1023u) & ~1023u;  // 41984
+// the unit's diagonal matrices, double-buffered by unit after the ring:
+// D (9 planes x 32 sites x 16 B), then B (9 planes x 32 sites x 8 B)
+constexpr uint32_t kDiagD = 9u * kUnit * 16u;          // 4608
+constexpr uint32_t kDiagB = 9u * kUnit * 8u;           // 2304
+constexpr uint32_t kDiagStride = 7168u;
+constexpr uint32_t kOffDiag = kBufs * kBufBytes;       // 209920
+constexpr uint32_t kSmemBytes = kOffDiag + 2u * kDiagStride + 1024u;           // 225280
+static_assert(kOffW % 128 == 0 && kOffX % 128 == 0 && kColStride % 128 == 0 && kColStride >= kColBytes &&
+                  kBufBytes % 1024 == 0 && kDiagStride % 128 == 0 && kDiagD + kDiagB <= kDiagStride,
               "layout");
-static_assert(kSmemBytes <= 232448, "shared memory");
+static_assert(kSmemBytes + 1024 <= 232448, "shared memory");
 static_assert(kMaxReg * 32 * 3 <= 16384, "registers of an SM quarter (three warps)");
 }  // namespace mv5
 
@@ -139,10 +144,30 @@ __global__ void __launch_bounds__(256) k_cn_blocks5(Lat L, CnCoef C, const doubl
 
 namespace {
 
-// the six periodic neighbours (+x,-x,+y,-y,+z,-z) of site s (V < 2^31)
-__device__ __forceinline__ void neighbours5(const Lat &L, int s, int (&nb)[6]) {
+// Coordinates of a unit's first site, from two integer divisions per unit;
+// everything else the pipeline needs follows from them by additions.
+struct UnitPos {
+  int x0, cx, cy, cz;
+};
+__device__ __forceinline__ UnitPos unit_pos(const Lat &L, int x0) {
+  const int nx = (int)L.nx, ny = (int)L.ny;
+  const int t = x0 / nx, z = t / ny;
+  return {x0, x0 - t * nx, t - z * ny, z};
+}
+
+// the six periodic neighbours (+x,-x,+y,-y,+z,-z) of the site l sites after
+// the unit's first (V < 2^31); its coordinates by carrying from the unit's
+__device__ __forceinline__ void neighbours5(const Lat &L, const UnitPos &P, int l, int (&nb)[6]) {
   const int nx = (int)L.nx, ny = (int)L.ny, nz = (int)L.nz;
-  const int t = s / nx, x = s - t * nx, z = t / ny, y = t - z * ny;
+  int x = P.cx + l, y = P.cy, z = P.cz;
+  while (x >= nx) {  // at most kUnit / nx + 1 rows
+    x -= nx;
+    if (++y == ny) {
+      y = 0;
+      ++z;
+    }
+  }
+  const int s = P.x0 + l;
   const int row = nx, plane = nx * ny;
   nb[0] = x + 1 < nx ? s + 1 : s - (nx - 1);
   nb[1] = x > 0 ? s - 1 : s + (nx - 1);
@@ -152,18 +177,18 @@ __device__ __forceinline__ void neighbours5(const Lat &L, int s, int (&nb)[6]) {
   nb[5] = z > 0 ? s - plane : s + (nz - 1) * plane;
 }
 
-// first site of the spinor tile of stage stg of the unit at x0 (stage 0:
+// first site of the spinor tile of stage stg of the unit (stage 0:
 // x0 - 1; stages 1-4: the +y, -y, +z, -z neighbours of x0)
-__device__ __forceinline__ int spin_start5(const Lat &L, int x0, int stg) {
+__device__ __forceinline__ int spin_start5(const Lat &L, const UnitPos &P, int stg) {
+  const int x0 = P.x0;
   if (stg == 0) return x0 - 1;
-  const int nx = (int)L.nx, ny = (int)L.ny, nz = (int)L.nz;
-  const int t = x0 / nx, z = t / ny, y = t - z * ny;
-  const int row = nx, plane = nx * ny;
+  const int ny = (int)L.ny, nz = (int)L.nz;
+  const int row = (int)L.nx, plane = (int)(L.nx * L.ny);
   switch (stg) {
-    case 1: return y + 1 < ny ? x0 + row : x0 - (ny - 1) * row;
-    case 2: return y > 0 ? x0 - row : x0 + (ny - 1) * row;
-    case 3: return z + 1 < nz ? x0 + plane : x0 - (nz - 1) * plane;
-    default: return z > 0 ? x0 - plane : x0 + (nz - 1) * plane;
+    case 1: return P.cy + 1 < ny ? x0 + row : x0 - (ny - 1) * row;
+    case 2: return P.cy > 0 ? x0 - row : x0 + (ny - 1) * row;
+    case 3: return P.cz + 1 < nz ? x0 + plane : x0 - (nz - 1) * plane;
+    default: return P.cz > 0 ? x0 - plane : x0 + (nz - 1) * plane;
   }
 }
 // first site of the block tile of a stage: forward stages read the blocks
@@ -174,16 +199,15 @@ __device__ __forceinline__ int blk_start5(int x0, int spin_start, int stg) {
   return spin_start;
 }
 
-// Sites of the unit at x0 whose x neighbour wraps outside the stage-0 tile
-// (rows of at least kUnit + 2 sites: one x = 0 and one x = nx - 1 site per
-// unit at most): yl = the -x neighbour of its x = 0 site, yr = the +x
-// neighbour of its x = nx - 1 site; -1 where the unit has no such site.
-__device__ __forceinline__ void x_wraps5(const Lat &L, int x0, int &yl, int &yr) {
-  const int nx = (int)L.nx, V = (int)L.V;
+// Sites of the unit whose x neighbour wraps outside the stage-0 tile (rows
+// of at least kUnit + 2 sites: one x = 0 and one x = nx - 1 site per unit at
+// most): yl = the -x neighbour of its x = 0 site, yr = the +x neighbour of
+// its x = nx - 1 site; -1 where the unit has no such site.
+__device__ __forceinline__ void x_wraps5(const Lat &L, const UnitPos &P, int &yl, int &yr) {
+  const int nx = (int)L.nx, V = (int)L.V, x0 = P.x0;
   yl = yr = -1;
   if (nx < mv5::kTileS) return;
-  const int cx0 = x0 % nx;
-  const int pl = cx0 == 0 ? 0 : nx - cx0, pr = nx - 1 - cx0;
+  const int pl = P.cx == 0 ? 0 : nx - P.cx, pr = nx - 1 - P.cx;
   if (pl < mv5::kUnit && x0 + pl < V) yl = x0 + pl + nx - 1;
   if (pr < mv5::kUnit && x0 + pr < V) yr = x0 + pr - (nx - 1);
 }
@@ -201,22 +225,21 @@ __device__ __forceinline__ double lds_d1(uint32_t a) {
 }
 
 // The thread's tile (rows 2c + s, c = 0..2; columns 3h + k, k = 0..2) +=
-// sum over q of w[c][q] psi[q][3h + k].  Forward: w[c][q] = sgn
-// W(x)[2c+s][q], entry (2c+s)*6 + q; backward: w[c][q] = -sgn
-// conj(W(y)[q][2c+s]), entry q*6 + 2c + s.  load_w(e) reads entry e of the
+// sum over q of w[c][q] psi[q][3h + k].  Forward: w[c][q] = W(x)[2c+s][q],
+// entry (2c+s)*6 + q; backward: w[c][q] = -conj(W(y)[q][2c+s]), entry
+// q*6 + 2c + s.  load_w(e) reads entry e of the
 // block, load_p(e) plane e of the spinor (species planes), from the shared
 // tiles or global memory.
 template <bool BWD, typename LW, typename LP>
-__device__ __forceinline__ void nb_products(double (&acc)[3][3][2], int s, int h, double sgn, LW load_w,
-                                            LP load_p) {
+__device__ __forceinline__ void nb_products(double (&acc)[3][3][2], int s, int h, LW load_w, LP load_p) {
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     double wr[3], wi[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const double2 wv = load_w(BWD ? q * 6 + 2 * c + s : (2 * c + s) * 6 + q);
-      wr[c] = BWD ? -sgn * wv.x : sgn * wv.x;
-      wi[c] = sgn * wv.y;
+      wr[c] = BWD ? -wv.x : wv.x;
+      wi[c] = wv.y;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -238,7 +261,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
              MvArgs A, int nunits, int *err, long long wait_cycles, int stall_load) {
   using namespace mv5;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kBufs], empty_bar[kBufs];
+  __shared__ __align__(8) uint64_t full_bar[kBufs], empty_bar[kBufs], dfull[2], dempty[2];
   __shared__ double red[kWarps][3][3];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -248,6 +271,10 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     for (int b = 0; b < kBufs; ++b) {
       mbar_init(&full_bar[b], 1);
       mbar_init(&empty_bar[b], 4);  // the four consumer warps of the load's species
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&dfull[b], 1);
+      mbar_init(&dempty[b], kWarps);  // every consumer warp
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -270,7 +297,8 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     if (lane == 0) {
       const int stop = stall_load >= 0 ? min(stall_load, total) : total;
       bool ok = true;
-      int i = 0;
+      int i = 0, ndiag = 0;
+      UnitPos P{0, 0, 0, 0};
       for (; i < stop && ok; ++i) {
         const int b = i % kBufs;
         if (i >= kBufs) {
@@ -281,22 +309,33 @@ __global__ void __maxnreg__(mv5::kMaxReg)
           if (!ok) break;
         }
         const int li = i % kLoads, stg = li >> 1, sp = li & 1;
-        const int x0 = ((int)blockIdx.x + (i / kLoads) * (int)gridDim.x) * kUnit;
-        const int ss = spin_start5(L, x0, stg);
+        if (li == 0) P = unit_pos(L, ((int)blockIdx.x + (i / kLoads) * (int)gridDim.x) * kUnit);
+        const int x0 = P.x0;
+        if (li == 0) {  // the unit's diagonal matrices, with its first load
+          const int k = i / kLoads, db = k & 1;
+          if (k >= 2) {
+            const uint32_t dpar = (uint32_t)((k / 2 - 1) & 1);
+            ok = wait(&dempty[db], dpar) && mbar_wait(&dfull[db], dpar);
+            if (!ok) break;
+          }
+          unsigned char *dd = smem + kOffDiag + db * kDiagStride;
+          mbar_expect_tx(&dfull[db], kDiagD + kDiagB);
+          tma_2d(dd, &maps.D, 2 * x0, 0, &dfull[db]);
+          tma_2d(dd + kDiagD, &maps.B, x0, 0, &dfull[db]);
+          ++ndiag;
+        }
+        const int ss = spin_start5(L, P, stg);
         const int ws = blk_start5(x0, ss, stg);
         const int I = stg == 0 ? 0 : (stg + 1) / 2;
         unsigned char *bb = smem + b * kBufBytes;
         int yl = -1, yr = -1;
-        if (stg == 0) x_wraps5(L, x0, yl, yr);
+        if (stg == 0) x_wraps5(L, P, yl, yr);
         uint32_t tx = 2u * kTileBytes;
-        if (stg == 0) tx += 9u * kUnit * 16u + 9u * kUnit * 8u + (yl >= 0 ? 2u : 0u) * kColBytes +
-                            (yr >= 0 ? kColBytes : 0u);
+        if (stg == 0) tx += (yl >= 0 ? 2u : 0u) * kColBytes + (yr >= 0 ? kColBytes : 0u);
         mbar_expect_tx(&full_bar[b], tx);
         tma_2d(bb, &maps.spin, 2 * ss, sp * 36, &full_bar[b]);
         tma_2d(bb + kOffW, &maps.W, 2 * ws, (I * 2 + sp) * 36, &full_bar[b]);
         if (stg == 0) {
-          tma_2d(bb + kOffD, &maps.D, 2 * x0, 0, &full_bar[b]);
-          tma_2d(bb + kOffB, &maps.B, x0, 0, &full_bar[b]);
           if (yl >= 0) {
             tma_2d(bb + kOffX, &maps.spin1, 2 * yl, sp * 36, &full_bar[b]);
             tma_2d(bb + kOffX + kColStride, &maps.W1, 2 * yl, sp * 36, &full_bar[b]);
@@ -309,6 +348,11 @@ __global__ void __maxnreg__(mv5::kMaxReg)
       // kBufs were waited for above
       for (int k = max(0, i - kBufs); k < i; ++k)
         if (!mbar_wait(&full_bar[k % kBufs], (uint32_t)((k / kBufs) & 1))) {
+          atomicExch(err, NRQ_ERR_TIMEOUT);
+          break;
+        }
+      for (int k = max(0, ndiag - 2); k < ndiag; ++k)
+        if (!mbar_wait(&dfull[k & 1], (uint32_t)((k >> 1) & 1))) {
           atomicExch(err, NRQ_ERR_TIMEOUT);
           break;
         }
@@ -331,12 +375,15 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   bool dead = false;
 
   for (int u = 0; u < my_units; ++u) {
-    const int x0 = ((int)blockIdx.x + u * (int)gridDim.x) * kUnit;
+    const UnitPos P = unit_pos(L, ((int)blockIdx.x + u * (int)gridDim.x) * kUnit);
+    const int x0 = P.x0;
     const int x = x0 + site_in_unit;
     const bool act = x < V;
     const int xs = act ? x : V - 1;  // a valid site for the addresses of idle lanes
     int nb[6];
-    neighbours5(L, xs, nb);
+    neighbours5(L, P, xs - x0, nb);
+    int yl = -1, yr = -1;
+    x_wraps5(L, P, yl, yr);
     double acc[3][3][2];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -360,7 +407,9 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             asm volatile("prefetch.global.L1 [%0];" ::"l"(epi_src + (int64_t)(sp * 36 + (3 * h + k) * 6 + 2 * c + s) * V +
                                                           xs));
       }
-      const bool expired = !dead && !wait(&full_bar[b], (uint32_t)((ld / kBufs) & 1));
+      bool expired = !dead && !wait(&full_bar[b], (uint32_t)((ld / kBufs) & 1));
+      // stage 0 also reads the unit's diagonal matrices
+      if (stg == 0 && !dead && !expired) expired = !wait(&dfull[u & 1], (uint32_t)((u >> 1) & 1));
       // warp-uniform: the products below use warp votes
       if (__any_sync(0xffffffffu, expired) && !dead) {
         dead = true;
@@ -369,15 +418,14 @@ __global__ void __maxnreg__(mv5::kMaxReg)
       const unsigned char *bb = smem + b * kBufBytes;
       const uint32_t s_tile = smem_u32(bb), s_w = smem_u32(bb + kOffW);
       if (!dead) {
-        const int ss = spin_start5(L, x0, stg);
+        const int ss = spin_start5(L, P, stg);
         const int ws = blk_start5(x0, ss, stg);
-        int yl = -1, yr = -1;
-        if (stg == 0) x_wraps5(L, x0, yl, yr);
         if (stg == 0) {
           // diagonal (colour only): row (c, s) takes input rows (j, s);
           // x - ss = site_in_unit + 1 lies inside the tile for every lane
-          const uint32_t s_d = smem_u32(bb + kOffD) + (uint32_t)(site_in_unit * 16);
-          const uint32_t s_b = smem_u32(bb + kOffB) + (uint32_t)(site_in_unit * 8);
+          const unsigned char *dd = smem + kOffDiag + (u & 1) * kDiagStride;
+          const uint32_t s_d = smem_u32(dd) + (uint32_t)(site_in_unit * 16);
+          const uint32_t s_b = smem_u32(dd + kDiagD) + (uint32_t)(site_in_unit * 8);
           const uint32_t s_own = s_tile + (uint32_t)((site_in_unit + 1) * 16 + s * kTileS * 16);
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
@@ -389,6 +437,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
               const double bv = lds_d1(s_b + (uint32_t)(e * kUnit * 8));
               cd[c] = ad * cplx{dv.x, dv.y} + bv * am;
               if (j == c) cd[c] = cd[c] + dg;
+              cd[c] = nb_sign * cd[c];  // see the epilogue
             }
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -425,18 +474,18 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             auto lw = [&](int e) { return lds_d2(wa + (uint32_t)e * wst); };
             auto lp = [&](int e) { return lds_d2(pa + (uint32_t)e * pst); };
             if (bwd)
-              nb_products<true>(acc, s, h, nb_sign, lw, lp);
+              nb_products<true>(acc, s, h, lw, lp);
             else
-              nb_products<false>(acc, s, h, nb_sign, lw, lp);
+              nb_products<false>(acc, s, h, lw, lp);
           } else if (__all_sync(0xffffffffu, (ps && wsh) || !act)) {
             // every operand of the warp in shared memory
             const uint32_t wa = s_w + (uint32_t)((m - ws) * 16), pa = s_tile + (uint32_t)((y - ss) * 16);
             auto lw = [&](int e) { return lds_d2(wa + (uint32_t)(e * kTileS * 16)); };
             auto lp = [&](int e) { return lds_d2(pa + (uint32_t)(e * kTileS * 16)); };
             if (bwd)
-              nb_products<true>(acc, s, h, nb_sign, lw, lp);
+              nb_products<true>(acc, s, h, lw, lp);
             else
-              nb_products<false>(acc, s, h, nb_sign, lw, lp);
+              nb_products<false>(acc, s, h, lw, lp);
           } else if (act) {
             // some lanes' operands outside the tiles (periodic wraps, tile
             // edges): those lanes read global memory, the others the tiles
@@ -447,14 +496,17 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             auto lw = [&](int e) { return wp[e * wst]; };
             auto lp = [&](int e) { return pp[e * pst]; };
             if (bwd)
-              nb_products<true>(acc, s, h, nb_sign, lw, lp);
+              nb_products<true>(acc, s, h, lw, lp);
             else
-              nb_products<false>(acc, s, h, nb_sign, lw, lp);
+              nb_products<false>(acc, s, h, lw, lp);
           }
         }
       }
       __syncwarp();
-      if (lane == 0) mbar_arrive(&empty_bar[b]);
+      if (lane == 0) {
+        mbar_arrive(&empty_bar[b]);
+        if (stg == 0) mbar_arrive(&dempty[u & 1]);
+      }
     }
 
     // ---------------------------------------------------------- epilogue
@@ -464,7 +516,9 @@ __global__ void __maxnreg__(mv5::kMaxReg)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const int64_t off = (int64_t)(sp * 36 + (3 * h + k) * 6 + 2 * c + s) * V + x;
-          const cplx y_ = {acc[c][k][0], acc[c][k][1]};
+          // D in + sgn N in = sgn (sgn D in + N in), sgn = +-1: the diagonal
+          // was scaled by sgn and the neighbour sum was not
+          const cplx y_ = {nb_sign * acc[c][k][0], nb_sign * acc[c][k][1]};
           const cplx ev = MODE == MV_PLAIN ? cplx{0.0, 0.0} : ldg(epi_src + off);
           if (MODE == MV_PLAIN) {
             st(A.out + off, y_);
