@@ -7,6 +7,7 @@
 #include <complex>
 #include <cstring>
 #include <new>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -28,8 +29,32 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 // per-column Krylov scalars followed by one int error flag written by the
 // stencil kernels (NRQ_ERR_TIMEOUT when a bounded wait expired)
 constexpr size_t kScalDoubles = (size_t)nrq::CN_COLS * nrq::SC_STRIDE;
-constexpr size_t kScalBytes = sizeof(double) * (kScalDoubles + 2);
+// after the scalars: 16 ints of the stencils' error record (the flag, and
+// where a bounded wait expired)
+constexpr size_t kScalBytes = sizeof(double) * (kScalDoubles + 8);
 inline int *scal_err(double *scal) { return (int *)(scal + kScalDoubles); }
+// the stencils' record of an expired pipeline wait (4 ints after the
+// scalars): the message of the update that reports it, and a reset
+std::string timeout_message(const double *h_scal) {
+  const int *e = (const int *)(h_scal + kScalDoubles);
+  static const char *roles[] = {"a consumer's wait for a load", "a consumer's wait for the diagonal matrices",
+                                "the loader's wait for a released buffer", "the loader's wait for a landed load",
+                                "the loader's final drain"};
+  const int stencil = e[1] / 16, role = e[1] % 16;
+  std::string m = "CN stencil: a bounded pipeline wait expired";
+  if (e[1] != 0) {
+    m += " (k_cn_mv" + std::to_string(stencil) + ", " + (role >= 0 && role < 5 ? roles[role] : "?") +
+         ", load " + std::to_string(e[2]) + ", CTA " + std::to_string(e[3]);
+    if (e[4] != 0) {  // the FMA stencil's detail: the loader's progress and the barrier's word
+      char buf[96];
+      snprintf(buf, sizeof buf, ", loads issued %d, barrier %08x%08x, parity %d", e[4] - 1, (unsigned)e[6],
+               (unsigned)e[5], e[7]);
+      m += buf;
+    }
+    m += ")";
+  }
+  return m;
+}
 
 int ensure_stage(nrq_ctx *ctx, size_t bytes) {
   if (ctx->stage_bytes >= bytes) return NRQ_OK;
@@ -1436,8 +1461,8 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(hs, cn->scal, kScalBytes, cudaMemcpyDeviceToHost, st));
     NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (*scal_err(hs) != 0) {
-      NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, sizeof(int), st));
-      ctx->last_error = "CN stencil: a bounded pipeline wait expired";
+      NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, 16 * sizeof(int), st));
+      ctx->last_error = timeout_message(hs);
       return NRQ_ERR_TIMEOUT;
     }
     bool all = true, nonfin = false;
@@ -1648,8 +1673,8 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (*scal_err(hs) != 0) {
       status = NRQ_ERR_TIMEOUT;
-      ctx->last_error = "CN stencil: a bounded pipeline wait expired";
-      NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, sizeof(int), st));
+      ctx->last_error = timeout_message(hs);
+      NRQ_CUDA_TRY(ctx, cudaMemsetAsync(scal_err(cn->scal), 0, 16 * sizeof(int), st));
       break;
     }
     {

@@ -165,13 +165,13 @@ __global__ void __launch_bounds__(mv3::kThreads, 1)
       if (issue(issued)) ++issued;
       else {
         prod_dead = true;
-        atomicExch(err, NRQ_ERR_TIMEOUT);
+        record_timeout(err, 3, 0, -1);
       }
     }
     const int buf = (int)(kk % kBufs);
     if (!dead && !mbar_wait(&full_bar[buf], (uint32_t)((kk / kBufs) & 1))) {
       dead = true;
-      atomicExch(err, NRQ_ERR_TIMEOUT);
+      record_timeout(err, 3, 0, -1);
     }
     return smem + buf * kBufBytes;
   };
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(mv3::kThreads, 1)
   // error path: copies issued ahead of the consumers must land before exit
   if (threadIdx.x == 0 && dead)
     for (int64_t kk = k; kk < issued; ++kk)
-      if (!mbar_wait(&full_bar[kk % kBufs], (uint32_t)((kk / kBufs) & 1))) atomicExch(err, NRQ_ERR_TIMEOUT);
+      if (!mbar_wait(&full_bar[kk % kBufs], (uint32_t)((kk / kBufs) & 1))) record_timeout(err, 3, 0, -1);
 }
 
 // ------------------------------------------------------------------ host

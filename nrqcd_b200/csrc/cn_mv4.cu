@@ -405,7 +405,7 @@ __global__ void __maxnreg__(mv4::kMaxReg)
         ok = mbar_wait(&empty_bar[kStages - 1], (uint32_t)((my_units - 1) & 1));
         if (ok) store_results(((int)blockIdx.x + (my_units - 1) * (int)gridDim.x) * kUnit);
       }
-      if (!ok) atomicExch(err, NRQ_ERR_TIMEOUT);
+      if (!ok) record_timeout(err, 4, 0, -1);
       bulk_wait_all();
       // error path: copies issued ahead of the consumers must land before
       // exit (the last use of each buffer; earlier uses were consumed)
@@ -418,7 +418,7 @@ __global__ void __maxnreg__(mv4::kMaxReg)
   auto stage_begin = [&](int stg) -> const unsigned char * {
     if (!dead && !mbar_wait(&full_bar[stg], c_par)) {
       dead = true;
-      atomicExch(err, NRQ_ERR_TIMEOUT);
+      record_timeout(err, 4, 0, -1);
     }
     return smem + buf_off(stg);
   };

@@ -26,7 +26,7 @@
 // 32-site unit) and one producer warp.  Ten loads per unit, per stage and species
 // (stage 0: diagonal matrices, +x and -x; 1: +y; 2: -y; 3: +z; 4: -z): a
 // spinor tile (34 sites x 36 planes) and a block tile (34 sites x 36 entry
-// planes) by TMA, into a ring of five shared-memory buffers completed on
+// planes) by TMA, into a ring of four shared-memory buffers completed on
 // mbarriers; the unit's diagonal matrices go with its first load into one
 // of two further buffers.  The producer refills a buffer once the four consumer warps of
 // its species released it and its previous load has landed.  The periodic
@@ -62,7 +62,14 @@ constexpr int kThreads = (kWarps + 1) * 32;
 constexpr int kMaxReg = 168;              // three warps on one SM quarter: 3 x 32 x 168 <= 16384
 constexpr int kStages = 5;                // stages per unit
 constexpr int kLoads = 2 * kStages;       // loads per unit: (stage, species)
-constexpr int kBufs = 5;                  // ring of load buffers
+// Ring of load buffers.  Loads alternate between the species, and a
+// consumer waits on a buffer's full barrier by phase parity, which is only
+// sound while it never waits more than one phase ahead of the barrier's
+// last completed phase.  With an even ring every use of a buffer belongs to
+// one species, whose warps released the previous use themselves; an odd
+// ring would let one species wait two phases ahead of a load of the other
+// that is still in flight, and pass the wait on a stale parity.
+constexpr int kBufs = 4;
 constexpr int kTileS = kUnit + 2;         // tile width in sites (x0 - 1 .. x0 + 32)
 constexpr uint32_t kTileBytes = 36u * kTileS * 16u;    // 19584: 36 planes x 34 sites
 constexpr uint32_t kOffW = kTileBytes;                 // block tile (36 entry planes)
@@ -78,12 +85,13 @@ constexpr uint32_t kBufBytes = ((kOffX + 3u * kColStride) + 1023u) & ~1023u;  //
 constexpr uint32_t kDiagD = 9u * kUnit * 16u;          // 4608
 constexpr uint32_t kDiagB = 9u * kUnit * 8u;           // 2304
 constexpr uint32_t kDiagStride = 7168u;
-constexpr uint32_t kOffDiag = kBufs * kBufBytes;       // 209920
-constexpr uint32_t kSmemBytes = kOffDiag + 2u * kDiagStride + 1024u;           // 225280
+constexpr uint32_t kOffDiag = kBufs * kBufBytes;       // 167936
+constexpr uint32_t kSmemBytes = kOffDiag + 2u * kDiagStride + 1024u;           // 183296
 static_assert(kOffW % 128 == 0 && kOffX % 128 == 0 && kColStride % 128 == 0 && kColStride >= kColBytes &&
                   kBufBytes % 1024 == 0 && kDiagStride % 128 == 0 && kDiagD + kDiagB <= kDiagStride,
               "layout");
 static_assert(kSmemBytes + 1024 <= 232448, "shared memory");
+static_assert(kBufs % 2 == 0 && kLoads % 2 == 0, "a buffer's uses must all belong to one species");
 static_assert(kMaxReg * 32 * 3 <= 16384, "registers of an SM quarter (three warps)");
 }  // namespace mv5
 
@@ -262,12 +270,14 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   using namespace mv5;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[kBufs], empty_bar[kBufs], dfull[2], dempty[2];
+  __shared__ volatile int s_issued;  // loads the producer issued (diagnostics of an expired wait)
   __shared__ double red[kWarps][3][3];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int V = (int)L.V;  // the launcher admits V < 2^31 only
 
   if (threadIdx.x == 0) {
+    s_issued = 0;
     for (int b = 0; b < kBufs; ++b) {
       mbar_init(&full_bar[b], 1);
       mbar_init(&empty_bar[b], 4);  // the four consumer warps of the load's species
@@ -305,7 +315,13 @@ __global__ void __maxnreg__(mv5::kMaxReg)
           const uint32_t par = (uint32_t)((i / kBufs - 1) & 1);
           // every consumer warp of the species released the buffer, and its
           // previous load landed
-          ok = wait(&empty_bar[b], par) && mbar_wait(&full_bar[b], par);
+          if (!wait(&empty_bar[b], par)) {
+            record_timeout(err, 5, 2, i);
+            ok = false;
+          } else if (!mbar_wait(&full_bar[b], par)) {
+            record_timeout(err, 5, 3, i);
+            ok = false;
+          }
           if (!ok) break;
         }
         const int li = i % kLoads, stg = li >> 1, sp = li & 1;
@@ -315,7 +331,13 @@ __global__ void __maxnreg__(mv5::kMaxReg)
           const int k = i / kLoads, db = k & 1;
           if (k >= 2) {
             const uint32_t dpar = (uint32_t)((k / 2 - 1) & 1);
-            ok = wait(&dempty[db], dpar) && mbar_wait(&dfull[db], dpar);
+            if (!wait(&dempty[db], dpar)) {
+              record_timeout(err, 5, 2, i);
+              ok = false;
+            } else if (!mbar_wait(&dfull[db], dpar)) {
+              record_timeout(err, 5, 3, i);
+              ok = false;
+            }
             if (!ok) break;
           }
           unsigned char *dd = smem + kOffDiag + db * kDiagStride;
@@ -342,18 +364,18 @@ __global__ void __maxnreg__(mv5::kMaxReg)
           }
           if (yr >= 0) tma_2d(bb + kOffX + 2 * kColStride, &maps.spin1, 2 * yr, sp * 36, &full_bar[b]);
         }
+        s_issued = i + 1;
       }
-      if (!ok) atomicExch(err, NRQ_ERR_TIMEOUT);
       // every issued load lands before the CTA exits: loads before the last
       // kBufs were waited for above
       for (int k = max(0, i - kBufs); k < i; ++k)
         if (!mbar_wait(&full_bar[k % kBufs], (uint32_t)((k / kBufs) & 1))) {
-          atomicExch(err, NRQ_ERR_TIMEOUT);
+          record_timeout(err, 5, 4, k);
           break;
         }
       for (int k = max(0, ndiag - 2); k < ndiag; ++k)
         if (!mbar_wait(&dfull[k & 1], (uint32_t)((k >> 1) & 1))) {
-          atomicExch(err, NRQ_ERR_TIMEOUT);
+          record_timeout(err, 5, 4, -1 - k);
           break;
         }
     }
@@ -407,13 +429,23 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             asm volatile("prefetch.global.L1 [%0];" ::"l"(epi_src + (int64_t)(sp * 36 + (3 * h + k) * 6 + 2 * c + s) * V +
                                                           xs));
       }
-      bool expired = !dead && !wait(&full_bar[b], (uint32_t)((ld / kBufs) & 1));
+      int role = -1;
+      if (!dead && !wait(&full_bar[b], (uint32_t)((ld / kBufs) & 1))) role = 0;
       // stage 0 also reads the unit's diagonal matrices
-      if (stg == 0 && !dead && !expired) expired = !wait(&dfull[u & 1], (uint32_t)((u >> 1) & 1));
+      if (stg == 0 && !dead && role < 0 && !wait(&dfull[u & 1], (uint32_t)((u >> 1) & 1))) role = 1;
       // warp-uniform: the products below use warp votes
-      if (__any_sync(0xffffffffu, expired) && !dead) {
+      if (__any_sync(0xffffffffu, role >= 0) && !dead) {
         dead = true;
-        if (lane == 0) atomicExch(err, NRQ_ERR_TIMEOUT);
+        if (role >= 0) {
+          record_timeout(err, 5, role, ld);
+          if (err[3] == (int)blockIdx.x && err[2] == ld) {  // this thread's record: add the detail
+            const uint64_t word = role == 0 ? *(volatile uint64_t *)&full_bar[b] : *(volatile uint64_t *)&dfull[u & 1];
+            err[4] = s_issued + 1;
+            err[5] = (int)(uint32_t)word;
+            err[6] = (int)(uint32_t)(word >> 32);
+            err[7] = role == 0 ? (ld / kBufs) & 1 : (u >> 1) & 1;
+          }
+        }
       }
       const unsigned char *bb = smem + b * kBufBytes;
       const uint32_t s_tile = smem_u32(bb), s_w = smem_u32(bb + kOffW);

@@ -12,6 +12,7 @@
 #include <cudaTypedefs.h>
 
 #include "nrq_common.cuh"
+#include "../../include/nrqcd_b200.h"
 
 namespace nrq {
 
@@ -59,6 +60,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
   }
   return true;
 }
+// Record an expired pipeline wait: err[0] = NRQ_ERR_TIMEOUT; the first
+// expiry of a launch also records where (err[1] = stencil * 16 + role,
+// err[2] = the load's index in its CTA, err[3] = the CTA).  Roles: 0 a
+// consumer's wait for a load, 1 for the diagonal matrices, 2 the loader's
+// wait for a released buffer, 3 for a landed load, 4 its final drain.
+__device__ __forceinline__ void record_timeout(int *err, int stencil, int role, int load) {
+  atomicExch(err, NRQ_ERR_TIMEOUT);
+  if (atomicCAS(err + 1, 0, stencil * 16 + role) == 0) {
+    atomicExch(err + 2, load);
+    atomicExch(err + 3, (int)blockIdx.x);
+  }
+}
+
 // 2D tile of a tensor map at (c0, c1) into shared memory
 __device__ __forceinline__ void tma_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
   asm volatile(
