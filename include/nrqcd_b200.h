@@ -87,6 +87,16 @@ void *nrq_cuda_stream(nrq_ctx *ctx);
 enum { NRQ_PROF_CLASSES = 6 };
 int nrq_profile_enable(nrq_ctx *ctx, int enable);
 int nrq_profile_read(nrq_ctx *ctx, int64_t launches[6], double milliseconds[6], double bytes[6]);
+/* The initial conditions' random stream drawn on the device (no reference
+ * counterpart: a check of the device draw against the reference's
+ * generator, src/ranlxd_generator.f90:251-350).  normals = 0: count numbers
+ * (count even) from number `first` (even) of the ranlxd stream of (level,
+ * seed); normals = 1: the real parts of the Box-Muller normals of count
+ * consecutive pairs from `first` (src/random.f90:238-255).  Into the host
+ * array out.                                                             */
+int nrq_ranlxd_draw(nrq_ctx *ctx, int level, int64_t seed, uint64_t first, int64_t count, int normals,
+                    double *out);
+
 /* ---- gauge configuration: src/gaugeconfiguration_su3.f90:33-116 -------- */
 int nrq_gauge_create(nrq_ctx *ctx, nrq_gauge **g);      /* Allocate (:124-140)   */
 int nrq_gauge_destroy(nrq_gauge *g);                    /* Deallocate            */

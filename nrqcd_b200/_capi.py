@@ -61,6 +61,7 @@ SIGNATURES = {
     "nrq_cuda_stream": (ctypes.c_void_p, [_vp]),
     "nrq_profile_enable": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_profile_read": (ctypes.c_int, [_vp, _i64p, _dp, _dp]),
+    "nrq_ranlxd_draw": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int, _dp]),
     "nrq_gauge_create": (ctypes.c_int, [_vp, _pp]),
     "nrq_gauge_destroy": (ctypes.c_int, [_vp]),
     "nrq_gauge_upload": (ctypes.c_int, [_vp, _dp, _dp]),

@@ -15,6 +15,7 @@
 #include "nrq_internal.h"
 #include "nrq_kernels.cuh"
 #include "ranlxd_host.h"
+#include "ranlxd_dev.cuh"
 
 using nrq::cplx;
 using nrqh::check_launch;
@@ -419,18 +420,6 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
     ctx->last_error = "transverse_box_init: seed must lie in [1, 2^31-1]";
     return NRQ_ERR_BAD_ARG;
   }
-  // real parts of complex Box-Muller normals, per site, per polarisation
-  // (gauge:1334-1340, random.f90:238-255): plane (pol*8 + a)
-  // (pair e = 16 s + 8 pol + a of the stream; drawn on host threads that
-  // jump to their share)
-  std::vector<double2> R((size_t)16 * V);
-  const double twopi = 2.0 * std::acos(-1.0);
-  if (!nrqh::draw_pairs_noexcept(2, seed, 0, (size_t)16 * V, [&](size_t e, double u1, double u2) {
-        R[(e % 16) * (size_t)V + e / 16] = make_double2(std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2), 0.0);
-      })) {
-    ctx->last_error = "transverse_box_init: the random stream could not be positioned or drawn";
-    return NRQ_ERR_BAD_ARG;
-  }
   // backward-derivative momentum per direction and coordinate (lattice:963-979):
   // component (re, im) and modulus, in the host's arithmetic
   std::vector<double> mtab;
@@ -482,9 +471,15 @@ extern "C" int nrq_gauge_transverse_box_init(nrq_gauge *g, double Q, double n0, 
   p24 = true;
   cufftSetStream(plan16, ctx->stream);
   cufftSetStream(plan24, ctx->stream);
-  if (cudaMemcpyAsync(dR, R.data(), sizeof(double2) * 16 * V, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
-      cudaMemcpyAsync(dM, mtab.data(), sizeof(double) * mtab.size(), cudaMemcpyHostToDevice, ctx->stream) !=
-          cudaSuccess) {
+  // real parts of complex Box-Muller normals, per site, per polarisation
+  // (gauge:1334-1340, random.f90:238-255): plane (pol*8 + a), pair
+  // e = 16 s + 8 pol + a of the stream, drawn on the device
+  if ((rc = nrq::device_draw_pairs(ctx, 2, seed, 0, 16 * V, nrq::BoxPairs{dR, V}))) {
+    cleanup();
+    return rc;
+  }
+  if (cudaMemcpyAsync(dM, mtab.data(), sizeof(double) * mtab.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+      cudaSuccess) {
     cleanup();
     return NRQ_ERR_CUDA;
   }
@@ -701,24 +696,14 @@ extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nef
   if ((rc = check_launch(ctx, "k_cold"))) return rc;
   if ((rc = gauge_written64(g))) return rc;
   const double sigma = std::sqrt(4.0 / beta), a0 = ctx->a[0];
-  const double twopi = 2.0 * std::acos(-1.0);
-  std::vector<double> ef((size_t)24 * V);  // the reference's efield(8,3,V)
   for (int64_t r = 0; r < nefieldinit; ++r) {
     // Box-Muller pairs in the reference's order: site, direction, generator
     // (random.f90:238-255); the real part, times sigma, times a0.  Round r
-    // starts at number 48 V r of the stream; host threads jump to their share.
-    if (!nrqh::draw_pairs_noexcept(2, seed, (uint64_t)r * ef.size() * 2, ef.size(),
-                                   [&](size_t i, double u1, double u2) {
-          ef[i] = (sigma * (std::sqrt(-2.0 * std::log(u1)) * std::cos(twopi * u2))) * a0;
-        })) {
-      ctx->last_error = "equilibrium_init: the random stream could not be positioned or drawn";
-      return NRQ_ERR_BAD_ARG;
-    }
-    if ((rc = ensure_stage(ctx, sizeof(double) * 24 * V))) return rc;
-    NRQ_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_stage, ef.data(), sizeof(double) * 24 * V, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-    nrq::k_efield_f2soa<<<nblk(V, 256), 256, 0, ctx->stream>>>((const double *)ctx->d_stage, g->E, V);
-    if ((rc = check_launch(ctx, "k_efield_f2soa"))) return rc;
+    // starts at number 48 V r of the stream; drawn on the device, straight
+    // into the field's planes.
+    if ((rc = nrq::device_draw_pairs(ctx, 2, seed, (uint64_t)r * 48 * (uint64_t)V, 24 * V,
+                                     nrq::ThermalPairs{g->E, V, sigma, a0})))
+      return rc;
     int64_t it = 0;
     rc = gauss_project(g, tol, max_sweeps, &it, nullptr);
     if (sweeps) sweeps[r] = it;
@@ -729,6 +714,22 @@ extern "C" int nrq_gauge_equilibrium_init(nrq_gauge *g, double beta, int64_t nef
     if (deviations && (rc = nrq_gauge_gauss(g, nullptr, &deviations[r]))) return rc;
   }
   return NRQ_OK;
+}
+
+extern "C" int nrq_ranlxd_draw(nrq_ctx *ctx, int level, int64_t seed, uint64_t first, int64_t count, int normals,
+                               double *out) {
+  if (!ctx || !out || count < 0 || (first & 1) || (!normals && (count & 1)) || (level != 1 && level != 2) ||
+      seed < 1 || seed > 2147483647LL)
+    return NRQ_ERR_BAD_ARG;
+  int rc = set_device(ctx);
+  if (rc || count == 0) return rc;
+  double *d = nullptr;
+  NRQ_CUDA_TRY(ctx, cudaMalloc(&d, sizeof(double) * count));
+  rc = normals ? nrq::device_draw_pairs(ctx, level, seed, first, count, nrq::NormalPairs{d})
+               : nrq::device_draw_pairs(ctx, level, seed, first, count / 2, nrq::UniformPairs{d});
+  if (!rc && cudaMemcpy(out, d, sizeof(double) * count, cudaMemcpyDeviceToHost) != cudaSuccess) rc = NRQ_ERR_CUDA;
+  cudaFree(d);
+  return rc;
 }
 
 // ---------------------------------------------------------------- gluon distribution

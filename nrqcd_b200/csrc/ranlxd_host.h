@@ -207,6 +207,15 @@ class Ranlxd {
     }
     return out_[next_++];
   }
+  // continue from a block-start state (words oldest first, borrow 0): the
+  // next call of next() refills and returns that block's first number
+  void load_block_state(const int64_t *w) {
+    for (int k = 0; k < 12; ++k) x_[k] = w[k];
+    carry_ = 0;
+    next_ = 12;
+  }
+  const int64_t *seeded_words() const { return seeded_; }
+  int steps_per_block() const { return pr_; }
 
  private:
   // one recurrence step on ring slot i (the oldest word) with lag slot j
@@ -242,6 +251,58 @@ class Ranlxd {
   double out_[12] = {};
   int pr_ = 397, next_ = 12;
 };
+
+// The generator's state at the start of blocks first_block + t * stride
+// (t < nstates) of the stream of (level, seed): for each t, the 12 words
+// (oldest first, borrow 0) whose next refill delivers that block, into
+// words[12 t .. 12 t + 12).  One jump per host thread and one modular
+// multiplication per further state (Z_{t+1} = Z_t b^(-pr stride)), split
+// over up to max_threads host threads.  False for a seed or level that init
+// refuses, or a position the 64-bit step count cannot reach.
+inline bool block_states(int level, int64_t seed, uint64_t first_block, uint64_t stride, size_t nstates,
+                         int64_t *words, unsigned max_threads = 32) noexcept {
+  try {
+    Ranlxd probe;
+    if (!probe.init(level, seed)) return false;
+    const uint64_t pr = (uint64_t)probe.steps_per_block();
+    if (nstates == 0) return true;
+    const uint64_t last = first_block + stride * (uint64_t)(nstates - 1);
+    if ((stride && (uint64_t)(nstates - 1) > (UINT64_MAX - first_block) / stride) || last > UINT64_MAX / pr)
+      return false;
+    const swb::Num z0 = swb::to_lcg(probe.seeded_words(), 0);
+    const swb::Num inv = swb::inverse_base();
+    const swb::Num step = swb::pow(inv, stride * pr);
+    unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), max_threads));
+    nt = (unsigned)std::min<size_t>(nt, (nstates + 63) / 64);
+    std::vector<char> ok(nt, 1);
+    auto share = [&](unsigned t) {
+      const size_t lo = nstates * t / nt, hi = nstates * (t + 1) / nt;
+      swb::Num z = swb::mul(swb::pow(inv, (first_block + stride * (uint64_t)lo) * pr), z0);
+      for (size_t k = lo; k < hi; ++k) {
+        if (!swb::from_lcg(z, words + 12 * k)) {
+          ok[t] = 0;
+          return;
+        }
+        z = swb::mul(z, step);
+      }
+    };
+    std::vector<std::thread> pool;
+    unsigned started = 1;
+    try {
+      pool.reserve(nt);
+      for (; started < nt; ++started) pool.emplace_back(share, started);
+    } catch (...) {  // no more threads: the remaining shares run here
+    }
+    share(0);
+    for (unsigned t = started; t < nt; ++t) share(t);
+    for (auto &th : pool) th.join();
+    for (char c : ok)
+      if (!c) return false;
+    return true;
+  } catch (...) {
+    return false;
+  }
+}
 
 // f(i, u[first + 2i], u[first + 2i + 1]) for i < count, u the stream of
 // (level, seed), on up to max_threads host threads, each starting its share

@@ -121,7 +121,7 @@ int main(void) {
 # header must be added to or removed from this list as well
 EXPECTED_SYMBOLS = {
     "nrq_init", "nrq_finalize", "nrq_synchronize", "nrq_cuda_stream", "nrq_status_string", "nrq_last_error",
-    "nrq_profile_enable", "nrq_profile_read",
+    "nrq_profile_enable", "nrq_profile_read", "nrq_ranlxd_draw",
     "nrq_gauge_create", "nrq_gauge_destroy", "nrq_gauge_upload", "nrq_gauge_download", "nrq_gauge_copy",
     "nrq_gauge_cold_init", "nrq_gauge_transverse_box_init", "nrq_gauge_update", "nrq_gauge_set_precision",
     "nrq_gauge_unitarity", "nrq_gauge_energy", "nrq_gauge_gauss", "nrq_gauge_gauss_project",

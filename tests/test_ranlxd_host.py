@@ -67,6 +67,7 @@ JUMP_SRC = r'''
 // mode 1: jump(n) against jump(n - d) and d calls of next(), far into the stream
 // mode 2: draw_pairs on several threads against one sequential pass
 // mode 3: an exception thrown by the callback reaches the caller
+// mode 4: block_states against jumps to the same blocks
 int main(int argc, char **argv) {
   const int mode = std::atoi(argv[1]), level = std::atoi(argv[2]);
   const long seed = std::atol(argv[3]);
@@ -99,6 +100,23 @@ int main(int argc, char **argv) {
   }
   const size_t count = std::atol(argv[4]);
   const unsigned long long first = std::strtoull(argv[5], nullptr, 10);
+  if (mode == 4) {  // block_states: every state continues the stream at its block
+    const unsigned long long first_block = count, stride = first;
+    const size_t n = std::atol(argv[6]);
+    std::vector<int64_t> w(12 * n);
+    if (!nrqh::block_states(level, seed, first_block, stride, n, w.data(), 8)) return 3;
+    long bad = 0;
+    for (size_t t = 0; t < n; ++t) {
+      nrqh::Ranlxd a, b;
+      a.init(level, seed);
+      b.init(level, seed);
+      a.load_block_state(&w[12 * t]);
+      if (!b.jump(12 * (first_block + stride * t))) return 3;
+      for (int i = 0; i < 36; ++i) bad += a.next() != b.next();
+    }
+    std::printf("%ld\n", bad);
+    return 0;
+  }
   if (mode == 3) {  // the callback throws at pair argv[6]: caught here, after every worker joined
     const size_t bad_at = std::atol(argv[6]);
     try {
@@ -214,3 +232,15 @@ def test_threaded_draw_passes_a_callback_exception_to_the_caller(jump_exe, bad_a
     has joined, instead of terminating the process."""
     r = subprocess.run([str(jump_exe), "3", "2", "3", "40000", "0", str(bad_at)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.split() == ["caught", "planted"], (r.returncode, r.stdout, r.stderr)
+
+
+@pytest.mark.parametrize("level,first_block,stride,n", [(2, 0, 37, 300), (2, 5, 1, 40), (1, 1000, 523, 70),
+                                                       (2, 10 ** 9, 12345, 20)])
+def test_block_states_continue_the_stream(jump_exe, level, first_block, stride, n):
+    """The device draw's starting states (one jump per host thread, one
+    modular multiplication per further state) continue the stream exactly
+    where a jump to the same block does (the jumps themselves are checked
+    against the oracle's stream above)."""
+    r = subprocess.run([str(jump_exe), "4", str(level), "11", str(first_block), str(stride), str(n)],
+                       capture_output=True, text=True, check=True)
+    assert r.stdout.split() == ["0"]
