@@ -528,7 +528,7 @@ extern "C" int nrq_gauge_update(nrq_gauge *g, double dt) {
       nrq::k_update_efield32<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U32, g->E, dt);
     } else {
       ProfScope ps(ctx, 5, V * (432.0 + 192.0 + 192.0));
-      nrq::k_update_efield<<<nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
+      nrq::k_update_efield<<<3 * nb_, 128, 0, ctx->stream>>>(ctx->lat, g->U, g->E, dt);
     }
   };
   // Update_Leapfrog ordering (gauge:2100-2110)

@@ -80,37 +80,45 @@ __global__ void __launch_bounds__(128) k_update_links(Lat L, double2 *__restrict
   }
 }
 
-__global__ void __launch_bounds__(128) k_update_efield(Lat L, const double2 *__restrict__ U,
+// blocks per SM the force kernel's registers are sized for
+#ifndef NRQ_EFIELD_MIN_BLOCKS
+#define NRQ_EFIELD_MIN_BLOCKS 3
+#endif
+
+// One thread per (site, direction i): the force on link (x, i) from its
+// four staples, k != i in ascending order as gauge:2147-2198 sums them.
+// Block b of the grid holds 128 consecutive sites of direction b % 3, so
+// the three directions of a site range run next to each other and share the
+// neighbour links in L2.
+__global__ void __launch_bounds__(128, NRQ_EFIELD_MIN_BLOCKS) k_update_efield(Lat L, const double2 *__restrict__ U,
                                                        double *__restrict__ E, double dt) {
-  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int i = (int)(blockIdx.x % 3);
+  const int64_t s = (int64_t)(blockIdx.x / 3) * blockDim.x + threadIdx.x;
   if (s >= L.V) return;
   const int64_t V = L.V;
-#pragma unroll 1
-  for (int i = 0; i < 3; ++i) {
-    m3 sum = m3_zero();
-    const int64_t xpi = nb(L, s, i, +1);
-#pragma unroll 1
-    for (int k = 0; k < 3; ++k) {
-      if (k == i) continue;
-      const double r = L.a0 / L.a[k];
-      const double coef = dt * (r * r);
-      const int64_t xpk = nb(L, s, k, +1), xmk = nb(L, s, k, -1);
-      const int64_t xpimk = nb(L, xmk, i, +1);
-      // U staple  U_k(x+i) U_i(x+k)^+ U_k(x)^+
-      m3 su = mul_nd(mul_nd(load_link(U, V, xpi, k), load_link(U, V, xpk, i)), load_link(U, V, s, k));
-      // D staple  U_k(x+i-k)^+ U_i(x-k)^+ U_k(x-k)
-      m3 sd = mul(dag(mul(load_link(U, V, xmk, i), load_link(U, V, xpimk, k))), load_link(U, V, xmk, k));
+  m3 sum = m3_zero();
+  const int64_t xpi = nb(L, s, i, +1);
 #pragma unroll
-      for (int m = 0; m < 9; ++m) sum.e[m] = sum.e[m] + coef * (su.e[m] + sd.e[m]);
-    }
-    m3 ls = mul(load_link(U, V, s, i), sum);
-    cplx tr[8];
-    traces_with_generators(ls, tr);
+  for (int k = 0; k < 3; ++k) {
+    if (k == i) continue;
+    const double r = L.a0 / L.a[k];
+    const double coef = dt * (r * r);
+    const int64_t xpk = nb(L, s, k, +1), xmk = nb(L, s, k, -1);
+    const int64_t xpimk = nb(L, xmk, i, +1);
+    // U staple  U_k(x+i) U_i(x+k)^+ U_k(x)^+
+    m3 su = mul_nd(mul_nd(load_link(U, V, xpi, k), load_link(U, V, xpk, i)), load_link(U, V, s, k));
+    // D staple  U_k(x+i-k)^+ U_i(x-k)^+ U_k(x-k)
+    m3 sd = mul(dag(mul(load_link(U, V, xmk, i), load_link(U, V, xpimk, k))), load_link(U, V, xmk, k));
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      double *e = E + (int64_t)(i * 8 + a) * V + s;
-      *e = *e - 2.0 * tr[a].im;
-    }
+    for (int m = 0; m < 9; ++m) sum.e[m] = sum.e[m] + coef * (su.e[m] + sd.e[m]);
+  }
+  m3 ls = mul(load_link(U, V, s, i), sum);
+  cplx tr[8];
+  traces_with_generators(ls, tr);
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double *e = E + (int64_t)(i * 8 + a) * V + s;
+    *e = *e - 2.0 * tr[a].im;
   }
 }
 
