@@ -41,11 +41,17 @@ MASS = 1.0
 WILSON = [1.0, 1.0, 1.0, 1.0]
 A = (0.05, 1.0, 1.0, 1.0)
 TOL = 1e-12
-# DRAM bytes per site of an average tensor-core stencil launch of the plain
-# solve, from one ncu capture of a 64^3 update (dram__bytes_read.sum +
-# dram__bytes_write.sum over its 2 residual, 4 v and 3 t launches: 10,773,
-# 7,760 and 6,377 B/site)
-STENCIL_DRAM_BYTES_PER_SITE = 7968.0
+# DRAM bytes per site of an average stencil launch of a plain 64^3 update
+# (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of the
+# update's 9 launches), by NRQ_STENCIL_* index: the tensor-core stencil (2
+# residual, 4 v and 3 t launches: 10,773, 7,760 and 6,377 B/site) and the
+# FMA stencil (1 right-hand side, 2 residual, 3 v and 3 t launches: 7,573,
+# 10,413, 7,500 and 6,199 B/site)
+STENCIL_DRAM_BYTES_PER_SITE = {2: 7968.0, 3: 7722.0}
+# FP64 arithmetic of the leapfrog force per site: 3 directions x (4 staples
+# of 2 products + the product with the link) = 27 complex 3x3 products of
+# 27 complex multiply-adds, 4 real FMAs each, 2 flops per FMA
+LEAPFROG_FORCE_FLOPS_PER_SITE = 27 * 27 * 4 * 2
 # FP64 stencils of the solver, by NRQ_STENCIL_* index
 STENCIL_NAMES = {0: "k_cn_mv2 (register-tiled)", 1: "k_cn_mv3 (TMA-staged)", 2: "k_cn_mv4 (FP64 tensor cores)",
                  3: "k_cn_mv5 (FP64 FMA on cached blocks)"}
@@ -242,9 +248,9 @@ def measure_thermal_ic(L, seed=1, cpu=True, cpu_sweeps=4, max_sweeps=200000):
            "algorithmic_bytes_per_site_sweep": THERMAL_BYTES_SITE_SWEEP,
            "algorithmic_GBps": THERMAL_BYTES_SITE_SWEEP * V * sweeps / (ms / 1000.0) / 1e9,
            "draw_ms": draw_ms,
-           "draw_note": "cold links, host ranlxd draw of the thermal field (the reference's one stream, split "
-                        "over host threads that jump to their share) and its upload",
-           "draw_threads": min(os.cpu_count() or 1, 32)}
+           "draw_note": "cold links and the device ranlxd draw of the thermal field: the reference's one "
+                        "stream, each device thread from a starting state the host jumps to (one modular "
+                        "multiplication per state), written into the field's planes"}
     if cpu:
         from oracle import oracle as oc
         n = (L, L, L)
@@ -679,6 +685,23 @@ def measure_fp64_peak(n=8192, reps=5):
     return 2.0 * n ** 3 / (best / 1000.0) / 1e12
 
 
+def leapfrog_summary(ms_per_step, prof, V, peak_gbps, fp64_tflops):
+    """Leapfrog-only steps: site-updates/s, and the force kernel against the
+    HBM and FP64 rooflines (its 816 B and 5,832 flops per site put it above
+    the FP64 ridge, so the FP64 peak bounds it)."""
+    ef, lk = prof["leapfrog_efield"], prof["leapfrog_links"]
+    ef_ms = ef["ms"] / max(1, ef["launches"])
+    out = {"ms_per_step": ms_per_step, "site_updates_per_s": V / (ms_per_step / 1000.0),
+           "links_ms": lk["ms"] / max(1, lk["launches"]), "force_ms": ef_ms}
+    if ef_ms > 0:
+        gbps = ef["bytes"] / max(1, ef["launches"]) / (ef_ms / 1000.0) / 1e9
+        tf = LEAPFROG_FORCE_FLOPS_PER_SITE * V / (ef_ms / 1000.0) / 1e12
+        out["force"] = {"algorithmic_GBps": gbps, "hbm_frac": gbps / peak_gbps, "fp64_tflops": tf,
+                        "fp64_frac": tf / fp64_tflops, "flops_per_site": LEAPFROG_FORCE_FLOPS_PER_SITE,
+                        "bytes_per_site": 816}
+    return out
+
+
 def member_seed(rank):
     """ranlxd seed of the ensemble member a rank evolves (replicas)."""
     return 1 + rank
@@ -867,6 +890,14 @@ def main():
                                         "k_cn_mv4_with_vec_s": float(tune_ms[2]),
                                         "k_cn_mv5_with_vec_s": float(tune_ms[3])}}
 
+    # ---------------- leapfrog-only steps (the long leapfrog phases before the
+    # propagators start), CUDA events on the library stream
+    lf_steps = 50
+    _capi.profile_enable(ctx, True)
+    lf_ms = timed_steps(lambda: g.Update(1.0), lf_steps, dist, CudaEventTimer(stream)) / lf_steps
+    lf_prof = _capi.profile_read(ctx)
+    _capi.profile_enable(ctx, False)
+
     # ---------------- end-to-end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -964,7 +995,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "CN 12-column stencil: " + stencil["in_use"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                         "traffic": (STENCIL_DRAM_BYTES_PER_SITE * V / 1e9 if tensor else None),
+                         "traffic": (STENCIL_DRAM_BYTES_PER_SITE[which] * V / 1e9
+                                     if which in STENCIL_DRAM_BYTES_PER_SITE else None),
                          "traffic_unit": "GB per launch (ncu capture of one 64^3 update, per site x V)",
                          "algorithmic_GB_per_launch": sten["bytes"] / max(1, sten["launches"]) / 1e9,
                          "algorithmic_bytes": "per 12-column launch: U and E once per species (2 x 624 B/site) "
@@ -979,6 +1011,7 @@ def main():
                          "fp64": {"flops_per_site_per_launch": flops_site, "achieved_tflops": fp64_achieved,
                                   "peak_tflops": p64, "peak_source": "measured (cuBLAS DGEMM, torch.matmul)",
                                   "frac": fp64_achieved / p64 if fp64_achieved else None}},
+            "leapfrog_only": leapfrog_summary(lf_ms, lf_prof, V, peak, p64),
             "kernel_classes": prof,
             "stencil": stencil,
             "cn": {"iterations_per_step": float(np.mean(its)) if its else None,
