@@ -344,6 +344,8 @@ def measure_gluon_distribution(L, cpu=True, steps=10):
 FORMS = {"plain_fp64_bicgstab": (0, 1), "plain_fp64_bicgstab_no_history": (0, 0),
          "precision_fp32_chebyshev_fp64_refinement": (1, 1), "learned_guess_precision": (2, 1)}
 FORMS_SIZES = (64, 96, 128)
+# lattices of the precision form's drift (the precision configuration names 64^3 and 96^3)
+DRIFT_SIZES = (64, 96)
 
 
 def train_learned(tol=1e-10, masses=(MASS,)):
@@ -444,9 +446,10 @@ def measure_all_forms(steps, sizes=FORMS_SIZES, learned=None):
 def measure_precision_drift(L, n0, steps, seed=1):
     """The precision form end to end (FP32-link leapfrog with FP64
     reunitarisation every 10 steps, FP32 Chebyshev CN with FP64 refinement
-    at 1e-10) against the FP64 path (FP64 leapfrog, plain FP64 CN at 1e-12)
-    from the same seeded fields: the drift of every observable after `steps`
-    coupled steps, and the s/step of both paths (CUDA events)."""
+    at 1e-10), its CN half alone on FP64 links, and the FP64 path at 1e-10,
+    against the FP64 path (FP64 leapfrog, plain FP64 CN at 1e-12) from the
+    same seeded fields: the drift of every observable after `steps` coupled
+    steps, and the s/step of every path (CUDA events)."""
     import torch
     from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice
     lib = _capi.load()
@@ -456,7 +459,12 @@ def measure_precision_drift(L, n0, steps, seed=1):
     try:
         stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(lat.ctx))
         paths = {}
-        for name, form, tol, prec in (("fp64", 0, 1e-12, 0), ("precision", 1, 1e-10, 1)):
+        # the FP64 path at the headline residual (the drift reference), the
+        # FP64 path at the forms' residual 1e-10, the whole precision form
+        # (FP32-link leapfrog and FP32 Chebyshev CN with FP64 refinement), and
+        # its CN half alone on FP64 links
+        for name, form, tol, prec in (("fp64", 0, 1e-12, 0), ("fp64_1e-10", 0, 1e-10, 0),
+                                      ("precision", 1, 1e-10, 1), ("precision_cn_fp64_links", 1, 1e-10, 0)):
             g = GaugeConfiguration(lat=lat)
             g.TransversePolarisedOccupiedInit_Box(0.5, n0, 0.0, RandomSeed=seed, identity_links=True)
             if prec:
@@ -497,18 +505,24 @@ def measure_precision_drift(L, n0, steps, seed=1):
                          "norm_antiq_minus_1": h.GetNorm_AntiQ() - 1.0,
                          "unitarity_max_dev": g.GetUnitarityDeviation()[0]}
         la, ea = paths["fp64"]["g"].download()
-        lb, eb = paths["precision"]["g"].download()
         qa, aa = paths["fp64"]["h"].download()
-        qb, ab = paths["precision"]["h"].download()
-        out["fp64"] = res["fp64"]
-        out["precision"] = res["precision"]
-        out["drift_vs_fp64"] = {
-            "energy_rel": abs(res["precision"]["energy"] - res["fp64"]["energy"]) / abs(res["fp64"]["energy"]),
-            "gauss_max_norm_abs": abs(res["precision"]["gauss_max_norm"] - res["fp64"]["gauss_max_norm"]),
-            "links_max_abs": float(np.abs(lb - la).max()), "efield_max_abs": float(np.abs(eb - ea).max()),
-            "propagator_max_abs": float(max(np.abs(qb - qa).max(), np.abs(ab - aa).max())),
-            "norm_abs": abs(res["precision"]["norm_quark_minus_1"] - res["fp64"]["norm_quark_minus_1"])}
+
+        def drift(name):
+            lb, eb = paths[name]["g"].download()
+            qb, ab = paths[name]["h"].download()
+            r, f = res[name], res["fp64"]
+            return {"energy_rel": abs(r["energy"] - f["energy"]) / abs(f["energy"]),
+                    "gauss_max_norm_abs": abs(r["gauss_max_norm"] - f["gauss_max_norm"]),
+                    "links_max_abs": float(np.abs(lb - la).max()), "efield_max_abs": float(np.abs(eb - ea).max()),
+                    "propagator_max_abs": float(max(np.abs(qb - qa).max(), np.abs(ab - aa).max())),
+                    "norm_abs": abs(r["norm_quark_minus_1"] - f["norm_quark_minus_1"])}
+        for name in res:
+            out[name] = res[name]
+        out["drift_vs_fp64"] = drift("precision")
+        out["drift_vs_fp64_by_path"] = {name: drift(name) for name in res if name != "fp64"}
         out["speedup_coupled_step"] = res["fp64"]["s_per_step"] / res["precision"]["s_per_step"]
+        out["speedup_vs_fp64_at_1e-10"] = {name: res["fp64_1e-10"]["s_per_step"] / res[name]["s_per_step"]
+                                           for name in ("precision", "precision_cn_fp64_links")}
         for p in paths.values():
             lib.nrq_cn_finalize(p["cn"])
             p["h"].Destructor()
@@ -805,7 +819,7 @@ def main():
     if args.only_drift:
         import torch
         torch.cuda.set_device(local)
-        out = [measure_precision_drift(args.size, n0, 20) for n0 in (0.5, 1.0, 2.0)]
+        out = [measure_precision_drift(size, n0, 20) for size in DRIFT_SIZES for n0 in (0.5, 1.0, 2.0)]
         if rank == 0:
             print(json.dumps({"precision_drift": out}), flush=True)
         return
@@ -947,7 +961,7 @@ def main():
 
     drift = None
     if not args.no_drift and world == 1:
-        drift = [measure_precision_drift(L, n0, 20) for n0 in (0.5, 1.0, 2.0)]
+        drift = [measure_precision_drift(size, n0, 20) for size in DRIFT_SIZES for n0 in (0.5, 1.0, 2.0)]
 
     forms = None
     if not args.no_forms and world == 1:
