@@ -10,34 +10,42 @@
 // coefficients the backward block is -W_I(x-I)^H, read from the forward
 // block of x-I, and A^H differs from A by the sign of the neighbour sum.
 //
-// Products.  A thread owns a 3 x 3 tile of one site and species: the three
-// output rows of one spin (the three colours) and three of the six columns,
-// 18 doubles in registers.  Per neighbour and input row q it reads 3 block
-// entries and 3 spinor entries from shared memory and does 36 FP64 FMAs,
-// none of them padding.  On B200 the FP64 FMA pipe and the FP64 tensor pipe
-// have the same peak, and the tensor pipe's 16x8 tiles hold 12 x 6 useful
-// entries.  A 16-byte shared-memory load costs four wavefronts per warp
-// whether or not lanes share addresses, so every warp holds 32 consecutive
-// sites of one (species, spin, column half): each load then delivers 512
-// distinct bytes without bank conflicts, and the tile size sets the traffic.
+// Products.  Four threads share the 6x6 product of one site, species and
+// neighbour: thread (kh, h) accumulates all six output rows of columns
+// 3h .. 3h+2 over the input rows q = 3kh .. 3kh+2, 36 doubles in registers.
+// Per input row it reads 6 block entries and 3 spinor entries from shared
+// memory and does 72 FP64 FMAs, none of them padding: 108 16-byte loads per
+// site, species and neighbour, against 144 for four 3x3 tiles over all six
+// input rows.  On B200 the FP64 FMA pipe and the FP64 tensor pipe have the
+// same peak, and the tensor pipe's 16x8 tiles hold 12 x 6 useful entries.  A
+// 16-byte shared-memory load costs four wavefronts per warp whether or not
+// lanes share addresses, so every warp holds 32 consecutive sites of one
+// (row half, species, column half): each load then delivers 512 distinct
+// bytes without bank conflicts, and the loads per site set the traffic.
+// After a unit's last stage the two row-half warps of a (species, column
+// half) sum their partial tiles through tensor memory (each keeps three of
+// the six rows; exchange_halves), which takes no shared memory.
 //
-// Pipeline.  Persistent, one CTA per SM: 8 consumer warps (species 0 in
-// warps 0-3, species 1 in 4-7; a warp holds one spin and column half of a
-// 32-site unit) and one producer warp.  Ten loads per unit, per stage and species
-// (stage 0: diagonal matrices, +x and -x; 1: +y; 2: -y; 3: +z; 4: -z): a
-// spinor tile (34 sites x 36 planes) and a block tile (34 sites x 36 entry
-// planes) by TMA, into a ring of four shared-memory buffers completed on
-// mbarriers; the unit's diagonal matrices go with its first load into one
-// of two further buffers.  The producer refills a buffer once the four consumer warps of
-// its species released it and its previous load has landed.  The periodic
-// x neighbours that wrap outside a unit's tile (one site at each row end)
-// arrive as two extra one-site spinor columns and one block column with
-// stage 0; a lane whose neighbour or block lies anywhere else outside the
-// tiles (rows shorter than the tile) reads it from global memory.  Results go straight to global
-// memory; the epilogue's operand at the own site is prefetched into L1 two
-// stages before the epilogue reads it; the residual and dot-product
-// partial sums stay in registers over all units of the CTA (one partial row
-// per CTA).
+// Pipeline.  Persistent, one CTA per SM: 8 consumer warps (warp 4kh + 2sp +
+// h) and a producer warpgroup, whose first warp issues the loads and which
+// hands its registers to the consumers (setmaxnreg: 232 per consumer thread,
+// which the 36 accumulators and the epilogue's operands need).  Ten loads per
+// unit, per stage and species (stage 0: diagonal matrices, +x and -x; 1: +y;
+// 2: -y; 3: +z; 4: -z): a spinor tile (34 sites x 36 planes) and a block tile
+// (34 sites x 36 entry planes) by TMA, into a ring of five shared-memory
+// buffers completed on mbarriers, one full barrier per buffer and species;
+// the unit's diagonal matrices go with its first load into one of two
+// further buffers.  The producer refills a buffer once the four consumer
+// warps of its species released it and its previous load has landed.  The
+// periodic x neighbours that wrap outside a unit's tile (one site at each
+// row end) arrive as two extra one-site spinor columns and one block column
+// with stage 0; a lane whose neighbour or block lies anywhere else outside
+// the tiles (rows shorter than the tile) reads it from global memory.
+// Results go straight to global memory; the epilogue's operand at the own
+// site is loaded into registers two stages before the epilogue (the ring
+// takes nearly all of the shared memory, so L1 is too small to hold it);
+// the residual and dot-product partial sums stay in registers over all
+// units of the CTA (one partial row per CTA).
 //
 // Every mbarrier wait is bounded (wait_cycles); on expiry the thread records
 // NRQ_ERR_TIMEOUT in *err and skips the remaining work.  The producer never
@@ -52,24 +60,33 @@
 #include "../../include/nrqcd_b200.h"
 #include "nrq_kernels.cuh"
 #include "stage.cuh"
+#include "tc.cuh"
 
 namespace nrq {
 
 namespace mv5 {
 constexpr int kUnit = 32;                 // sites per work unit (one per lane)
 constexpr int kWarps = 8;                 // consumer warps: (species, spin, column half)
-constexpr int kThreads = (kWarps + 1) * 32;
-constexpr int kMaxReg = 168;              // three warps on one SM quarter: 3 x 32 x 168 <= 16384
+// the producer warpgroup (warps 8-11: warp 8 loads, 9-11 leave) gives its
+// registers to the two consumer warpgroups (setmaxnreg)
+constexpr int kThreads = (kWarps + 4) * 32;
+constexpr int kMaxReg = 168;              // at launch: 12 warps x 32 x 168 = 64512 registers
+constexpr int kProdReg = 40, kConsReg = 232;
 constexpr int kStages = 5;                // stages per unit
 constexpr int kLoads = 2 * kStages;       // loads per unit: (stage, species)
-// Ring of load buffers.  Loads alternate between the species, and a
-// consumer waits on a buffer's full barrier by phase parity, which is only
-// sound while it never waits more than one phase ahead of the barrier's
-// last completed phase.  With an even ring every use of a buffer belongs to
-// one species, whose warps released the previous use themselves; an odd
-// ring would let one species wait two phases ahead of a load of the other
-// that is still in flight, and pass the wait on a stale parity.
-constexpr int kBufs = 4;
+// Ring of load buffers.  Loads alternate between the species (load i is of
+// species i & 1), and a consumer waits on a full barrier by phase parity,
+// which is only sound while it never waits more than one phase ahead of the
+// barrier's last completed phase.  Each buffer therefore has one full
+// barrier per species, completed only by that species' loads: the k-th load
+// of a species into a buffer is load i with i / kPer = k, and its consumers
+// released the (k-1)-th themselves.  With an odd ring the uses of a buffer
+// alternate species; a single full barrier per buffer would then let one
+// species wait two phases ahead of a load of the other still in flight and
+// pass the wait on a stale parity.  The empty barriers have one waiter, the
+// producer, which takes every use of a buffer in order.
+constexpr int kBufs = 5;
+constexpr int kPer = (kBufs % 2) ? 2 * kBufs : kBufs;  // loads between two uses of one (buffer, species)
 constexpr int kTileS = kUnit + 2;         // tile width in sites (x0 - 1 .. x0 + 32)
 constexpr uint32_t kTileBytes = 36u * kTileS * 16u;    // 19584: 36 planes x 34 sites
 constexpr uint32_t kOffW = kTileBytes;                 // block tile (36 entry planes)
@@ -85,14 +102,17 @@ constexpr uint32_t kBufBytes = ((kOffX + 3u * kColStride) + 1023u) & ~1023u;  //
 constexpr uint32_t kDiagD = 9u * kUnit * 16u;          // 4608
 constexpr uint32_t kDiagB = 9u * kUnit * 8u;           // 2304
 constexpr uint32_t kDiagStride = 7168u;
-constexpr uint32_t kOffDiag = kBufs * kBufBytes;       // 167936
-constexpr uint32_t kSmemBytes = kOffDiag + 2u * kDiagStride + 1024u;           // 183296
+constexpr uint32_t kOffDiag = kBufs * kBufBytes;       // 209920
+constexpr uint32_t kSmemBytes = kOffDiag + 2u * kDiagStride + 1024u;           // 225280
+constexpr uint32_t kTmemCols = 128;  // the exchange: columns 0-35 and 64-99 of every lane
 static_assert(kOffW % 128 == 0 && kOffX % 128 == 0 && kColStride % 128 == 0 && kColStride >= kColBytes &&
                   kBufBytes % 1024 == 0 && kDiagStride % 128 == 0 && kDiagD + kDiagB <= kDiagStride,
               "layout");
 static_assert(kSmemBytes + 1024 <= 232448, "shared memory");
-static_assert(kBufs % 2 == 0 && kLoads % 2 == 0, "a buffer's uses must all belong to one species");
-static_assert(kMaxReg * 32 * 3 <= 16384, "registers of an SM quarter (three warps)");
+static_assert(kLoads % 2 == 0, "load i is of species i & 1");
+static_assert(kMaxReg * kThreads <= 65536 && kMaxReg * 32 * 3 <= 16384, "registers at launch");
+static_assert(kProdReg * 128 + kConsReg * 256 <= kMaxReg * kThreads && (2 * kConsReg + kProdReg) * 32 <= 16384,
+              "the split draws only on the launch's registers and fits each SM quarter");
 }  // namespace mv5
 
 struct Mv5Maps {
@@ -232,33 +252,121 @@ __device__ __forceinline__ double lds_d1(uint32_t a) {
   return v;
 }
 
-// The thread's tile (rows 2c + s, c = 0..2; columns 3h + k, k = 0..2) +=
-// sum over q of w[c][q] psi[q][3h + k].  Forward: w[c][q] = W(x)[2c+s][q],
-// entry (2c+s)*6 + q; backward: w[c][q] = -conj(W(y)[q][2c+s]), entry
-// q*6 + 2c + s.  load_w(e) reads entry e of the
-// block, load_p(e) plane e of the spinor (species planes), from the shared
-// tiles or global memory.
+// The thread's partial tile (rows r = 0..5; columns 3h + k, k = 0..2) +=
+// sum over its three input rows q = 3 kh + qq of w[r][q] psi[q][3h + k].
+// Forward: w[r][q] = W(x)[r][q], entry r*6 + q; backward: w[r][q] =
+// -conj(W(y)[q][r]), entry q*6 + r.  load_w(e) reads entry e of the block,
+// load_p(e) plane e of the spinor (species planes), from the shared tiles
+// or global memory.
 template <bool BWD, typename LW, typename LP>
-__device__ __forceinline__ void nb_products(double (&acc)[3][3][2], int s, int h, LW load_w, LP load_p) {
+__device__ __forceinline__ void nb_products(double (&acc)[6][3][2], int kh, int h, LW load_w, LP load_p) {
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    double wr[3], wi[3];
+  for (int qq = 0; qq < 3; ++qq) {
+    const int q = 3 * kh + qq;
+    double wr[6], wi[6];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const double2 wv = load_w(BWD ? q * 6 + 2 * c + s : (2 * c + s) * 6 + q);
-      wr[c] = BWD ? -wv.x : wv.x;
-      wi[c] = wv.y;
+    for (int r = 0; r < 6; ++r) {
+      const double2 wv = load_w(BWD ? q * 6 + r : r * 6 + q);
+      wr[r] = BWD ? -wv.x : wv.x;
+      wi[r] = wv.y;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const double2 p = load_p((3 * h + k) * 6 + q);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        acc[c][k][0] = fma(wr[c], p.x, fma(-wi[c], p.y, acc[c][k][0]));
-        acc[c][k][1] = fma(wr[c], p.y, fma(wi[c], p.x, acc[c][k][1]));
+      for (int r = 0; r < 6; ++r) {
+        acc[r][k][0] = fma(wr[r], p.x, fma(-wi[r], p.y, acc[r][k][0]));
+        acc[r][k][1] = fma(wr[r], p.y, fma(wi[r], p.x, acc[r][k][1]));
       }
     }
   }
+}
+
+// The diagonal (colour only) of the thread's input rows q = 3 KH + qq: row
+// 2c + (q & 1) takes cd[c][q >> 1] psi[q], cd from the unit's D and B tiles.
+template <int KH>
+__device__ __forceinline__ void diag_products(double (&acc)[6][3][2], int h, uint32_t s_d, uint32_t s_b,
+                                              uint32_t s_own, cplx ad, cplx am, cplx dg, double nb_sign) {
+#pragma unroll
+  for (int qq = 0; qq < 3; ++qq) {
+    constexpr int kTile = mv5::kTileS * 16;
+    const int q = 3 * KH + qq, j = q >> 1, sq = q & 1;
+    cplx cd[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int e = j * 3 + c;
+      const double2 dv = lds_d2(s_d + (uint32_t)(e * mv5::kUnit * 16));
+      const double bv = lds_d1(s_b + (uint32_t)(e * mv5::kUnit * 8));
+      cd[c] = ad * cplx{dv.x, dv.y} + bv * am;
+      if (j == c) cd[c] = cd[c] + dg;
+      cd[c] = nb_sign * cd[c];  // see the epilogue
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double2 p = lds_d2(s_own + (uint32_t)(((3 * h + k) * 6 + q) * kTile));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        acc[2 * c + sq][k][0] = fma(cd[c].re, p.x, fma(-cd[c].im, p.y, acc[2 * c + sq][k][0]));
+        acc[2 * c + sq][k][1] = fma(cd[c].re, p.y, fma(cd[c].im, p.x, acc[2 * c + sq][k][1]));
+      }
+    }
+  }
+}
+
+// Tensor memory as the scratch of the exchange: 36 columns of 32 bits per
+// lane (nine complex doubles), the lane quarter of the warp.
+__device__ __forceinline__ void tmem_st36(uint32_t taddr, const uint32_t (&w)[36]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr), "r"(w[0]), "r"(w[1]), "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7]), "r"(w[8]), "r"(w[9]), "r"(w[10]), "r"(w[11]), "r"(w[12]), "r"(w[13]), "r"(w[14]), "r"(w[15]), "r"(w[16]), "r"(w[17]), "r"(w[18]), "r"(w[19]), "r"(w[20]), "r"(w[21]), "r"(w[22]), "r"(w[23]), "r"(w[24]), "r"(w[25]), "r"(w[26]), "r"(w[27]), "r"(w[28]), "r"(w[29]), "r"(w[30]), "r"(w[31]) : "memory");
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr + 32u), "r"(w[32]),
+               "r"(w[33]), "r"(w[34]), "r"(w[35])
+               : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld36(uint32_t taddr, uint32_t (&w)[36]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7]), "=r"(w[8]), "=r"(w[9]), "=r"(w[10]), "=r"(w[11]), "=r"(w[12]), "=r"(w[13]), "=r"(w[14]), "=r"(w[15]), "=r"(w[16]), "=r"(w[17]), "=r"(w[18]), "=r"(w[19]), "=r"(w[20]), "=r"(w[21]), "=r"(w[22]), "=r"(w[23]), "=r"(w[24]), "=r"(w[25]), "=r"(w[26]), "=r"(w[27]), "=r"(w[28]), "=r"(w[29]), "=r"(w[30]), "=r"(w[31]) : "r"(taddr) : "memory");
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(w[32]), "=r"(w[33]), "=r"(w[34]), "=r"(w[35])
+               : "r"(taddr + 32u)
+               : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// The two warps of a (species, column half) hold partial tiles over the two
+// halves of the input rows; warp kh keeps output rows 3 kh .. 3 kh + 2.  Both
+// share a tensor-memory lane quarter (warp & 3): each writes the other's
+// three rows into its own 36 columns (64 kh ..), and after the pair's
+// barrier reads the partner's columns and adds them to its rows.
+template <int KH>
+__device__ __forceinline__ void exchange_halves(const double (&acc)[6][3][2], double (&res)[3][3][2],
+                                                uint32_t tbase, int warp, int bar_id) {
+  const uint32_t quarter = tbase + ((uint32_t)(32 * (warp & 3)) << 16);
+  uint32_t w[36];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri) {
+        const double v = acc[3 * (1 - KH) + i][k][ri];
+        w[(i * 3 + k) * 4 + 2 * ri] = (uint32_t)__double2loint(v);
+        w[(i * 3 + k) * 4 + 2 * ri + 1] = (uint32_t)__double2hiint(v);
+      }
+  tmem_st36(quarter + 64u * KH, w);
+  tc::fence_before_sync();
+  named_bar_sync(bar_id, 64);
+  tc::fence_after_sync();
+  tmem_ld36(quarter + 64u * (1 - KH), w);
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int ri = 0; ri < 2; ++ri)
+        res[i][k][ri] = acc[3 * KH + i][k][ri] +
+                        __hiloint2double((int)w[(i * 3 + k) * 4 + 2 * ri + 1], (int)w[(i * 3 + k) * 4 + 2 * ri]);
+  tc::fence_before_sync();
+  named_bar_sync(bar_id, 64);  // the columns are free for the next unit
+  tc::fence_after_sync();
 }
 
 }  // namespace
@@ -269,8 +377,9 @@ __global__ void __maxnreg__(mv5::kMaxReg)
              MvArgs A, int nunits, int *err, long long wait_cycles, int stall_load) {
   using namespace mv5;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[kBufs], empty_bar[kBufs], dfull[2], dempty[2];
+  __shared__ __align__(8) uint64_t full_bar[kBufs][2], empty_bar[kBufs], dfull[2], dempty[2];
   __shared__ volatile int s_issued;  // loads the producer issued (diagnostics of an expired wait)
+  __shared__ uint32_t s_tmem;        // the exchange's tensor-memory columns
   __shared__ double red[kWarps][3][3];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -279,7 +388,8 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   if (threadIdx.x == 0) {
     s_issued = 0;
     for (int b = 0; b < kBufs; ++b) {
-      mbar_init(&full_bar[b], 1);
+      mbar_init(&full_bar[b][0], 1);
+      mbar_init(&full_bar[b][1], 1);
       mbar_init(&empty_bar[b], 4);  // the four consumer warps of the load's species
     }
     for (int b = 0; b < 2; ++b) {
@@ -288,7 +398,11 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (warp == 0) tc::tmem_alloc(&s_tmem, kTmemCols);
+  tc::fence_before_sync();
   __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = s_tmem;
 
   const int my_units = (nunits - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   const int total = my_units * kLoads;
@@ -303,8 +417,9 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   };
 
   // ---------------------------------------------------------- producer
-  if (warp == kWarps) {
-    if (lane == 0) {
+  if (warp >= kWarps) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kProdReg));
+    if (warp == kWarps && lane == 0) {
       const int stop = stall_load >= 0 ? min(stall_load, total) : total;
       bool ok = true;
       int i = 0, ndiag = 0;
@@ -313,12 +428,13 @@ __global__ void __maxnreg__(mv5::kMaxReg)
         const int b = i % kBufs;
         if (i >= kBufs) {
           const uint32_t par = (uint32_t)((i / kBufs - 1) & 1);
+          const int j = i - kBufs;  // the buffer's previous load
           // every consumer warp of the species released the buffer, and its
           // previous load landed
           if (!wait(&empty_bar[b], par)) {
             record_timeout(err, 5, 2, i);
             ok = false;
-          } else if (!mbar_wait(&full_bar[b], par)) {
+          } else if (!mbar_wait(&full_bar[b][j & 1], (uint32_t)((j / kPer) & 1))) {
             record_timeout(err, 5, 3, i);
             ok = false;
           }
@@ -354,22 +470,23 @@ __global__ void __maxnreg__(mv5::kMaxReg)
         if (stg == 0) x_wraps5(L, P, yl, yr);
         uint32_t tx = 2u * kTileBytes;
         if (stg == 0) tx += (yl >= 0 ? 2u : 0u) * kColBytes + (yr >= 0 ? kColBytes : 0u);
-        mbar_expect_tx(&full_bar[b], tx);
-        tma_2d(bb, &maps.spin, 2 * ss, sp * 36, &full_bar[b]);
-        tma_2d(bb + kOffW, &maps.W, 2 * ws, (I * 2 + sp) * 36, &full_bar[b]);
+        uint64_t *fb = &full_bar[b][sp];
+        mbar_expect_tx(fb, tx);
+        tma_2d(bb, &maps.spin, 2 * ss, sp * 36, fb);
+        tma_2d(bb + kOffW, &maps.W, 2 * ws, (I * 2 + sp) * 36, fb);
         if (stg == 0) {
           if (yl >= 0) {
-            tma_2d(bb + kOffX, &maps.spin1, 2 * yl, sp * 36, &full_bar[b]);
-            tma_2d(bb + kOffX + kColStride, &maps.W1, 2 * yl, sp * 36, &full_bar[b]);
+            tma_2d(bb + kOffX, &maps.spin1, 2 * yl, sp * 36, fb);
+            tma_2d(bb + kOffX + kColStride, &maps.W1, 2 * yl, sp * 36, fb);
           }
-          if (yr >= 0) tma_2d(bb + kOffX + 2 * kColStride, &maps.spin1, 2 * yr, sp * 36, &full_bar[b]);
+          if (yr >= 0) tma_2d(bb + kOffX + 2 * kColStride, &maps.spin1, 2 * yr, sp * 36, fb);
         }
         s_issued = i + 1;
       }
       // every issued load lands before the CTA exits: loads before the last
       // kBufs were waited for above
       for (int k = max(0, i - kBufs); k < i; ++k)
-        if (!mbar_wait(&full_bar[k % kBufs], (uint32_t)((k / kBufs) & 1))) {
+        if (!mbar_wait(&full_bar[k % kBufs][k & 1], (uint32_t)((k / kPer) & 1))) {
           record_timeout(err, 5, 4, k);
           break;
         }
@@ -381,12 +498,16 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     }
     return;
   }
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kConsReg));
 
   // ---------------------------------------------------------- consumers
-  // warp w = 4 sp + 2 s + h: species sp, spin s, column half h; lane = site
-  // of the 32-site unit.  The thread owns rows 2c + s (c = 0..2) and columns
-  // 3h .. 3h + 2 of its site and species.
-  const int sp = warp >> 2, s = (warp >> 1) & 1, h = warp & 1;
+  // warp w = 4 kh + 2 sp + h: input-row half kh, species sp, column half h;
+  // lane = site of the 32-site unit.  The thread accumulates all six output
+  // rows of columns 3h .. 3h + 2 over input rows 3 kh .. 3 kh + 2 of its site
+  // and species; after the unit's last stage it keeps rows 3 kh .. 3 kh + 2
+  // of the sum (exchange_halves with warp w ^ 4).
+  const int kh = warp >> 2, sp = (warp >> 1) & 1, h = warp & 1;
+  const int pair_bar = 2 + (warp & 3);  // named barrier of the warp pair (ids 2-5)
   const int site_in_unit = lane;
   constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
   double qs[3][3];
@@ -406,31 +527,29 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     neighbours5(L, P, xs - x0, nb);
     int yl = -1, yr = -1;
     x_wraps5(L, P, yl, yr);
-    double acc[3][3][2];
+    double acc[6][3][2];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 6; ++r)
 #pragma unroll
-      for (int k = 0; k < 3; ++k) acc[c][k][0] = acc[c][k][1] = 0.0;
+      for (int k = 0; k < 3; ++k) acc[r][k][0] = acc[r][k][1] = 0.0;
     // the epilogue's operand at the own site: b for the residuals, rh for V,
     // the input itself for RHS and T
     const double2 *epi_src = (MODE == MV_V) ? A.in2 : (MODE == MV_RES || MODE == MV_RESC) ? A.bvec : A.in;
+    cplx ev[3][3];
 
 #pragma unroll
     for (int stg = 0; stg < kStages; ++stg) {
       const int ld = u * kLoads + stg * 2 + sp;
       const int b = ld % kBufs;
       if (stg == kStages - 2 && MODE != MV_PLAIN) {
-        // brought into L1 two stages ahead (no registers held), read there
-        // in the epilogue
+        // the epilogue's operand, loaded into registers two stages ahead
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int k = 0; k < 3; ++k)
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(epi_src + (int64_t)(sp * 36 + (3 * h + k) * 6 + 2 * c + s) * V +
-                                                          xs));
+          for (int k = 0; k < 3; ++k) ev[i][k] = ldg(epi_src + (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + xs);
       }
       int role = -1;
-      if (!dead && !wait(&full_bar[b], (uint32_t)((ld / kBufs) & 1))) role = 0;
+      if (!dead && !wait(&full_bar[b][sp], (uint32_t)((ld / kPer) & 1))) role = 0;
       // stage 0 also reads the unit's diagonal matrices
       if (stg == 0 && !dead && role < 0 && !wait(&dfull[u & 1], (uint32_t)((u >> 1) & 1))) role = 1;
       // warp-uniform: the products below use warp votes
@@ -439,11 +558,12 @@ __global__ void __maxnreg__(mv5::kMaxReg)
         if (role >= 0) {
           record_timeout(err, 5, role, ld);
           if (err[3] == (int)blockIdx.x && err[2] == ld) {  // this thread's record: add the detail
-            const uint64_t word = role == 0 ? *(volatile uint64_t *)&full_bar[b] : *(volatile uint64_t *)&dfull[u & 1];
+            const uint64_t word =
+                role == 0 ? *(volatile uint64_t *)&full_bar[b][sp] : *(volatile uint64_t *)&dfull[u & 1];
             err[4] = s_issued + 1;
             err[5] = (int)(uint32_t)word;
             err[6] = (int)(uint32_t)(word >> 32);
-            err[7] = role == 0 ? (ld / kBufs) & 1 : (u >> 1) & 1;
+            err[7] = role == 0 ? (ld / kPer) & 1 : (u >> 1) & 1;
           }
         }
       }
@@ -458,29 +578,11 @@ __global__ void __maxnreg__(mv5::kMaxReg)
           const unsigned char *dd = smem + kOffDiag + (u & 1) * kDiagStride;
           const uint32_t s_d = smem_u32(dd) + (uint32_t)(site_in_unit * 16);
           const uint32_t s_b = smem_u32(dd + kDiagD) + (uint32_t)(site_in_unit * 8);
-          const uint32_t s_own = s_tile + (uint32_t)((site_in_unit + 1) * 16 + s * kTileS * 16);
-#pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            cplx cd[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-              const int e = j * 3 + c;
-              const double2 dv = lds_d2(s_d + (uint32_t)(e * kUnit * 16));
-              const double bv = lds_d1(s_b + (uint32_t)(e * kUnit * 8));
-              cd[c] = ad * cplx{dv.x, dv.y} + bv * am;
-              if (j == c) cd[c] = cd[c] + dg;
-              cd[c] = nb_sign * cd[c];  // see the epilogue
-            }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-              const double2 p = lds_d2(s_own + (uint32_t)(((3 * h + k) * 6 + 2 * j) * kTileS * 16));
-#pragma unroll
-              for (int c = 0; c < 3; ++c) {
-                acc[c][k][0] = fma(cd[c].re, p.x, fma(-cd[c].im, p.y, acc[c][k][0]));
-                acc[c][k][1] = fma(cd[c].re, p.y, fma(cd[c].im, p.x, acc[c][k][1]));
-              }
-            }
-          }
+          const uint32_t s_own = s_tile + (uint32_t)((site_in_unit + 1) * 16);
+          if (kh == 0)
+            diag_products<0>(acc, h, s_d, s_b, s_own, ad, am, dg, nb_sign);
+          else
+            diag_products<1>(acc, h, s_d, s_b, s_own, ad, am, dg, nb_sign);
         }
         // neighbours of this stage: stage 0 = +x (forward) and -x (backward)
 #pragma unroll
@@ -506,18 +608,18 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             auto lw = [&](int e) { return lds_d2(wa + (uint32_t)e * wst); };
             auto lp = [&](int e) { return lds_d2(pa + (uint32_t)e * pst); };
             if (bwd)
-              nb_products<true>(acc, s, h, lw, lp);
+              nb_products<true>(acc, kh, h, lw, lp);
             else
-              nb_products<false>(acc, s, h, lw, lp);
+              nb_products<false>(acc, kh, h, lw, lp);
           } else if (__all_sync(0xffffffffu, (ps && wsh) || !act)) {
             // every operand of the warp in shared memory
             const uint32_t wa = s_w + (uint32_t)((m - ws) * 16), pa = s_tile + (uint32_t)((y - ss) * 16);
             auto lw = [&](int e) { return lds_d2(wa + (uint32_t)(e * kTileS * 16)); };
             auto lp = [&](int e) { return lds_d2(pa + (uint32_t)(e * kTileS * 16)); };
             if (bwd)
-              nb_products<true>(acc, s, h, lw, lp);
+              nb_products<true>(acc, kh, h, lw, lp);
             else
-              nb_products<false>(acc, s, h, lw, lp);
+              nb_products<false>(acc, kh, h, lw, lp);
           } else if (act) {
             // some lanes' operands outside the tiles (periodic wraps, tile
             // edges): those lanes read global memory, the others the tiles
@@ -528,9 +630,9 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             auto lw = [&](int e) { return wp[e * wst]; };
             auto lp = [&](int e) { return pp[e * pst]; };
             if (bwd)
-              nb_products<true>(acc, s, h, lw, lp);
+              nb_products<true>(acc, kh, h, lw, lp);
             else
-              nb_products<false>(acc, s, h, lw, lp);
+              nb_products<false>(acc, kh, h, lw, lp);
           }
         }
       }
@@ -542,45 +644,52 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     }
 
     // ---------------------------------------------------------- epilogue
+    // every warp of the pair takes both barriers of the exchange, dead or
+    // not, active lanes or not
+    double res[3][3][2];
+    if (kh == 0)
+      exchange_halves<0>(acc, res, tbase, warp, pair_bar);
+    else
+      exchange_halves<1>(acc, res, tbase, warp, pair_bar);
     if (!dead && act) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
+      for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const int64_t off = (int64_t)(sp * 36 + (3 * h + k) * 6 + 2 * c + s) * V + x;
+          const int64_t off = (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + x;
           // D in + sgn N in = sgn (sgn D in + N in), sgn = +-1: the diagonal
           // was scaled by sgn and the neighbour sum was not
-          const cplx y_ = {nb_sign * acc[c][k][0], nb_sign * acc[c][k][1]};
-          const cplx ev = MODE == MV_PLAIN ? cplx{0.0, 0.0} : ldg(epi_src + off);
+          const cplx y_ = {nb_sign * res[i][k][0], nb_sign * res[i][k][1]};
+          const cplx ev_ = ev[i][k];
           if (MODE == MV_PLAIN) {
             st(A.out + off, y_);
           } else if (MODE == MV_RHS) {
             st(A.out + off, y_);
-            st(A.out2 + off, 2.0 * y_ - ev);
+            st(A.out2 + off, 2.0 * y_ - ev_);
           } else if (MODE == MV_RES) {
-            const cplx rv = ev - y_;
+            const cplx rv = ev_ - y_;
             st(A.out + off, rv);
             st(A.out2 + off, rv);
             st(A.out3 + off, rv);
             qs[k][0] += norm2(rv);
-            qs[k][1] += norm2(ev);
+            qs[k][1] += norm2(ev_);
           } else if (MODE == MV_V) {
             st(A.out + off, y_);
             cplx dd = {0.0, 0.0};
-            cmac_cj(dd, ev, y_);
+            cmac_cj(dd, ev_, y_);
             qs[k][0] += dd.re;
             qs[k][1] += dd.im;
           } else if (MODE == MV_RESC) {
-            const cplx rv = ev - y_;
+            const cplx rv = ev_ - y_;
             const cplx dv = rv * A.inv_theta[sp];
             A.r32[off] = make_float2((float)rv.re, (float)rv.im);
             A.d32[off] = make_float2((float)dv.re, (float)dv.im);
             qs[k][0] += norm2(rv);
-            qs[k][1] += norm2(ev);
+            qs[k][1] += norm2(ev_);
           } else {  // MV_T: in = s
             st(A.out + off, y_);
             cplx dd = {0.0, 0.0};
-            cmac_cj(dd, y_, ev);
+            cmac_cj(dd, y_, ev_);
             qs[k][0] += dd.re;
             qs[k][1] += dd.im;
             qs[k][2] += norm2(y_);
@@ -589,8 +698,15 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     }
   }
 
+  // every consumer warp is done with the tensor memory before warp 0 frees it
+  tc::fence_before_sync();
+  named_bar_sync(1, kWarps * 32);
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tbase, kTmemCols);
+
   // one partial row per CTA: each column summed over the warp's lanes, then
-  // over the two spin warps of its species and half in a fixed order
+  // over the two row-half warps of its species and column half in a fixed
+  // order
   if constexpr (NQ > 0) {
 #pragma unroll
     for (int k = 0; k < 3; ++k)
@@ -605,9 +721,9 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     if (threadIdx.x < CN_COLS * NQ) {
       const int col12 = threadIdx.x / NQ, kk = threadIdx.x % NQ;
       const int spc = col12 / 6, n = col12 % 6, hc = n / 3, k = n % 3;
-      // warps 4 spc + 2 s + hc for s = 0, 1
+      // warps 4 kh + 2 spc + hc for kh = 0, 1
       A.partials[((int64_t)blockIdx.x * CN_COLS + col12) * NQ + kk] =
-          red[4 * spc + hc][k][kk] + red[4 * spc + 2 + hc][k][kk];
+          red[2 * spc + hc][k][kk] + red[4 + 2 * spc + hc][k][kk];
     }
   }
 }
