@@ -217,6 +217,19 @@ int nrq_cn_set_wait_test(nrq_cn *cn, int64_t wait_cycles, int stall_load);
 /* Force a stencil (NRQ_STENCIL_*) or restore the timed choice (-1).
  * NRQ_ERR_BAD_ARG if the stencil cannot describe this lattice.            */
 int nrq_cn_set_stencil(nrq_cn *cn, int stencil);
+/* The FP32 Chebyshev step of the precision forms (forms 1 and 2; no
+ * reference counterpart).  REGISTER: the operator assembled from FP32 links
+ * and field strengths per launch; BLOCKS: FP32 FMAs on per-update 6x6
+ * blocks staged by TMA (V a multiple of 4, V >= 36, nx even).  -1 (the
+ * default) times both on the first update where BLOCKS applies and keeps
+ * the faster; forcing BLOCKS on a lattice it cannot describe is
+ * NRQ_ERR_BAD_ARG.  nrq_cn_cheb_info gives the step the last update ran
+ * (-1 before any) and the per-launch milliseconds of each (index NRQ_CHEB_*;
+ * -1 where not timed); either pointer may be NULL.                        */
+#define NRQ_CHEB_REGISTER 0
+#define NRQ_CHEB_BLOCKS 1
+int nrq_cn_set_cheb_stencil(nrq_cn *cn, int which);
+int nrq_cn_cheb_info(const nrq_cn *cn, int *last, double ms[2]);
 /* Plain form (form 0; no reference counterpart): on = 1 (the default)
  * starts every solve from 2b - psi + 2 t1 - t2, t1 and t2 the corrections
  * to that start of the field's last two steps (one step: + t1), kept per
@@ -281,12 +294,20 @@ int nrq_cn_batch_attach_learned(nrq_cn_batch *batch, struct nrq_learn *net);
 int nrq_cn_batch_residuals(const nrq_cn_batch *batch, double *rel);
 /* Tuning and schedule: the chosen Chebyshev kernel variant (0: one field
  * per tile, 2 blocks per SM; 1: one field per tile, 3 blocks per SM; 2: two
- * fields of one mass per tile) and block order (0: field fastest, 1: site
- * block fastest), the measured milliseconds per launch of every candidate
- * (index variant*2 + order; -1 where not applicable), and the inner steps
- * of each refinement pass (up to 16).                                     */
-int nrq_cn_batch_info(const nrq_cn_batch *batch, int *variant, int *order, double candidate_ms[6],
+ * fields of one mass per tile; 3: the FP32 block step, per-update blocks of
+ * every mass staged by TMA with the fields' vectors, where the lattice
+ * allows it: V a multiple of 4, V >= 36, nx even) and block order (0: field
+ * fastest, 1: site block fastest), the measured milliseconds per launch of
+ * every candidate (NRQ_BATCH_CANDIDATES entries, index variant*2 + order;
+ * -1 where not applicable), and the inner steps of each refinement pass (up
+ * to 16).                                                                 */
+#define NRQ_BATCH_CANDIDATES 8
+int nrq_cn_batch_info(const nrq_cn_batch *batch, int *variant, int *order, double candidate_ms[8],
                       int *npasses, int steps[16]);
+/* Force the Chebyshev kernel variant and block order (as in
+ * nrq_cn_batch_info; NRQ_ERR_BAD_ARG where the variant does not apply) or
+ * restore the timed choice (variant -1).  The next update recalibrates.    */
+int nrq_cn_batch_set_variant(nrq_cn_batch *batch, int variant, int order);
 
 /* An ensemble of independent members (batch[i], gauge[i]); the members may
  * sit on contexts of different lattice sizes on the same device.  One step

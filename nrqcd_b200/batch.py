@@ -75,16 +75,24 @@ class CNBatch:
         _capi.check(_capi.load().nrq_cn_batch_residuals(self._h, _capi.dptr(out)), self._ctx, "residuals")
         return out
 
+    VARIANTS = ("tile1_2blocks", "tile1_3blocks", "tile2_1block", "fp32_blocks_tma")
+
+    def set_variant(self, variant=None, order=0):
+        """Force the Chebyshev kernel (a name of VARIANTS or its index) and
+        block order; None restores the timed choice."""
+        v = -1 if variant is None else (self.VARIANTS.index(variant) if isinstance(variant, str) else int(variant))
+        _capi.check(_capi.load().nrq_cn_batch_set_variant(self._h, v, int(order)), self._ctx, "set_variant")
+
     def info(self) -> dict:
         var, order, npass = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        ms = np.zeros(6)
+        ms = np.zeros(8)
         steps = (ctypes.c_int * 16)()
         _capi.check(_capi.load().nrq_cn_batch_info(self._h, ctypes.byref(var), ctypes.byref(order), _capi.dptr(ms),
                                                    ctypes.byref(npass), steps), self._ctx, "info")
-        names = ("tile1_2blocks", "tile1_3blocks", "tile2_1block")
+        names = self.VARIANTS
         return {"variant": names[var.value], "fields_per_tile": 2 if var.value == 2 else 1,
                 "block_order": order.value,
-                "candidate_ms": {f"{names[v]}_order{o}": float(ms[2 * v + o]) for v in range(3) for o in range(2)},
+                "candidate_ms": {f"{names[v]}_order{o}": float(ms[2 * v + o]) for v in range(4) for o in range(2)},
                 "schedule": [int(steps[k]) for k in range(npass.value)]}
 
 

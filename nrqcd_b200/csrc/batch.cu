@@ -64,7 +64,11 @@ struct nrq_cn_batch {
   std::vector<int> schedule;
   bool tuned = false;
   int variant = 0, order = 0;  // Chebyshev kernel variant (nrq_kernels.cuh) and block order
-  double cand_ms[2 * nrq::BATCH_CHEB_VARIANTS] = {-1, -1, -1, -1, -1, -1};
+  double cand_ms[2 * nrq::BATCH_CHEB_VARIANTS] = {-1, -1, -1, -1, -1, -1, -1, -1};
+  // FP32 blocks of every distinct mass (Chebyshev variant 3; null where the
+  // lattice does not allow it) and the bounded waits' error record
+  float2 *W5f = nullptr;
+  int *err = nullptr, *h_err = nullptr;
   // generation: changes with every new schedule, tuning or key
   uint64_t gen = 0;
   // graph of one scheduled step (CN only), with the generation and gauge
@@ -143,6 +147,7 @@ void fill_table(nrq_cn_batch *b, const double c[8], double dt) {
     f.bounds = b->bounds + 4 * b->mass_of[i];
     f.tau = dt * ctx->a[0] / 2.0;
     f.mass = m;
+    f.wblk = b->mass_of[i];
     if (learned_on(b)) {
       nrq_heavy *h = b->fields[i];
       f.h1 = hist_v1(h);
@@ -175,6 +180,12 @@ int enq_prepare(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double d
     ProfScope ps(ctx, 3, (double)V * (1080.0 + 540.0));
     nrq::launch_cn_to_f32(V, b->U64, b->DE, b->Dsum, b->Bsum, b->U32, b->DE32, b->D32, b->B32, st);
   }
+  if (b->W5f && (!b->tuned || b->variant == 3))  // FP32 blocks of every mass (Chebyshev variant 3)
+    for (size_t k = 0; k < b->masses.size(); ++k) {
+      ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 1728.0));
+      const nrq::CnCoef CH = nrqh::make_coef(ctx, b->masses[k], c, dt, true);
+      nrq::launch_cn_blocks5(L, CH, b->U64, b->DE, nullptr, b->W5f + (int64_t)k * nrq::cn_mv5_block_entries(V), st);
+    }
   const double tau = dt * ctx->a[0] / 2.0;
   for (size_t k = 0; k < b->masses.size(); ++k) {
     ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 216.0));
@@ -217,14 +228,26 @@ int enq_residual(nrq_cn_batch *b, cudaStream_t st, bool first) {
   return check_launch(ctx, "batch residual");
 }
 
+// Chebyshev step `step` of every field with kernel variant / block order
+// (nonzero: the variant does not apply)
+int launch_cheb(nrq_cn_batch *b, int step, int variant, int order, cudaStream_t st) {
+  nrq_ctx *ctx = b->ctx;
+  if (variant == 3)
+    return b->W5f ? nrq::launch_batch_cheb5f(step, order, ctx->lat, b->W5f, (int)b->masses.size(), b->D32, b->B32,
+                                             b->dA_all, b->dB_all, b->d_tab, b->nf, b->err, ctx->sm_count, st,
+                                             nrq_wait_cycles_default)
+                  : 1;
+  return nrq::launch_batch_cheb(step, variant, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf,
+                                st);
+}
+
 // m FP32 Chebyshev steps on A^H e = r, then x += e
 int enq_inner(nrq_cn_batch *b, int m, cudaStream_t st) {
   nrq_ctx *ctx = b->ctx;
   const double V = (double)ctx->lat.V;
   for (int k = 0; k < m; ++k) {
     ProfScope ps(ctx, 0, V * (b->nf * 576.0 * 6 + 756.0));
-    if (nrq::launch_batch_cheb(k, b->variant, b->order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf,
-                               st)) {
+    if (launch_cheb(b, k, b->variant, b->order, st)) {
       ctx->last_error = "batch: unsupported Chebyshev tile";
       return NRQ_ERR_BAD_ARG;
     }
@@ -240,6 +263,7 @@ int enq_readback(nrq_cn_batch *b, cudaStream_t st) {
   NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(b->h_scal, b->scal_all, sizeof(double) * kFieldScal * b->nf,
                                        cudaMemcpyDeviceToHost, st));
   NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(b->h_flags, b->flags, sizeof(int) * b->nf, cudaMemcpyDeviceToHost, st));
+  NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(b->h_err, b->err, sizeof(int) * 16, cudaMemcpyDeviceToHost, st));
   return NRQ_OK;
 }
 
@@ -259,11 +283,12 @@ int enq_scheduled(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double
 
 // ---- host-side checks -------------------------------------------------------
 struct Check {
-  bool conv = true, nonfin = false, badbounds = false;
+  bool conv = true, nonfin = false, badbounds = false, timeout = false;
   double worst = 0.0;
 };
 Check check(const nrq_cn_batch *b) {
   Check r;
+  r.timeout = b->h_err[0] != 0;
   for (int i = 0; i < b->nf; ++i) {
     if (b->h_flags[i]) r.badbounds = true;
     const double *s = b->h_scal + (size_t)i * kFieldScal;
@@ -318,14 +343,11 @@ int autotune(nrq_cn_batch *b, cudaStream_t st) {
     for (int order = 0; order < 2; ++order) {
       const int idx = variant * 2 + order;
       b->cand_ms[idx] = -1.0;
-      if (variant == 2 && !even) continue;
+      if ((variant == 2 && !even) || (variant == 3 && !b->W5f)) continue;
       // warm-up launch, then timed repetitions
-      int bad =
-          nrq::launch_batch_cheb(0, variant, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf, st);
+      int bad = launch_cheb(b, 0, variant, order, st);
       cudaEventRecord(e0, st);
-      for (int r = 0; r < reps && !bad; ++r)
-        bad = nrq::launch_batch_cheb(0, variant, order, ctx->lat, b->U32, b->D32, b->B32, b->DE32, b->d_tab, b->nf,
-                                     st);
+      for (int r = 0; r < reps && !bad; ++r) bad = launch_cheb(b, 0, variant, order, st);
       cudaEventRecord(e1, st);
       if (bad) continue;
       int rc = check_launch(ctx, "batch autotune");
@@ -357,7 +379,7 @@ int autotune(nrq_cn_batch *b, cudaStream_t st) {
 // `budget` passes ran.  Appends the step counts used to `used`.
 int refine_adaptive(nrq_cn_batch *b, double dt, cudaStream_t st, int budget, std::vector<int> &used, Check &chk) {
   nrq_ctx *ctx = b->ctx;
-  for (int p = 0; p < budget && !chk.conv && !chk.nonfin && !chk.badbounds; ++p) {
+  for (int p = 0; p < budget && !chk.conv && !chk.nonfin && !chk.badbounds && !chk.timeout; ++p) {
     const int m = steps_for(b, dt, chk.worst / (0.3 * b->tol));
     int rc = enq_inner(b, m, st);
     if (!rc) rc = enq_residual(b, st, false);
@@ -401,7 +423,7 @@ int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], dou
 int finish_step(nrq_cn_batch *b, double dt, cudaStream_t st, Check &chk, bool *schedule_changed) {
   chk = check(b);
   *schedule_changed = false;
-  if (!chk.conv && !chk.nonfin && !chk.badbounds) {
+  if (!chk.conv && !chk.nonfin && !chk.badbounds && !chk.timeout) {
     NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(b->h_bounds, b->bounds, sizeof(double) * 4 * b->masses.size(),
                                          cudaMemcpyDeviceToHost, st));
     NRQ_CUDA_TRY(b->ctx, cudaStreamSynchronize(st));
@@ -420,7 +442,7 @@ int finish_step(nrq_cn_batch *b, double dt, cudaStream_t st, Check &chk, bool *s
 int conclude(nrq_cn_batch *b, const Check &chk, int64_t inner, int64_t passes) {
   // results: the iterate becomes the field, the old field the next work
   // buffer; a learned step leaves the new history in the field
-  const bool keep = learned_on(b) && chk.conv && !chk.nonfin && !chk.badbounds;
+  const bool keep = learned_on(b) && chk.conv && !chk.nonfin && !chk.badbounds && !chk.timeout;
   for (int i = 0; i < b->nf; ++i) {
     std::swap(b->fields[i]->P, b->xbuf[i]);
     if (keep) hist_push(b->fields[i]);
@@ -431,6 +453,13 @@ int conclude(nrq_cn_batch *b, const Check &chk, int64_t inner, int64_t passes) {
   b->last_matvecs = 1 + (passes + 1) + inner;
   b->last_maxrel = chk.worst;
   b->last_conv = chk.conv;
+  if (chk.timeout) {
+    b->ctx->last_error = "batch Chebyshev stencil: a bounded pipeline wait expired (load " +
+                         std::to_string(b->h_err[2]) + ", CTA " + std::to_string(b->h_err[3]) + ")";
+    cudaMemsetAsync(b->err, 0, sizeof(int) * 16, b->ctx->stream);
+    b->h_err[0] = 0;
+    return NRQ_ERR_TIMEOUT;
+  }
   if (chk.badbounds) {
     b->ctx->last_error = "batch: invalid spectral bounds";
     return NRQ_ERR_NONFINITE;
@@ -564,6 +593,9 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
   NRQ_B_ALLOC(b->scal_all, sizeof(double) * kFieldScal * nfields);
   NRQ_B_ALLOC(b->flags, sizeof(int) * nfields);
   NRQ_B_ALLOC(b->d_tab, sizeof(nrq::BatchField) * nfields);
+  NRQ_B_ALLOC(b->err, sizeof(int) * 16);
+  if (nrq::cheb5f_applicable(ctx->lat))
+    NRQ_B_ALLOC(b->W5f, sizeof(float2) * nrq::cn_mv5_block_entries(V) * b->masses.size());
   b->xbuf.assign(nfields, nullptr);
   for (int i = 0; i < nfields; ++i) NRQ_B_ALLOC(b->xbuf[i], sizeof(double2) * P);
 #undef NRQ_B_ALLOC
@@ -571,6 +603,9 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
   if ((e = cudaMallocHost(&b->h_scal, sizeof(double) * kFieldScal * nfields)) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&b->h_flags, sizeof(int) * nfields)) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&b->h_bounds, sizeof(double) * 4 * b->masses.size())) != cudaSuccess) return fail(e);
+  if ((e = cudaMallocHost(&b->h_err, sizeof(int) * 16)) != cudaSuccess) return fail(e);
+  std::memset(b->h_err, 0, sizeof(int) * 16);
+  if ((e = cudaMemsetAsync(b->err, 0, sizeof(int) * 16, ctx->stream)) != cudaSuccess) return fail(e);
   // defined contents for the FP32 vectors and flags the tuner's first launches read
   for (float2 *p : {b->r32_all, b->dA_all, b->dB_all, b->e32_all})
     if ((e = cudaMemsetAsync(p, 0, sizeof(float2) * P * nfields, ctx->stream)) != cudaSuccess) return fail(e);
@@ -590,11 +625,11 @@ extern "C" int nrq_cn_batch_destroy(nrq_cn_batch *b) {
                   (void *)b->D32, (void *)b->B32, (void *)b->bpart, (void *)b->bounds, (void *)b->b_all,
                   (void *)b->r32_all, (void *)b->dA_all, (void *)b->dB_all, (void *)b->e32_all, (void *)b->part_all,
                   (void *)b->scal_all, (void *)b->flags, (void *)b->d_tab, (void *)b->lgf, (void *)b->lfeat,
-                  (void *)b->lomega})
+                  (void *)b->lomega, (void *)b->W5f, (void *)b->err})
     if (p) cudaFree(p);
   for (double2 *p : b->xbuf)
     if (p) cudaFree(p);
-  for (void *p : {(void *)b->h_tab, (void *)b->h_scal, (void *)b->h_flags, (void *)b->h_bounds})
+  for (void *p : {(void *)b->h_tab, (void *)b->h_scal, (void *)b->h_flags, (void *)b->h_bounds, (void *)b->h_err})
     if (p) cudaFreeHost(p);
   delete b;
   return NRQ_OK;
@@ -711,7 +746,7 @@ extern "C" int nrq_cn_batch_residuals(const nrq_cn_batch *b, double *rel) {
   return NRQ_OK;
 }
 
-extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *variant, int *order, double candidate_ms[6],
+extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *variant, int *order, double candidate_ms[8],
                                  int *npasses, int steps[16]) {
   if (!b) return NRQ_ERR_BAD_ARG;
   if (variant) *variant = b->variant;
@@ -721,6 +756,31 @@ extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *variant, int *order
   if (npasses) *npasses = (int)b->schedule.size();
   if (steps)
     for (int k = 0; k < 16; ++k) steps[k] = k < (int)b->schedule.size() ? b->schedule[k] : 0;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_batch_set_variant(nrq_cn_batch *b, int variant, int order) {
+  if (!b || variant < -1 || variant >= nrq::BATCH_CHEB_VARIANTS || order < 0 || order > 1) return NRQ_ERR_BAD_ARG;
+  if (variant == 2) {
+    for (int n : b->group_size)
+      if (n % 2) {
+        b->ctx->last_error = "batch: two-field tiles need an even number of fields per mass";
+        return NRQ_ERR_BAD_ARG;
+      }
+  }
+  if (variant == 3 && !b->W5f) {
+    b->ctx->last_error = "batch: the FP32 block step needs V a multiple of 4, V >= 36, nx even";
+    return NRQ_ERR_BAD_ARG;
+  }
+  if (variant < 0) {
+    b->tuned = false;
+  } else {
+    b->variant = variant;
+    b->order = order;
+    b->tuned = true;
+  }
+  b->have_key = false;  // recalibrate the schedule with the new kernel
+  b->gen++;
   return NRQ_OK;
 }
 

@@ -44,7 +44,8 @@ std::string timeout_message(const double *h_scal) {
   const int stencil = e[1] / 16, role = e[1] % 16;
   std::string m = "CN stencil: a bounded pipeline wait expired";
   if (e[1] != 0) {
-    m += " (k_cn_mv" + std::to_string(stencil) + ", " + (role >= 0 && role < 5 ? roles[role] : "?") +
+    m += std::string(" (") + (stencil == 6 ? "k_cheb5f" : "k_cn_mv" + std::to_string(stencil)) + ", " +
+         (role >= 0 && role < 5 ? roles[role] : "?") +
          ", load " + std::to_string(e[2]) + ", CTA " + std::to_string(e[3]);
     if (e[4] != 0) {  // the FMA stencil's detail: the loader's progress and the barrier's word
       char buf[96];
@@ -1078,6 +1079,25 @@ extern "C" int nrq_cn_set_stencil(nrq_cn *cn, int stencil) {
   return NRQ_OK;
 }
 
+extern "C" int nrq_cn_set_cheb_stencil(nrq_cn *cn, int which) {
+  if (!cn || which < -1 || which > NRQ_CHEB_BLOCKS) return NRQ_ERR_BAD_ARG;
+  if (which == NRQ_CHEB_BLOCKS && !nrq::cheb5f_applicable(cn->ctx->lat)) {
+    cn->ctx->last_error = "nrq_cn_set_cheb_stencil: the FP32 block step needs V a multiple of 4, V >= 36, nx even";
+    return NRQ_ERR_BAD_ARG;
+  }
+  cn->cheb_stencil = which;
+  cn->cheb_tuned = false;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_cheb_info(const nrq_cn *cn, int *last, double ms[2]) {
+  if (!cn) return NRQ_ERR_BAD_ARG;
+  if (last) *last = cn->last_cheb;
+  if (ms)
+    for (int k = 0; k < 2; ++k) ms[k] = cn->cheb_ms[k];
+  return NRQ_OK;
+}
+
 extern "C" int nrq_cn_set_history_guess(nrq_cn *cn, int on) {
   if (!cn || on < 0 || on > 1) return NRQ_ERR_BAD_ARG;
   cn->history_guess = on != 0;
@@ -1092,7 +1112,7 @@ extern "C" int nrq_cn_finalize(nrq_cn *cn) {
                   (void *)cn->rh, (void *)cn->p, (void *)cn->v, (void *)cn->t, (void *)cn->s, (void *)cn->scal,
                   (void *)cn->partials, (void *)cn->U32, (void *)cn->DE32, (void *)cn->D32, (void *)cn->B32,
                   (void *)cn->r32, (void *)cn->dA32, (void *)cn->dB32, (void *)cn->e32, (void *)cn->bounds,
-                  (void *)cn->Wblk, (void *)cn->Wblk5})
+                  (void *)cn->Wblk, (void *)cn->Wblk5, (void *)cn->Wblk5f})
     if (p) cudaFree(p);
   if (cn->h_scal) cudaFreeHost(cn->h_scal);
   if (cn->h_bounds) cudaFreeHost(cn->h_bounds);
@@ -1144,20 +1164,41 @@ int ensure_blocks(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *
   *sign = 1.0;
   return check_launch(ctx, "k_cn_blocks");
 }
-// the FMA stencil's blocks (row-major, 37 entries per block)
-int ensure_blocks5(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *sign) {
+// whether the precision form's inner steps run on the FP32 blocks: forced,
+// or the faster of the two on the first update (before it, the blocks are
+// built so that the timing can run)
+bool use_cheb5f(const nrq_cn *cn) {
+  if (cn->form < 1 || cn->cheb_stencil == NRQ_CHEB_REGISTER || !nrq::cheb5f_applicable(cn->ctx->lat)) return false;
+  return cn->cheb_stencil == NRQ_CHEB_BLOCKS || !cn->cheb_tuned || cn->cheb_choice == NRQ_CHEB_BLOCKS;
+}
+// The FMA stencil's blocks (FP64, f32 = false) or the FP32 Chebyshev step's
+// (f32 = true), with the coefficients C.  Where the other precision is
+// missing for the same coefficients and the update will need it too, one
+// pass writes both.
+int ensure_blocks5(nrq_cn *cn, const nrq::CnCoef &C, const nrq_gauge *g, double *sign, bool f32 = false) {
   nrq_ctx *ctx = cn->ctx;
-  *sign = blocks_sign(cn->w5_valid, cn->w5_coef, C);
+  *sign = f32 ? blocks_sign(cn->w5f_valid, cn->w5f_coef, C) : blocks_sign(cn->w5_valid, cn->w5_coef, C);
   if (*sign != 0.0) return NRQ_OK;
   const int64_t V = ctx->lat.V;
-  if (!cn->Wblk5)
+  const bool want64 = !f32 || (cn->stencil == NRQ_STENCIL_FMA && blocks_sign(cn->w5_valid, cn->w5_coef, C) == 0.0);
+  const bool want32 = f32 || (use_cheb5f(cn) && blocks_sign(cn->w5f_valid, cn->w5f_coef, C) == 0.0);
+  if (want64 && !cn->Wblk5)
     NRQ_CUDA_TRY(ctx, cudaMalloc((void **)&cn->Wblk5, sizeof(double2) * nrq::cn_mv5_block_entries(V)));
+  if (want32 && !cn->Wblk5f)
+    NRQ_CUDA_TRY(ctx, cudaMalloc((void **)&cn->Wblk5f, sizeof(float2) * nrq::cn_mv5_block_entries(V)));
   {
-    ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 3552.0));
-    nrq::launch_cn_blocks5(ctx->lat, C, g->U, cn->DE, cn->Wblk5, ctx->stream);
+    ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + (want64 ? 3456.0 : 0.0) + (want32 ? 1728.0 : 0.0)));
+    nrq::launch_cn_blocks5(ctx->lat, C, g->U, cn->DE, want64 ? cn->Wblk5 : nullptr, want32 ? cn->Wblk5f : nullptr,
+                           ctx->stream);
   }
-  cn->w5_coef = C;
-  cn->w5_valid = true;
+  if (want64) {
+    cn->w5_coef = C;
+    cn->w5_valid = true;
+  }
+  if (want32) {
+    cn->w5f_coef = C;
+    cn->w5f_valid = true;
+  }
   *sign = 1.0;
   return check_launch(ctx, "k_cn_blocks5");
 }
@@ -1323,6 +1364,7 @@ int cn_prepare(nrq_cn *cn, const nrq_gauge *g) {
   nrq::launch_cn_prepare(ctx->lat, g->U, g->E, cn->Dsum, cn->Bsum, cn->DE, ctx->stream);
   cn->w_valid = false;  // the cached blocks follow the new gauge field on demand
   cn->w5_valid = false;
+  cn->w5f_valid = false;
   return check_launch(ctx, "k_cn_prepare");
 }
 }  // namespace
@@ -1348,6 +1390,50 @@ using nrqh::ChebSeg;
 using nrqh::cheb_gain;
 using nrqh::cheb_segment;
 namespace {
+// The first update's choice between the two FP32 Chebyshev steps: one warm-up
+// and three timed launches of each as a first step, reading d = dA32 and
+// writing only e32 and dB32 (the r operand pointed at e32 as well), which the
+// solve's real first step rewrites before it reads them.
+int tune_cheb(nrq_cn *cn, const nrq::CnCoef &CH, const nrq::ChebCoef &K, double wsign) {
+  nrq_ctx *ctx = cn->ctx;
+  cn->cheb_tuned = true;
+  cn->cheb_choice = NRQ_CHEB_REGISTER;
+  if (!nrq::cheb5f_applicable(ctx->lat)) return NRQ_OK;
+  cudaStream_t st = ctx->stream;
+  const bool prof = ctx->prof;
+  ctx->prof = false;
+  cudaEvent_t e0, e1;
+  NRQ_CUDA_TRY(ctx, cudaEventCreate(&e0));
+  NRQ_CUDA_TRY(ctx, cudaEventCreate(&e1));
+  const int reps = 3;
+  for (int which = 0; which < 2; ++which) {
+    cn->cheb_ms[which] = -1.0;
+    bool ok = true;
+    for (int r = 0; r < reps + 1 && ok; ++r) {
+      if (r == 1) cudaEventRecord(e0, st);
+      if (which == NRQ_CHEB_BLOCKS)
+        ok = nrq::launch_cheb5f(true, ctx->lat, CH, wsign, cn->Wblk5f, cn->D32, cn->B32, cn->dA32, cn->dB32, cn->e32,
+                                cn->e32, K, scal_err(cn->scal), ctx->sm_count, st, cn->wait_cycles) == 0;
+      else
+        nrq::launch_cheb32(true, ctx->lat, CH, cn->U32, cn->D32, cn->B32, cn->DE32, cn->dA32, cn->dB32, cn->e32,
+                           cn->e32, K, st);
+    }
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ok) cn->cheb_ms[which] = ms / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx->prof = prof;
+  int rc = check_launch(ctx, "Chebyshev step timing");
+  if (rc) return rc;
+  if (cn->cheb_ms[NRQ_CHEB_BLOCKS] > 0.0 && cn->cheb_ms[NRQ_CHEB_BLOCKS] < cn->cheb_ms[NRQ_CHEB_REGISTER])
+    cn->cheb_choice = NRQ_CHEB_BLOCKS;
+  return NRQ_OK;
+}
+
 // Precision form: FP64 refinement around FP32 Chebyshev inner solves.
 int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass, const double c[8], double dt,
                         nrq_cn_stats *stats) {
@@ -1495,10 +1581,23 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     if (m <= 0) break;
     // FP32 inner Chebyshev solve of A^H e = r, then x += e
     float2 *dcur = cn->dA32, *dnext = cn->dB32;
+    double wsign = 0.0;
+    if (use_cheb5f(cn) && (rc = ensure_blocks5(cn, CH, g, &wsign, true))) return rc;
+    if (cn->cheb_stencil < 0 && !cn->cheb_tuned && (rc = tune_cheb(cn, CH, coef[0], wsign))) return rc;
+    const bool blk = use_cheb5f(cn);
     for (int k = 0; k < m; ++k) {
       ProfScope ps(ctx, 0, (double)V * (576.0 * 6 + 756.0));
-      nrq::launch_cheb32(k == 0, L, CH, cn->U32, cn->D32, cn->B32, cn->DE32, dcur, dnext, cn->r32, cn->e32, coef[k],
-                         st);
+      if (blk)
+        rc = nrq::launch_cheb5f(k == 0, L, CH, wsign, cn->Wblk5f, cn->D32, cn->B32, dcur, dnext, cn->r32, cn->e32,
+                                coef[k], scal_err(cn->scal), ctx->sm_count, st, cn->wait_cycles);
+      if (!blk || rc) {
+        rc = NRQ_OK;
+        nrq::launch_cheb32(k == 0, L, CH, cn->U32, cn->D32, cn->B32, cn->DE32, dcur, dnext, cn->r32, cn->e32,
+                           coef[k], st);
+        cn->last_cheb = NRQ_CHEB_REGISTER;
+      } else {
+        cn->last_cheb = NRQ_CHEB_BLOCKS;
+      }
       std::swap(dcur, dnext);
     }
     inner += m;

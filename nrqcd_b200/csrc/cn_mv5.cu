@@ -138,9 +138,12 @@ __device__ __forceinline__ cplx pauli_t5(int k, int s, int t) {
 }
 
 // One thread per (direction I, species, row g, site): row g of the forward
-// block W_I(x) of that species, into planes (I*2 + sp)*36 + g*6 + column.
+// block W_I(x) of that species, into planes (I*2 + sp)*36 + g*6 + column, in
+// FP64 (W) and/or rounded to FP32 (Wf, the FP32 Chebyshev stencil's blocks).
+template <bool F64, bool F32>
 __global__ void __launch_bounds__(256) k_cn_blocks5(Lat L, CnCoef C, const double2 *__restrict__ U,
-                                                    const double2 *__restrict__ DE, double2 *__restrict__ W) {
+                                                    const double2 *__restrict__ DE, double2 *__restrict__ W,
+                                                    float2 *__restrict__ Wf) {
   const int64_t V = L.V;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= 36 * V) return;
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(256) k_cn_blocks5(Lat L, CnCoef C, const doubl
   const int K0 = (I + 2) % 3, K1 = (I + 1) % 3;
   const cplx ck = (-0.5 * C.inva2[I]) * C.kin[sp];
   const cplx cs0 = times_i(C.so[sp]), cs1 = -times_i(C.so[sp]);
-  double2 *row = W + ((int64_t)isp * 36 + g * 6) * V + x;
+  const int64_t row = ((int64_t)isp * 36 + g * 6) * V + x;
 #pragma unroll
   for (int cp = 0; cp < 3; ++cp) {
     const int e = cp * 3 + c;  // M^T[c][cp] = M[cp][c]
@@ -165,7 +168,8 @@ __global__ void __launch_bounds__(256) k_cn_blocks5(Lat L, CnCoef C, const doubl
     for (int t = 0; t < 2; ++t) {
       cplx v = (s == t) ? ku : cplx{0.0, 0.0};
       v = v + pauli_t5(K0, s, t) * e0 + pauli_t5(K1, s, t) * e1;
-      st(row + (int64_t)(2 * cp + t) * V, v);
+      if (F64) st(W + row + (int64_t)(2 * cp + t) * V, v);
+      if (F32) Wf[row + (int64_t)(2 * cp + t) * V] = make_float2((float)v.re, (float)v.im);
     }
   }
 }
@@ -255,24 +259,25 @@ __device__ __forceinline__ double lds_d1(uint32_t a) {
 // The thread's partial tile (rows r = 0..5; columns 3h + k, k = 0..2) +=
 // sum over its three input rows q = 3 kh + qq of w[r][q] psi[q][3h + k].
 // Forward: w[r][q] = W(x)[r][q], entry r*6 + q; backward: w[r][q] =
-// -conj(W(y)[q][r]), entry q*6 + r.  load_w(e) reads entry e of the block,
-// load_p(e) plane e of the spinor (species planes), from the shared tiles
-// or global memory.
+// -conj(W(y)[q][r]), entry q*6 + r.  load_w(e) reads entry e + (3 kh,
+// backward 18 kh) of the block and load_p(e) plane e + 18 h + 3 kh of the
+// spinor (species planes), from the shared tiles or global memory: the
+// callers fold the thread's offsets into their base addresses, so that e
+// is a constant of the unrolled loops.
 template <bool BWD, typename LW, typename LP>
-__device__ __forceinline__ void nb_products(double (&acc)[6][3][2], int kh, int h, LW load_w, LP load_p) {
+__device__ __forceinline__ void nb_products(double (&acc)[6][3][2], LW load_w, LP load_p) {
 #pragma unroll
   for (int qq = 0; qq < 3; ++qq) {
-    const int q = 3 * kh + qq;
     double wr[6], wi[6];
 #pragma unroll
     for (int r = 0; r < 6; ++r) {
-      const double2 wv = load_w(BWD ? q * 6 + r : r * 6 + q);
+      const double2 wv = load_w(BWD ? qq * 6 + r : r * 6 + qq);
       wr[r] = BWD ? -wv.x : wv.x;
       wi[r] = wv.y;
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      const double2 p = load_p((3 * h + k) * 6 + q);
+      const double2 p = load_p(k * 6 + qq);
 #pragma unroll
       for (int r = 0; r < 6; ++r) {
         acc[r][k][0] = fma(wr[r], p.x, fma(-wi[r], p.y, acc[r][k][0]));
@@ -508,6 +513,8 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   // of the sum (exchange_halves with warp w ^ 4).
   const int kh = warp >> 2, sp = (warp >> 1) & 1, h = warp & 1;
   const int pair_bar = 2 + (warp & 3);  // named barrier of the warp pair (ids 2-5)
+  // the thread's first spinor plane and block entries (see nb_products)
+  const int pofs = 18 * h + 3 * kh, wofs_f = 3 * kh, wofs_b = 18 * kh;
   const int site_in_unit = lane;
   constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
   double qs[3][3];
@@ -602,37 +609,42 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             // shared memory, a lane's operands in the tile or in a wrap
             // column (per-lane strides)
             const uint32_t xc = smem_u32(bb + kOffX);
-            const uint32_t wa = ww ? xc + kColStride : s_w + (uint32_t)((m - ws) * 16);
-            const uint32_t pa = pw ? xc + (bwd ? 0u : 2u * kColStride) : s_tile + (uint32_t)((y - ss) * 16);
             const uint32_t wst = ww ? 16u : (uint32_t)kTileS * 16u, pst = pw ? 16u : (uint32_t)kTileS * 16u;
+            const uint32_t wa = (ww ? xc + kColStride : s_w + (uint32_t)((m - ws) * 16)) +
+                                (uint32_t)(bwd ? wofs_b : wofs_f) * wst;
+            const uint32_t pa =
+                (pw ? xc + (bwd ? 0u : 2u * kColStride) : s_tile + (uint32_t)((y - ss) * 16)) + (uint32_t)pofs * pst;
             auto lw = [&](int e) { return lds_d2(wa + (uint32_t)e * wst); };
             auto lp = [&](int e) { return lds_d2(pa + (uint32_t)e * pst); };
             if (bwd)
-              nb_products<true>(acc, kh, h, lw, lp);
+              nb_products<true>(acc, lw, lp);
             else
-              nb_products<false>(acc, kh, h, lw, lp);
+              nb_products<false>(acc, lw, lp);
           } else if (__all_sync(0xffffffffu, (ps && wsh) || !act)) {
             // every operand of the warp in shared memory
-            const uint32_t wa = s_w + (uint32_t)((m - ws) * 16), pa = s_tile + (uint32_t)((y - ss) * 16);
-            auto lw = [&](int e) { return lds_d2(wa + (uint32_t)(e * kTileS * 16)); };
-            auto lp = [&](int e) { return lds_d2(pa + (uint32_t)(e * kTileS * 16)); };
+            constexpr uint32_t kPl = kTileS * 16u;  // plane stride of the tiles
+            const uint32_t wa = s_w + (uint32_t)((m - ws) * 16) + (uint32_t)(bwd ? wofs_b : wofs_f) * kPl;
+            const uint32_t pa = s_tile + (uint32_t)((y - ss) * 16) + (uint32_t)pofs * kPl;
+            auto lw = [&](int e) { return lds_d2(wa + (uint32_t)e * kPl); };
+            auto lp = [&](int e) { return lds_d2(pa + (uint32_t)e * kPl); };
             if (bwd)
-              nb_products<true>(acc, kh, h, lw, lp);
+              nb_products<true>(acc, lw, lp);
             else
-              nb_products<false>(acc, kh, h, lw, lp);
+              nb_products<false>(acc, lw, lp);
           } else if (act) {
             // some lanes' operands outside the tiles (periodic wraps, tile
             // edges): those lanes read global memory, the others the tiles
-            const double2 *wp = wsh ? (const double2 *)(bb + kOffW) + (m - ws)
-                                    : W + (int64_t)((I * 2 + sp) * 36) * V + m;
-            const double2 *pp = ps ? (const double2 *)bb + (y - ss) : A.in + (int64_t)(sp * 36) * V + y;
             const int64_t wst = wsh ? kTileS : V, pst = ps ? kTileS : V;
+            const double2 *wp = (wsh ? (const double2 *)(bb + kOffW) + (m - ws)
+                                     : W + (int64_t)((I * 2 + sp) * 36) * V + m) +
+                                (bwd ? wofs_b : wofs_f) * wst;
+            const double2 *pp = (ps ? (const double2 *)bb + (y - ss) : A.in + (int64_t)(sp * 36) * V + y) + pofs * pst;
             auto lw = [&](int e) { return wp[e * wst]; };
             auto lp = [&](int e) { return pp[e * pst]; };
             if (bwd)
-              nb_products<true>(acc, kh, h, lw, lp);
+              nb_products<true>(acc, lw, lp);
             else
-              nb_products<false>(acc, kh, h, lw, lp);
+              nb_products<false>(acc, lw, lp);
           }
         }
       }
@@ -729,10 +741,16 @@ __global__ void __maxnreg__(mv5::kMaxReg)
 }
 
 // ------------------------------------------------------------------ host
-void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, cudaStream_t st) {
+void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, float2 *Wf,
+                       cudaStream_t st) {
   const int64_t n = 36 * L.V;
   const unsigned grid = (unsigned)((n + 255) / 256);
-  k_cn_blocks5<<<grid, 256, 0, st>>>(L, C, U, DE, W);
+  if (W && Wf)
+    k_cn_blocks5<true, true><<<grid, 256, 0, st>>>(L, C, U, DE, W, Wf);
+  else if (W)
+    k_cn_blocks5<true, false><<<grid, 256, 0, st>>>(L, C, U, DE, W, Wf);
+  else if (Wf)
+    k_cn_blocks5<false, true><<<grid, 256, 0, st>>>(L, C, U, DE, W, Wf);
 }
 
 int64_t cn_mv5_units(int64_t V) { return (V + mv5::kUnit - 1) / mv5::kUnit; }

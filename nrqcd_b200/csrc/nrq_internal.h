@@ -155,10 +155,22 @@ struct nrq_cn {
   double2 *Wblk = nullptr;
   bool w_valid = false;
   nrq::CnCoef w_coef{};
-  // FP64 FMA stencil: the same blocks, row-major, 37 entries per block
+  // FP64 FMA stencil: the same blocks as 216 planes
   double2 *Wblk5 = nullptr;
   bool w5_valid = false;
   nrq::CnCoef w5_coef{};
+  // the FP32 Chebyshev step of the precision forms: the same blocks rounded
+  // to FP32, and which step kernel runs (-1: k_cheb5f where it applies, else
+  // k_cheb32; NRQ_CHEB_* forces one); last_cheb: the one the last update ran
+  float2 *Wblk5f = nullptr;
+  bool w5f_valid = false;
+  nrq::CnCoef w5f_coef{};
+  int cheb_stencil = -1;
+  int last_cheb = -1;
+  // the timed choice between the two steps (per-launch ms; -1 not timed)
+  bool cheb_tuned = false;
+  int cheb_choice = -1;
+  double cheb_ms[2] = {-1.0, -1.0};
   // bound of the FMA stencil's pipeline waits (clock cycles) and, for the
   // test of the timeout path, the load its producer stops before (-1: none)
   long long wait_cycles = nrq_wait_cycles_default;

@@ -136,12 +136,15 @@ int64_t cn_mv4_units(int64_t V);
 int64_t cn_mv4_rows(int64_t V, int sm_count);
 int launch_cn_mv4(int mode, Lat L, const CnCoef &C, double nb_sign, const double2 *W, const double2 *Dsum,
                   const double *Bsum, const MvArgs &a, int *err, int sm_count, cudaStream_t st);
-// FP64 FMA stencil (cn_mv5.cu) on the same forward blocks, stored row-major
-// with 37 entries per block (cn_mv5_block_entries complex in all); the same
-// conditions as the tensor-core stencil.  wait_cycles bounds every pipeline
-// wait; stall_load >= 0 stops the producer before that load (the test of the
-// timeout path).  One partial row per CTA (cn_mv5_rows).
-void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, cudaStream_t st);
+// FP64 FMA stencil (cn_mv5.cu) on the same forward blocks, stored as 216
+// planes (direction, species, row, column; cn_mv5_block_entries complex in
+// all); the same conditions as the tensor-core stencil.  wait_cycles bounds
+// every pipeline wait; stall_load >= 0 stops the producer before that load
+// (the test of the timeout path).  One partial row per CTA (cn_mv5_rows).
+// launch_cn_blocks5 writes the blocks in FP64 (W), rounded to FP32 (Wf), or
+// both in one pass; a null pointer skips that precision.
+void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, float2 *Wf,
+                       cudaStream_t st);
 int64_t cn_mv5_units(int64_t V);
 int64_t cn_mv5_rows(int64_t V, int sm_count);
 int64_t cn_mv5_block_entries(int64_t V);
@@ -162,6 +165,7 @@ struct BatchField {
   const double *bounds;          // spectral enclosure of this field's mass (lo0, hi0, lo1, hi1)
   double tau;                    // dt a0 / 2 (signed)
   double mass;                   // heavy mass of this field
+  int wblk;                      // the field's FP32 block set (its distinct mass)
   // learned initial guess: the field's history (v1 newest, v2 older; null
   // when absent) and the slot the new history goes to (null: no learned guess)
   const float2 *h1, *h2;
@@ -184,9 +188,18 @@ void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2
 // registers); 1 = one field per tile, 3 blocks/SM (113 registers); 2 = two
 // fields of one mass per tile, 1 block/SM.  Returns nonzero for an
 // unsupported variant (a two-field tile needs an even count per mass).
-constexpr int BATCH_CHEB_VARIANTS = 3;
+constexpr int BATCH_CHEB_VARIANTS = 4;
 int launch_batch_cheb(int step, int variant, int order, Lat L, const float2 *U, const float2 *Dsum,
                       const float *Bsum, const float2 *DE, const BatchField *tab, int nfields, cudaStream_t st);
+// Variant 3 of the batched Chebyshev step: the FP32 block step of
+// launch_cheb5f over every field (work items (field, unit), field fastest
+// for order 0), on the block sets Wf (nblk of 216 planes, one per distinct
+// mass, built with that mass's A^H coefficients) and the fields' d vectors
+// (dA_all / dB_all by the step's parity, 72 planes per field).  Returns
+// nonzero where it does not apply.
+int launch_batch_cheb5f(int step, int order, Lat L, const float2 *Wf, int nblk, const float2 *Dsum,
+                        const float *Bsum, const float2 *dA_all, const float2 *dB_all, const BatchField *tab,
+                        int nfields, int *err, int sm_count, cudaStream_t st, long long wait_cycles);
 void launch_batch_add_e(int64_t n, const BatchField *tab, int nfields, cudaStream_t st);
 // Chebyshev coefficients of every field from its mass's bounds; sets
 // flags[f] = 1 for non-finite bounds
@@ -200,6 +213,15 @@ void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, cons
 void launch_cheb32(bool first, Lat L, const CnCoef &C, const float2 *U, const float2 *Dsum, const float *Bsum,
                    const float2 *DE, const float2 *D, float2 *Dn, float2 *R, float2 *E, const ChebCoef &K,
                    cudaStream_t st);
+// The same Chebyshev step on the FP32 blocks of launch_cn_blocks5 (Wf, built
+// with the coefficients C; nb_sign as for the FP64 FMA stencil), staged by
+// TMA (cn_cheb5f.cu).  cheb5f_applicable: the lattices it describes (V a
+// multiple of 4, at least 36 sites, nx even, V < 2^31).  Returns nonzero if
+// the tensor maps cannot be made; wait_cycles bounds every pipeline wait.
+bool cheb5f_applicable(const Lat &L);
+int launch_cheb5f(bool first, Lat L, const CnCoef &C, double nb_sign, const float2 *Wf, const float2 *Dsum,
+                  const float *Bsum, const float2 *D, float2 *Dn, float2 *R, float2 *E, const ChebCoef &K, int *err,
+                  int sm_count, cudaStream_t st, long long wait_cycles);
 void launch_add_e(int64_t n, double2 *X, const float2 *E, cudaStream_t st);
 void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st);
 void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);

@@ -81,6 +81,28 @@ def SetStencil(stencil=None):
                 f"Error in {modulename}: stencil")
 
 
+CHEB_REGISTER, CHEB_BLOCKS = 0, 1
+
+
+def SetChebStencil(which=None):
+    """Precision forms: force the FP32 Chebyshev step (CHEB_REGISTER: the
+    operator assembled per launch; CHEB_BLOCKS: FP32 blocks staged by TMA);
+    None restores the default (blocks where the lattice allows)."""
+    _capi.check(_capi.load().nrq_cn_set_cheb_stencil(solver_handle(), -1 if which is None else int(which)),
+                lattice.context(), f"Error in {modulename}: Chebyshev stencil")
+
+
+def ChebInfo(with_times=False):
+    """The FP32 Chebyshev step the last update ran (CHEB_*; -1 before any);
+    with_times: also the per-launch ms of each step timed on the first
+    update (-1 where not timed)."""
+    last = ctypes.c_int()
+    ms = np.zeros(2)
+    _capi.check(_capi.load().nrq_cn_cheb_info(solver_handle(), ctypes.byref(last), _capi.dptr(ms)),
+                lattice.context(), f"Error in {modulename}: Chebyshev info")
+    return (int(last.value), ms) if with_times else int(last.value)
+
+
 def SetHistoryGuess(on=True):
     """Plain form: start each solve from the extrapolation 2b - psi plus
     2 t1 - t2 of the field's last two corrections (FP32 history; the

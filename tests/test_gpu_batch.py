@@ -249,3 +249,52 @@ def test_batch_with_learned_guess_matches_single_updates(oracle):
         bl.Destructor()
         bp.Destructor()
         net.Destructor()
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (36, 4, 4)])
+@pytest.mark.parametrize("order", [0, 1])
+def test_batch_fp32_block_step(oracle, n, order):
+    """The batch forced onto the FP32 block Chebyshev step (variant 3): every
+    field equals its single-field update to within the tolerance, and two
+    fields the oracle.  36 x 4 x 4 has rows long enough for the x-wrap
+    columns; 2 masses x 3 sources use two block sets."""
+    V = int(np.prod(n))
+    masses = [1.0, 1.5]
+    srcs = _sources(V, 3, 13)
+    tol = 1e-10
+    with lattice_ctx(n, A, cn=(masses[0], C, 1.0, tol, 10000, FORM_PRECISION)):
+        g, links, ef = _hot_gauge(oracle, n, 9)
+        hs = _fields(V, srcs) + _fields(V, srcs)
+        ms = [masses[0]] * 3 + [masses[1]] * 3
+        b = CNBatch(hs, ms, tol)
+        b.set_variant("fp32_blocks_tma", order)
+        singles = _fields(V, srcs) + _fields(V, srcs)
+        for step in range(3):
+            st = b.Update(g, C, 1.0, use_graph=step > 0)
+            assert st["converged"] == 1 and st["max_rel_residual"] <= tol
+            for h, m in zip(singles, ms):
+                assert h.Update(g, m, C, 1.0)["converged"] == 1
+        info = b.info()
+        assert info["variant"] == "fp32_blocks_tma" and info["block_order"] == order
+        for hb, hsg in zip(hs, singles):
+            qb, ab = hb.download()
+            qs, as_ = hsg.download()
+            assert np.abs(qb - qs).max() < 5e-10 and np.abs(ab - as_).max() < 5e-10
+        for idx in (0, 3):
+            lq, la = srcs[idx % 3]
+            q = oracle.single_point(n, lq)
+            an = oracle.single_point(n, la)
+            for _ in range(3):
+                oracle.cn_update(n, A, links, ef, ms[idx], C, 1.0, q, an, tol=1e-14)
+            qb, ab = hs[idx].download()
+            assert np.abs(qb - q).max() < 5e-10 and np.abs(ab - an).max() < 5e-10
+        b.Destructor()
+
+
+def test_batch_fp32_block_step_refused_for_odd_rows():
+    with lattice_ctx((5, 4, 4), A, cn=(1.0, C, 1.0, 1e-10, 10000, FORM_PRECISION)):
+        hs = _fields(80, [(1, 1), (2, 2)])
+        b = CNBatch(hs, [1.0, 1.0], 1e-10)
+        with pytest.raises(NrqcdError):
+            b.set_variant("fp32_blocks_tma", 0)
+        b.Destructor()

@@ -137,3 +137,60 @@ def test_precision_form_drift_against_fp64_oracle(oracle, n0):
     assert abs(en - e_ref) <= 1e-5 * max(abs(e_ref), 1e-12)
     assert np.abs(gq - q).max() < 1e-6 and np.abs(ga - an).max() < 1e-6
     assert abs(nq - 1) < 1e-9 and abs(na - 1) < 1e-9
+
+
+@pytest.mark.parametrize("n", [(6, 6, 6), (36, 4, 4), (40, 6, 4), (64, 4, 4), (16, 16, 16)])
+@pytest.mark.parametrize("cheb", ["register", "blocks"])
+def test_precision_form_chebyshev_steps(oracle, n, cheb):
+    """Both FP32 Chebyshev steps (operator assembled per launch; FP32 blocks
+    staged by TMA) against the FP64 oracle at outer residual 1e-10.  The
+    lattices cover rows shorter than a tile, rows long enough for the x-wrap
+    columns (36), units spanning rows (40 x 6) and several units per row."""
+    from nrqcd_b200 import nrqcd
+    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 7, identity_links=False)
+    M, c = 1.0, [1, 1, 1, 1]
+    q = oracle.single_point(n, 3)
+    an = oracle.single_point(n, 3)
+    want = nrqcd.CHEB_BLOCKS if cheb == "blocks" else nrqcd.CHEB_REGISTER
+    with lattice_ctx(n, A, cn=(M, c, 1.0, 1e-10, 10000, FORM_PRECISION)):
+        nrqcd.SetChebStencil(want)
+        g = GaugeConfiguration()
+        g.upload(links, ef)
+        h = NRQCDField()
+        h.InitSinglePoint(3, 3)
+        for _ in range(3):
+            st = h.Update(g, M, c, 1.0)
+            assert st["converged"] == 1 and st["max_rel_residual"] <= 1e-10
+            oracle.cn_update(n, A, links, ef, M, c, 1.0, q, an, tol=1e-14)
+        assert nrqcd.ChebInfo() == want
+        gq, ga = h.download()
+    assert np.abs(gq - q).max() < 3e-10 and np.abs(ga - an).max() < 3e-10
+
+
+def test_chebyshev_blocks_need_even_rows():
+    """nx odd: the default runs the per-launch step, forcing the block step
+    is refused."""
+    from nrqcd_b200 import NrqcdError, nrqcd
+    with lattice_ctx((5, 4, 4), A, cn=(1.0, [1, 1, 1, 1], 1.0, 1e-10, 10000, FORM_PRECISION)):
+        with pytest.raises(NrqcdError):
+            nrqcd.SetChebStencil(nrqcd.CHEB_BLOCKS)
+        g = GaugeConfiguration()
+        g.ColdInit()
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        assert h.Update(g, 1.0, [1, 1, 1, 1], 1.0)["converged"] == 1
+        assert nrqcd.ChebInfo() == nrqcd.CHEB_REGISTER
+
+
+def test_chebyshev_step_timed_choice():
+    """By default the first update times both FP32 steps and runs the faster."""
+    from nrqcd_b200 import nrqcd
+    n = (16, 16, 16)
+    with lattice_ctx(n, A, cn=(1.0, [1, 1, 1, 1], 1.0, 1e-10, 10000, FORM_PRECISION)):
+        g = GaugeConfiguration()
+        g.ColdInit()
+        h = NRQCDField()
+        h.InitSinglePoint(1, 1)
+        assert h.Update(g, 1.0, [1, 1, 1, 1], 1.0)["converged"] == 1
+        last, ms = nrqcd.ChebInfo(with_times=True)
+    assert (ms > 0).all() and last == int(np.argmin(ms))
