@@ -308,6 +308,13 @@ int nrq_cn_batch_info(const nrq_cn_batch *batch, int *variant, int *order, doubl
  * nrq_cn_batch_info; NRQ_ERR_BAD_ARG where the variant does not apply) or
  * restore the timed choice (variant -1).  The next update recalibrates.    */
 int nrq_cn_batch_set_variant(nrq_cn_batch *batch, int variant, int order);
+/* The FP64 stencil of the batch's right-hand side and residuals: 0 the
+ * register-tiled one, 1 FP64 FMAs on per-update blocks of every mass staged
+ * by TMA (V even, V >= 34).  The batch times both with its Chebyshev
+ * candidates on the first update (ms, index = which; -1 where not timed);
+ * nrq_cn_batch_set_fp64 forces one (the next update recalibrates).        */
+int nrq_cn_batch_fp64_info(const nrq_cn_batch *batch, int *which, double ms[2]);
+int nrq_cn_batch_set_fp64(nrq_cn_batch *batch, int which);
 
 /* An ensemble of independent members (batch[i], gauge[i]); the members may
  * sit on contexts of different lattice sizes on the same device.  One step

@@ -83,6 +83,12 @@ class CNBatch:
         v = -1 if variant is None else (self.VARIANTS.index(variant) if isinstance(variant, str) else int(variant))
         _capi.check(_capi.load().nrq_cn_batch_set_variant(self._h, v, int(order)), self._ctx, "set_variant")
 
+    def set_fp64(self, which):
+        """Force the FP64 stencil of the right-hand side and residuals:
+        "register" (0) or "blocks" (1)."""
+        w = {"register": 0, "blocks": 1}.get(which, which)
+        _capi.check(_capi.load().nrq_cn_batch_set_fp64(self._h, int(w)), self._ctx, "set_fp64")
+
     def info(self) -> dict:
         var, order, npass = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         ms = np.zeros(8)
@@ -93,7 +99,15 @@ class CNBatch:
         return {"variant": names[var.value], "fields_per_tile": 2 if var.value == 2 else 1,
                 "block_order": order.value,
                 "candidate_ms": {f"{names[v]}_order{o}": float(ms[2 * v + o]) for v in range(4) for o in range(2)},
-                "schedule": [int(steps[k]) for k in range(npass.value)]}
+                "schedule": [int(steps[k]) for k in range(npass.value)], **self._fp64_info()}
+
+    def _fp64_info(self) -> dict:
+        which = ctypes.c_int()
+        ms = np.zeros(2)
+        _capi.check(_capi.load().nrq_cn_batch_fp64_info(self._h, ctypes.byref(which), _capi.dptr(ms)), self._ctx,
+                    "fp64 info")
+        names = ("register", "blocks")
+        return {"fp64_stencil": names[which.value], "fp64_candidate_ms": {n: float(ms[k]) for k, n in enumerate(names)}}
 
 
 class Ensemble:

@@ -69,6 +69,14 @@ struct nrq_cn_batch {
   // lattice does not allow it) and the bounded waits' error record
   float2 *W5f = nullptr;
   int *err = nullptr, *h_err = nullptr;
+  // the FP64 stencil of the right-hand side and residuals: per-update FP64
+  // blocks of every distinct mass and every field's tensor maps (null where
+  // the lattice does not allow it); fp64 = 1 runs it, 0 the register-tiled
+  // one (timed with the Chebyshev candidates)
+  double2 *W5 = nullptr;
+  nrq::CnBatchMaps *d_fmaps = nullptr, *h_fmaps = nullptr;
+  int fp64 = 0;
+  double fp64_ms[2] = {-1, -1};
   // generation: changes with every new schedule, tuning or key
   uint64_t gen = 0;
   // graph of one scheduled step (CN only), with the generation and gauge
@@ -148,6 +156,7 @@ void fill_table(nrq_cn_batch *b, const double c[8], double dt) {
     f.tau = dt * ctx->a[0] / 2.0;
     f.mass = m;
     f.wblk = b->mass_of[i];
+    if (b->h_fmaps && !nrq::batch_mv5_field_maps(b->h_fmaps + i, ctx->lat, f.psi, f.x)) b->fp64 = 0;
     if (learned_on(b)) {
       nrq_heavy *h = b->fields[i];
       f.h1 = hist_v1(h);
@@ -160,10 +169,24 @@ void fill_table(nrq_cn_batch *b, const double c[8], double dt) {
 int upload_table(nrq_cn_batch *b, cudaStream_t st) {
   NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(b->d_tab, b->h_tab, sizeof(nrq::BatchField) * b->nf,
                                        cudaMemcpyHostToDevice, st));
+  if (b->d_fmaps)
+    NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(b->d_fmaps, b->h_fmaps, sizeof(nrq::CnBatchMaps) * b->nf,
+                                         cudaMemcpyHostToDevice, st));
   return NRQ_OK;
 }
 
 // ---- enqueue helpers (no host synchronisation) ----------------------------
+// the FP64 stencil of every field: MV_RHS or MV_RESC, the FMA stencil on the
+// blocks (fp64 = 1, where it applies) or the register-tiled one
+void launch_fp64(nrq_cn_batch *b, int mode, int fp64, int skip_done, cudaStream_t st) {
+  nrq_ctx *ctx = b->ctx;
+  if (fp64 == 1 && b->W5 &&
+      nrq::launch_batch_mv5(mode, b->order, ctx->lat, b->W5, (int)b->masses.size(), b->Dsum, b->Bsum, b->d_fmaps,
+                            b->d_tab, b->nf, skip_done, b->err, ctx->sm_count, st, nrq_wait_cycles_default) == 0)
+    return;
+  nrq::launch_batch_mv(mode, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, skip_done, st);
+}
+
 // gauge-derived data of this step: link copy, CN blocks, FP32 copies, the
 // spectral enclosure of every mass and the Chebyshev coefficients of every
 // field
@@ -180,11 +203,16 @@ int enq_prepare(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double d
     ProfScope ps(ctx, 3, (double)V * (1080.0 + 540.0));
     nrq::launch_cn_to_f32(V, b->U64, b->DE, b->Dsum, b->Bsum, b->U32, b->DE32, b->D32, b->B32, st);
   }
-  if (b->W5f && (!b->tuned || b->variant == 3))  // FP32 blocks of every mass (Chebyshev variant 3)
+  // per-update blocks of every mass: FP32 for Chebyshev variant 3, FP64 for
+  // the FP64 FMA stencil (the tuner times both before it chooses)
+  const bool want32 = b->W5f && (!b->tuned || b->variant == 3), want64 = b->W5 && (!b->tuned || b->fp64 == 1);
+  if (want32 || want64)
     for (size_t k = 0; k < b->masses.size(); ++k) {
-      ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + 1728.0));
+      ProfScope ps(ctx, 3, (double)V * (432.0 + 864.0 + (want32 ? 1728.0 : 0.0) + (want64 ? 3456.0 : 0.0)));
       const nrq::CnCoef CH = nrqh::make_coef(ctx, b->masses[k], c, dt, true);
-      nrq::launch_cn_blocks5(L, CH, b->U64, b->DE, nullptr, b->W5f + (int64_t)k * nrq::cn_mv5_block_entries(V), st);
+      const int64_t off = (int64_t)k * nrq::cn_mv5_block_entries(V);
+      nrq::launch_cn_blocks5(L, CH, b->U64, b->DE, want64 ? b->W5 + off : nullptr, want32 ? b->W5f + off : nullptr,
+                             st);
     }
   const double tau = dt * ctx->a[0] / 2.0;
   for (size_t k = 0; k < b->masses.size(); ++k) {
@@ -201,7 +229,7 @@ int enq_rhs(nrq_cn_batch *b, const nrq_gauge *g, cudaStream_t st) {
   nrq_ctx *ctx = b->ctx;
   {
     ProfScope ps(ctx, 0, (double)ctx->lat.V * (b->nf * 1152.0 * 3 + 432.0 + 192.0));
-    nrq::launch_batch_mv(nrq::MV_RHS, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf, 0, st);
+    launch_fp64(b, nrq::MV_RHS, b->fp64, 0, st);
   }
   int rc = check_launch(ctx, "batch rhs");
   if (!rc && learned_on(b)) {
@@ -218,8 +246,7 @@ int enq_residual(nrq_cn_batch *b, cudaStream_t st, bool first) {
   nrq_ctx *ctx = b->ctx;
   {
     ProfScope ps(ctx, 0, (double)ctx->lat.V * (b->nf * (1152.0 * 2 + 576.0 * 2) + 432.0 + 192.0));
-    nrq::launch_batch_mv(nrq::MV_RESC, b->order, ctx->lat, b->U64, b->Dsum, b->Bsum, b->DE, b->d_tab, b->nf,
-                         first ? 0 : 1, st);
+    launch_fp64(b, nrq::MV_RESC, b->fp64, first ? 0 : 1, st);
   }
   {
     ProfScope ps(ctx, 2, (double)b->nf * b->nsb * nrq::CN_COLS * 2 * 8);
@@ -366,10 +393,32 @@ int autotune(nrq_cn_batch *b, cudaStream_t st) {
         best_order = order;
       }
     }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   b->variant = best_variant;
   b->order = best_order;
+  // the FP64 residual stencil (it writes r32, d of the first slot and the
+  // partials, which the solve's first residual rewrites), in the chosen order
+  b->fp64 = 0;
+  for (int which = 0; which < 2; ++which) {
+    b->fp64_ms[which] = -1.0;
+    if (which == 1 && !b->W5) continue;
+    launch_fp64(b, nrq::MV_RESC, which, 0, st);
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < reps; ++r) launch_fp64(b, nrq::MV_RESC, which, 0, st);
+    cudaEventRecord(e1, st);
+    int rc = check_launch(ctx, "batch autotune");
+    if (rc) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return rc;
+    }
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    b->fp64_ms[which] = ms / reps;
+  }
+  if (b->fp64_ms[1] > 0.0 && b->fp64_ms[1] < b->fp64_ms[0]) b->fp64 = 1;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   b->tuned = true;
   return NRQ_OK;
 }
@@ -454,7 +503,8 @@ int conclude(nrq_cn_batch *b, const Check &chk, int64_t inner, int64_t passes) {
   b->last_maxrel = chk.worst;
   b->last_conv = chk.conv;
   if (chk.timeout) {
-    b->ctx->last_error = "batch Chebyshev stencil: a bounded pipeline wait expired (load " +
+    b->ctx->last_error = std::string("batch stencil: a bounded pipeline wait expired (") +
+                         (b->h_err[1] / 16 == 7 ? "k_batch_mv5" : "k_cheb5f") + ", load " +
                          std::to_string(b->h_err[2]) + ", CTA " + std::to_string(b->h_err[3]) + ")";
     cudaMemsetAsync(b->err, 0, sizeof(int) * 16, b->ctx->stream);
     b->h_err[0] = 0;
@@ -596,6 +646,10 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
   NRQ_B_ALLOC(b->err, sizeof(int) * 16);
   if (nrq::cheb5f_applicable(ctx->lat))
     NRQ_B_ALLOC(b->W5f, sizeof(float2) * nrq::cn_mv5_block_entries(V) * b->masses.size());
+  if (nrq::batch_mv5_applicable(ctx->lat)) {
+    NRQ_B_ALLOC(b->W5, sizeof(double2) * nrq::cn_mv5_block_entries(V) * b->masses.size());
+    NRQ_B_ALLOC(b->d_fmaps, sizeof(nrq::CnBatchMaps) * nfields);
+  }
   b->xbuf.assign(nfields, nullptr);
   for (int i = 0; i < nfields; ++i) NRQ_B_ALLOC(b->xbuf[i], sizeof(double2) * P);
 #undef NRQ_B_ALLOC
@@ -604,6 +658,8 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
   if ((e = cudaMallocHost(&b->h_flags, sizeof(int) * nfields)) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&b->h_bounds, sizeof(double) * 4 * b->masses.size())) != cudaSuccess) return fail(e);
   if ((e = cudaMallocHost(&b->h_err, sizeof(int) * 16)) != cudaSuccess) return fail(e);
+  if (b->d_fmaps && (e = cudaMallocHost(&b->h_fmaps, sizeof(nrq::CnBatchMaps) * nfields)) != cudaSuccess)
+    return fail(e);
   std::memset(b->h_err, 0, sizeof(int) * 16);
   if ((e = cudaMemsetAsync(b->err, 0, sizeof(int) * 16, ctx->stream)) != cudaSuccess) return fail(e);
   // defined contents for the FP32 vectors and flags the tuner's first launches read
@@ -625,11 +681,12 @@ extern "C" int nrq_cn_batch_destroy(nrq_cn_batch *b) {
                   (void *)b->D32, (void *)b->B32, (void *)b->bpart, (void *)b->bounds, (void *)b->b_all,
                   (void *)b->r32_all, (void *)b->dA_all, (void *)b->dB_all, (void *)b->e32_all, (void *)b->part_all,
                   (void *)b->scal_all, (void *)b->flags, (void *)b->d_tab, (void *)b->lgf, (void *)b->lfeat,
-                  (void *)b->lomega, (void *)b->W5f, (void *)b->err})
+                  (void *)b->lomega, (void *)b->W5f, (void *)b->err, (void *)b->W5, (void *)b->d_fmaps})
     if (p) cudaFree(p);
   for (double2 *p : b->xbuf)
     if (p) cudaFree(p);
-  for (void *p : {(void *)b->h_tab, (void *)b->h_scal, (void *)b->h_flags, (void *)b->h_bounds, (void *)b->h_err})
+  for (void *p : {(void *)b->h_tab, (void *)b->h_scal, (void *)b->h_flags, (void *)b->h_bounds, (void *)b->h_err,
+                  (void *)b->h_fmaps})
     if (p) cudaFreeHost(p);
   delete b;
   return NRQ_OK;
@@ -759,6 +816,26 @@ extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *variant, int *order
   return NRQ_OK;
 }
 
+extern "C" int nrq_cn_batch_fp64_info(const nrq_cn_batch *b, int *which, double ms[2]) {
+  if (!b) return NRQ_ERR_BAD_ARG;
+  if (which) *which = b->fp64;
+  if (ms)
+    for (int k = 0; k < 2; ++k) ms[k] = b->fp64_ms[k];
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_batch_set_fp64(nrq_cn_batch *b, int which) {
+  if (!b || which < 0 || which > 1) return NRQ_ERR_BAD_ARG;
+  if (which == 1 && !b->W5) {
+    b->ctx->last_error = "batch: the FP64 block stencil needs an even V of at least 34 sites";
+    return NRQ_ERR_BAD_ARG;
+  }
+  b->fp64 = which;
+  b->have_key = false;
+  b->gen++;
+  return NRQ_OK;
+}
+
 extern "C" int nrq_cn_batch_set_variant(nrq_cn_batch *b, int variant, int order) {
   if (!b || variant < -1 || variant >= nrq::BATCH_CHEB_VARIANTS || order < 0 || order > 1) return NRQ_ERR_BAD_ARG;
   if (variant == 2) {
@@ -777,6 +854,7 @@ extern "C" int nrq_cn_batch_set_variant(nrq_cn_batch *b, int variant, int order)
   } else {
     b->variant = variant;
     b->order = order;
+    if (b->fp64 < 0 || !b->tuned) b->fp64 = b->W5 ? 1 : 0;  // untimed: the FMA stencil where it applies
     b->tuned = true;
   }
   b->have_key = false;  // recalibrate the schedule with the new kernel
@@ -851,6 +929,13 @@ extern "C" int nrq_ensemble_step(nrq_ensemble *e, const double c[8], double dt, 
     if (!e->exec) {
       cudaGraph_t master = nullptr;
       NRQ_CUDA_TRY(ctx0, cudaGraphCreate(&master, 0));
+      // members run as concurrent branches, except where a member uses the
+      // persistent block stencils: those size their grids to every SM and
+      // hold most of an SM's shared memory, so concurrent members only
+      // fragment the GPU, and the members' steps are chained instead
+      bool chain = false;
+      for (nrq_cn_batch *b : e->batches) chain = chain || b->variant == 3 || b->fp64 == 1;
+      cudaGraphNode_t prev = nullptr;
       for (int i = 0; i < n; ++i) {
         cudaGraph_t child = nullptr;
         StepArgs a{e->batches[i], e->gauges[i], c, dt, true};
@@ -860,8 +945,10 @@ extern "C" int nrq_ensemble_step(nrq_ensemble *e, const double c[8], double dt, 
           return rc;
         }
         cudaGraphNode_t node;
-        cudaError_t er = cudaGraphAddChildGraphNode(&node, master, nullptr, 0, child);
+        cudaError_t er = cudaGraphAddChildGraphNode(&node, master, chain && prev ? &prev : nullptr,
+                                                    chain && prev ? 1 : 0, child);
         cudaGraphDestroy(child);
+        prev = node;
         if (er != cudaSuccess) {
           cudaGraphDestroy(master);
           ctx0->last_error = std::string("cudaGraphAddChildGraphNode: ") + cudaGetErrorString(er);

@@ -1,6 +1,8 @@
 // Kernel declarations shared between the kernel translation units and the
 // C-ABI translation unit.
 #pragma once
+#include <cuda.h>
+
 #include "nrq_common.cuh"
 
 namespace nrq {
@@ -184,6 +186,25 @@ __device__ __forceinline__ bool batch_field_done(const BatchField &f) {
 // fields alone (their iterate did not change since their last check)
 void launch_batch_mv(int mode, int order, Lat L, const double2 *U, const double2 *Dsum, const double *Bsum,
                      const double2 *DE, const BatchField *tab, int nfields, int skip_done, cudaStream_t st);
+// The same two modes (MV_RHS, MV_RESC) on the FP64 FMA stencil's blocks
+// (cn_batch_mv5.cu): W holds nblk block sets of 216 planes, one per distinct
+// mass, built with that mass's A^H coefficients (the field's wblk); fmaps[f]
+// the tensor maps of field f's psi and iterate x (written by
+// batch_mv5_field_maps before every step; device memory).  The residual's
+// partials are one row per (field, 32-site unit), the rows of
+// launch_batch_finalize.  Returns nonzero where it does not apply (V even,
+// at least 34 sites, V < 2^31).
+struct CnBatchMaps {
+  struct {
+    CUtensorMap spin;   // 72 planes x 2V doubles, box {68, 36}
+    CUtensorMap spin1;  // one site, box {2, 36}
+  } in[2];              // 0: psi, 1: the iterate x
+};
+bool batch_mv5_applicable(const Lat &L);
+bool batch_mv5_field_maps(CnBatchMaps *m, const Lat &L, const double2 *psi, const double2 *x);
+int launch_batch_mv5(int mode, int order, Lat L, const double2 *W, int nblk, const double2 *Dsum, const double *Bsum,
+                     const CnBatchMaps *fmaps, const BatchField *tab, int nfields, int skip_done, int *err,
+                     int sm_count, cudaStream_t st, long long wait_cycles);
 // Chebyshev kernel variants: 0 = one field per tile, 2 blocks/SM (168
 // registers); 1 = one field per tile, 3 blocks/SM (113 registers); 2 = two
 // fields of one mass per tile, 1 block/SM.  Returns nonzero for an

@@ -253,11 +253,13 @@ def test_batch_with_learned_guess_matches_single_updates(oracle):
 
 @pytest.mark.parametrize("n", [(8, 8, 8), (36, 4, 4)])
 @pytest.mark.parametrize("order", [0, 1])
-def test_batch_fp32_block_step(oracle, n, order):
-    """The batch forced onto the FP32 block Chebyshev step (variant 3): every
-    field equals its single-field update to within the tolerance, and two
-    fields the oracle.  36 x 4 x 4 has rows long enough for the x-wrap
-    columns; 2 masses x 3 sources use two block sets."""
+@pytest.mark.parametrize("fp64", ["register", "blocks"])
+def test_batch_fp32_block_step(oracle, n, order, fp64):
+    """The batch forced onto the FP32 block Chebyshev step (variant 3) with
+    either FP64 stencil for the right-hand side and residuals: every field
+    equals its single-field update to within the tolerance, and two fields
+    the oracle.  36 x 4 x 4 has rows long enough for the x-wrap columns;
+    2 masses x 3 sources use two block sets."""
     V = int(np.prod(n))
     masses = [1.0, 1.5]
     srcs = _sources(V, 3, 13)
@@ -268,6 +270,7 @@ def test_batch_fp32_block_step(oracle, n, order):
         ms = [masses[0]] * 3 + [masses[1]] * 3
         b = CNBatch(hs, ms, tol)
         b.set_variant("fp32_blocks_tma", order)
+        b.set_fp64(fp64)
         singles = _fields(V, srcs) + _fields(V, srcs)
         for step in range(3):
             st = b.Update(g, C, 1.0, use_graph=step > 0)
@@ -276,6 +279,7 @@ def test_batch_fp32_block_step(oracle, n, order):
                 assert h.Update(g, m, C, 1.0)["converged"] == 1
         info = b.info()
         assert info["variant"] == "fp32_blocks_tma" and info["block_order"] == order
+        assert info["fp64_stencil"] == fp64
         for hb, hsg in zip(hs, singles):
             qb, ab = hb.download()
             qs, as_ = hsg.download()
