@@ -740,6 +740,385 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   }
 }
 
+// The same stencil over every field of a batch (the batching form's
+// right-hand side and refinement residual; k_batch_mv2 in cn_mv.cu is the
+// register-tiled alternative): work items (field, unit), field fastest
+// (order 0) or unit fastest (order 1).  MV_RHS reads psi (b = A psi, x = 2b
+// - psi), MV_RESC the iterate x (r = b - A^H x rounded to FP32, d = r /
+// theta), each from the field's own tensor maps (fmaps), both on the field's
+// block set (wblk: blocks built with that mass's A^H coefficients, so A is
+// the neighbour sum negated).  A field that converged sits a residual out
+// (skip_done).  The residual's partial sums form one row per (field, unit),
+// the rows launch_batch_finalize reads, summed in a fixed order.
+template <int MODE>
+__global__ void __maxnreg__(mv5::kMaxReg)
+    k_batch_mv5(Lat L, const __grid_constant__ Mv5Maps maps, const double2 *__restrict__ W, int nunits, int *err,
+                long long wait_cycles, const BatchField *__restrict__ tab, const CnBatchMaps *__restrict__ fmaps,
+                int nfields, int order, int skip_done) {
+  using namespace mv5;
+  static_assert(MODE == MV_RHS || MODE == MV_RESC, "batch modes");
+  const int nwork = nfields * nunits;
+  auto item = [&](int w, int &f, int &u) {
+    if (order == 0) {
+      f = w % nfields;
+      u = w / nfields;
+    } else {
+      f = w / nunits;
+      u = w % nunits;
+    }
+  };
+  auto skip = [&](int f) { return MODE == MV_RESC && skip_done && batch_field_done(tab[f]); };
+  constexpr int kIn = MODE == MV_RHS ? 0 : 1;  // the field's input: psi or x
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[kBufs][2], empty_bar[kBufs], dfull[2], dempty[2];
+  __shared__ volatile int s_issued;  // loads the producer issued (diagnostics of an expired wait)
+  __shared__ uint32_t s_tmem;        // the exchange's tensor-memory columns
+  __shared__ double redb[2][2][2][3][2];  // per item parity, species, column half, column, sum
+  unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int V = (int)L.V;  // the launcher admits V < 2^31 only
+
+  if (threadIdx.x == 0) {
+    s_issued = 0;
+    for (int b = 0; b < kBufs; ++b) {
+      mbar_init(&full_bar[b][0], 1);
+      mbar_init(&full_bar[b][1], 1);
+      mbar_init(&empty_bar[b], 4);  // the four consumer warps of the load's species
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&dfull[b], 1);
+      mbar_init(&dempty[b], kWarps);  // every consumer warp
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tc::tmem_alloc(&s_tmem, kTmemCols);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = s_tmem;
+
+
+  // bounded wait with this launch's limit
+  auto wait = [&](uint64_t *bar, uint32_t parity) -> bool {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+      if (clock64() - t0 > wait_cycles) return false;
+    return true;
+  };
+
+  // ---------------------------------------------------------- producer
+  if (warp >= kWarps) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kProdReg));
+    if (warp == kWarps && lane == 0) {
+      bool ok = true;
+      int i = 0, ndiag = 0, k = 0;  // loads issued, diagonal loads issued, items begun
+      for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x) {
+        int f, u;
+        item(w, f, u);
+        if (skip(f)) continue;
+        const UnitPos P = unit_pos(L, u * kUnit);
+        const int x0 = P.x0;
+        const CUtensorMap *spin = &fmaps[f].in[kIn].spin, *spin1 = &fmaps[f].in[kIn].spin1;
+        const int wrow = tab[f].wblk * 216;
+        {  // the unit's diagonal matrices, with its first load
+          const int db = k & 1;
+          if (k >= 2) {
+            const uint32_t dpar = (uint32_t)((k / 2 - 1) & 1);
+            if (!wait(&dempty[db], dpar)) {
+              record_timeout(err, 5, 2, i);
+              ok = false;
+            } else if (!mbar_wait(&dfull[db], dpar)) {
+              record_timeout(err, 5, 3, i);
+              ok = false;
+            }
+            if (!ok) break;
+          }
+          unsigned char *dd = smem + kOffDiag + db * kDiagStride;
+          mbar_expect_tx(&dfull[db], kDiagD + kDiagB);
+          tma_2d(dd, &maps.D, 2 * x0, 0, &dfull[db]);
+          tma_2d(dd + kDiagD, &maps.B, x0, 0, &dfull[db]);
+          ++ndiag;
+        }
+        for (int li = 0; li < kLoads && ok; ++li, ++i) {
+          const int b = i % kBufs;
+          if (i >= kBufs) {
+            const uint32_t par = (uint32_t)((i / kBufs - 1) & 1);
+            const int j = i - kBufs;  // the buffer's previous load
+            // every consumer warp of the species released the buffer, and
+            // its previous load landed
+            if (!wait(&empty_bar[b], par)) {
+              record_timeout(err, 5, 2, i);
+              ok = false;
+            } else if (!mbar_wait(&full_bar[b][j & 1], (uint32_t)((j / kPer) & 1))) {
+              record_timeout(err, 5, 3, i);
+              ok = false;
+            }
+            if (!ok) break;
+          }
+          const int stg = li >> 1, sp = li & 1;
+          const int ss = spin_start5(L, P, stg);
+          const int ws = blk_start5(x0, ss, stg);
+          const int I = stg == 0 ? 0 : (stg + 1) / 2;
+          unsigned char *bb = smem + b * kBufBytes;
+          int yl = -1, yr = -1;
+          if (stg == 0) x_wraps5(L, P, yl, yr);
+          uint32_t tx = 2u * kTileBytes;
+          if (stg == 0) tx += (yl >= 0 ? 2u : 0u) * kColBytes + (yr >= 0 ? kColBytes : 0u);
+          uint64_t *fb = &full_bar[b][sp];
+          mbar_expect_tx(fb, tx);
+          tma_2d(bb, spin, 2 * ss, sp * 36, fb);
+          tma_2d(bb + kOffW, &maps.W, 2 * ws, wrow + (I * 2 + sp) * 36, fb);
+          if (stg == 0) {
+            if (yl >= 0) {
+              tma_2d(bb + kOffX, spin1, 2 * yl, sp * 36, fb);
+              tma_2d(bb + kOffX + kColStride, &maps.W1, 2 * yl, wrow + sp * 36, fb);
+            }
+            if (yr >= 0) tma_2d(bb + kOffX + 2 * kColStride, spin1, 2 * yr, sp * 36, fb);
+          }
+          s_issued = i + 1;
+        }
+        ++k;
+      }
+      // every issued load lands before the CTA exits: loads before the last
+      // kBufs were waited for above
+      for (int k = max(0, i - kBufs); k < i; ++k)
+        if (!mbar_wait(&full_bar[k % kBufs][k & 1], (uint32_t)((k / kPer) & 1))) {
+          record_timeout(err, 5, 4, k);
+          break;
+        }
+      for (int k = max(0, ndiag - 2); k < ndiag; ++k)
+        if (!mbar_wait(&dfull[k & 1], (uint32_t)((k >> 1) & 1))) {
+          record_timeout(err, 5, 4, -1 - k);
+          break;
+        }
+    }
+    return;
+  }
+  asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kConsReg));
+
+  // ---------------------------------------------------------- consumers
+  // warp w = 4 kh + 2 sp + h: input-row half kh, species sp, column half h;
+  // lane = site of the 32-site unit.  The thread accumulates all six output
+  // rows of columns 3h .. 3h + 2 over input rows 3 kh .. 3 kh + 2 of its site
+  // and species; after the unit's last stage it keeps rows 3 kh .. 3 kh + 2
+  // of the sum (exchange_halves with warp w ^ 4).
+  const int kh = warp >> 2, sp = (warp >> 1) & 1, h = warp & 1;
+  const int pair_bar = 2 + (warp & 3);  // named barrier of the warp pair (ids 2-5)
+  // the thread's first spinor plane and block entries (see nb_products)
+  const int pofs = 18 * h + 3 * kh, wofs_f = 3 * kh, wofs_b = 18 * kh;
+  const int site_in_unit = lane;
+  bool dead = false;
+
+  int it = 0;  // items begun
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    int f, u;
+    item(w, f, u);
+    if (skip(f)) continue;
+    // the item's operator, input and block set (the field's own)
+    const BatchField *F = tab + f;
+    const CnCoef &Ci = MODE == MV_RHS ? F->CA : F->CH;
+    const double nb_sign = MODE == MV_RHS ? -1.0 : 1.0;
+    const double2 *in = MODE == MV_RHS ? F->psi : F->x;
+    const double2 *Wb = W + (int64_t)F->wblk * 216 * V;
+    const cplx ak = Ci.kin[sp], am = Ci.mag[sp], ad = Ci.dar[sp];
+    const cplx dg = Ci.dkin * ak + cplx{1.0, 0.0};
+    const UnitPos P = unit_pos(L, u * kUnit);
+    const int x0 = P.x0;
+    const int x = x0 + site_in_unit;
+    const bool act = x < V;
+    const int xs = act ? x : V - 1;  // a valid site for the addresses of idle lanes
+    int nb[6];
+    neighbours5(L, P, xs - x0, nb);
+    int yl = -1, yr = -1;
+    x_wraps5(L, P, yl, yr);
+    double acc[6][3][2];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) acc[r][k][0] = acc[r][k][1] = 0.0;
+    // the epilogue's operand at the own site: b for the residuals, rh for V,
+    // the input itself for RHS and T
+    const double2 *epi_src = MODE == MV_RHS ? F->psi : F->b;
+    cplx ev[3][3];
+
+#pragma unroll
+    for (int stg = 0; stg < kStages; ++stg) {
+      const int ld = it * kLoads + stg * 2 + sp;
+      const int b = ld % kBufs;
+      if (stg == kStages - 2) {
+        // the epilogue's operand, loaded into registers two stages ahead
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int k = 0; k < 3; ++k) ev[i][k] = ldg(epi_src + (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + xs);
+      }
+      int role = -1;
+      if (!dead && !wait(&full_bar[b][sp], (uint32_t)((ld / kPer) & 1))) role = 0;
+      // stage 0 also reads the unit's diagonal matrices
+      if (stg == 0 && !dead && role < 0 && !wait(&dfull[it & 1], (uint32_t)((it >> 1) & 1))) role = 1;
+      // warp-uniform: the products below use warp votes
+      if (__any_sync(0xffffffffu, role >= 0) && !dead) {
+        dead = true;
+        if (role >= 0) {
+          record_timeout(err, 5, role, ld);
+          if (err[3] == (int)blockIdx.x && err[2] == ld) {  // this thread's record: add the detail
+            const uint64_t word =
+                role == 0 ? *(volatile uint64_t *)&full_bar[b][sp] : *(volatile uint64_t *)&dfull[it & 1];
+            err[4] = s_issued + 1;
+            err[5] = (int)(uint32_t)word;
+            err[6] = (int)(uint32_t)(word >> 32);
+            err[7] = role == 0 ? (ld / kPer) & 1 : (it >> 1) & 1;
+          }
+        }
+      }
+      const unsigned char *bb = smem + b * kBufBytes;
+      const uint32_t s_tile = smem_u32(bb), s_w = smem_u32(bb + kOffW);
+      if (!dead) {
+        const int ss = spin_start5(L, P, stg);
+        const int ws = blk_start5(x0, ss, stg);
+        if (stg == 0) {
+          // diagonal (colour only): row (c, s) takes input rows (j, s);
+          // x - ss = site_in_unit + 1 lies inside the tile for every lane
+          const unsigned char *dd = smem + kOffDiag + (it & 1) * kDiagStride;
+          const uint32_t s_d = smem_u32(dd) + (uint32_t)(site_in_unit * 16);
+          const uint32_t s_b = smem_u32(dd + kDiagD) + (uint32_t)(site_in_unit * 8);
+          const uint32_t s_own = s_tile + (uint32_t)((site_in_unit + 1) * 16);
+          if (kh == 0)
+            diag_products<0>(acc, h, s_d, s_b, s_own, ad, am, dg, nb_sign);
+          else
+            diag_products<1>(acc, h, s_d, s_b, s_own, ad, am, dg, nb_sign);
+        }
+        // neighbours of this stage: stage 0 = +x (forward) and -x (backward)
+#pragma unroll
+        for (int hh = 0; hh < (stg == 0 ? 2 : 1); ++hh) {
+          const bool bwd = stg == 0 ? (hh == 1) : (stg % 2 == 0);
+          const int d = stg == 0 ? hh : stg + 1;  // neighbour index in nb[]
+          const int I = d >> 1;
+          const int y = nb[d];                   // neighbour site
+          const int m = bwd ? y : xs;            // site of the forward block
+          const bool ps = (unsigned)(y - ss) < (unsigned)kTileS;  // spinor in the tile
+          const bool wsh = (unsigned)(m - ws) < (unsigned)kTileS; // block in the tile
+          // stage 0: a wrapped x neighbour in the wrap columns
+          const bool pw = stg == 0 && !ps && y == (bwd ? yl : yr);
+          const bool ww = stg == 0 && bwd && !wsh && m == yl;
+          if (stg == 0 && __any_sync(0xffffffffu, act && (pw || ww)) &&
+              __all_sync(0xffffffffu, ((ps || pw) && (wsh || ww)) || !act)) {
+            // shared memory, a lane's operands in the tile or in a wrap
+            // column (per-lane strides)
+            const uint32_t xc = smem_u32(bb + kOffX);
+            const uint32_t wst = ww ? 16u : (uint32_t)kTileS * 16u, pst = pw ? 16u : (uint32_t)kTileS * 16u;
+            const uint32_t wa = (ww ? xc + kColStride : s_w + (uint32_t)((m - ws) * 16)) +
+                                (uint32_t)(bwd ? wofs_b : wofs_f) * wst;
+            const uint32_t pa =
+                (pw ? xc + (bwd ? 0u : 2u * kColStride) : s_tile + (uint32_t)((y - ss) * 16)) + (uint32_t)pofs * pst;
+            auto lw = [&](int e) { return lds_d2(wa + (uint32_t)e * wst); };
+            auto lp = [&](int e) { return lds_d2(pa + (uint32_t)e * pst); };
+            if (bwd)
+              nb_products<true>(acc, lw, lp);
+            else
+              nb_products<false>(acc, lw, lp);
+          } else if (__all_sync(0xffffffffu, (ps && wsh) || !act)) {
+            // every operand of the warp in shared memory
+            constexpr uint32_t kPl = kTileS * 16u;  // plane stride of the tiles
+            const uint32_t wa = s_w + (uint32_t)((m - ws) * 16) + (uint32_t)(bwd ? wofs_b : wofs_f) * kPl;
+            const uint32_t pa = s_tile + (uint32_t)((y - ss) * 16) + (uint32_t)pofs * kPl;
+            auto lw = [&](int e) { return lds_d2(wa + (uint32_t)e * kPl); };
+            auto lp = [&](int e) { return lds_d2(pa + (uint32_t)e * kPl); };
+            if (bwd)
+              nb_products<true>(acc, lw, lp);
+            else
+              nb_products<false>(acc, lw, lp);
+          } else if (act) {
+            // some lanes' operands outside the tiles (periodic wraps, tile
+            // edges): those lanes read global memory, the others the tiles
+            const int64_t wst = wsh ? kTileS : V, pst = ps ? kTileS : V;
+            const double2 *wp = (wsh ? (const double2 *)(bb + kOffW) + (m - ws)
+                                     : Wb + (int64_t)((I * 2 + sp) * 36) * V + m) +
+                                (bwd ? wofs_b : wofs_f) * wst;
+            const double2 *pp = (ps ? (const double2 *)bb + (y - ss) : in + (int64_t)(sp * 36) * V + y) + pofs * pst;
+            auto lw = [&](int e) { return wp[e * wst]; };
+            auto lp = [&](int e) { return pp[e * pst]; };
+            if (bwd)
+              nb_products<true>(acc, lw, lp);
+            else
+              nb_products<false>(acc, lw, lp);
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&empty_bar[b]);
+        if (stg == 0) mbar_arrive(&dempty[it & 1]);
+      }
+    }
+
+    // ---------------------------------------------------------- epilogue
+    // every warp of the pair takes both barriers of the exchange, dead or
+    // not, active lanes or not
+    double res[3][3][2];
+    if (kh == 0)
+      exchange_halves<0>(acc, res, tbase, warp, pair_bar);
+    else
+      exchange_halves<1>(acc, res, tbase, warp, pair_bar);
+    double qb[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};  // the residual: this item's sums
+    if (!dead && act) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int64_t off = (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + x;
+          // D in + sgn N in = sgn (sgn D in + N in), sgn = +-1: the diagonal
+          // was scaled by sgn and the neighbour sum was not
+          const cplx y_ = {nb_sign * res[i][k][0], nb_sign * res[i][k][1]};
+          const cplx ev_ = ev[i][k];
+          if (MODE == MV_RHS) {
+            st(F->b + off, y_);
+            st(F->x + off, 2.0 * y_ - ev_);
+          } else {
+            const cplx rv = ev_ - y_;
+            const cplx dv = rv * F->inv_theta[sp];
+            F->r32[off] = make_float2((float)rv.re, (float)rv.im);
+            F->dA[off] = make_float2((float)dv.re, (float)dv.im);
+            qb[k][0] += norm2(rv);
+            qb[k][1] += norm2(ev_);
+          }
+        }
+    }
+    if (MODE == MV_RESC) {
+      // the item's partial row: each column over the lanes, then over the
+      // warp pair (the row half kh = 1 hands its sums to kh = 0)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) qb[k][j] += __shfl_xor_sync(0xffffffffu, qb[k][j], o);
+      if (kh == 1 && lane == 0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) redb[it & 1][sp][h][k][j] = qb[k][j];
+      named_bar_sync(pair_bar, 64);
+      if (kh == 0 && lane < 6 && !dead) {
+        double v = 0.0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t)
+          if (t == lane) v = qb[t >> 1][t & 1];
+        const int k = lane >> 1, j = lane & 1;
+        F->partials[((int64_t)u * CN_COLS + sp * 6 + 3 * h + k) * 2 + j] = v + redb[it & 1][sp][h][k][j];
+      }
+    }
+    ++it;
+  }
+
+  // every consumer warp is done with the tensor memory before warp 0 frees it
+  tc::fence_before_sync();
+  named_bar_sync(1, kWarps * 32);
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tbase, kTmemCols);
+}
+
 // ------------------------------------------------------------------ host
 void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, float2 *Wf,
                        cudaStream_t st) {
@@ -785,6 +1164,49 @@ int launch_cn_mv5(int mode, Lat L, const CnCoef &C, double nb_sign, const double
     case MV_RESC: go(k_cn_mv5<MV_RESC>); break;
     default: go(k_cn_mv5<MV_T>); break;
   }
+  return 0;
+}
+
+
+bool batch_mv5_applicable(const Lat &L) { return L.V >= mv5::kTileS && L.V <= 0x7fffffffLL && (L.V & 1) == 0; }
+
+bool batch_mv5_field_maps(CnBatchMaps *m, const Lat &L, const double2 *psi, const double2 *x) {
+  using namespace mv5;
+  const uint64_t V = (uint64_t)L.V;
+  memset(m, 0, sizeof(*m));
+  const double2 *src[2] = {psi, x};
+  for (int k = 0; k < 2; ++k)
+    if (!stage::encode(&m->in[k].spin, src[k], 2 * V, 72, 2 * kTileS, 36) ||
+        !stage::encode(&m->in[k].spin1, src[k], 2 * V, 72, 2, 36))
+      return false;
+  return true;
+}
+
+int launch_batch_mv5(int mode, int order, Lat L, const double2 *W, int nblk, const double2 *Dsum, const double *Bsum,
+                     const CnBatchMaps *fmaps, const BatchField *tab, int nfields, int skip_done, int *err,
+                     int sm_count, cudaStream_t st, long long wait_cycles) {
+  using namespace mv5;
+  if (!batch_mv5_applicable(L) || nfields <= 0 || order < 0 || order > 1 || (mode != MV_RHS && mode != MV_RESC))
+    return -1;
+  const int64_t nunits = cn_mv5_units(L.V);
+  if (nunits * nfields > 0x7fffffffLL) return -1;
+  const uint64_t V = (uint64_t)L.V;
+  Mv5Maps maps;  // the fields' spinor maps come from fmaps
+  memset(&maps, 0, sizeof(maps));
+  if (!stage::encode(&maps.W, W, 2 * V, 216ull * nblk, 2 * kTileS, 36) ||
+      !stage::encode(&maps.W1, W, 2 * V, 216ull * nblk, 2, 36) || !stage::encode(&maps.D, Dsum, 2 * V, 9, 2 * kUnit, 9) ||
+      !stage::encode(&maps.B, Bsum, V, 9, kUnit, 9))
+    return -1;
+  const unsigned grid = (unsigned)std::min<int64_t>(nunits * nfields, sm_count);
+  auto go = [&](auto kern) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+    kern<<<grid, kThreads, kSmemBytes, st>>>(L, maps, W, (int)nunits, err, wait_cycles, tab, fmaps, nfields, order,
+                                            skip_done);
+  };
+  if (mode == MV_RHS)
+    go(k_batch_mv5<MV_RHS>);
+  else
+    go(k_batch_mv5<MV_RESC>);
   return 0;
 }
 
