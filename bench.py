@@ -93,53 +93,109 @@ def workload_config(L, n_gpus):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """SM clocks and clock-event reasons of this rank's GPU during the timed
+    region: NVML polled every 10 ms from a thread (started before the
+    warm-up, so that the timed region is covered from its first
+    millisecond; mark() and stop() bound the window), else nvidia-smi at
+    50 ms.  Reads only; changes no setting of the GPU."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index):
         self.dev = device_index
+        self.samples = []  # (time, sm MHz, max MHz, reasons)
+        self.t0 = None
         self.proc = None
-        self.lines = []
+        self.stop_ev = threading.Event()
+        self.thread = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.dev)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def poll():
+                while not self.stop_ev.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((time.perf_counter(), sm, smax,
+                                             {k for k, bit in bits.items() if r & bit}))
+                    except Exception:
+                        pass
+                    self.stop_ev.wait(0.01)
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            self.source = "nvml"
+            return
+        except Exception:
+            pass
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "50", "-i", str(self.dev)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+
+            def read():
+                for line in self.proc.stdout:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm, smax = float(parts[1]), float(parts[2])
+                    except ValueError:
+                        continue
+                    self.samples.append((time.perf_counter(), sm, smax,
+                                         {nm for nm, v in zip(self.NAMES, parts[5:9]) if v.lower() == "active"}))
+            self.thread = threading.Thread(target=read, daemon=True)
+            self.thread.start()
+            self.source = "nvidia-smi"
         except Exception:
             self.proc = None
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def mark(self):
+        """The timed region begins now."""
+        self.t0 = time.perf_counter()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 9:
-                continue
+        t1 = time.perf_counter()
+        if self.source is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        time.sleep(0.03)  # the sample that straddles the end
+        self.stop_ev.set()
+        if self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        t0 = self.t0 if self.t0 is not None else 0.0
+        inside = [s for s in self.samples if t0 <= s[0] <= t1 + 0.02]
+        sm = [s[1] for s in inside]
+        reasons = set().union(*[s[3] for s in inside]) if inside else set()
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(s[2] for s in inside) if inside else None,
+                "sm_min_mhz": min(sm) if sm else None, "reasons": sorted(reasons), "samples": len(sm),
+                "source": self.source}
 
 
 # ------------------------------------------------------------------ reference arm
@@ -881,14 +937,15 @@ def main():
         iters.append(st)
         g.Update(1.0)
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(max(3, args.warmup)):
         step()
     lattice.synchronize()
     iters.clear()
     # ---------------- timed region
-    clocks = ClockSampler(local)
-    clocks.start()
     torch.cuda.synchronize()
+    clocks.mark()
     _capi.profile_enable(ctx, True)
     ms = timed_steps(step, args.steps, dist, CudaEventTimer(stream))
     prof = _capi.profile_read(ctx)
