@@ -187,6 +187,28 @@ __device__ __forceinline__ UnitPos unit_pos(const Lat &L, int x0) {
   return {x0, x0 - t * nx, t - z * ny, z};
 }
 
+// Position of work unit u (32 consecutive sites along x).  Where every row
+// holds whole units (nx a multiple of 32) and ny, nz are multiples of 8, the
+// units are taken in blocks of 8 x 8 rows (x fastest, then y and z within
+// the block, then the blocks), so that the +-y and +-z tiles a unit shares
+// with its neighbours are read within a few hundred units of each other,
+// while L2 still holds them, at any lattice size (in site order the +-z
+// tiles are a whole plane of units apart: 127 MB of loads at 128^3);
+// otherwise in site order.
+__device__ __forceinline__ UnitPos unit_pos_of(const Lat &L, int u) {
+  const int nx = (int)L.nx, ny = (int)L.ny, nz = (int)L.nz;
+  if ((nx & 31) || (ny & 7) || (nz & 7)) return unit_pos(L, u * mv5::kUnit);
+  const int nxu = nx >> 5;
+  int t = u / nxu;
+  const int cx = (u - t * nxu) << 5;
+  const int yi = t & 7, zi = (t >> 3) & 7;
+  t >>= 6;
+  const int nby = ny >> 3;
+  const int bz = t / nby, by = t - bz * nby;
+  const int cy = (by << 3) + yi, cz = (bz << 3) + zi;
+  return {cx + nx * (cy + ny * cz), cx, cy, cz};
+}
+
 // the six periodic neighbours (+x,-x,+y,-y,+z,-z) of the site l sites after
 // the unit's first (V < 2^31); its coordinates by carrying from the unit's
 __device__ __forceinline__ void neighbours5(const Lat &L, const UnitPos &P, int l, int (&nb)[6]) {
@@ -446,7 +468,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
           if (!ok) break;
         }
         const int li = i % kLoads, stg = li >> 1, sp = li & 1;
-        if (li == 0) P = unit_pos(L, ((int)blockIdx.x + (i / kLoads) * (int)gridDim.x) * kUnit);
+        if (li == 0) P = unit_pos_of(L, (int)blockIdx.x + (i / kLoads) * (int)gridDim.x);
         const int x0 = P.x0;
         if (li == 0) {  // the unit's diagonal matrices, with its first load
           const int k = i / kLoads, db = k & 1;
@@ -525,7 +547,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   bool dead = false;
 
   for (int u = 0; u < my_units; ++u) {
-    const UnitPos P = unit_pos(L, ((int)blockIdx.x + u * (int)gridDim.x) * kUnit);
+    const UnitPos P = unit_pos_of(L, (int)blockIdx.x + u * (int)gridDim.x);
     const int x0 = P.x0;
     const int x = x0 + site_in_unit;
     const bool act = x < V;
@@ -817,7 +839,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
         int f, u;
         item(w, f, u);
         if (skip(f)) continue;
-        const UnitPos P = unit_pos(L, u * kUnit);
+        const UnitPos P = unit_pos_of(L, u);
         const int x0 = P.x0;
         const CUtensorMap *spin = &fmaps[f].in[kIn].spin, *spin1 = &fmaps[f].in[kIn].spin1;
         const int wrow = tab[f].wblk * 216;
@@ -923,7 +945,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     const double2 *Wb = W + (int64_t)F->wblk * 216 * V;
     const cplx ak = Ci.kin[sp], am = Ci.mag[sp], ad = Ci.dar[sp];
     const cplx dg = Ci.dkin * ak + cplx{1.0, 0.0};
-    const UnitPos P = unit_pos(L, u * kUnit);
+    const UnitPos P = unit_pos_of(L, u);
     const int x0 = P.x0;
     const int x = x0 + site_in_unit;
     const bool act = x < V;
