@@ -103,6 +103,24 @@ __device__ __forceinline__ UnitPos5f unit_pos5f(const Lat &L, int x0) {
   return {x0, x0 - t * nx, t - z * ny, z};
 }
 
+// Position of work unit u: in blocks of 8 x 8 rows where the lattice allows
+// (nx a multiple of 32, ny and nz of 8), so that neighbouring units' +-y and
+// +-z tiles come from L2, as in the FP64 FMA stencil (cn_mv5.cu); otherwise
+// in site order.
+__device__ __forceinline__ UnitPos5f unit_pos5f_of(const Lat &L, int u) {
+  const int nx = (int)L.nx, ny = (int)L.ny, nz = (int)L.nz;
+  if ((nx & 31) || (ny & 7) || (nz & 7)) return unit_pos5f(L, u * c5f::kUnit);
+  const int nxu = nx >> 5;
+  int t = u / nxu;
+  const int cx = (u - t * nxu) << 5;
+  const int yi = t & 7, zi = (t >> 3) & 7;
+  t >>= 6;
+  const int nby = ny >> 3;
+  const int bz = t / nby, by = t - bz * nby;
+  const int cy = (by << 3) + yi, cz = (bz << 3) + zi;
+  return {cx + nx * (cy + ny * cz), cx, cy, cz};
+}
+
 // the six periodic neighbours (+x,-x,+y,-y,+z,-z) of the site l sites after
 // the unit's first (V < 2^31), its coordinates by carrying from the unit's
 __device__ __forceinline__ void neighbours5f(const Lat &L, const UnitPos5f &P, int l, int (&nb)[6]) {
@@ -282,7 +300,7 @@ __global__ void __launch_bounds__(c5f::kThreads, 1)
         int f, u;
         cheb5f_item<BATCH>(A, w, f, u);
         if (cheb5f_skip<BATCH>(A, f)) continue;
-        const UnitPos5f P = unit_pos5f(L, u * kUnit);
+        const UnitPos5f P = unit_pos5f_of(L, u);
         const int x0 = P.x0;
         const int srow = BATCH ? f * 72 : 0;                   // the field's planes
         const int wrow = BATCH ? A.tab[f].wblk * 216 : 0;      // its block set
@@ -384,7 +402,7 @@ __global__ void __launch_bounds__(c5f::kThreads, 1)
     const cfl dg = {(float)C.dkin * ak.re + 1.f, (float)C.dkin * ak.im};
     const cfl c1 = {(float)K.c1[sp].re, (float)K.c1[sp].im}, c2 = {(float)K.c2[sp].re, (float)K.c2[sp].im};
 
-    const UnitPos5f P = unit_pos5f(L, u * kUnit);
+    const UnitPos5f P = unit_pos5f_of(L, u);
     const int x0 = P.x0;
     const int x = x0 + site_in_unit;
     const bool act = x < V;
