@@ -654,7 +654,7 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
         _capi.profile_enable(lats[L].ctx, False)
     info = {L: b.info() for (L, _, _, _), b in zip(members, batches)}
     # forms combined: every batch starts its solves from the learned guess
-    t_learned, info_learned, learned_stats = None, None, []
+    t_learned, info_learned, learned_stats, gates_learned = None, None, [], None
     if learned_params is not None:
         from nrqcd_b200.learned import LearnedGuess
         nets = {}
@@ -664,10 +664,17 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
             nets[L].set_trained(True)
         for (L, _, _, _), b in zip(members, batches):
             b.attach_learned(nets[L])
-        for _ in range(max(4, warmup + 2)):  # history fills (depth 0, 1, 2), then calibration and capture
+        # history fills (depth 0, 1, 2), the gate decides at depth 2, then
+        # calibration (with the guess or, gated off, without) and capture
+        for _ in range(max(6, warmup + 3)):
             ens.Step(WILSON, 1.0, use_graph=True)
         t_learned = timed(lambda: learned_stats.append(ens.Step(WILSON, 1.0, use_graph=True)), steps)
         info_learned = {L: b.info() for (L, _, _, _), b in zip(members, batches)}
+        gates_learned = {}
+        for (L, _, _, _), b in zip(members, batches):
+            gi = b.learned_info()
+            gates_learned.setdefault(f"{L}^3", []).append(
+                {"gate": gi["gate"], "guess_ms": round(gi["guess_ms"], 3), "saving_ms": round(gi["saving_ms"], 3)})
         for b in batches:
             b.attach_learned(None)
         for net in nets.values():
@@ -719,7 +726,8 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
             "s_per_step": t_learned, "field_site_updates_per_s": per_step / t_learned,
             "speedup_vs_serial": t_serial / t_learned,
             "max_rel_residual": max(st["max_rel_residual"] for st in learned_stats),
-            "schedules": {f"{L}^3": v["schedule"] for L, v in info_learned.items()}},
+            "schedules": {f"{L}^3": v["schedule"] for L, v in info_learned.items()},
+            "gates": gates_learned},
         "max_rel_residual": max(s["max_rel_residual"] for s in stats),
         "converged": all(s["converged"] == 1 for s in stats),
         "tuning": {f"{L}^3": v for L, v in info.items()},

@@ -314,6 +314,15 @@ int nrq_cn_batch_set_variant(nrq_cn_batch *batch, int variant, int order);
  * candidates on the first update (ms, index = which; -1 where not timed);
  * nrq_cn_batch_set_fp64 forces one (the next update recalibrates).        */
 int nrq_cn_batch_fp64_info(const nrq_cn_batch *batch, int *which, double ms[2]);
+/* The gate of an attached learned guess: the calibration with the guess's
+ * full two-step history measures the guess's cost and prices the inner
+ * steps and refinement passes it saved against the last schedule without
+ * it (same step width and coefficients); when the saving is below 1.25
+ * times the cost the guess is switched off (gate 0) and the batch runs the
+ * plain start.  gate: -2 no guess attached, -1 not decided yet, 1 on, 0
+ * off; guess_ms, saving_ms: the measured cost and the value of the saving
+ * (-1 before).                                                             */
+int nrq_cn_batch_learned_info(const nrq_cn_batch *batch, int *gate, double *guess_ms, double *saving_ms);
 int nrq_cn_batch_set_fp64(nrq_cn_batch *batch, int which);
 
 /* An ensemble of independent members (batch[i], gauge[i]); the members may

@@ -101,6 +101,16 @@ class CNBatch:
                 "candidate_ms": {f"{names[v]}_order{o}": float(ms[2 * v + o]) for v in range(4) for o in range(2)},
                 "schedule": [int(steps[k]) for k in range(npass.value)], **self._fp64_info()}
 
+    def learned_info(self) -> dict:
+        """The attached learned guess's gate ("none", "undecided", "on",
+        "off"), its measured cost and the value of the steps it saved (ms)."""
+        gate = ctypes.c_int()
+        cost, saving = ctypes.c_double(), ctypes.c_double()
+        _capi.check(_capi.load().nrq_cn_batch_learned_info(self._h, ctypes.byref(gate), ctypes.byref(cost),
+                                                           ctypes.byref(saving)), self._ctx, "learned info")
+        names = {-2: "none", -1: "undecided", 0: "off", 1: "on"}
+        return {"gate": names[gate.value], "guess_ms": cost.value, "saving_ms": saving.value}
+
     def _fp64_info(self) -> dict:
         which = ctypes.c_int()
         ms = np.zeros(2)

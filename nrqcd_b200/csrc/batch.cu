@@ -90,6 +90,16 @@ struct nrq_cn_batch {
   float4 *lgf = nullptr, *lomega = nullptr;
   float *lfeat = nullptr;
   int key_depth = -1;
+  // the guess's gate: -1 undecided, 1 on, 0 off (it cost more than the
+  // Chebyshev steps and passes it saved, measured at the calibration with
+  // the full two-step history); the last schedule calibrated without the
+  // guess, the measured cost of the guess and the value of what it saved
+  int learn_gate = -1;
+  bool have_plain = false;
+  double plain_dt = 0.0, plain_c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<int> plain_schedule;
+  bool time_guess = false;
+  double guess_ms = -1.0, guess_saving_ms = -1.0;
   // statistics of the last update
   int64_t last_inner = 0, last_passes = 0, last_matvecs = 0;
   double last_maxrel = 0.0, last_initial = 0.0;
@@ -115,7 +125,9 @@ void free_graph(cudaGraphExec_t &g) {
   g = nullptr;
 }
 
-bool learned_on(const nrq_cn_batch *b) { return b->learn && nrqh::learned_ready(b->learn); }
+bool learned_on(const nrq_cn_batch *b) {
+  return b->learn && nrqh::learned_ready(b->learn) && b->learn_gate != 0;
+}
 
 // history depth of the learned guess (every field's count, capped at 2), -1 without it
 int depth_of(const nrq_cn_batch *b) {
@@ -234,7 +246,22 @@ int enq_rhs(nrq_cn_batch *b, const nrq_gauge *g, cudaStream_t st) {
   int rc = check_launch(ctx, "batch rhs");
   if (!rc && learned_on(b)) {
     ProfScope ps(ctx, 3, (double)ctx->lat.V * b->nf * (1152.0 * 4 + 576.0 * 5 + 128.0));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (b->time_guess) {  // the gate's measurement of the guess's cost
+      NRQ_CUDA_TRY(ctx, cudaEventCreate(&e0));
+      NRQ_CUDA_TRY(ctx, cudaEventCreate(&e1));
+      cudaEventRecord(e0, st);
+    }
     rc = nrqh::learned_guess_batch(b->learn, ctx, b->d_tab, b->nf, b->U64, g->E, b->lgf, b->lfeat, b->lomega, st);
+    if (b->time_guess) {
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      b->guess_ms = ms;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
   }
   return rc;
 }
@@ -442,6 +469,12 @@ int refine_adaptive(nrq_cn_batch *b, double dt, cudaStream_t st, int budget, std
 }
 
 // calibration step: adaptive passes with host synchronisation; records the
+int64_t sum(const std::vector<int> &v) {
+  int64_t s = 0;
+  for (int x : v) s += x;
+  return s;
+}
+
 // schedule and tunes the kernels on the first call
 int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double dt, cudaStream_t st,
                      Check &chk) {
@@ -452,12 +485,39 @@ int update_calibrate(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], dou
                                     cudaMemcpyDeviceToHost, st));
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (!b->tuned && (rc = autotune(b, st))) return rc;
-  if ((rc = enq_rhs(b, g, st)) || (rc = enq_residual(b, st, true)) || (rc = enq_readback(b, st))) return rc;
+  const bool deciding = learned_on(b) && b->learn_gate < 0 && depth_of(b) == 2;
+  b->time_guess = deciding;
+  rc = enq_rhs(b, g, st);
+  b->time_guess = false;
+  if (rc || (rc = enq_residual(b, st, true)) || (rc = enq_readback(b, st))) return rc;
   NRQ_CUDA_TRY(ctx, cudaStreamSynchronize(st));
   chk = check(b);
   b->last_initial = chk.worst;
   std::vector<int> used;
   if ((rc = refine_adaptive(b, dt, st, kMaxPasses, used, chk))) return rc;
+  if (!learned_on(b)) {  // the plain schedule, for the gate of a later guess
+    b->have_plain = true;
+    b->plain_schedule = used;
+    b->plain_dt = dt;
+    std::memcpy(b->plain_c, c, sizeof(b->plain_c));
+  } else if (deciding) {
+    // the gate: the inner steps and passes the guess saved against the last
+    // plain schedule of the same step width and coefficients, at the
+    // measured time of a Chebyshev launch and of a residual launch, against
+    // the guess's measured cost (and a quarter more for its history
+    // updates); no plain schedule to compare with keeps the guess on
+    bool same = b->have_plain && b->plain_dt == dt;
+    for (int k = 0; k < 8 && same; ++k) same = b->plain_c[k] == c[k];
+    b->learn_gate = 1;
+    if (same && b->guess_ms >= 0.0) {
+      const double cheb = b->cand_ms[2 * b->variant + b->order];
+      const double resc = b->fp64_ms[b->fp64] > 0.0 ? b->fp64_ms[b->fp64] : cheb;
+      const double steps = (double)(sum(b->plain_schedule) - sum(used));
+      const double passes = (double)b->plain_schedule.size() - (double)used.size();
+      b->guess_saving_ms = std::max(0.0, steps) * std::max(0.0, cheb) + std::max(0.0, passes) * resc;
+      if (b->guess_saving_ms < 1.25 * b->guess_ms) b->learn_gate = 0;
+    }
+  }
   b->schedule = used;
   b->have_key = true;
   b->key_depth = depth_of(b);
@@ -531,11 +591,6 @@ void fill_stats(const nrq_cn_batch *b, nrq_cn_stats *s) {
   s->initial_rel_residual = b->last_initial;
 }
 
-int64_t sum(const std::vector<int> &v) {
-  int64_t s = 0;
-  for (int x : v) s += x;
-  return s;
-}
 
 int capture(nrq_ctx *ctx, cudaStream_t st, cudaGraph_t *graph, int (*body)(void *), void *arg) {
   const bool prof = ctx->prof;
@@ -784,6 +839,8 @@ extern "C" int nrq_cn_batch_attach_learned(nrq_cn_batch *b, nrq_learn *net) {
       if ((rc = nrqh::ensure_hist(h))) return rc;
   }
   b->learn = net;
+  b->learn_gate = -1;
+  b->guess_ms = b->guess_saving_ms = -1.0;
   b->have_key = false;  // recalibrate (and recapture) with or without the guess
   b->gen++;
   return NRQ_OK;
@@ -813,6 +870,14 @@ extern "C" int nrq_cn_batch_info(const nrq_cn_batch *b, int *variant, int *order
   if (npasses) *npasses = (int)b->schedule.size();
   if (steps)
     for (int k = 0; k < 16; ++k) steps[k] = k < (int)b->schedule.size() ? b->schedule[k] : 0;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_batch_learned_info(const nrq_cn_batch *b, int *gate, double *guess_ms, double *saving_ms) {
+  if (!b) return NRQ_ERR_BAD_ARG;
+  if (gate) *gate = b->learn ? b->learn_gate : -2;
+  if (guess_ms) *guess_ms = b->guess_ms;
+  if (saving_ms) *saving_ms = b->guess_saving_ms;
   return NRQ_OK;
 }
 

@@ -251,6 +251,50 @@ def test_batch_with_learned_guess_matches_single_updates(oracle):
         net.Destructor()
 
 
+def test_batch_learned_guess_gate(oracle):
+    """A guess attached after plain steps is gated at the calibration with
+    its full history: its cost and the value of the steps it saved are
+    measured, the gate is decided, and the fields keep their single-field
+    results either way (once off, the batch runs the plain start)."""
+    from nrqcd_b200.learned import LearnedGuess
+    n = (8, 8, 8)
+    V = int(np.prod(n))
+    tol = 1e-10
+    with lattice_ctx(n, A, cn=(1.0, C, 1.0, tol, 10000, FORM_PRECISION)):
+        net = LearnedGuess(seed=3)
+        net.reserve(16 * 2 * V)
+        g0, _, _ = _hot_gauge(oracle, n, 51)
+        h0 = NRQCDField()
+        h0.InitSinglePoint(5, 9)
+        for _ in range(8):
+            net.record(h0, g0, 1.0, C, 1.0)
+            g0.Update(1.0)
+        net.train(300, batch=2048, lr=2e-3, seed=3)
+        g, _, _ = _hot_gauge(oracle, n, 52)
+        srcs = _sources(V, 2, 19)
+        ms = [1.0, 1.0, 1.5, 1.5]
+        hb = _fields(V, srcs + srcs)
+        singles = _fields(V, srcs + srcs)
+        b = CNBatch(hb, ms, tol)
+        assert b.learned_info()["gate"] == "none"
+        for step in range(7):
+            if step == 2:
+                b.attach_learned(net)
+                assert b.learned_info()["gate"] == "undecided"
+            assert b.Update(g, C, 1.0, use_graph=True)["converged"] == 1
+            for h, m in zip(singles, ms):
+                h.Update(g, m, C, 1.0)
+        info = b.learned_info()
+        assert info["gate"] in ("on", "off") and info["guess_ms"] > 0 and info["saving_ms"] >= 0
+        for a_, b_ in zip(hb, singles):
+            qa, aa = a_.download()
+            qb, ab = b_.download()
+            assert np.abs(qa - qb).max() < 5e-10 and np.abs(aa - ab).max() < 5e-10
+        b.attach_learned(None)
+        b.Destructor()
+        net.Destructor()
+
+
 @pytest.mark.parametrize("n", [(8, 8, 8), (36, 4, 4)])
 @pytest.mark.parametrize("order", [0, 1])
 @pytest.mark.parametrize("fp64", ["register", "blocks"])
