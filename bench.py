@@ -69,6 +69,12 @@ def parse():
     p.add_argument("--no-forms", action="store_true")
     p.add_argument("--no-ensemble", action="store_true")
     p.add_argument("--only-ensemble", action="store_true", help="print only the batching-ensemble JSON")
+    p.add_argument("--ensemble-members", default=None,
+                   help="with --only-ensemble: members as EXTENTxCOUNT[,...] (default the C4 ensemble)")
+    p.add_argument("--ensemble-sources", type=int, default=None,
+                   help="with --only-ensemble: point sources per member and mass (default 16)")
+    p.add_argument("--ensemble-no-learned", action="store_true",
+                   help="with --only-ensemble: skip the learned-guess leg")
     p.add_argument("--only-forms", action="store_true", help="print only the CN-forms JSON")
     p.add_argument("--forms-sizes", type=int, nargs="+", default=list(FORMS_SIZES))
     p.add_argument("--no-drift", action="store_true")
@@ -596,25 +602,26 @@ ENS_SOURCES = 16
 ENS_MASSES = (1.0, 1.5)
 
 
-def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
+def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None, ensemble=ENSEMBLE, sources=ENS_SOURCES):
     """Aggregate field-site updates/s of the uneven ensemble: one CUDA graph
     launch per coupled step, the same batched launches issued eagerly, and a
     serial loop of single-field precision-form updates (nrq_heavy_update_cn
-    per field, then the leapfrog per member)."""
+    per field, then the leapfrog per member).  ensemble: (extent, members)
+    pairs; sources: point sources per member and mass."""
     import torch
     from nrqcd_b200 import GaugeConfiguration, NRQCDField, _capi, lattice
     from nrqcd_b200.batch import CNBatch, Ensemble
     lib = _capi.load()
-    lats = {L: lattice.Lattice((L, L, L), A) for L, _ in ENSEMBLE}
+    lats = {L: lattice.Lattice((L, L, L), A) for L, _ in ensemble}
     members = []
     seed = 1000
-    for L, count in ENSEMBLE:
+    for L, count in ensemble:
         for _ in range(count):
             seed += 1
             g = GaugeConfiguration(lat=lats[L])
             g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=seed, identity_links=True)
             rng = np.random.default_rng(seed)
-            srcs = rng.integers(0, L ** 3, size=(ENS_SOURCES, 2)) + 1
+            srcs = rng.integers(0, L ** 3, size=(sources, 2)) + 1
             fields, masses = [], []
             for m in ENS_MASSES:
                 for lq, la in srcs:
@@ -624,7 +631,7 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
                     masses.append(m)
             members.append((L, g, fields, masses))
     per_step = sum(L ** 3 * len(f) for L, _, f, _ in members)
-    streams = [torch.cuda.ExternalStream(lib.nrq_cuda_stream(lats[L].ctx)) for L, _ in ENSEMBLE]
+    streams = [torch.cuda.ExternalStream(lib.nrq_cuda_stream(lats[L].ctx)) for L, _ in ensemble]
     s0 = streams[0]
 
     def timed(fn, n):
@@ -712,7 +719,8 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None):
         sten[f"{L}^3"] = {"launches": c0["launches"], "ms": c0["ms"],
                           "achieved_GBps": c0["bytes"] / (c0["ms"] / 1000.0) / 1e9 if c0["ms"] > 0 else None}
     out = {
-        "workload": "uneven ensemble 8 x 24^3 + 4 x 32^3 + 2 x 48^3, 16 point sources at random sites x aM = 1.0, "
+        "workload": "uneven ensemble " + " + ".join(f"{n} x {L}^3" for L, n in ensemble) +
+                    f", {sources} point sources at random sites x aM = 1.0, "
                     "1.5 per member, coupled step (CN of every field, then the member's leapfrog), "
                     "precision-form CN at residual 1e-10",
         "field_site_updates_per_step": per_step,
@@ -890,7 +898,12 @@ def main():
     if args.only_ensemble:
         import torch
         torch.cuda.set_device(local)
-        out = measure_ensemble(args.steps, args.warmup, learned_params=train_learned(masses=ENS_MASSES)[0])
+        ens = ENSEMBLE
+        if args.ensemble_members:
+            ens = tuple((int(a), int(b)) for a, b in (m.split("x") for m in args.ensemble_members.split(",")))
+        learned = None if args.ensemble_no_learned else train_learned(masses=ENS_MASSES)[0]
+        out = measure_ensemble(args.steps, args.warmup, learned_params=learned, ensemble=ens,
+                               sources=args.ensemble_sources or ENS_SOURCES)
         if rank == 0:
             print(json.dumps({"batching_ensemble": out}), flush=True)
         return
