@@ -399,12 +399,15 @@ def measure_gluon_distribution(L, cpu=True, steps=10):
 
 
 # ------------------------------------------------------------------ CN forms
-# name -> (form, history start of the plain form); the speed-ups are
-# against plain_fp64_bicgstab, the library's default plain solve (with the
-# start extrapolated from the field's history); the plain solve from 2b - psi
-# alone is reported beside it
-FORMS = {"plain_fp64_bicgstab": (0, 1), "plain_fp64_bicgstab_no_history": (0, 0),
-         "precision_fp32_chebyshev_fp64_refinement": (1, 1), "learned_guess_precision": (2, 1)}
+# name -> (form, history start, merged update, confirm every solve) of the
+# plain form; the speed-ups are against plain_fp64_bicgstab, the library's
+# default plain solve (start extrapolated from the field's history, x, r and
+# p updated in one pass, the recursive residual accepted with the measured
+# margin); beside it the plain solve from 2b - psi alone and the plain solve
+# with two update passes and every solve confirmed by the true residual
+FORMS = {"plain_fp64_bicgstab": (0, 1, 1, 0), "plain_fp64_bicgstab_no_history": (0, 0, 1, 0),
+         "plain_fp64_bicgstab_two_pass_confirmed": (0, 1, 0, 1),
+         "precision_fp32_chebyshev_fp64_refinement": (1, 1, 1, 0), "learned_guess_precision": (2, 1, 1, 0)}
 FORMS_SIZES = (64, 96, 128)
 # lattices of the precision form's drift (the precision configuration names 64^3 and 96^3)
 DRIFT_SIZES = (64, 96)
@@ -441,11 +444,13 @@ def measure_cn_forms(L, steps, params, tol=1e-10, seed=1):
         g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=seed, identity_links=True)
         stream = torch.cuda.ExternalStream(lib.nrq_cuda_stream(lat.ctx))
         cw = _capi.coeffs(WILSON)
-        for name, (form, hist) in FORMS.items():
+        for name, (form, hist, merged, confirm) in FORMS.items():
             cn = ctypes.c_void_p()
             _capi.check(lib.nrq_cn_init(lat.ctx, MASS, _capi.dptr(cw), 1.0, tol, 10000, form, ctypes.byref(cn)),
                         lat.ctx, "nrq_cn_init")
             _capi.check(lib.nrq_cn_set_history_guess(cn, hist), lat.ctx, "history guess")
+            _capi.check(lib.nrq_cn_set_merged_update(cn, merged), lat.ctx, "merged update")
+            _capi.check(lib.nrq_cn_set_true_residual(cn, confirm), lat.ctx, "true residual")
             net = None
             if form == 2:
                 net = LearnedGuess(lat=lat)

@@ -3,6 +3,7 @@
 // initial-condition pipeline (host ranlxd stream, cuFFT, device kernels).
 #include <cufft.h>
 
+#include <cfloat>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -1098,6 +1099,24 @@ extern "C" int nrq_cn_cheb_info(const nrq_cn *cn, int *last, double ms[2]) {
   return NRQ_OK;
 }
 
+extern "C" int nrq_cn_set_merged_update(nrq_cn *cn, int on) {
+  if (!cn || on < 0 || on > 1) return NRQ_ERR_BAD_ARG;
+  cn->merged_update = on != 0;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_set_true_residual(nrq_cn *cn, int always) {
+  if (!cn || always < 0 || always > 1) return NRQ_ERR_BAD_ARG;
+  cn->confirm_always = always != 0;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_true_residual_info(const nrq_cn *cn, int *last_true) {
+  if (!cn || !last_true) return NRQ_ERR_BAD_ARG;
+  *last_true = cn->last_true ? 1 : 0;
+  return NRQ_OK;
+}
+
 extern "C" int nrq_cn_set_history_guess(nrq_cn *cn, int on) {
   if (!cn || on < 0 || on > 1) return NRQ_ERR_BAD_ARG;
   cn->history_guess = on != 0;
@@ -1127,7 +1146,7 @@ namespace {
 // formed.  Derived data a stencil reads instead (the tensor-core stencil's
 // cached blocks) is extra traffic and is not counted.
 double mv_bytes(const nrq_ctx *ctx, int mode) {
-  const int streams[6] = {2, 3, 5, 3, 2, 3};  // PLAIN, RHS, RES, V, T, RESC
+  const int streams[7] = {2, 3, 5, 3, 2, 3, 3};  // PLAIN, RHS, RES, V, T, RESC, T2
   return (double)ctx->lat.V * (1152.0 * streams[mode] + 2.0 * (432.0 + 192.0));
 }
 // the tensor-core stencil's backward blocks are -W^H of the forward ones,
@@ -1219,6 +1238,10 @@ int mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq
       return NRQ_OK;
     }
   }
+  if (mode == nrq::MV_T2) {  // the solve asks for it only after an FMA launch
+    ctx->last_error = "cn stencil: the merged update needs the FMA stencil";
+    return NRQ_ERR_BAD_ARG;
+  }
   if (cn->stencil == NRQ_STENCIL_TENSOR && offdiag_imaginary(C)) {
     double sign = 0.0;
     int rc = ensure_blocks(cn, C, g, &sign);
@@ -1258,7 +1281,8 @@ void fin(nrq_cn *cn, int stage) {
   int64_t rows = cn->nblocks;
   if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TMA) rows = 3 * cn->nblocks;
   if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TENSOR) rows = nrq::cn_mv4_rows(ctx->lat.V, ctx->sm_count);
-  if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_FMA) rows = nrq::cn_mv5_rows(ctx->lat.V, ctx->sm_count);
+  if ((stage <= 2 || stage == 5) && cn->last_stencil == NRQ_STENCIL_FMA)
+    rows = nrq::cn_mv5_rows(ctx->lat.V, ctx->sm_count);
   ProfScope ps(ctx, 2, (double)rows * 12 * 3 * 8);
   nrq::launch_cn_finalize(stage, rows, cn->partials, cn->scal, cn->tol, ctx->stream);
 }
@@ -1638,6 +1662,30 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
 }
 }  // namespace
 
+// The per-column recursive relative residuals at a convergence, from the
+// scalars read back from the device; half: at the half-step exit, where the
+// columns that met the tolerance there have |s| and the others (converged
+// before) their last r.
+static void recursive_rel(const double *hs, bool half, double rel[nrq::CN_COLS]) {
+  for (int k = 0; k < nrq::CN_COLS; ++k) {
+    const double *sc = hs + k * nrq::SC_STRIDE;
+    const double q = (half && sc[nrq::SC_CONV] == 0.0) ? sc[nrq::SC_SS] : sc[nrq::SC_RR];
+    rel[k] = sc[nrq::SC_BB] > 0.0 ? std::sqrt(q / sc[nrq::SC_BB]) : 0.0;
+  }
+}
+// Whether a converged solve may end on its recursive residual: every column's
+// plus four times the largest recursive-to-true gap that this solver's
+// confirmed solves showed (at least 4 eps of ||b||) meets the tolerance.  The
+// gap comes from rounding in the x and r updates (x carries about eps ||A||
+// ||x|| per iteration that r does not); it is measured, not assumed.
+static bool accept_recursive(const nrq_cn *cn, const double rel[nrq::CN_COLS]) {
+  if (cn->confirm_always || cn->gap_rel < 0.0 || cn->since_confirm >= nrq_cn::kReconfirm) return false;
+  const double margin = 4.0 * std::max(cn->gap_rel, 4.0 * DBL_EPSILON);
+  for (int k = 0; k < nrq::CN_COLS; ++k)
+    if (!(rel[k] + margin <= cn->tol)) return false;
+  return true;
+}
+
 extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mass, const double c[8],
                                    double dt, nrq_cn_stats *stats) {
   if (!cn || !h || !g || !c) return NRQ_ERR_BAD_ARG;
@@ -1669,6 +1717,11 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     vstreams += 2;
   }
   bool restart = true, just_restarted = false;
+  bool half_accept = false;  // ended at a half step on the recursive |s|
+  // a restart pass confirming a convergence measures the recursive-to-true
+  // gap against the recursive residuals of that convergence
+  bool gap_pending = false;
+  double rec[nrq::CN_COLS];
   int64_t its = 0;
   int status = NRQ_OK;
   double *hs = cn->h_scal;
@@ -1733,11 +1786,24 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
             half = half && (sc[nrq::SC_CONV] != 0.0 || sc[nrq::SC_HALF] != 0.0);
           }
           if (half && *scal_err(hs) == 0) {
-            ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 3);
-            nrq::launch_vec_xp(L, cn->x, cn->p, cn->scal, st);
+            {
+              ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 3);
+              nrq::launch_vec_xp(L, cn->x, cn->p, cn->scal, st);
+            }
             matvecs += 1;
             vstreams += 3;
             ++its;
+            // the same acceptance as below, on |s| for the columns that met
+            // the tolerance here
+            recursive_rel(hs, true, rec);
+            if (accept_recursive(cn, rec)) {
+              half_accept = true;
+              cn->last_true = false;
+              ++cn->since_confirm;
+              if ((rc = check_launch(ctx, "cn half step"))) return rc;
+              break;
+            }
+            gap_pending = true;
             restart = true;
             continue;
           }
@@ -1749,23 +1815,37 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       b.out = cn->t;
       b.partials = cn->partials;
       b.scal = cn->scal;
-      if ((rc = mv(cn, nrq::MV_T, CH, g, b))) return rc;
-      fin(cn, 2);
-      if (tma) {
-        ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 7);
-        nrq::launch_vec_xr_s(L, cn->x, cn->r, cn->p, cn->s, cn->t, cn->rh, cn->scal, cn->partials, st);
-        vstreams -= 1;
+      // the merged update: the t launch also reduces rh.t, which gives beta
+      // before r is formed, so that x, r and p are updated in one pass
+      const bool merged = tma && cn->merged_update && cn->last_stencil == NRQ_STENCIL_FMA;
+      if (merged) b.in2 = cn->rh;
+      if ((rc = mv(cn, merged ? nrq::MV_T2 : nrq::MV_T, CH, g, b))) return rc;
+      if (merged) {
+        fin(cn, 5);
+        {
+          ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 8);
+          nrq::launch_vec_xrp(L, cn->x, cn->r, cn->p, cn->s, cn->t, cn->v, cn->scal, cn->partials, st);
+        }
+        fin(cn, 6);
+        vstreams += 1 + 1 + 8;  // rh read by the v and t launches, the merged pass
       } else {
-        ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 8);
-        nrq::launch_vec_xr(L, cn->x, cn->r, cn->p, cn->v, cn->t, cn->rh, cn->scal, cn->partials, st);
-      }
-      fin(cn, 3);
-      {
-        ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 4);
-        nrq::launch_vec_p(L, cn->p, cn->r, cn->v, cn->scal, st);
+        fin(cn, 2);
+        if (tma) {
+          ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 7);
+          nrq::launch_vec_xr_s(L, cn->x, cn->r, cn->p, cn->s, cn->t, cn->rh, cn->scal, cn->partials, st);
+          vstreams -= 1;
+        } else {
+          ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 8);
+          nrq::launch_vec_xr(L, cn->x, cn->r, cn->p, cn->v, cn->t, cn->rh, cn->scal, cn->partials, st);
+        }
+        fin(cn, 3);
+        {
+          ProfScope ps(ctx, 1, (double)L.V * 1152.0 * 4);
+          nrq::launch_vec_p(L, cn->p, cn->r, cn->v, cn->scal, st);
+        }
+        vstreams += 1 + 1 + 8 + 4;
       }
       matvecs += 2;
-      vstreams += 1 + 1 + 8 + 4;
       ++its;
     }
     if ((rc = check_launch(ctx, "cn iteration"))) return rc;
@@ -1807,10 +1887,32 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       ctx->last_error = "CN solve: non-finite residual";
       break;
     }
+    if (just_restarted && gap_pending) {  // the true residual beside the recursive one
+      double gap = 0.0;
+      for (int k = 0; k < nrq::CN_COLS; ++k) {
+        const double *sc = hs + k * nrq::SC_STRIDE;
+        if (sc[nrq::SC_BB] > 0.0) gap = std::max(gap, std::fabs(std::sqrt(sc[nrq::SC_RR] / sc[nrq::SC_BB]) - rec[k]));
+      }
+      cn->gap_rel = std::max(cn->gap_rel, gap);
+      cn->since_confirm = 0;
+      gap_pending = false;
+    }
     if (all) {
       // every column below tolerance: accept once a true residual b - A^H x
-      // (the restart pass) confirms it, otherwise recompute it first
-      if (just_restarted) break;
+      // (the restart pass) confirms it, or at once on the recursive residual
+      // where it meets the tolerance with the measured margin (PETSc's KSP
+      // tests its recursive residual alone); otherwise recompute it first
+      if (just_restarted) {
+        cn->last_true = true;
+        break;
+      }
+      recursive_rel(hs, false, rec);
+      if (accept_recursive(cn, rec)) {
+        cn->last_true = false;
+        ++cn->since_confirm;
+        break;
+      }
+      gap_pending = true;
       restart = true;
       continue;
     }
@@ -1834,9 +1936,11 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   bool conv = true;
   for (int k = 0; k < nrq::CN_COLS; ++k) {
     const double *s = hs + k * nrq::SC_STRIDE;
-    double rel = s[nrq::SC_BB] > 0 ? std::sqrt(s[nrq::SC_RR] / s[nrq::SC_BB]) : 0.0;
+    const bool at_half = half_accept && s[nrq::SC_CONV] == 0.0;  // met the tolerance at the half step
+    const double q = at_half ? s[nrq::SC_SS] : s[nrq::SC_RR];
+    double rel = s[nrq::SC_BB] > 0 ? std::sqrt(q / s[nrq::SC_BB]) : 0.0;
     maxrel = std::max(maxrel, rel);
-    conv = conv && s[nrq::SC_CONV] != 0.0;
+    conv = conv && (s[nrq::SC_CONV] != 0.0 || (at_half && s[nrq::SC_HALF] != 0.0));
   }
   cn->last_iterations = its;
   cn->last_matvecs = matvecs;

@@ -313,6 +313,42 @@ __global__ void __launch_bounds__(384) k_vec_xr_s(int64_t V, double2 *__restrict
     for (int k = 0; k < 3; ++k) partials[((int64_t)blockIdx.x * CN_COLS + w) * 3 + k] = q[k];
 }
 
+// The merged update after t = A^H s (MV_T2 left omega and beta):
+// x += alpha p + omega s ; r = s - omega t ; p = r + beta (p - omega v) ;
+// partials (r.r).  One pass of 5 reads and 3 writes in place of the x, r
+// update (5 reads, rh included, 2 writes) and the p update (3 reads, 1 write).
+__global__ void __launch_bounds__(384) k_vec_xrp(int64_t V, double2 *__restrict__ X, double2 *__restrict__ R,
+                                                 double2 *__restrict__ P, const double2 *__restrict__ S,
+                                                 const double2 *__restrict__ T, const double2 *__restrict__ Vv,
+                                                 const double *__restrict__ scal, double *__restrict__ partials) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t x0 = (int64_t)blockIdx.x * CN_SITES_PER_BLOCK + lane;
+  const int64_t pb = (int64_t)(w * 6) * V;
+  const cplx al = scal_c(scal, w, SC_ALPHA), om = scal_c(scal, w, SC_OMEGA), be = scal_c(scal, w, SC_BETA);
+  double q = 0.0;
+  if (x0 < V) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      const int64_t o = pb + (int64_t)r * V + x0;
+      const cplx s = ldg(S + o), p = ld(P + o);
+      const cplx rn = s - om * ldg(T + o);
+      st(X + o, ld(X + o) + al * p + om * s);
+      st(R + o, rn);
+      st(P + o, rn + be * (p - om * ldg(Vv + o)));
+      q += norm2(rn);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
+  if (lane == 0) partials[(int64_t)blockIdx.x * CN_COLS + w] = q;
+}
+
+void launch_vec_xrp(Lat L, double2 *x, double2 *r, double2 *p, const double2 *s, const double2 *t,
+                    const double2 *v, const double *scal, double *partials, cudaStream_t st) {
+  unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
+  k_vec_xrp<<<nb_, 32 * CN_COLS, 0, st>>>(L.V, x, r, p, s, t, v, scal, partials);
+}
+
 void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st,
                   double *partials) {
   unsigned nb_ = (unsigned)((L.V + CN_SITES_PER_BLOCK - 1) / CN_SITES_PER_BLOCK);
@@ -344,16 +380,16 @@ __device__ __forceinline__ cplx cdiv_safe(cplx a, cplx b) { return cdiv(a, b); }
 __global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restrict__ partials,
                               double *__restrict__ scal, double tol) {
   const int col = blockIdx.x;
-  const int nq = stage == 4 ? 1 : (stage == 0 || stage == 1) ? 2 : 3;
-  __shared__ double sh[3][256];
-  double acc[3] = {0.0, 0.0, 0.0};
+  const int nq = (stage == 4 || stage == 6) ? 1 : stage == 5 ? 5 : (stage == 0 || stage == 1) ? 2 : 3;
+  __shared__ double sh[5][256];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x)
     for (int k = 0; k < nq; ++k) acc[k] += partials[(b * CN_COLS + col) * nq + k];
-  for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = acc[k];
+  for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] = acc[k];
   __syncthreads();
   for (int wd = blockDim.x / 2; wd > 0; wd >>= 1) {
     if (threadIdx.x < wd)
-      for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + wd];
+      for (int k = 0; k < 5; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + wd];
     __syncthreads();
   }
   if (threadIdx.x != 0) return;
@@ -384,6 +420,39 @@ __global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restri
     if (!conv && q2 > 0.0) om = (1.0 / q2) * cplx{q0, q1};
     sc[SC_OMEGA] = om.re;
     sc[SC_OMEGA + 1] = om.im;
+  } else if (stage == 5) {  // omega = (t.s)/(t.t) and beta, ahead of the merged update
+    // rh.s = rh.r - alpha rh.v = 0 by the choice of alpha, so
+    // rho_new = rh.(s - omega t) = -omega rh.t, and beta =
+    // (rho_new / rho)(alpha / omega) = -alpha (rh.t) / rho
+    if (!conv) {
+      cplx om = {0.0, 0.0};
+      if (q2 > 0.0) om = (1.0 / q2) * cplx{q0, q1};
+      const cplx rht = {sh[3][0], sh[4][0]};
+      const cplx rho = {sc[SC_RHO], sc[SC_RHO + 1]};
+      const cplx al = {sc[SC_ALPHA], sc[SC_ALPHA + 1]};
+      cplx be = {0.0, 0.0}, rhon = {0.0, 0.0};
+      if ((om.re == 0.0 && om.im == 0.0) || (rho.re == 0.0 && rho.im == 0.0)) {
+        sc[SC_BREAK] = 1.0;
+      } else {
+        rhon = -(om * rht);
+        be = -cdiv(al * rht, rho);
+      }
+      if (!isfinite(rht.re) || !isfinite(rht.im)) sc[SC_NONFIN] = 1.0;
+      sc[SC_OMEGA] = om.re;
+      sc[SC_OMEGA + 1] = om.im;
+      sc[SC_BETA] = be.re;
+      sc[SC_BETA + 1] = be.im;
+      sc[SC_RHO] = rhon.re;
+      sc[SC_RHO + 1] = rhon.im;
+    } else {
+      sc[SC_OMEGA] = sc[SC_OMEGA + 1] = sc[SC_BETA] = sc[SC_BETA + 1] = 0.0;
+    }
+  } else if (stage == 6) {  // rr = r.r after the merged update
+    if (!conv) {
+      sc[SC_RR] = q0;
+      if (!isfinite(q0)) sc[SC_NONFIN] = 1.0;
+      if (q0 <= tol * tol * sc[SC_BB]) sc[SC_CONV] = 1.0;
+    }
   } else if (stage == 4) {  // half step: |s|^2 against the tolerance
     sc[SC_SS] = q0;
     sc[SC_HALF] = (!conv && q0 <= tol * tol * sc[SC_BB]) ? 1.0 : 0.0;

@@ -407,7 +407,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   __shared__ __align__(8) uint64_t full_bar[kBufs][2], empty_bar[kBufs], dfull[2], dempty[2];
   __shared__ volatile int s_issued;  // loads the producer issued (diagnostics of an expired wait)
   __shared__ uint32_t s_tmem;        // the exchange's tensor-memory columns
-  __shared__ double red[kWarps][3][3];
+  __shared__ double red[kWarps][3][MODE == MV_T2 ? 5 : 3];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int V = (int)L.V;  // the launcher admits V < 2^31 only
@@ -538,10 +538,16 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   // the thread's first spinor plane and block entries (see nb_products)
   const int pofs = 18 * h + 3 * kh, wofs_f = 3 * kh, wofs_b = 18 * kh;
   const int site_in_unit = lane;
-  constexpr int NQ = (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
+  constexpr int NQ = MODE == MV_T2 ? 5 : (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
+  // the first three sums per column in registers; MV_T2's rh.t (4th and
+  // 5th) summed over the warp after every unit into the warp's own slots of
+  // red, which keeps them out of the registers of the stage loop
   double qs[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) qs[k][0] = qs[k][1] = qs[k][2] = 0.0;
+  if (MODE == MV_T2 && lane == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) red[warp][k][3] = red[warp][k][4] = 0.0;
   const cplx ak = C.kin[sp], am = C.mag[sp], ad = C.dar[sp];
   const cplx dg = C.dkin * ak + cplx{1.0, 0.0};
   bool dead = false;
@@ -565,6 +571,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     // the input itself for RHS and T
     const double2 *epi_src = (MODE == MV_V) ? A.in2 : (MODE == MV_RES || MODE == MV_RESC) ? A.bvec : A.in;
     cplx ev[3][3];
+    cplx eh[3][3];  // MV_T2: rh at the own site
 
 #pragma unroll
     for (int stg = 0; stg < kStages; ++stg) {
@@ -680,11 +687,19 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     // ---------------------------------------------------------- epilogue
     // every warp of the pair takes both barriers of the exchange, dead or
     // not, active lanes or not
+    cplx ht[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};  // MV_T2: this unit's rh.t per column
     double res[3][3][2];
     if (kh == 0)
       exchange_halves<0>(acc, res, tbase, warp, pair_bar);
     else
       exchange_halves<1>(acc, res, tbase, warp, pair_bar);
+    // MV_T2: rh at the own site (loaded here, after the accumulators are
+    // released: ahead of the exchange it spills)
+    if (MODE == MV_T2)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) eh[i][k] = ldg(A.in2 + (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + xs);
     if (!dead && act) {
 #pragma unroll
       for (int i = 0; i < 3; ++i)
@@ -720,15 +735,31 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             A.d32[off] = make_float2((float)dv.re, (float)dv.im);
             qs[k][0] += norm2(rv);
             qs[k][1] += norm2(ev_);
-          } else {  // MV_T: in = s
+          } else {  // MV_T, MV_T2: in = s
             st(A.out + off, y_);
             cplx dd = {0.0, 0.0};
             cmac_cj(dd, y_, ev_);
             qs[k][0] += dd.re;
             qs[k][1] += dd.im;
             qs[k][2] += norm2(y_);
+            if (MODE == MV_T2) cmac_cj(ht[k], eh[i][k], y_);
           }
         }
+    }
+    if (MODE == MV_T2) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double re = ht[k].re, im = ht[k].im;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          re += __shfl_xor_sync(0xffffffffu, re, o);
+          im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) {
+          red[warp][k][3] += re;
+          red[warp][k][4] += im;
+        }
+      }
     }
   }
 
@@ -745,7 +776,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int kk = 0; kk < NQ; ++kk) {
+      for (int kk = 0; kk < (NQ < 3 ? NQ : 3); ++kk) {  // MV_T2's 4th and 5th are in red already
         double v = qs[k][kk];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -1184,6 +1215,7 @@ int launch_cn_mv5(int mode, Lat L, const CnCoef &C, double nb_sign, const double
     case MV_RES: go(k_cn_mv5<MV_RES>); break;
     case MV_V: go(k_cn_mv5<MV_V>); break;
     case MV_RESC: go(k_cn_mv5<MV_RESC>); break;
+    case MV_T2: go(k_cn_mv5<MV_T2>); break;
     default: go(k_cn_mv5<MV_T>); break;
   }
   return 0;

@@ -149,6 +149,22 @@ struct nrq_cn {
   // plain form: start from 2b - psi + 2 t1 - t2 with the field's history of
   // corrections (FP32); on by default
   bool history_guess = true;
+  // plain form: confirm every converged solve with the true residual (a
+  // residual pass), or (false, the default) accept the recursive residual
+  // where it meets the tolerance with a margin of four times the largest
+  // recursive-to-true gap measured on this solver's confirmed solves (gap_rel,
+  // relative to ||b||; -1 before the first), confirming again after
+  // kReconfirm unconfirmed solves; last_true: the last update's reported
+  // residual is the true one
+  static constexpr int kReconfirm = 16;
+  bool confirm_always = false;
+  bool last_true = true;
+  double gap_rel = -1.0;
+  int since_confirm = 0;
+  // plain form on the FMA stencil: the x, r and p updates of an iteration in
+  // one pass, beta from the rh.t the t = A^H s launch reduces (false: the
+  // x, r update and the p update as two passes)
+  bool merged_update = true;
   // tensor-core stencil: forward 6x6 blocks (6 per site: direction x
   // species, 36 complex each) built for the coefficients w_coef from the
   // current gauge field (w_valid cleared by every preparation)

@@ -69,11 +69,13 @@ struct CnCoef {
   double inva2[3];   // 1/a_i^2
 };
 
-enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4, MV_RESC = 5 };
+// MV_T2 (FMA stencil only): MV_T on a materialised s that also reduces
+// rh^H t (in2 = rh), from which the merged BiCGStab update takes beta
+enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4, MV_RESC = 5, MV_T2 = 6 };
 
 struct MvArgs {
   const double2 *in;  // operand (PLAIN/RHS: psi, RES: x, V: p, T: r)
-  const double2 *in2; // T: v ; RHS: (unused)
+  const double2 *in2; // T: v ; T2: rh ; RHS: (unused)
   double2 *out;       // PLAIN: A in ; RHS: b ; RES: r ; V: v ; T: t
   double2 *out2;      // RHS: x0 = 2b - psi ; RES: rh
   double2 *out3;      // RES: p
@@ -120,6 +122,8 @@ void launch_vec_p(Lat L, double2 *p, const double2 *r, const double2 *v, const d
 void launch_vec_s(Lat L, double2 *s, const double2 *r, const double2 *v, const double *scal, cudaStream_t st,
                   double *partials = nullptr);
 void launch_vec_xp(Lat L, double2 *x, const double2 *p, const double *scal, cudaStream_t st);
+void launch_vec_xrp(Lat L, double2 *x, double2 *r, double2 *p, const double2 *s, const double2 *t,
+                    const double2 *v, const double *scal, double *partials, cudaStream_t st);
 void launch_vec_xr_s(Lat L, double2 *x, double2 *r, const double2 *p, const double2 *s, const double2 *t,
                      const double2 *rh, const double *scal, double *partials, cudaStream_t st);
 // TMA-staged stencil (cn_mv3.cu); returns nonzero if the tensor maps cannot

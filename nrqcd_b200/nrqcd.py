@@ -103,6 +103,30 @@ def ChebInfo(with_times=False):
     return (int(last.value), ms) if with_times else int(last.value)
 
 
+def SetMergedUpdate(on=True):
+    """Plain form on the FMA stencil: update x, r and p of an iteration in one
+    pass (on=True, the default) or in two (x and r, then p)."""
+    _capi.check(_capi.load().nrq_cn_set_merged_update(solver_handle(), int(bool(on))), lattice.context(),
+                f"Error in {modulename}: merged update")
+
+
+def SetTrueResidual(always=True):
+    """Plain form: confirm every converged solve with the true residual
+    (always=True), or accept the recursive residual where it meets the
+    tolerance with a margin of four times the recursive-to-true gap measured
+    on the solver's confirmed solves (False, the default)."""
+    _capi.check(_capi.load().nrq_cn_set_true_residual(solver_handle(), int(bool(always))), lattice.context(),
+                f"Error in {modulename}: true residual")
+
+
+def LastResidualIsTrue():
+    """Whether the last update's max_rel_residual is the true residual."""
+    v = ctypes.c_int()
+    _capi.check(_capi.load().nrq_cn_true_residual_info(solver_handle(), ctypes.byref(v)), lattice.context(),
+                f"Error in {modulename}: true residual info")
+    return bool(v.value)
+
+
 def SetHistoryGuess(on=True):
     """Plain form: start each solve from the extrapolation 2b - psi plus
     2 t1 - t2 of the field's last two corrections (FP32 history; the
