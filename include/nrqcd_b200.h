@@ -57,7 +57,9 @@ typedef struct {
   int64_t iterations;      /* Krylov iterations of the last update (max over columns) */
   int64_t matvecs;         /* stencil applications (12 columns each)  */
   int64_t vector_streams;  /* 12-column vector passes (read or write)  */
-  double max_rel_residual; /* max over the 12 columns of ||b-Ax||/||b|| (true residual) */
+  double max_rel_residual; /* max over the 12 columns of ||b-Ax||/||b||: the true
+                              residual, or the recursive one where the plain
+                              solve ended on it (nrq_cn_true_residual_info) */
   int converged;           /* 1 when every column reached the tolerance */
   double initial_rel_residual; /* the same maximum for the starting guess
                                   (0 where a batch step did not read it back) */
