@@ -1146,7 +1146,8 @@ namespace {
 // formed.  Derived data a stencil reads instead (the tensor-core stencil's
 // cached blocks) is extra traffic and is not counted.
 double mv_bytes(const nrq_ctx *ctx, int mode) {
-  const int streams[7] = {2, 3, 5, 3, 2, 3, 3};  // PLAIN, RHS, RES, V, T, RESC, T2
+  // PLAIN, RHS, RES, V, T, RESC, T2, RES2, V2 (the FP32 shadow residual half a stream)
+  const double streams[9] = {2, 3, 5, 3, 2, 3, 2.5, 4.5, 2.5};
   return (double)ctx->lat.V * (1152.0 * streams[mode] + 2.0 * (432.0 + 192.0));
 }
 // the tensor-core stencil's backward blocks are -W^H of the forward ones,
@@ -1238,7 +1239,7 @@ int mv(nrq_cn *cn, int mode, const nrq::CnCoef &C, const nrq_gauge *g, const nrq
       return NRQ_OK;
     }
   }
-  if (mode == nrq::MV_T2) {  // the solve asks for it only after an FMA launch
+  if (mode == nrq::MV_T2 || mode == nrq::MV_RES2 || mode == nrq::MV_V2) {  // asked for only after an FMA launch
     ctx->last_error = "cn stencil: the merged update needs the FMA stencil";
     return NRQ_ERR_BAD_ARG;
   }
@@ -1281,7 +1282,7 @@ void fin(nrq_cn *cn, int stage) {
   int64_t rows = cn->nblocks;
   if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TMA) rows = 3 * cn->nblocks;
   if (stage <= 2 && cn->last_stencil == NRQ_STENCIL_TENSOR) rows = nrq::cn_mv4_rows(ctx->lat.V, ctx->sm_count);
-  if ((stage <= 2 || stage == 5) && cn->last_stencil == NRQ_STENCIL_FMA)
+  if ((stage <= 2 || stage == 5 || stage == 7) && cn->last_stencil == NRQ_STENCIL_FMA)
     rows = nrq::cn_mv5_rows(ctx->lat.V, ctx->sm_count);
   ProfScope ps(ctx, 2, (double)rows * 12 * 3 * 8);
   nrq::launch_cn_finalize(stage, rows, cn->partials, cn->scal, cn->tol, ctx->stream);
@@ -1716,6 +1717,12 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     nrq::launch_hist_extrapolate(72 * L.V, cn->x, hist_v1(h), hist_v2(h), st);
     vstreams += 2;
   }
+  // the merged update on the FMA stencil (the right-hand side ran on it)
+  // keeps the shadow residual rh in FP32, in the first half of the rh
+  // buffer: any fixed shadow vector serves BiCGStab, and every product
+  // with it (rho_0 included) uses the same rounded values
+  const bool merged = cn->merged_update && cn->last_stencil == NRQ_STENCIL_FMA;
+  float2 *const sh32 = merged ? reinterpret_cast<float2 *>(cn->rh) : nullptr;
   bool restart = true, just_restarted = false;
   bool half_accept = false;  // ended at a half step on the recursive |s|
   // a restart pass confirming a convergence measures the recursive-to-true
@@ -1739,9 +1746,10 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       a.out = cn->r;
       a.out2 = cn->rh;
       a.out3 = cn->p;
+      a.sh32 = sh32;
       a.partials = cn->partials;
-      if ((rc = mv(cn, nrq::MV_RES, CH, g, a))) return rc;
-      fin(cn, 0);
+      if ((rc = mv(cn, merged ? nrq::MV_RES2 : nrq::MV_RES, CH, g, a))) return rc;
+      fin(cn, merged ? 7 : 0);
       matvecs += 1;
       vstreams += 3;  // b read, rh and p writes
       restart = false;
@@ -1755,10 +1763,11 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       nrq::MvArgs a{};
       a.in = cn->p;
       a.in2 = cn->rh;
+      a.sh32 = sh32;
       a.out = cn->v;
       a.partials = cn->partials;
       a.scal = cn->scal;
-      if ((rc = mv(cn, nrq::MV_V, CH, g, a))) return rc;
+      if ((rc = mv(cn, merged ? nrq::MV_V2 : nrq::MV_V, CH, g, a))) return rc;
       fin(cn, 1);
       const bool tma = mv_t_needs_s(cn, CH);
       // half-step exit: close to the tolerance, |s| = |r - alpha v| is
@@ -1817,8 +1826,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
       b.scal = cn->scal;
       // the merged update: the t launch also reduces rh.t, which gives beta
       // before r is formed, so that x, r and p are updated in one pass
-      const bool merged = tma && cn->merged_update && cn->last_stencil == NRQ_STENCIL_FMA;
-      if (merged) b.in2 = cn->rh;
+      b.sh32 = sh32;
       if ((rc = mv(cn, merged ? nrq::MV_T2 : nrq::MV_T, CH, g, b))) return rc;
       if (merged) {
         fin(cn, 5);

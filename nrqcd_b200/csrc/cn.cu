@@ -380,7 +380,7 @@ __device__ __forceinline__ cplx cdiv_safe(cplx a, cplx b) { return cdiv(a, b); }
 __global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restrict__ partials,
                               double *__restrict__ scal, double tol) {
   const int col = blockIdx.x;
-  const int nq = (stage == 4 || stage == 6) ? 1 : stage == 5 ? 5 : (stage == 0 || stage == 1) ? 2 : 3;
+  const int nq = (stage == 4 || stage == 6) ? 1 : stage == 5 ? 5 : stage == 7 ? 4 : (stage == 0 || stage == 1) ? 2 : 3;
   __shared__ double sh[5][256];
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x)
@@ -396,11 +396,11 @@ __global__ void k_cn_finalize(int stage, int64_t nblocks, const double *__restri
   double *sc = scal + col * SC_STRIDE;
   const double q0 = sh[0][0], q1 = sh[1][0], q2 = sh[2][0];
   const bool conv = sc[SC_CONV] != 0.0;
-  if (stage == 0) {  // rr, bb after a (re)start
+  if (stage == 0 || stage == 7) {  // rr, bb after a (re)start; rho = rh.r (7: FP32 shadow rh)
     sc[SC_RR] = q0;
     sc[SC_BB] = q1;
-    sc[SC_RHO] = q0;
-    sc[SC_RHO + 1] = 0.0;
+    sc[SC_RHO] = stage == 7 ? q2 : q0;
+    sc[SC_RHO + 1] = stage == 7 ? sh[3][0] : 0.0;
     sc[SC_CONV] = (q0 <= tol * tol * q1 || q1 == 0.0) ? 1.0 : 0.0;
     sc[SC_BREAK] = 0.0;
     sc[SC_NONFIN] = (isfinite(q0) && isfinite(q1)) ? 0.0 : 1.0;

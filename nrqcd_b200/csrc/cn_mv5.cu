@@ -398,6 +398,38 @@ __device__ __forceinline__ void exchange_halves(const double (&acc)[6][3][2], do
 
 }  // namespace
 
+// Sum of six doubles over the warp by halving exchanges (8 shuffles where
+// six butterflies take 30): after the exchange across lane bit 4 each half
+// of the warp carries three of the values, across bit 3 two (the third
+// padded), across bit 2 one, then bits 1 and 0 finish the sum.  Lane L ends
+// with value 3 (L >> 4) + 2 ((L >> 3) & 1) + ((L >> 2) & 1) (index 3 of a
+// half is the padding); warp_sum6_slot gives that index, or -1.
+__device__ __forceinline__ double warp_sum6(const double v[6], int lane) {
+  const bool b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1, b2 = (lane >> 2) & 1;
+  double w[4];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const double mine = b4 ? v[j + 3] : v[j], other = b4 ? v[j] : v[j + 3];
+    w[j] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
+  }
+  w[3] = 0.0;
+  double y[2];
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const double mine = b3 ? w[j + 2] : w[j], other = b3 ? w[j] : w[j + 2];
+    y[j] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
+  }
+  double z = (b2 ? y[1] : y[0]) + __shfl_xor_sync(0xffffffffu, b2 ? y[0] : y[1], 4);
+  z += __shfl_xor_sync(0xffffffffu, z, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
+__device__ __forceinline__ int warp_sum6_slot(int lane) {
+  if (lane & 3) return -1;
+  const int idx = 2 * ((lane >> 3) & 1) + ((lane >> 2) & 1);
+  return idx < 3 ? 3 * (lane >> 4) + idx : -1;
+}
+
 template <int MODE>
 __global__ void __maxnreg__(mv5::kMaxReg)
     k_cn_mv5(Lat L, CnCoef C, double nb_sign, const __grid_constant__ Mv5Maps maps, const double2 *__restrict__ W,
@@ -407,7 +439,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   __shared__ __align__(8) uint64_t full_bar[kBufs][2], empty_bar[kBufs], dfull[2], dempty[2];
   __shared__ volatile int s_issued;  // loads the producer issued (diagnostics of an expired wait)
   __shared__ uint32_t s_tmem;        // the exchange's tensor-memory columns
-  __shared__ double red[kWarps][3][MODE == MV_T2 ? 5 : 3];
+  __shared__ double red[kWarps][3][MODE == MV_T2 ? 5 : MODE == MV_RES2 ? 4 : 3];
   unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int V = (int)L.V;  // the launcher admits V < 2^31 only
@@ -538,16 +570,24 @@ __global__ void __maxnreg__(mv5::kMaxReg)
   // the thread's first spinor plane and block entries (see nb_products)
   const int pofs = 18 * h + 3 * kh, wofs_f = 3 * kh, wofs_b = 18 * kh;
   const int site_in_unit = lane;
-  constexpr int NQ = MODE == MV_T2 ? 5 : (MODE == MV_T) ? 3 : ((MODE == MV_RES || MODE == MV_V || MODE == MV_RESC) ? 2 : 0);
-  // the first three sums per column in registers; MV_T2's rh.t (4th and
-  // 5th) summed over the warp after every unit into the warp's own slots of
-  // red, which keeps them out of the registers of the stage loop
+  constexpr int NQ = MODE == MV_T2 ? 5 : MODE == MV_RES2 ? 4 : (MODE == MV_T) ? 3
+                   : ((MODE == MV_RES || MODE == MV_V || MODE == MV_V2 || MODE == MV_RESC) ? 2 : 0);
+  // the products with the FP32 shadow residual (MV_T2: rh.t, MV_RES2:
+  // rh.r) are summed over the warp after every unit into the warp's own
+  // slots XQ, XQ + 1 of red, which keeps them out of the registers of the
+  // stage loop; the other sums (NR per column) stay in registers
+  constexpr int XQ = MODE == MV_T2 ? 3 : MODE == MV_RES2 ? 2 : -1;
+  constexpr int NR = XQ >= 0 ? XQ : NQ;
+  constexpr bool kShadow = MODE == MV_T2 || MODE == MV_V2;  // reads sh32
   double qs[3][3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) qs[k][0] = qs[k][1] = qs[k][2] = 0.0;
-  if (MODE == MV_T2 && lane == 0)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) red[warp][k][3] = red[warp][k][4] = 0.0;
+  // the lane that ends with value j of the per-unit sums (re and im of the
+  // three columns) owns its slot of red, which it clears here
+  if (XQ >= 0 && warp_sum6_slot(lane) >= 0) {
+    const int j = warp_sum6_slot(lane);
+    red[warp][j >> 1][XQ + (j & 1)] = 0.0;
+  }
   const cplx ak = C.kin[sp], am = C.mag[sp], ad = C.dar[sp];
   const cplx dg = C.dkin * ak + cplx{1.0, 0.0};
   bool dead = false;
@@ -568,21 +608,26 @@ __global__ void __maxnreg__(mv5::kMaxReg)
 #pragma unroll
       for (int k = 0; k < 3; ++k) acc[r][k][0] = acc[r][k][1] = 0.0;
     // the epilogue's operand at the own site: b for the residuals, rh for V,
-    // the input itself for RHS and T
-    const double2 *epi_src = (MODE == MV_V) ? A.in2 : (MODE == MV_RES || MODE == MV_RESC) ? A.bvec : A.in;
+    // the input itself for RHS and T; the FP32 shadow residual for V2, T2
+    const double2 *epi_src =
+        (MODE == MV_V) ? A.in2 : (MODE == MV_RES || MODE == MV_RES2 || MODE == MV_RESC) ? A.bvec : A.in;
     cplx ev[3][3];
-    cplx eh[3][3];  // MV_T2: rh at the own site
+    float2 eh[3][3];
 
 #pragma unroll
     for (int stg = 0; stg < kStages; ++stg) {
       const int ld = u * kLoads + stg * 2 + sp;
       const int b = ld % kBufs;
       if (stg == kStages - 2 && MODE != MV_PLAIN) {
-        // the epilogue's operand, loaded into registers two stages ahead
+        // the epilogue's operands, loaded into registers two stages ahead
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int k = 0; k < 3; ++k) ev[i][k] = ldg(epi_src + (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + xs);
+          for (int k = 0; k < 3; ++k) {
+            const int64_t o = (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + xs;
+            if (MODE != MV_V2) ev[i][k] = ldg(epi_src + o);
+            if (kShadow) eh[i][k] = __ldg(A.sh32 + o);
+          }
       }
       int role = -1;
       if (!dead && !wait(&full_bar[b][sp], (uint32_t)((ld / kPer) & 1))) role = 0;
@@ -687,19 +732,12 @@ __global__ void __maxnreg__(mv5::kMaxReg)
     // ---------------------------------------------------------- epilogue
     // every warp of the pair takes both barriers of the exchange, dead or
     // not, active lanes or not
-    cplx ht[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};  // MV_T2: this unit's rh.t per column
+    cplx ht[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};  // this unit's product with the shadow, per column
     double res[3][3][2];
     if (kh == 0)
       exchange_halves<0>(acc, res, tbase, warp, pair_bar);
     else
       exchange_halves<1>(acc, res, tbase, warp, pair_bar);
-    // MV_T2: rh at the own site (loaded here, after the accumulators are
-    // released: ahead of the exchange it spills)
-    if (MODE == MV_T2)
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int k = 0; k < 3; ++k) eh[i][k] = ldg(A.in2 + (int64_t)(sp * 36 + (3 * h + k) * 6 + 3 * kh + i) * V + xs);
     if (!dead && act) {
 #pragma unroll
       for (int i = 0; i < 3; ++i)
@@ -722,10 +760,25 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             st(A.out3 + off, rv);
             qs[k][0] += norm2(rv);
             qs[k][1] += norm2(ev_);
+          } else if (MODE == MV_RES2) {
+            const cplx rv = ev_ - y_;
+            const float2 f = make_float2((float)rv.re, (float)rv.im);
+            st(A.out + off, rv);
+            A.sh32[off] = f;
+            st(A.out3 + off, rv);
+            qs[k][0] += norm2(rv);
+            qs[k][1] += norm2(ev_);
+            cmac_cj(ht[k], cplx{(double)f.x, (double)f.y}, rv);
           } else if (MODE == MV_V) {
             st(A.out + off, y_);
             cplx dd = {0.0, 0.0};
             cmac_cj(dd, ev_, y_);
+            qs[k][0] += dd.re;
+            qs[k][1] += dd.im;
+          } else if (MODE == MV_V2) {
+            st(A.out + off, y_);
+            cplx dd = {0.0, 0.0};
+            cmac_cj(dd, cplx{(double)eh[i][k].x, (double)eh[i][k].y}, y_);
             qs[k][0] += dd.re;
             qs[k][1] += dd.im;
           } else if (MODE == MV_RESC) {
@@ -742,24 +795,15 @@ __global__ void __maxnreg__(mv5::kMaxReg)
             qs[k][0] += dd.re;
             qs[k][1] += dd.im;
             qs[k][2] += norm2(y_);
-            if (MODE == MV_T2) cmac_cj(ht[k], eh[i][k], y_);
+            if (MODE == MV_T2) cmac_cj(ht[k], cplx{(double)eh[i][k].x, (double)eh[i][k].y}, y_);
           }
         }
     }
-    if (MODE == MV_T2) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        double re = ht[k].re, im = ht[k].im;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          re += __shfl_xor_sync(0xffffffffu, re, o);
-          im += __shfl_xor_sync(0xffffffffu, im, o);
-        }
-        if (lane == 0) {
-          red[warp][k][3] += re;
-          red[warp][k][4] += im;
-        }
-      }
+    if (XQ >= 0) {
+      const double hv[6] = {ht[0].re, ht[0].im, ht[1].re, ht[1].im, ht[2].re, ht[2].im};
+      const double z = warp_sum6(hv, lane);
+      const int j = warp_sum6_slot(lane);  // recomputed: a register held across the stages spills
+      if (j >= 0) red[warp][j >> 1][XQ + (j & 1)] += z;
     }
   }
 
@@ -776,7 +820,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
-      for (int kk = 0; kk < (NQ < 3 ? NQ : 3); ++kk) {  // MV_T2's 4th and 5th are in red already
+      for (int kk = 0; kk < NR; ++kk) {  // the shadow products are in red already
         double v = qs[k][kk];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -1216,6 +1260,8 @@ int launch_cn_mv5(int mode, Lat L, const CnCoef &C, double nb_sign, const double
     case MV_V: go(k_cn_mv5<MV_V>); break;
     case MV_RESC: go(k_cn_mv5<MV_RESC>); break;
     case MV_T2: go(k_cn_mv5<MV_T2>); break;
+    case MV_RES2: go(k_cn_mv5<MV_RES2>); break;
+    case MV_V2: go(k_cn_mv5<MV_V2>); break;
     default: go(k_cn_mv5<MV_T>); break;
   }
   return 0;

@@ -69,13 +69,19 @@ struct CnCoef {
   double inva2[3];   // 1/a_i^2
 };
 
-// MV_T2 (FMA stencil only): MV_T on a materialised s that also reduces
-// rh^H t (in2 = rh), from which the merged BiCGStab update takes beta
-enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4, MV_RESC = 5, MV_T2 = 6 };
+// FMA stencil only, the plain solve with the merged update and the shadow
+// residual rh kept in FP32 (sh32; any fixed shadow vector serves BiCGStab,
+// and every product with it uses the same rounded values):
+//   MV_RES2: MV_RES writing rh = f32(r) to sh32 and reducing rh^H r (rho_0);
+//   MV_V2:   MV_V with rh^H v from sh32;
+//   MV_T2:   MV_T on a materialised s that also reduces rh^H t from sh32,
+//            from which the merged update takes beta
+enum MvMode { MV_PLAIN = 0, MV_RHS = 1, MV_RES = 2, MV_V = 3, MV_T = 4, MV_RESC = 5, MV_T2 = 6, MV_RES2 = 7,
+              MV_V2 = 8 };
 
 struct MvArgs {
   const double2 *in;  // operand (PLAIN/RHS: psi, RES: x, V: p, T: r)
-  const double2 *in2; // T: v ; T2: rh ; RHS: (unused)
+  const double2 *in2; // T: v ; RHS: (unused)
   double2 *out;       // PLAIN: A in ; RHS: b ; RES: r ; V: v ; T: t
   double2 *out2;      // RHS: x0 = 2b - psi ; RES: rh
   double2 *out3;      // RES: p
@@ -87,6 +93,7 @@ struct MvArgs {
   float2 *r32;
   float2 *d32;
   cplx inv_theta[2];
+  float2 *sh32;       // RES2: FP32 shadow residual written; V2, T2: read
 };
 
 // per-species coefficients of one Chebyshev step: d' = c1 d + c2 r
