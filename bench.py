@@ -85,6 +85,8 @@ def parse():
     p.add_argument("--stencil", default="timed", choices=["timed", "register", "tma", "tensor", "fma"],
                    help="FP64 stencil of the headline step (default: the solver's timed choice)")
     p.add_argument("--only-drift", action="store_true", help="print only the precision-drift JSON")
+    p.add_argument("--two-pass", action="store_true",
+                   help="headline step: the two-pass BiCGStab update in place of the merged one")
     return p.parse_args()
 
 
@@ -925,6 +927,8 @@ def main():
     if args.stencil != "timed":
         nrqcd.SetStencil({"register": nrqcd.STENCIL_REGISTER, "tma": nrqcd.STENCIL_TMA,
                           "tensor": nrqcd.STENCIL_TENSOR, "fma": nrqcd.STENCIL_FMA}[args.stencil])
+    if args.two_pass:
+        nrqcd.SetMergedUpdate(False)
     g = GaugeConfiguration()
     g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=member_seed(rank), identity_links=True)
     h = NRQCDField()
@@ -1088,7 +1092,8 @@ def main():
             "metric": METRIC, "value": value, "unit": "site-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(L, world),
+            "config": dict(workload_config(L, world),
+                           bicgstab_update="two-pass" if args.two_pass else "merged"),
             "roofline": {"bound": "hbm", "kernel": "CN 12-column stencil: " + stencil["in_use"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
