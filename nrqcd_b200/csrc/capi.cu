@@ -1354,12 +1354,17 @@ int tune_stencil(nrq_cn *cn, const nrq::CnCoef &CH, const nrq_gauge *g) {
   for (int which : {NRQ_STENCIL_TENSOR, NRQ_STENCIL_FMA}) {
     if (rc || cn->tune_ms[which] <= 0.0) continue;
     double sign = 0.0;
+    // a first, untimed build allocates the block sets (once per solver);
+    // the timed one is the rebuild every update makes
+    rc = which == NRQ_STENCIL_TENSOR ? ensure_blocks(cn, CH, g, &sign) : ensure_blocks5(cn, CH, g, &sign);
+    if (rc) continue;
     cudaEventRecord(e0, st);
     if (which == NRQ_STENCIL_TENSOR) {
       cn->w_valid = false;
       rc = ensure_blocks(cn, CH, g, &sign);
     } else {
       cn->w5_valid = false;
+      cn->w5f_valid = false;
       rc = ensure_blocks5(cn, CH, g, &sign);
     }
     cudaEventRecord(e1, st);
