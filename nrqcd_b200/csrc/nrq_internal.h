@@ -161,6 +161,12 @@ struct nrq_cn {
   bool last_true = true;
   double gap_rel = -1.0;
   int since_confirm = 0;
+  // precision forms: the largest ratio of the true residual to the
+  // Chebyshev prediction (previous residual / the pass's guaranteed gain)
+  // measured on confirmed passes (-1 before the first), and the updates
+  // accepted on the prediction since the last confirmation
+  double cheb_ratio = -1.0;
+  int cheb_unconfirmed = 0;
   // plain form on the FMA stencil: the x, r and p updates of an iteration in
   // one pass, beta from the rh.t the t = A^H s launch reduces (false: the
   // x, r update and the p update as two passes)

@@ -194,3 +194,44 @@ def test_chebyshev_step_timed_choice():
         assert h.Update(g, 1.0, [1, 1, 1, 1], 1.0)["converged"] == 1
         last, ms = nrqcd.ChebInfo(with_times=True)
     assert (ms > 0).all() and last == int(np.argmin(ms))
+
+
+@pytest.mark.parametrize("tol", [1e-10, 1e-12])
+def test_precision_form_prediction_acceptance(oracle, tol):
+    """The precision form ends an update on the Chebyshev prediction of its
+    last pass (previous residual over the pass's guaranteed gain, scaled by
+    the true-to-predicted ratio its confirmed passes measured) where that
+    meets the tolerance: the true residual of every update, recomputed by the
+    oracle from the downloaded fields, is within the tolerance, some updates
+    end on the prediction, and the always-confirm mode agrees with it."""
+    from nrqcd_b200 import nrqcd
+    from tests.test_gpu_cn import _true_rel_residuals
+    n = (16, 16, 16)
+    M, c = 1.0, np.array([1, 1, 1, 1], dtype=complex)
+    runs = {}
+    for always in (False, True):
+        with lattice_ctx(n, A, cn=(M, list(c), 1.0, tol, 10000, FORM_PRECISION)):
+            nrqcd.SetTrueResidual(always)
+            links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 4, identity_links=False)
+            g = GaugeConfiguration()
+            g.upload(links, ef)
+            h = NRQCDField()
+            h.InitSinglePoint(1, 1)
+            predicted, mv = 0, 0
+            for _ in range(6):
+                old = h.download()
+                gl, ge = g.download()
+                st = h.Update(g, M, list(c), 1.0)
+                assert st["converged"] == 1 and st["max_rel_residual"] <= tol
+                if not nrqcd.LastResidualIsTrue():
+                    predicted += 1
+                assert _true_rel_residuals(oracle, n, gl, ge, M, c, old, h.download()) <= tol
+                mv += st["matvecs"]
+                g.Update(1.0)
+            q, a = h.download()
+            del g, h
+        runs[always] = (q, a, predicted, mv)
+    assert runs[True][2] == 0
+    assert runs[False][2] > 0 and runs[False][3] < runs[True][3]
+    assert np.abs(runs[True][0] - runs[False][0]).max() < 50 * tol
+    assert np.abs(runs[True][1] - runs[False][1]).max() < 50 * tol
