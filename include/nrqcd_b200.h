@@ -241,15 +241,19 @@ int nrq_cn_cheb_info(const nrq_cn *cn, int *last, double ms[2]);
  * its start: its refinement passes are set by the FP32 gain per pass, and
  * the smaller start did not remove one at 64^3 or 96^3.)                  */
 int nrq_cn_set_history_guess(nrq_cn *cn, int on);
-/* Plain form (form 0): the solve's acceptance.  always = 1 confirms every
- * converged solve with the true residual b - A^H x (one residual pass); 0
- * (the default) accepts BiCGStab's recursive residual, as PETSc's KSP
- * (src/nrqcd.f90:803) tests its recursive residual, where every column's
- * meets the tolerance with a margin of four times the largest gap between
- * recursive and true residual that this solver's confirmed solves showed;
+/* The solve's acceptance.  always = 1 confirms every converged solve with
+ * the true residual b - A^H x (one residual pass); 0 (the default) accepts,
+ * as PETSc's KSP (src/nrqcd.f90:803) tests its recursive residual:
+ *  - plain form: BiCGStab's recursive residual, where every column's meets
+ *    the tolerance with a margin of four times the largest gap between
+ *    recursive and true residual that this solver's confirmed solves showed;
+ *  - precision forms: the Chebyshev prediction of the last pass (the
+ *    previous residual over the pass's guaranteed gain), where twice it,
+ *    scaled by the largest true-to-predicted ratio of this solver's
+ *    confirmed passes, meets the tolerance;
  * the first solve and every 16th after an unconfirmed run confirm.
  * nrq_cn_true_residual_info: whether the last update's max_rel_residual is
- * the true residual (1) or the recursive one (0).                         */
+ * the true residual (1) or the recursive or predicted one (0).            */
 /* Plain form on the FMA stencil: on = 1 (the default) updates x, r and p of
  * an iteration in one pass, beta taken from rh.t, which the t = A^H s launch
  * reduces (rh.s vanishes by the choice of alpha, so rho_new = -omega rh.t);

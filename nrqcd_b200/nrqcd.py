@@ -111,10 +111,10 @@ def SetMergedUpdate(on=True):
 
 
 def SetTrueResidual(always=True):
-    """Plain form: confirm every converged solve with the true residual
-    (always=True), or accept the recursive residual where it meets the
-    tolerance with a margin of four times the recursive-to-true gap measured
-    on the solver's confirmed solves (False, the default)."""
+    """Confirm every converged solve with the true residual (always=True), or
+    (False, the default) accept the plain form's recursive residual, or the
+    precision forms' Chebyshev prediction, where it meets the tolerance with
+    a margin measured on the solver's confirmed solves."""
     _capi.check(_capi.load().nrq_cn_set_true_residual(solver_handle(), int(bool(always))), lattice.context(),
                 f"Error in {modulename}: true residual")
 
