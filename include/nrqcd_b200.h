@@ -346,6 +346,16 @@ int nrq_cn_batch_fp64_info(const nrq_cn_batch *batch, int *which, double ms[2]);
  * off; guess_ms, saving_ms: the measured cost and the value of the saving
  * (-1 before).                                                             */
 int nrq_cn_batch_learned_info(const nrq_cn_batch *batch, int *gate, double *guess_ms, double *saving_ms);
+/* The scheduled steps' predicted acceptance (no reference counterpart):
+ * after the last pass each unconverged column's residual is predicted from
+ * its residual before the pass and the pass's guaranteed Chebyshev gain;
+ * where twice the prediction, scaled by the largest true-to-predicted
+ * ratio the measured columns showed, meets the tolerance, the column is
+ * accepted on it and the final residual check skips the fields accepted in
+ * full (the first scheduled step and every 16th predict nothing).  ratio:
+ * that largest ratio (-1 before the first measurement); steps: scheduled
+ * steps taken.  Synchronises the batch's stream.                          */
+int nrq_cn_batch_prediction_info(const nrq_cn_batch *batch, double *ratio, int64_t *steps);
 int nrq_cn_batch_set_fp64(nrq_cn_batch *batch, int which);
 
 /* An ensemble of independent members (batch[i], gauge[i]); the members may

@@ -111,6 +111,15 @@ class CNBatch:
         names = {-2: "none", -1: "undecided", 0: "off", 1: "on"}
         return {"gate": names[gate.value], "guess_ms": cost.value, "saving_ms": saving.value}
 
+    def prediction_info(self) -> dict:
+        """The scheduled steps' predicted acceptance: the largest measured
+        ratio of true to predicted residual (-1 before the first) and the
+        scheduled steps taken."""
+        ratio, steps = ctypes.c_double(), ctypes.c_int64()
+        _capi.check(_capi.load().nrq_cn_batch_prediction_info(self._h, ctypes.byref(ratio), ctypes.byref(steps)),
+                    self._ctx, "prediction info")
+        return {"ratio": ratio.value, "steps": steps.value}
+
     def _fp64_info(self) -> dict:
         which = ctypes.c_int()
         ms = np.zeros(2)

@@ -51,6 +51,9 @@ struct nrq_cn_batch {
   double2 *b_all = nullptr;
   float2 *r32_all = nullptr, *dA_all = nullptr, *dB_all = nullptr, *e32_all = nullptr;
   double *part_all = nullptr, *scal_all = nullptr;
+  // the scheduled steps' predicted acceptance: {largest true-to-predicted
+  // ratio measured (-1: none), scheduled steps taken} (device)
+  double *pstate = nullptr;
   int *flags = nullptr;
   int64_t nsb = 0;  // 32-site blocks
   // device table and pinned mirrors
@@ -277,7 +280,7 @@ int enq_residual(nrq_cn_batch *b, cudaStream_t st, bool first) {
   }
   {
     ProfScope ps(ctx, 2, (double)b->nf * b->nsb * nrq::CN_COLS * 2 * 8);
-    nrq::launch_batch_finalize(b->d_tab, b->nf, b->nsb, b->tol, st);
+    nrq::launch_batch_finalize(b->d_tab, b->nf, b->nsb, b->tol, first ? 0 : 1, st);
   }
   return check_launch(ctx, "batch residual");
 }
@@ -322,7 +325,10 @@ int enq_readback(nrq_cn_batch *b, cudaStream_t st) {
 }
 
 // the scheduled step: prepare, RHS, the scheduled passes, the final residual
-// check and its read-back
+// check and its read-back.  After the last pass its Chebyshev prediction
+// marks the columns it brings within the tolerance (with the measured
+// margin) as converged, so that the final check skips the fields it
+// predicts in full; the check's measured columns then calibrate the margin.
 int enq_scheduled(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double dt, cudaStream_t st) {
   int rc = enq_prepare(b, g, c, dt, st);
   if (!rc) rc = enq_rhs(b, g, st);
@@ -330,7 +336,13 @@ int enq_scheduled(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double
     rc = enq_residual(b, st, p == 0);
     if (!rc) rc = enq_inner(b, b->schedule[p], st);
   }
+  const bool predict = !b->schedule.empty();
+  if (!rc && predict) nrq::launch_batch_predict(b->d_tab, b->nf, b->schedule.back(), b->tol, b->pstate, st);
   if (!rc) rc = enq_residual(b, st, b->schedule.empty());
+  if (!rc && predict) {
+    nrq::launch_batch_calibrate(b->d_tab, b->nf, b->pstate, st);
+    rc = check_launch(b->ctx, "batch prediction");
+  }
   if (!rc) rc = enq_readback(b, st);
   return rc;
 }
@@ -696,6 +708,7 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
   NRQ_B_ALLOC(b->e32_all, sizeof(float2) * P * nfields);
   NRQ_B_ALLOC(b->part_all, sizeof(double) * b->nsb * nrq::CN_COLS * 2 * nfields);
   NRQ_B_ALLOC(b->scal_all, sizeof(double) * kFieldScal * nfields);
+  NRQ_B_ALLOC(b->pstate, sizeof(double) * 2);
   NRQ_B_ALLOC(b->flags, sizeof(int) * nfields);
   NRQ_B_ALLOC(b->d_tab, sizeof(nrq::BatchField) * nfields);
   NRQ_B_ALLOC(b->err, sizeof(int) * 16);
@@ -722,6 +735,10 @@ extern "C" int nrq_cn_batch_create(nrq_ctx *ctx, int nfields, nrq_heavy *const *
     if ((e = cudaMemsetAsync(p, 0, sizeof(float2) * P * nfields, ctx->stream)) != cudaSuccess) return fail(e);
   if ((e = cudaMemsetAsync(b->scal_all, 0, sizeof(double) * kFieldScal * nfields, ctx->stream)) != cudaSuccess)
     return fail(e);
+  {
+    const double p0[2] = {-1.0, 0.0};  // no ratio measured, no scheduled step taken
+    if ((e = cudaMemcpy(b->pstate, p0, sizeof(p0), cudaMemcpyHostToDevice)) != cudaSuccess) return fail(e);
+  }
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e);
   *out = b;
   return NRQ_OK;
@@ -736,7 +753,8 @@ extern "C" int nrq_cn_batch_destroy(nrq_cn_batch *b) {
                   (void *)b->D32, (void *)b->B32, (void *)b->bpart, (void *)b->bounds, (void *)b->b_all,
                   (void *)b->r32_all, (void *)b->dA_all, (void *)b->dB_all, (void *)b->e32_all, (void *)b->part_all,
                   (void *)b->scal_all, (void *)b->flags, (void *)b->d_tab, (void *)b->lgf, (void *)b->lfeat,
-                  (void *)b->lomega, (void *)b->W5f, (void *)b->err, (void *)b->W5, (void *)b->d_fmaps})
+                  (void *)b->lomega, (void *)b->W5f, (void *)b->err, (void *)b->W5, (void *)b->d_fmaps,
+                  (void *)b->pstate})
     if (p) cudaFree(p);
   for (double2 *p : b->xbuf)
     if (p) cudaFree(p);
@@ -878,6 +896,18 @@ extern "C" int nrq_cn_batch_learned_info(const nrq_cn_batch *b, int *gate, doubl
   if (gate) *gate = b->learn ? b->learn_gate : -2;
   if (guess_ms) *guess_ms = b->guess_ms;
   if (saving_ms) *saving_ms = b->guess_saving_ms;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_batch_prediction_info(const nrq_cn_batch *b, double *ratio, int64_t *steps) {
+  if (!b) return NRQ_ERR_BAD_ARG;
+  int rc = set_device(b->ctx);
+  if (rc) return rc;
+  double p[2] = {-1.0, 0.0};
+  NRQ_CUDA_TRY(b->ctx, cudaMemcpyAsync(p, b->pstate, sizeof(p), cudaMemcpyDeviceToHost, b->ctx->stream));
+  NRQ_CUDA_TRY(b->ctx, cudaStreamSynchronize(b->ctx->stream));
+  if (ratio) *ratio = p[0];
+  if (steps) *steps = (int64_t)p[1];
   return NRQ_OK;
 }
 

@@ -511,7 +511,12 @@ __global__ void k_batch_coef(BatchField *__restrict__ tab, int nfields, int *__r
     const cplx sigma = cdiv(theta, delta);
     f.inv_theta[sp] = cdiv(one, theta);
     cplx rho = cdiv(one, sigma);
+    // rho_k = T_k(sigma) / T_{k+1}(sigma), so m steps gain 1/|rho_0 ... rho_{m-1}|
+    cplx prod = one;
+    f.gain[sp][0] = 1.0;
     for (int k = 0; k < BATCH_MAX_CHEB; ++k) {
+      prod = prod * rho;
+      f.gain[sp][k + 1] = 1.0 / sqrt(norm2(prod));
       const cplx rn = cdiv(one, 2.0 * sigma - rho);
       f.cheb[k].c1[sp] = rn * rho;
       f.cheb[k].c2[sp] = cdiv(2.0 * rn, delta);
@@ -526,9 +531,13 @@ void launch_batch_coef(BatchField *tab, int nfields, int *flags, cudaStream_t st
 
 // (r.r, b.b) of every column of every field from the residual stencil's
 // partial rows; sets the convergence and non-finite flags of each column.
-__global__ void k_batch_finalize(const BatchField *__restrict__ tab, int64_t nrows, double tol) {
+__global__ void k_batch_finalize(const BatchField *__restrict__ tab, int64_t nrows, double tol, int skip_done) {
   const int col = blockIdx.x;
   const BatchField &f = tab[blockIdx.y];
+  // a field the residual launch skipped keeps its scalars (another column's
+  // block may mark its column converged meanwhile: then this column had
+  // converged before, and keeps its scalars too)
+  if (skip_done && batch_field_done(f)) return;
   __shared__ double sh[2][256];
   double acc[2] = {0.0, 0.0};
   for (int64_t b = threadIdx.x; b < nrows; b += blockDim.x)
@@ -548,8 +557,64 @@ __global__ void k_batch_finalize(const BatchField *__restrict__ tab, int64_t nro
   sc[SC_CONV] = (q0 <= tol * tol * q1 || q1 == 0.0) ? 1.0 : 0.0;
   sc[SC_NONFIN] = (isfinite(q0) && isfinite(q1)) ? 0.0 : 1.0;
 }
-void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, double tol, cudaStream_t st) {
-  k_batch_finalize<<<dim3(CN_COLS, (unsigned)nfields), 256, 0, st>>>(tab, nrows, tol);
+void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, double tol, int skip_done,
+                           cudaStream_t st) {
+  k_batch_finalize<<<dim3(CN_COLS, (unsigned)nfields), 256, 0, st>>>(tab, nrows, tol, skip_done);
+}
+
+__global__ void k_batch_predict(const BatchField *__restrict__ tab, int nfields, int m, double tol,
+                                const double *__restrict__ pstate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nfields * CN_COLS) return;
+  const BatchField &f = tab[i / CN_COLS];
+  const int col = i % CN_COLS;
+  double *sc = f.scal + col * SC_STRIDE;
+  sc[SC_HALF] = 0.0;
+  if (sc[SC_CONV] != 0.0 || !(sc[SC_BB] > 0.0)) return;
+  const double ratio = pstate[0];
+  const bool on = ratio >= 0.0 && fmod(pstate[1], 16.0) != 0.0;
+  const double pred = sqrt(sc[SC_RR] / sc[SC_BB]) / f.gain[col / 6][m];
+  const double scale = fmax(1.0, ratio);
+  sc[SC_SS] = pred;
+  if (on && 2.0 * scale * pred <= tol) {
+    sc[SC_CONV] = 1.0;
+    sc[SC_HALF] = 1.0;
+    sc[SC_RR] = (scale * pred) * (scale * pred) * sc[SC_BB];
+  } else {
+    sc[SC_HALF] = 2.0;
+  }
+}
+void launch_batch_predict(const BatchField *tab, int nfields, int m, double tol, const double *pstate,
+                          cudaStream_t st) {
+  const int n = nfields * CN_COLS;
+  m = m < 0 ? 0 : (m > BATCH_MAX_CHEB ? BATCH_MAX_CHEB : m);
+  k_batch_predict<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(tab, nfields, m, tol, pstate);
+}
+
+// one block: the largest true-to-predicted ratio of the columns the
+// residual check measured (SC_HALF = 2) into pstate[0]; pstate[1] += 1
+__global__ void k_batch_calibrate(const BatchField *__restrict__ tab, int nfields, double *__restrict__ pstate) {
+  __shared__ double sh[256];
+  double mx = -1.0;
+  for (int i = threadIdx.x; i < nfields * CN_COLS; i += blockDim.x) {
+    double *sc = tab[i / CN_COLS].scal + (i % CN_COLS) * SC_STRIDE;
+    if (sc[SC_HALF] == 2.0 && sc[SC_BB] > 0.0 && sc[SC_SS] > 0.0)
+      mx = fmax(mx, sqrt(sc[SC_RR] / sc[SC_BB]) / sc[SC_SS]);
+    sc[SC_HALF] = 0.0;
+  }
+  sh[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (sh[0] >= 0.0) pstate[0] = fmax(pstate[0], sh[0]);
+    pstate[1] += 1.0;
+  }
+}
+void launch_batch_calibrate(const BatchField *tab, int nfields, double *pstate, cudaStream_t st) {
+  k_batch_calibrate<<<1, 256, 0, st>>>(tab, nfields, pstate);
 }
 
 // ------------------------------------------------------------ propagator I/O, norms, correlators

@@ -185,6 +185,9 @@ struct BatchField {
   float2 *hnew;
   cplx inv_theta[2];             // 1/theta per species (written on the device)
   ChebCoef cheb[BATCH_MAX_CHEB]; // Chebyshev steps (written on the device)
+  // guaranteed gain |T_m(sigma)| of m Chebyshev steps per species (written
+  // on the device)
+  double gain[2][BATCH_MAX_CHEB + 1];
 };
 // every column of the field converged at its last residual check
 __device__ __forceinline__ bool batch_field_done(const BatchField &f) {
@@ -237,7 +240,23 @@ void launch_batch_add_e(int64_t n, const BatchField *tab, int nfields, cudaStrea
 // flags[f] = 1 for non-finite bounds
 void launch_batch_coef(BatchField *tab, int nfields, int *flags, cudaStream_t st);
 // stage-0 reduction of every field's residual partials (nrows rows per field)
-void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, double tol, cudaStream_t st);
+// skip_done: the residual launch skipped the fields whose every column had
+// converged (their scalars stay as they are)
+void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, double tol, int skip_done,
+                           cudaStream_t st);
+// The prediction of the scheduled step's last pass (m Chebyshev steps):
+// every unconverged column's residual before the pass over the pass's
+// guaranteed gain.  pstate = {ratio, steps}: the largest true-to-predicted
+// ratio measured so far (-1: none) and the scheduled steps taken.  Where
+// prediction is on (a ratio measured and steps not a multiple of 16) and
+// twice the prediction, scaled by max(1, ratio), meets tol, the column is
+// marked converged on it (SC_HALF = 1, SC_RR the scaled prediction);
+// otherwise it waits for the residual check (SC_HALF = 2, SC_SS the
+// prediction).  launch_batch_calibrate, after that check, takes the ratio
+// of the measured columns into pstate and counts the step.
+void launch_batch_predict(const BatchField *tab, int nfields, int m, double tol, const double *pstate,
+                          cudaStream_t st);
+void launch_batch_calibrate(const BatchField *tab, int nfields, double *pstate, cudaStream_t st);
 void launch_cn_to_f32(int64_t V, const double2 *U, const double2 *DE, const double2 *D, const double *B, float2 *U32,
                       float2 *DE32, float2 *D32, float *B32, cudaStream_t st);
 void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, const double2 *Dsum, const double *Bsum,

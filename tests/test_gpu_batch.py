@@ -84,6 +84,36 @@ def test_batch_matches_single_field_updates(oracle):
         b.Destructor()
 
 
+def test_batch_predicted_acceptance_true_residuals(oracle):
+    """The scheduled steps accept columns on the Chebyshev prediction of the
+    last pass (with the margin the measured columns calibrate): over graph
+    replays on an evolving 16^3 gauge field, the true residual of every
+    field, recomputed by the oracle from the downloaded fields, stays within
+    the tolerance, and the margin has been measured."""
+    from tests.test_gpu_cn import _true_rel_residuals
+    n = (16, 16, 16)
+    V = int(np.prod(n))
+    masses = [1.0, 1.5]
+    srcs = _sources(V, 2, 5)
+    tol = 1e-10
+    with lattice_ctx(n, A, cn=(masses[0], C, 1.0, tol, 10000, FORM_PRECISION)):
+        g, _, _ = _hot_gauge(oracle, n, 3)
+        hs = _fields(V, srcs) + _fields(V, srcs)
+        ms = [masses[0]] * 2 + [masses[1]] * 2
+        b = CNBatch(hs, ms, tol)
+        for _ in range(6):
+            olds = [h.download() for h in hs]
+            gl, ge = g.download()
+            st = b.Update(g, C, 1.0, use_graph=True)
+            assert st["converged"] == 1 and st["max_rel_residual"] <= tol
+            for h, m, old in zip(hs, ms, olds):
+                assert _true_rel_residuals(oracle, n, gl, ge, m, np.array(C, dtype=complex), old, h.download()) <= tol
+            g.Update(1.0)
+        info = b.prediction_info()
+        assert info["ratio"] >= 0.0 and info["steps"] >= 1
+        b.Destructor()
+
+
 def test_graph_replay_equals_eager_launches(oracle):
     """The captured step and the same launches issued one by one agree bit for bit."""
     n = (6, 6, 6)
