@@ -87,6 +87,8 @@ def parse():
     p.add_argument("--only-drift", action="store_true", help="print only the precision-drift JSON")
     p.add_argument("--two-pass", action="store_true",
                    help="headline step: the two-pass BiCGStab update in place of the merged one")
+    p.add_argument("--history-depth", type=int, default=None,
+                   help="headline step: history vectors of the plain solve's start (1-4; default the library's)")
     return p.parse_args()
 
 
@@ -929,6 +931,8 @@ def main():
                           "tensor": nrqcd.STENCIL_TENSOR, "fma": nrqcd.STENCIL_FMA}[args.stencil])
     if args.two_pass:
         nrqcd.SetMergedUpdate(False)
+    if args.history_depth is not None:
+        nrqcd.SetHistoryDepth(args.history_depth)
     g = GaugeConfiguration()
     g.TransversePolarisedOccupiedInit_Box(0.5, 1.0, 0.0, RandomSeed=member_seed(rank), identity_links=True)
     h = NRQCDField()
@@ -1093,7 +1097,8 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(workload_config(L, world),
-                           bicgstab_update="two-pass" if args.two_pass else "merged"),
+                           bicgstab_update="two-pass" if args.two_pass else "merged",
+                           history_depth=args.history_depth if args.history_depth is not None else "default"),
             "roofline": {"bound": "hbm", "kernel": "CN 12-column stencil: " + stencil["in_use"],
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,

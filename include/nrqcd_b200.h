@@ -241,6 +241,13 @@ int nrq_cn_cheb_info(const nrq_cn *cn, int *last, double ms[2]);
  * its start: its refinement passes are set by the FP32 gain per pass, and
  * the smaller start did not remove one at 64^3 or 96^3.)                  */
 int nrq_cn_set_history_guess(nrq_cn *cn, int on);
+/* Plain form: the history vectors the extrapolated start uses (1-4, default
+ * 4): x0 = 2b - psi + the degree depth - 1 extrapolation of the field's last
+ * depth corrections t (t1; 2 t1 - t2; 3 t1 - 3 t2 + t3; 4 t1 - 6 t2 + 4 t3
+ * - t4), fewer while the field has fewer steps of history.  Each history
+ * vector is 576 B per site (FP32).  No reference counterpart (PETSc's KSP
+ * starts from the previous solution, src/nrqcd.f90:1108-1123).             */
+int nrq_cn_set_history_depth(nrq_cn *cn, int depth);
 /* The solve's acceptance.  always = 1 confirms every converged solve with
  * the true residual b - A^H x (one residual pass); 0 (the default) accepts,
  * as PETSc's KSP (src/nrqcd.f90:803) tests its recursive residual:

@@ -99,6 +99,7 @@ SIGNATURES = {
     "nrq_cn_set_stencil": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_cn_set_cheb_stencil": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_cn_set_true_residual": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "nrq_cn_set_history_depth": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_cn_set_merged_update": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_cn_true_residual_info": (ctypes.c_int, [_vp, _ip]),
     "nrq_cn_batch_set_variant": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),

@@ -1117,6 +1117,12 @@ extern "C" int nrq_cn_true_residual_info(const nrq_cn *cn, int *last_true) {
   return NRQ_OK;
 }
 
+extern "C" int nrq_cn_set_history_depth(nrq_cn *cn, int depth) {
+  if (!cn || depth < 1 || depth > nrq_heavy::kMaxHist) return NRQ_ERR_BAD_ARG;
+  cn->history_depth = depth;
+  return NRQ_OK;
+}
+
 extern "C" int nrq_cn_set_history_guess(nrq_cn *cn, int on) {
   if (!cn || on < 0 || on > 1) return NRQ_ERR_BAD_ARG;
   cn->history_guess = on != 0;
@@ -1755,9 +1761,11 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
     matvecs += 1;
     vstreams += 1;  // extra write of x0
   }
-  if (cn->history_guess && h->hist_count >= 1) {  // x0 += 2 t1 - t2 (or t1)
-    ProfScope ps(ctx, 1, (double)L.V * (1152.0 * 2 + 576.0 * h->hist_count));
-    nrq::launch_hist_extrapolate(72 * L.V, cn->x, hist_v1(h), hist_v2(h), st);
+  if (cn->history_guess && h->hist_count >= 1) {  // x0 += the extrapolated t of the last steps
+    const int d = std::min(cn->history_depth, h->hist_count);
+    const float2 *t[4] = {hist_v(h, 1), hist_v(h, 2), hist_v(h, 3), hist_v(h, 4)};
+    ProfScope ps(ctx, 1, (double)L.V * (1152.0 * 2 + 576.0 * d));
+    nrq::launch_hist_extrapolate(72 * L.V, cn->x, t, d, st);
     vstreams += 2;
   }
   // the merged update on the FMA stencil (the right-hand side ran on it)
@@ -1973,7 +1981,7 @@ extern "C" int nrq_heavy_update_cn(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g,
   // (history_guess), otherwise a plain step leaves none
   bool keep = false;
   if (cn->history_guess && status == NRQ_OK) {
-    if ((rc = nrqh::ensure_hist(h))) return rc;
+    if ((rc = nrqh::ensure_hist(h, cn->history_depth))) return rc;
     ProfScope ps(ctx, 1, (double)L.V * (1152.0 * 3 + 576.0));
     nrq::launch_hist_store(72 * L.V, cn->x, cn->b, h->P, hist_next(h), st);
     if ((rc = check_launch(ctx, "k_hist_store"))) return rc;

@@ -818,19 +818,25 @@ void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &
 
 // ------------------------------------------------------------ history-extrapolated start
 // The plain solve's start 2b - psi misses t = x - (2b - psi); consecutive
-// steps' t are strongly correlated, so x0 = 2b - psi + 2 t1 - t2 (or + t1
-// with one step of history) starts closer.  The history is kept in FP32.
-__global__ void k_hist_extrapolate(int64_t n, double2 *__restrict__ X, const float2 *__restrict__ T1,
-                                   const float2 *__restrict__ T2) {
+// steps' t vary smoothly, so the start adds t extrapolated from the last d
+// steps by the polynomial of degree d - 1 through them: x0 = 2b - psi +
+// sum_k c_k t_k, c = (1), (2, -1), (3, -3, 1), (4, -6, 4, -1) (t_1 the
+// newest).  The history is kept in FP32.
+struct HistExtrap {
+  const float2 *t[4];
+  double c[4];
+};
+__global__ void k_hist_extrapolate(int64_t n, double2 *__restrict__ X, const HistExtrap H) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float2 a = T1[i];
-  double dx = a.x, dy = a.y;
-  if (T2) {
-    const float2 b = T2[i];
-    dx = 2.0 * dx - (double)b.x;
-    dy = 2.0 * dy - (double)b.y;
-  }
+  double dx = 0.0, dy = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (H.t[k]) {
+      const float2 a = H.t[k][i];
+      dx += H.c[k] * (double)a.x;
+      dy += H.c[k] * (double)a.y;
+    }
   const double2 x = X[i];
   X[i] = make_double2(x.x + dx, x.y + dy);
 }
@@ -842,8 +848,15 @@ __global__ void k_hist_store(int64_t n, const double2 *__restrict__ X, const dou
   const double2 x = X[i], b = B[i], p = Psi[i];
   T[i] = make_float2((float)(x.x - (2.0 * b.x - p.x)), (float)(x.y - (2.0 * b.y - p.y)));
 }
-void launch_hist_extrapolate(int64_t n, double2 *X, const float2 *T1, const float2 *T2, cudaStream_t st) {
-  k_hist_extrapolate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, X, T1, T2);
+void launch_hist_extrapolate(int64_t n, double2 *X, const float2 *const *t, int d, cudaStream_t st) {
+  static const double kCoef[4][4] = {{1, 0, 0, 0}, {2, -1, 0, 0}, {3, -3, 1, 0}, {4, -6, 4, -1}};
+  HistExtrap H{};
+  d = d < 1 ? 1 : (d > 4 ? 4 : d);
+  for (int k = 0; k < 4; ++k) {
+    H.t[k] = k < d ? t[k] : nullptr;
+    H.c[k] = kCoef[d - 1][k];
+  }
+  k_hist_extrapolate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, X, H);
 }
 void launch_hist_store(int64_t n, const double2 *X, const double2 *B, const double2 *Psi, float2 *T, cudaStream_t st) {
   k_hist_store<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, X, B, Psi, T);

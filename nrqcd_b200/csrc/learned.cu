@@ -1038,9 +1038,15 @@ int learned_guess_batch(nrq_learn *net, const nrq_ctx *ctx, const nrq::BatchFiel
                                     256, 0, st>>>(V, tab, omega);
   return check_launch(c, "batched learned guess");
 }
-int ensure_hist(nrq_heavy *h) {
-  for (int k = 0; k < 2; ++k)
+int ensure_hist(nrq_heavy *h, int depth) {
+  depth = std::min(std::max(depth, 2), (int)nrq_heavy::kMaxHist);
+  for (int k = 0; k < depth; ++k)
     if (!h->hist[k]) NRQ_CUDA_TRY(h->ctx, cudaMalloc(&h->hist[k], sizeof(float2) * 72 * h->ctx->lat.V));
+  if (depth > h->hist_cap) {  // a larger ring: its order starts afresh
+    h->hist_cap = depth;
+    h->hist_count = 0;
+    h->hist_head = 0;
+  }
   return NRQ_OK;
 }
 void add_e_hist(int64_t n, double2 *x, const float2 *e, float2 *hist, cudaStream_t st) {

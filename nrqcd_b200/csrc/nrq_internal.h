@@ -93,24 +93,29 @@ struct nrq_heavy {
   nrq_ctx *ctx = nullptr;
   // 72 planes of V complex: (species*36 + col*6 + row); species 0 quark, 1 antiquark
   double2 *P = nullptr;
-  // history of the learned initial guess (FP32, 72 planes each): what the
-  // extrapolation 2 RHS - psi missed in the last two steps.  hist_count
-  // vectors are valid (0..2; only after learned-form or recording updates),
-  // the newest in slot hist_head.
-  float2 *hist[2] = {nullptr, nullptr};
+  // history of the field's steps (FP32, 72 planes each): what the start
+  // 2 RHS - psi missed, t = x - (2 RHS - psi), in the last steps, for the
+  // plain solve's extrapolated start and the learned guess.  A ring of
+  // hist_cap slots (2, grown to the plain solve's history depth on demand);
+  // hist_count vectors are valid, the newest in slot hist_head.
+  static constexpr int kMaxHist = 4;
+  float2 *hist[kMaxHist] = {nullptr, nullptr, nullptr, nullptr};
+  int hist_cap = 2;
   int hist_count = 0;
   int hist_head = 0;
 };
 
-inline const float2 *hist_v1(const nrq_heavy *h) { return h->hist_count >= 1 ? h->hist[h->hist_head] : nullptr; }
-inline const float2 *hist_v2(const nrq_heavy *h) {
-  return h->hist_count >= 2 ? h->hist[1 - h->hist_head] : nullptr;
+// the k-th newest history vector (k = 1, 2, ...), null where not valid
+inline const float2 *hist_v(const nrq_heavy *h, int k) {
+  return h->hist_count >= k ? h->hist[(h->hist_head - (k - 1) + h->hist_cap) % h->hist_cap] : nullptr;
 }
+inline const float2 *hist_v1(const nrq_heavy *h) { return hist_v(h, 1); }
+inline const float2 *hist_v2(const nrq_heavy *h) { return hist_v(h, 2); }
 // slot the next history vector goes to (the oldest one)
-inline float2 *hist_next(nrq_heavy *h) { return h->hist[1 - h->hist_head]; }
+inline float2 *hist_next(nrq_heavy *h) { return h->hist[(h->hist_head + 1) % h->hist_cap]; }
 inline void hist_push(nrq_heavy *h) {
-  h->hist_head = 1 - h->hist_head;
-  h->hist_count = h->hist_count < 2 ? h->hist_count + 1 : 2;
+  h->hist_head = (h->hist_head + 1) % h->hist_cap;
+  h->hist_count = h->hist_count < h->hist_cap ? h->hist_count + 1 : h->hist_cap;
 }
 
 struct nrq_learn;
@@ -149,6 +154,7 @@ struct nrq_cn {
   // plain form: start from 2b - psi + 2 t1 - t2 with the field's history of
   // corrections (FP32); on by default
   bool history_guess = true;
+  int history_depth = 4;  // history vectors the start extrapolates from (1-4)
   // plain form: confirm every converged solve with the true residual (a
   // residual pass), or (false, the default) accept the recursive residual
   // where it meets the tolerance with a margin of four times the largest
@@ -258,8 +264,9 @@ const nrq_ctx *learned_ctx(const nrq_learn *net);
 int learn_record(nrq_learn *net, const nrq_ctx *ctx, const double2 *psi, const double2 *b, const double2 *x,
                  const float2 *v1, const float2 *v2, float2 *hnew, const double2 *U, const double *E, double mass,
                  double dt);
-// both history slots of h allocated
-int ensure_hist(nrq_heavy *h);
+// at least `depth` history slots of h allocated (2 by default); growing the
+// ring drops the history it held
+int ensure_hist(nrq_heavy *h, int depth = 2);
 // learned guess of every field of a batch table (learned.cu)
 int learned_guess_batch(nrq_learn *net, const nrq_ctx *ctx, const nrq::BatchField *tab, int nfields,
                         const double2 *U, const double *E, float4 *gf, float *fbuf, float4 *omega,

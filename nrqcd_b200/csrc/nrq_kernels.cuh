@@ -278,7 +278,9 @@ void launch_prop_f2soa(const double2 *f, double2 *P, int64_t V, cudaStream_t st)
 void launch_prop_soa2f(const double2 *P, double2 *f, int64_t V, cudaStream_t st);
 void launch_single_point(double2 *P, int64_t V, int64_t sq, int64_t sa, cudaStream_t st);
 void launch_norms(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st);
-void launch_hist_extrapolate(int64_t n, double2 *X, const float2 *T1, const float2 *T2, cudaStream_t st);
+// x += sum_k c_k t_k over the d newest history vectors t[0..d-1] (d = 1..4),
+// c the coefficients of the degree d - 1 extrapolation
+void launch_hist_extrapolate(int64_t n, double2 *X, const float2 *const *t, int d, cudaStream_t st);
 void launch_hist_store(int64_t n, const double2 *X, const double2 *B, const double2 *Psi, float2 *T, cudaStream_t st);
 void launch_correlators(const double2 *P, int64_t V, double *partials, int64_t &nblk, cudaStream_t st,
                         bool gconjg = false);

@@ -127,6 +127,12 @@ def LastResidualIsTrue():
     return bool(v.value)
 
 
+def SetHistoryDepth(depth=4):
+    """Plain form: the history vectors (1-4) the extrapolated start uses."""
+    _capi.check(_capi.load().nrq_cn_set_history_depth(solver_handle(), int(depth)), lattice.context(),
+                f"Error in {modulename}: history depth")
+
+
 def SetHistoryGuess(on=True):
     """Plain form: start each solve from the extrapolation 2b - psi plus
     2 t1 - t2 of the field's last two corrections (FP32 history; the

@@ -133,7 +133,7 @@ EXPECTED_SYMBOLS = {
     "nrq_cn_init", "nrq_cn_finalize", "nrq_cn_apply", "nrq_cn_stencil_info", "nrq_cn_set_stencil",
     "nrq_cn_set_history_guess", "nrq_cn_attach_learned", "nrq_cn_set_wait_test",
     "nrq_cn_set_cheb_stencil", "nrq_cn_cheb_info", "nrq_cn_set_true_residual", "nrq_cn_true_residual_info",
-    "nrq_cn_set_merged_update",
+    "nrq_cn_set_merged_update", "nrq_cn_set_history_depth",
     "nrq_cn_batch_create", "nrq_cn_batch_destroy", "nrq_cn_batch_update", "nrq_cn_batch_info",
     "nrq_cn_batch_set_variant", "nrq_cn_batch_set_fp64", "nrq_cn_batch_fp64_info", "nrq_cn_batch_learned_info",
     "nrq_cn_batch_prediction_info",

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from nrqcd_b200 import GaugeConfiguration, NRQCDField, nrqcd
+from nrqcd_b200 import GaugeConfiguration, NRQCDField, NrqcdError, nrqcd
 from tests.gpu_util import lattice_ctx
 
 pytestmark = pytest.mark.gpu
@@ -308,3 +308,40 @@ def test_merged_update_matches_two_pass(oracle, n):
     assert all(abs(x - y) <= 1 for x, y in zip(runs[True][2], runs[False][2]))
     assert np.abs(runs[True][0] - runs[False][0]).max() < 50 * tol
     assert np.abs(runs[True][1] - runs[False][1]).max() < 50 * tol
+
+
+def test_history_depth_lowers_the_start(oracle):
+    """The extrapolated start of degree depth - 1: over coupled steps on an
+    evolving 16^3 field, once the history is full each deeper extrapolation
+    starts lower (the field's t vary smoothly from step to step), every
+    update converges, and the evolutions agree to the tolerance's level."""
+    n = (16, 16, 16)
+    tol = 1e-12
+    M, c = 1.0, [1, 1, 1, 1]
+    links, ef = oracle.transverse_box(n, A, 2.0, 1.0, 0.0, 4, identity_links=False)
+    runs = {}
+    for depth in (2, 3, 4):
+        with lattice_ctx(n, A, cn=(M, c, 1.0, tol)):
+            nrqcd.SetHistoryDepth(depth)
+            g = GaugeConfiguration()
+            g.upload(links, ef)
+            h = NRQCDField()
+            h.InitSinglePoint(1, 1)
+            init = []
+            for _ in range(8):
+                st = h.Update(g, M, c, 1.0)
+                assert st["converged"] == 1 and st["max_rel_residual"] <= tol
+                init.append(st["initial_rel_residual"])
+                g.Update(1.0)
+            q, a = h.download()
+            del g, h
+        runs[depth] = (q, a, init)
+    for lo, hi in ((3, 2), (4, 3)):
+        assert all(x < 0.6 * y for x, y in zip(runs[lo][2][5:], runs[hi][2][5:]))
+    for d in (3, 4):
+        assert np.abs(runs[d][0] - runs[2][0]).max() < 50 * tol
+        assert np.abs(runs[d][1] - runs[2][1]).max() < 50 * tol
+    with lattice_ctx(n, A, cn=(M, c, 1.0, tol)):
+        for bad in (0, 5):
+            with pytest.raises(NrqcdError):
+                nrqcd.SetHistoryDepth(bad)
