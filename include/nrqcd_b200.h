@@ -232,16 +232,14 @@ int nrq_cn_set_stencil(nrq_cn *cn, int stencil);
 #define NRQ_CHEB_BLOCKS 1
 int nrq_cn_set_cheb_stencil(nrq_cn *cn, int which);
 int nrq_cn_cheb_info(const nrq_cn *cn, int *last, double ms[2]);
-/* Plain form (form 0; no reference counterpart): on = 1 (the default)
- * starts every solve from 2b - psi + 2 t1 - t2, t1 and t2 the corrections
- * to that start of the field's last two steps (one step: + t1), kept per
- * field in FP32 (2 x 576 B per site); 0 starts from 2b - psi.  Any upload,
- * copy or point source restarts the history.  The tolerance and the final
- * true-residual check are the same either way.  (The precision form keeps
- * its start: its refinement passes are set by the FP32 gain per pass, and
- * the smaller start did not remove one at 64^3 or 96^3.)                  */
+/* Plain and precision forms (no reference counterpart): on = 1 (the
+ * default) starts every solve from 2b - psi plus the extrapolation of the
+ * corrections t to that start of the field's last steps (the depth below),
+ * kept per field in FP32 (576 B per site and step); 0 starts from 2b - psi.
+ * Any upload, copy or point source restarts the history.  The tolerance is
+ * the same either way.  The learned form uses its network's start.        */
 int nrq_cn_set_history_guess(nrq_cn *cn, int on);
-/* Plain form: the history vectors the extrapolated start uses (1-4, default
+/* The history vectors the extrapolated start uses (1-4, default
  * 4): x0 = 2b - psi + the degree depth - 1 extrapolation of the field's last
  * depth corrections t (t1; 2 t1 - t2; 3 t1 - 3 t2 + t3; 4 t1 - 6 t2 + 4 t3
  * - t4), fewer while the field has fewer steps of history.  Each history

@@ -1512,6 +1512,15 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
   // learned form: x = 2 RHS - psi + w1 u + w2 v (network), history restarted
   // with the network's part; every refinement correction is added to it
   const bool learned = cn->form == 2 && nrqh::learned_ready(cn->learn);
+  // otherwise the plain solve's extrapolated start from the field's history
+  const bool hist = !learned && cn->history_guess;
+  if (hist && h->hist_count >= 1) {
+    const int d = std::min(cn->history_depth, h->hist_count);
+    const float2 *t[4] = {hist_v(h, 1), hist_v(h, 2), hist_v(h, 3), hist_v(h, 4)};
+    ProfScope ps(ctx, 1, (double)V * (1152.0 * 2 + 576.0 * d));
+    nrq::launch_hist_extrapolate(72 * V, cn->x, t, d, st);
+    vstreams += 2;
+  }
   if (learned) {
     if ((rc = nrqh::ensure_hist(h))) return rc;
     ProfScope ps(ctx, 3, (double)V * (1152.0 * 4 + 576.0 * 6 + 432.0 * 3 + 128.0));
@@ -1686,8 +1695,16 @@ int cn_update_precision(nrq_cn *cn, nrq_heavy *h, const nrq_gauge *g, double mas
     }
   }
   if (status == NRQ_OK && !conv) status = NRQ_ERR_NOT_CONVERGED;
+  bool keep = learned && status == NRQ_OK;
+  if (hist && status == NRQ_OK) {  // t = x - (2 RHS - psi) into the history
+    if ((rc = nrqh::ensure_hist(h, cn->history_depth))) return rc;
+    ProfScope ps(ctx, 1, (double)V * (1152.0 * 3 + 576.0));
+    nrq::launch_hist_store(72 * V, cn->x, cn->b, h->P, hist_next(h), st);
+    if ((rc = check_launch(ctx, "k_hist_store"))) return rc;
+    keep = true;
+  }
   std::swap(h->P, cn->x);
-  if (learned && status == NRQ_OK) hist_push(h);
+  if (keep) hist_push(h);
   else h->hist_count = 0;
   double maxrel = 0.0;
   for (int k = 0; k < nrq::CN_COLS; ++k) {

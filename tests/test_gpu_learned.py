@@ -102,8 +102,8 @@ def test_recorded_samples_match_oracle(oracle):
 
 def test_trained_guess_beats_plain_extrapolation(oracle):
     """Train on 8 recorded steps of two seeded 8^3 fields; a third field then
-    needs fewer inner steps with the learned start than without it, and the
-    two forms agree to the solve tolerance."""
+    needs fewer inner steps with the learned start than from 2b - psi, and
+    the two forms agree to the solve tolerance."""
     n = (8, 8, 8)
     V = int(np.prod(n))
     M, tol = 1.0, 1e-10
@@ -132,6 +132,7 @@ def test_trained_guess_beats_plain_extrapolation(oracle):
                 net.attach()
             else:
                 net.detach()
+                nrqcd.SetHistoryGuess(False)  # the start 2b - psi alone
             its, r0 = [], []
             for _ in range(5):
                 st = h.Update(g, M, C, 1.0)
@@ -140,6 +141,7 @@ def test_trained_guess_beats_plain_extrapolation(oracle):
                 r0.append(st["initial_rel_residual"])
                 g.Update(1.0)
             runs[use] = (its, h.download(), r0)
+            nrqcd.SetHistoryGuess(True)
         net.detach()
         net.Destructor()
     its_plain, (qp, ap), r0_plain = runs[False]
