@@ -658,7 +658,9 @@ def measure_ensemble(steps, warmup, tol=1e-10, learned_params=None, ensemble=ENS
     batches = [CNBatch(f, m, tol, lat=lats[L]) for L, _, f, m in members]
     ens = Ensemble(batches, [g for _, g, _, _ in members])
     stats = []
-    for _ in range(max(2, warmup)):  # calibration, then graph capture
+    # the fields' history fills (depth 0 to 4, a calibration at each), then
+    # the graph capture
+    for _ in range(max(6, warmup)):
         ens.Step(WILSON, 1.0, use_graph=True)
     t_graph = timed(lambda: stats.append(ens.Step(WILSON, 1.0, use_graph=True)), steps)
     # the same batched launches without the graph, with per-class kernel timing

@@ -361,6 +361,11 @@ int nrq_cn_batch_learned_info(const nrq_cn_batch *batch, int *gate, double *gues
  * that largest ratio (-1 before the first measurement); steps: scheduled
  * steps taken.  Synchronises the batch's stream.                          */
 int nrq_cn_batch_prediction_info(const nrq_cn_batch *batch, double *ratio, int64_t *steps);
+/* Without a learned guess every field of the batch starts from 2b - psi plus
+ * the cubic extrapolation of its last four corrections, as the single-field
+ * solves do (on = 1, the default); 0 starts from 2b - psi.  No reference
+ * counterpart.                                                             */
+int nrq_cn_batch_set_history(nrq_cn_batch *batch, int on);
 int nrq_cn_batch_set_fp64(nrq_cn_batch *batch, int which);
 
 /* An ensemble of independent members (batch[i], gauge[i]); the members may

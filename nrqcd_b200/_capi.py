@@ -107,6 +107,7 @@ SIGNATURES = {
     "nrq_cn_batch_fp64_info": (ctypes.c_int, [_vp, _ip, _dp]),
     "nrq_cn_batch_learned_info": (ctypes.c_int, [_vp, _ip, _dp, _dp]),
     "nrq_cn_batch_prediction_info": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_int64)]),
+    "nrq_cn_batch_set_history": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_cn_cheb_info": (ctypes.c_int, [_vp, _ip, _dp]),
     "nrq_cn_set_history_guess": (ctypes.c_int, [_vp, ctypes.c_int]),
     "nrq_heavy_update_cn": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double, _dp, ctypes.c_double,

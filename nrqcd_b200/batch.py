@@ -111,6 +111,11 @@ class CNBatch:
         names = {-2: "none", -1: "undecided", 0: "off", 1: "on"}
         return {"gate": names[gate.value], "guess_ms": cost.value, "saving_ms": saving.value}
 
+    def set_history(self, on=True):
+        """Start every field from 2b - psi plus the cubic extrapolation of its
+        history (True, the default) or from 2b - psi alone (False)."""
+        _capi.check(_capi.load().nrq_cn_batch_set_history(self._h, int(bool(on))), self._ctx, "set history")
+
     def prediction_info(self) -> dict:
         """The scheduled steps' predicted acceptance: the largest measured
         ratio of true to predicted residual (-1 before the first) and the

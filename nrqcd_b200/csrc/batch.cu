@@ -54,6 +54,10 @@ struct nrq_cn_batch {
   // the scheduled steps' predicted acceptance: {largest true-to-predicted
   // ratio measured (-1: none), scheduled steps taken} (device)
   double *pstate = nullptr;
+  // without a learned guess every field starts from 2b - psi plus the
+  // extrapolation of its last kBatchHistDepth corrections, as the
+  // single-field solves do
+  bool history = true;
   int *flags = nullptr;
   int64_t nsb = 0;  // 32-site blocks
   // device table and pinned mirrors
@@ -132,12 +136,26 @@ bool learned_on(const nrq_cn_batch *b) {
   return b->learn && nrqh::learned_ready(b->learn) && b->learn_gate != 0;
 }
 
-// history depth of the learned guess (every field's count, capped at 2), -1 without it
+constexpr int kBatchHistDepth = 4;
+bool hist_on(const nrq_cn_batch *b) { return b->history && !learned_on(b); }
+
+// history depth of the start (every field's count, capped at 2 for the
+// learned guess and at kBatchHistDepth for the extrapolation), -1 without one
 int depth_of(const nrq_cn_batch *b) {
-  if (!learned_on(b)) return -1;
-  int d = 2;
+  if (!learned_on(b) && !hist_on(b)) return -1;
+  int d = learned_on(b) ? 2 : kBatchHistDepth;
   for (const nrq_heavy *h : b->fields) d = std::min(d, h->hist_count);
   return d;
+}
+
+// every field's history ring holds the extrapolation's steps
+int ensure_batch_hist(nrq_cn_batch *b) {
+  if (!hist_on(b)) return NRQ_OK;
+  for (nrq_heavy *h : b->fields) {
+    const int rc = nrqh::ensure_hist(h, kBatchHistDepth);
+    if (rc) return rc;
+  }
+  return NRQ_OK;
 }
 
 bool same_key(const nrq_cn_batch *b, const double c[8], double dt) {
@@ -176,6 +194,13 @@ void fill_table(nrq_cn_batch *b, const double c[8], double dt) {
       nrq_heavy *h = b->fields[i];
       f.h1 = hist_v1(h);
       f.h2 = hist_v2(h);
+      f.hnew = hist_next(h);
+    } else if (hist_on(b)) {
+      nrq_heavy *h = b->fields[i];
+      f.h1 = hist_v(h, 1);
+      f.h2 = hist_v(h, 2);
+      f.h3 = hist_v(h, 3);
+      f.h4 = hist_v(h, 4);
       f.hnew = hist_next(h);
     }
   }
@@ -247,6 +272,11 @@ int enq_rhs(nrq_cn_batch *b, const nrq_gauge *g, cudaStream_t st) {
     launch_fp64(b, nrq::MV_RHS, b->fp64, 0, st);
   }
   int rc = check_launch(ctx, "batch rhs");
+  if (!rc && hist_on(b)) {
+    ProfScope ps(ctx, 1, (double)ctx->lat.V * b->nf * (1152.0 * 2 + 576.0 * (kBatchHistDepth + 1)));
+    nrq::launch_batch_hist_start(ctx->lat.V, b->d_tab, b->nf, st);
+    rc = check_launch(ctx, "batch history start");
+  }
   if (!rc && learned_on(b)) {
     ProfScope ps(ctx, 3, (double)ctx->lat.V * b->nf * (1152.0 * 4 + 576.0 * 5 + 128.0));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -563,7 +593,7 @@ int finish_step(nrq_cn_batch *b, double dt, cudaStream_t st, Check &chk, bool *s
 int conclude(nrq_cn_batch *b, const Check &chk, int64_t inner, int64_t passes) {
   // results: the iterate becomes the field, the old field the next work
   // buffer; a learned step leaves the new history in the field
-  const bool keep = learned_on(b) && chk.conv && !chk.nonfin && !chk.badbounds && !chk.timeout;
+  const bool keep = (learned_on(b) || hist_on(b)) && chk.conv && !chk.nonfin && !chk.badbounds && !chk.timeout;
   for (int i = 0; i < b->nf; ++i) {
     std::swap(b->fields[i]->P, b->xbuf[i]);
     if (keep) hist_push(b->fields[i]);
@@ -790,8 +820,10 @@ int check_member_gauge(nrq_cn_batch *b, const nrq_gauge *g) {
 int batch_update(nrq_cn_batch *b, const nrq_gauge *g, const double c[8], double dt, bool use_graph) {
   nrq_ctx *ctx = b->ctx;
   cudaStream_t st = ctx->stream;
+  int rc = ensure_batch_hist(b);
+  if (rc) return rc;
   fill_table(b, c, dt);
-  int rc = upload_table(b, st);
+  rc = upload_table(b, st);
   if (rc) return rc;
   Check chk;
   if (!same_key(b, c, dt)) {
@@ -896,6 +928,16 @@ extern "C" int nrq_cn_batch_learned_info(const nrq_cn_batch *b, int *gate, doubl
   if (gate) *gate = b->learn ? b->learn_gate : -2;
   if (guess_ms) *guess_ms = b->guess_ms;
   if (saving_ms) *saving_ms = b->guess_saving_ms;
+  return NRQ_OK;
+}
+
+extern "C" int nrq_cn_batch_set_history(nrq_cn_batch *b, int on) {
+  if (!b || on < 0 || on > 1) return NRQ_ERR_BAD_ARG;
+  if (b->history != (on != 0)) {
+    b->history = on != 0;
+    b->have_key = false;  // recalibrate (and recapture) with the other start
+    b->gen++;
+  }
   return NRQ_OK;
 }
 
@@ -1015,6 +1057,7 @@ extern "C" int nrq_ensemble_step(nrq_ensemble *e, const double c[8], double dt, 
   } else {
     cudaStream_t st0 = ctx0->stream;
     for (nrq_cn_batch *b : e->batches) {
+      if ((rc = ensure_batch_hist(b))) return rc;
       fill_table(b, c, dt);
       if ((rc = upload_table(b, st0))) return rc;
     }

@@ -24,6 +24,8 @@
 // The stencil kernels live in cn_mv3.cu (TMA-staged) and cn_mv.cu
 // (register-tiled); this file holds the per-step preparation, the BiCGStab
 // vector updates and scalar stages, and the propagator I/O and observables.
+#include <algorithm>
+
 #include "nrq_eigen.cuh"
 #include "nrq_kernels.cuh"
 
@@ -615,6 +617,30 @@ __global__ void k_batch_calibrate(const BatchField *__restrict__ tab, int nfield
 }
 void launch_batch_calibrate(const BatchField *tab, int nfields, double *pstate, cudaStream_t st) {
   k_batch_calibrate<<<1, 256, 0, st>>>(tab, nfields, pstate);
+}
+
+__global__ void k_batch_hist_start(int64_t n, const BatchField *__restrict__ tab) {
+  const BatchField &f = tab[blockIdx.y];
+  const float2 *h[4] = {f.h1, f.h2, f.h3, f.h4};
+  int d = 0;
+  while (d < 4 && h[d]) ++d;
+  const double cf[5][4] = {{0, 0, 0, 0}, {1, 0, 0, 0}, {2, -1, 0, 0}, {3, -3, 1, 0}, {4, -6, 4, -1}};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double dx = 0.0, dy = 0.0;
+    for (int k = 0; k < d; ++k) {  // read before hnew (which may be the oldest slot) is written
+      const float2 a = h[k][i];
+      dx += cf[d][k] * (double)a.x;
+      dy += cf[d][k] * (double)a.y;
+    }
+    const double2 x = f.x[i];
+    f.x[i] = make_double2(x.x + dx, x.y + dy);
+    f.hnew[i] = make_float2((float)dx, (float)dy);
+  }
+}
+void launch_batch_hist_start(int64_t V, const BatchField *tab, int nfields, cudaStream_t st) {
+  const int64_t n = 72 * V;
+  k_batch_hist_start<<<dim3((unsigned)std::min<int64_t>((n + 255) / 256, 2048), (unsigned)nfields), 256, 0, st>>>(
+      n, tab);
 }
 
 // ------------------------------------------------------------ propagator I/O, norms, correlators

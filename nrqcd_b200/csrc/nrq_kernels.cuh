@@ -183,6 +183,9 @@ struct BatchField {
   // when absent) and the slot the new history goes to (null: no learned guess)
   const float2 *h1, *h2;
   float2 *hnew;
+  // history start without the learned guess: the field's third and fourth
+  // newest history vectors (null when absent; h1, h2 the newest two)
+  const float2 *h3, *h4;
   cplx inv_theta[2];             // 1/theta per species (written on the device)
   ChebCoef cheb[BATCH_MAX_CHEB]; // Chebyshev steps (written on the device)
   // guaranteed gain |T_m(sigma)| of m Chebyshev steps per species (written
@@ -257,6 +260,11 @@ void launch_batch_finalize(const BatchField *tab, int nfields, int64_t nrows, do
 void launch_batch_predict(const BatchField *tab, int nfields, int m, double tol, const double *pstate,
                           cudaStream_t st);
 void launch_batch_calibrate(const BatchField *tab, int nfields, double *pstate, cudaStream_t st);
+// The history start of every field (no learned guess): with the field's
+// history vectors h1.. (d of them, the first null ends the list) x +=
+// sum_k c_k h_k, c of the degree d - 1 extrapolation, and hnew = the same
+// sum in FP32 (0 without history), to which every correction is added.
+void launch_batch_hist_start(int64_t V, const BatchField *tab, int nfields, cudaStream_t st);
 void launch_cn_to_f32(int64_t V, const double2 *U, const double2 *DE, const double2 *D, const double *B, float2 *U32,
                       float2 *DE32, float2 *D32, float *B32, cudaStream_t st);
 void launch_cn_bounds(Lat L, const CnCoef &C, double tau, const double2 *U, const double2 *Dsum, const double *Bsum,

@@ -136,7 +136,7 @@ EXPECTED_SYMBOLS = {
     "nrq_cn_set_merged_update", "nrq_cn_set_history_depth",
     "nrq_cn_batch_create", "nrq_cn_batch_destroy", "nrq_cn_batch_update", "nrq_cn_batch_info",
     "nrq_cn_batch_set_variant", "nrq_cn_batch_set_fp64", "nrq_cn_batch_fp64_info", "nrq_cn_batch_learned_info",
-    "nrq_cn_batch_prediction_info",
+    "nrq_cn_batch_prediction_info", "nrq_cn_batch_set_history",
     "nrq_cn_batch_residuals", "nrq_cn_batch_attach_learned",
     "nrq_ensemble_create", "nrq_ensemble_destroy", "nrq_ensemble_step",
     "nrq_learn_create", "nrq_learn_destroy", "nrq_learn_record", "nrq_learn_train", "nrq_learn_params",
