@@ -261,9 +261,11 @@ int nrq_cn_set_history_depth(nrq_cn *cn, int depth);
  * the true residual (1) or the recursive or predicted one (0).            */
 /* Plain form on the FMA stencil: on = 1 (the default) updates x, r and p of
  * an iteration in one pass, beta taken from rh.t, which the t = A^H s launch
- * reduces (rh.s vanishes by the choice of alpha, so rho_new = -omega rh.t);
- * 0 keeps two passes (x and r, then p) with rho_new = rh.r reduced.  No
- * reference counterpart (PETSc's KSPBCGS, src/nrqcd.f90:803).            */
+ * reduces (rh.s vanishes by the choice of alpha, so rho_new = -omega rh.t),
+ * with the shadow residual rh kept in FP32 (every product with it, rho_0
+ * included, uses the same rounded values); 0 keeps two passes (x and r,
+ * then p) with rho_new = rh.r reduced and rh in FP64.  No reference
+ * counterpart (PETSc's KSPBCGS, src/nrqcd.f90:803).                       */
 int nrq_cn_set_merged_update(nrq_cn *cn, int on);
 int nrq_cn_set_true_residual(nrq_cn *cn, int always);
 int nrq_cn_true_residual_info(const nrq_cn *cn, int *last_true);
