@@ -137,39 +137,50 @@ __device__ __forceinline__ cplx pauli_t5(int k, int s, int t) {
   return (s == 0) ? cplx{1.0, 0.0} : cplx{-1.0, 0.0};
 }
 
-// One thread per (direction I, species, row g, site): row g of the forward
-// block W_I(x) of that species, into planes (I*2 + sp)*36 + g*6 + column, in
-// FP64 (W) and/or rounded to FP32 (Wf, the FP32 Chebyshev stencil's blocks).
+// One thread per (direction I, colour row c, site): rows g = 2c + s of the
+// forward blocks W_I(x) of both species, column 2cp + t, into plane
+// (I*2 + sp)*36 + g*6 + column, in FP64 (W) and/or rounded to FP32 (Wf, the
+// FP32 Chebyshev stencil's blocks).  The entries (cp, c) of the link and
+// the two derived matrices belong to this c alone, so every input is read
+// once, and every store is coalesced over the warp's consecutive sites.
 template <bool F64, bool F32>
 __global__ void __launch_bounds__(256) k_cn_blocks5(Lat L, CnCoef C, const double2 *__restrict__ U,
                                                     const double2 *__restrict__ DE, double2 *__restrict__ W,
                                                     float2 *__restrict__ Wf) {
   const int64_t V = L.V;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= 36 * V) return;
+  if (tid >= 9 * V) return;
   const int64_t x = tid % V;
-  const int64_t r = tid / V;  // (I*2 + sp)*6 + g
-  const int g = (int)(r % 6);
-  const int isp = (int)(r / 6);
-  const int I = isp >> 1, sp = isp & 1;
-  const int c = g >> 1, s = g & 1;
+  const int r = (int)(tid / V);  // I*3 + c
+  const int I = r / 3, c = r % 3;
   const int K0 = (I + 2) % 3, K1 = (I + 1) % 3;
-  const cplx ck = (-0.5 * C.inva2[I]) * C.kin[sp];
-  const cplx cs0 = times_i(C.so[sp]), cs1 = -times_i(C.so[sp]);
-  const int64_t row = ((int64_t)isp * 36 + g * 6) * V + x;
+  cplx u[3], d0[3], d1[3];
 #pragma unroll
   for (int cp = 0; cp < 3; ++cp) {
     const int e = cp * 3 + c;  // M^T[c][cp] = M[cp][c]
-    const cplx u = ldg(U + (int64_t)(I * 9 + e) * V + x);
-    const cplx d0 = ldg(DE + (int64_t)((I * 2 + 0) * 9 + e) * V + x);
-    const cplx d1 = ldg(DE + (int64_t)((I * 2 + 1) * 9 + e) * V + x);
-    const cplx ku = ck * u, e0 = cs0 * d0, e1 = cs1 * d1;
+    u[cp] = ldg(U + (int64_t)(I * 9 + e) * V + x);
+    d0[cp] = ldg(DE + (int64_t)((I * 2 + 0) * 9 + e) * V + x);
+    d1[cp] = ldg(DE + (int64_t)((I * 2 + 1) * 9 + e) * V + x);
+  }
 #pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      cplx v = (s == t) ? ku : cplx{0.0, 0.0};
-      v = v + pauli_t5(K0, s, t) * e0 + pauli_t5(K1, s, t) * e1;
-      if (F64) st(W + row + (int64_t)(2 * cp + t) * V, v);
-      if (F32) Wf[row + (int64_t)(2 * cp + t) * V] = make_float2((float)v.re, (float)v.im);
+  for (int sp = 0; sp < 2; ++sp) {
+    const cplx ck = (-0.5 * C.inva2[I]) * C.kin[sp];
+    const cplx cs0 = times_i(C.so[sp]), cs1 = -times_i(C.so[sp]);
+#pragma unroll
+    for (int cp = 0; cp < 3; ++cp) {
+      const cplx ku = ck * u[cp], e0 = cs0 * d0[cp], e1 = cs1 * d1[cp];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int g = 2 * c + s;
+        const int64_t row = ((int64_t)(I * 2 + sp) * 36 + g * 6) * V + x;
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+          cplx v = (s == t) ? ku : cplx{0.0, 0.0};
+          v = v + pauli_t5(K0, s, t) * e0 + pauli_t5(K1, s, t) * e1;
+          if (F64) st(W + row + (int64_t)(2 * cp + t) * V, v);
+          if (F32) Wf[row + (int64_t)(2 * cp + t) * V] = make_float2((float)v.re, (float)v.im);
+        }
+      }
     }
   }
 }
@@ -1219,7 +1230,7 @@ __global__ void __maxnreg__(mv5::kMaxReg)
 // ------------------------------------------------------------------ host
 void launch_cn_blocks5(Lat L, const CnCoef &C, const double2 *U, const double2 *DE, double2 *W, float2 *Wf,
                        cudaStream_t st) {
-  const int64_t n = 36 * L.V;
+  const int64_t n = 9 * L.V;
   const unsigned grid = (unsigned)((n + 255) / 256);
   if (W && Wf)
     k_cn_blocks5<true, true><<<grid, 256, 0, st>>>(L, C, U, DE, W, Wf);
