@@ -244,7 +244,8 @@ int nrq_cn_set_history_guess(nrq_cn *cn, int on);
  * depth corrections t (t1; 2 t1 - t2; 3 t1 - 3 t2 + t3; 4 t1 - 6 t2 + 4 t3
  * - t4), fewer while the field has fewer steps of history.  Each history
  * vector is 576 B per site (FP32).  No reference counterpart (PETSc's KSP
- * starts from the previous solution, src/nrqcd.f90:1108-1123).             */
+ * starts from zero: the solution vector holds psi, src/nrqcd.f90:1108-1123,
+ * but KSPSetInitialGuessNonzero is never called).                          */
 int nrq_cn_set_history_depth(nrq_cn *cn, int depth);
 /* The solve's acceptance.  always = 1 confirms every converged solve with
  * the true residual b - A^H x (one residual pass); 0 (the default) accepts,
@@ -386,8 +387,8 @@ int nrq_ensemble_step(nrq_ensemble *ens, const double c[8], double stepwidth, in
                       nrq_cn_stats *stats);
 
 /* ---- learned initial guess (form 2) ----------------------------------- */
-/* No counterpart in the reference (PETSc KSP starts from the previous
- * propagator, src/nrqcd.f90:1112-1123).  Per sample (site, species) a
+/* No counterpart in the reference (PETSc KSP starts from zero,
+ * src/nrqcd.f90:1108-1123).  Per sample (site, species) a
  * 16 -> 64 -> 64 -> 6 MLP (ReLU, BF16 weights and activations, FP32
  * accumulation on the tensor cores) maps local invariants of the right-hand
  * side b = A psi, of the field's history and of the gauge field

@@ -1,8 +1,8 @@
 // Learned initial guess of the Crank-Nicolson solve (form 2), its training
 // and its C ABI (nrq_learn_*).
 //
-// The reference's solve starts from the previous propagator (PETSc KSP,
-// src/nrqcd.f90:1112-1123); the plain forms here start from the extrapolation
+// The reference's solve starts from zero (PETSc KSP, src/nrqcd.f90:1108-1123,
+// without KSPSetInitialGuessNonzero); the plain forms here start from the extrapolation
 // x0 = 2 RHS - psi.  The learned form adds, per sample (site, species),
 //   x0 = 2 b - psi + w1 u + w2 v,   u = b - psi,   v = history,
 // where the history v = x_prev - (2 b_prev - psi_prev) is what the

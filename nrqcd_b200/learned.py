@@ -7,7 +7,8 @@ of the solve A^H x = b (b = A psi), v1 and v2 being what the extrapolation
 2 b - psi missed in the field's previous two steps.  It is trained on the method's own
 solves (``record`` then ``train``); the solve's FP64 residual check decides
 convergence with or without it.  No counterpart in the reference, whose
-PETSc solve starts from the previous propagator (src/nrqcd.f90:1112-1123).
+PETSc solve starts from zero (src/nrqcd.f90:1108-1123; the solution vector
+holds psi, but KSPSetInitialGuessNonzero is never called).
 """
 from __future__ import annotations
 
