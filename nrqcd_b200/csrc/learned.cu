@@ -2,8 +2,9 @@
 // and its C ABI (nrq_learn_*).
 //
 // The reference's solve starts from zero (PETSc KSP, src/nrqcd.f90:1108-1123,
-// without KSPSetInitialGuessNonzero); the plain forms here start from the extrapolation
-// x0 = 2 RHS - psi.  The learned form adds, per sample (site, species),
+// without KSPSetInitialGuessNonzero); the plain and precision forms here
+// start from x0 = 2 RHS - psi plus the polynomial extrapolation of the
+// field's last corrections.  The learned form adds, per sample (site, species),
 //   x0 = 2 b - psi + w1 u + w2 v,   u = b - psi,   v = history,
 // where the history v = x_prev - (2 b_prev - psi_prev) is what the
 // extrapolation missed in the previous step and (w1, w2) complex come from a
