@@ -109,3 +109,20 @@ def test_history_coefficients_extrapolate_polynomials(d):
     poly[0] = 1.0
     ts = [np.polyval(poly, 10.0 - k) for k in range(1, d + 1)]
     assert abs(sum(c * t for c, t in zip(coef, ts)) - np.polyval(poly, 10.0)) > 0.5
+
+
+@pytest.mark.parametrize("sigma", [1.5 + 0.0j, 2.0 - 3.0j, 0.3 + 4.0j, -1.2 + 0.7j])
+def test_chebyshev_gain_from_the_coefficient_recurrence(sigma):
+    """The batch's guaranteed gain of m Chebyshev steps: the coefficient
+    recurrence rho_0 = 1/sigma, rho_{k+1} = 1/(2 sigma - rho_k) gives
+    rho_k = T_k(sigma) / T_{k+1}(sigma), so 1/|rho_0 ... rho_{m-1}| equals
+    |T_m(sigma)| (T the Chebyshev polynomials, T_{k+1} = 2 sigma T_k -
+    T_{k-1})."""
+    rho = 1.0 / sigma
+    prod = 1.0 + 0.0j
+    t_prev, t_cur = 1.0 + 0.0j, sigma
+    for m in range(1, 20):
+        prod *= rho
+        assert abs(1.0 / abs(prod) - abs(t_cur)) <= 1e-9 * abs(t_cur)
+        rho = 1.0 / (2.0 * sigma - rho)
+        t_prev, t_cur = t_cur, 2.0 * sigma * t_cur - t_prev
