@@ -181,8 +181,8 @@ def test_errors_fail_loudly():
 
 @pytest.mark.parametrize("tol", [1e-10, 1e-12])
 def test_history_start_and_half_step_exit(oracle, tol):
-    """The plain solve's start extrapolated from the field's last two
-    corrections (the default) and the half-step exit: over coupled steps on
+    """The plain solve's start extrapolated from the field's last
+    corrections (the default, up to four) and the half-step exit: over coupled steps on
     an evolving 16^3 field it starts at a smaller residual and needs fewer
     stencil launches than the start 2b - psi alone, ends at the same
     tolerance, and both evolutions agree to the tolerance's level (both
